@@ -1,0 +1,1160 @@
+// C-ABI of the devil B200 path: context, uploads, the fit pipeline in the
+// order of cpu_fit (R/main.R:375-523), the DE test and the single-step
+// entry points.  See include/devil_b200.h for the contract.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/devil_b200.h"
+#include "internal.h"
+
+using namespace devil;
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct devil_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int64_t launches = 0;
+    std::map<std::string, DevBuf> bufs;
+    int32_t* mapped_host = nullptr;   // pinned, mapped: active-gene count mirror
+    int32_t* mapped_dev = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int sm_count = 148;
+};
+
+namespace {
+
+struct Fail {
+    int code;
+};
+
+void set_err(devil_ctx* ctx, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+}
+
+#define CK(expr)                                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (expr);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            set_err(ctx, "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(e_),        \
+                    __FILE__, __LINE__);                                                \
+            throw Fail{e_ == cudaErrorMemoryAllocation ? DEVIL_ERR_NOMEM : DEVIL_ERR_CUDA}; \
+        }                                                                               \
+    } while (0)
+
+#define LAUNCH(expr)            \
+    do {                        \
+        CK(expr);               \
+        ctx->launches++;        \
+    } while (0)
+
+void fail(devil_ctx* ctx, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+    throw Fail{code};
+}
+
+// grow-only named device workspace
+template <class T>
+T* ws(devil_ctx* ctx, const std::string& name, size_t count) {
+    size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    DevBuf& b = ctx->bufs[name];
+    if (b.bytes < bytes) {
+        if (b.p) CK(cudaFree(b.p));
+        b.p = nullptr;
+        b.bytes = 0;
+        CK(cudaMalloc(&b.p, bytes));
+        b.bytes = bytes;
+    }
+    return static_cast<T*>(b.p);
+}
+
+template <class T>
+void h2d(devil_ctx* ctx, T* dst, const T* src, size_t count) {
+    if (count) CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+}
+template <class T>
+void d2h(devil_ctx* ctx, T* dst, const T* src, size_t count) {
+    if (count && dst) CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+}
+
+int pow2_floor(int v) {
+    int p = 1;
+    while (p * 2 <= v) p *= 2;
+    return p;
+}
+
+// ------------------------------------------------------------------
+// device-resident problem
+// ------------------------------------------------------------------
+struct DevProblem {
+    int64_t G = 0, n = 0;
+    int P = 0;
+    int xs = 0;
+    int val_u16 = 0;
+    const int64_t* rowptr = nullptr;
+    const int32_t* col = nullptr;
+    const void* val = nullptr;
+    int64_t nnz = 0;
+    const double* Xcm = nullptr;
+    float* Xrm = nullptr;
+    double* sf = nullptr;
+    double* off = nullptr;
+    float* off_f = nullptr;
+    double* stats = nullptr;
+    int nfine = 1;
+    int32_t* fine_bound = nullptr;
+    int64_t* fine_ptr = nullptr;
+};
+
+int xs_for(int P) {
+    if (P <= 8) return P <= 1 ? 1 : (P <= 2 ? 2 : (P <= 4 ? 4 : 8));
+    return (P + 3) & ~3;
+}
+
+void check_counts(devil_ctx* ctx, const devil_counts* c) {
+    if (!c) fail(ctx, DEVIL_ERR_ARG, "counts is NULL");
+    if (c->n_genes < 0 || c->n_cells < 2) fail(ctx, DEVIL_ERR_ARG, "need n_genes >= 0 and n_cells >= 2");
+    if (c->n_cells > INT32_MAX) fail(ctx, DEVIL_ERR_ARG, "n_cells must fit int32");
+    if (c->n_genes > INT32_MAX) fail(ctx, DEVIL_ERR_ARG, "n_genes must fit int32");
+    if (c->format < 0 || c->format > 4) fail(ctx, DEVIL_ERR_ARG, "unknown counts format %d", c->format);
+    if (c->n_genes > 0 && c->n_cells > 0 && !c->values && c->nnz != 0)
+        fail(ctx, DEVIL_ERR_ARG, "counts values is NULL");
+}
+
+// every kernel indexes the design with CSR cell indices: check them first
+void validate_csr(devil_ctx* ctx, const DevProblem& dp) {
+    int32_t* bad = ws<int32_t>(ctx, "csr_bad", 1);
+    CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), ctx->stream));
+    LAUNCH(launch_validate_csr(dp.rowptr, dp.col, dp.G, dp.n, dp.nnz, bad, ctx->stream));
+    int32_t h = 0;
+    CK(cudaMemcpyAsync(&h, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h)
+        fail(ctx, DEVIL_ERR_ARG,
+             "invalid CSR: row pointers must be non-decreasing and end at nnz, cell indices in "
+             "[0, n) and strictly increasing within each gene");
+}
+
+// upload host counts to a device CSR (gene-major)
+void upload_counts(devil_ctx* ctx, const devil_counts* c, DevProblem& dp) {
+    const int64_t G = c->n_genes, n = c->n_cells;
+    dp.G = G;
+    dp.n = n;
+    cudaStream_t st = ctx->stream;
+    switch (c->format) {
+        case DEVIL_COUNTS_CSR_U16:
+        case DEVIL_COUNTS_CSR_F32: {
+            if (!c->ptr || (!c->idx && c->nnz)) fail(ctx, DEVIL_ERR_ARG, "CSR needs ptr and idx");
+            int64_t nnz = c->ptr[G];
+            if (nnz != c->nnz) fail(ctx, DEVIL_ERR_ARG, "CSR nnz mismatch (%lld vs rowptr %lld)",
+                                    (long long)c->nnz, (long long)nnz);
+            int64_t* rp = ws<int64_t>(ctx, "rowptr", G + 1);
+            int32_t* col = ws<int32_t>(ctx, "col", nnz);
+            h2d(ctx, rp, c->ptr, G + 1);
+            h2d(ctx, col, c->idx, nnz);
+            if (c->format == DEVIL_COUNTS_CSR_U16) {
+                uint16_t* v = ws<uint16_t>(ctx, "val16", nnz);
+                h2d(ctx, v, static_cast<const uint16_t*>(c->values), nnz);
+                dp.val = v;
+                dp.val_u16 = 1;
+            } else {
+                float* v = ws<float>(ctx, "val32", nnz);
+                h2d(ctx, v, static_cast<const float*>(c->values), nnz);
+                dp.val = v;
+                dp.val_u16 = 0;
+            }
+            dp.rowptr = rp;
+            dp.col = col;
+            dp.nnz = nnz;
+            validate_csr(ctx, dp);
+            return;
+        }
+        case DEVIL_COUNTS_DENSE_F64:
+        case DEVIL_COUNTS_DENSE_F32: {
+            const int is64 = c->format == DEVIL_COUNTS_DENSE_F64;
+            const size_t esz = is64 ? 8 : 4;
+            void* Yd = ws<char>(ctx, "dense", (size_t)G * n * esz);
+            if (G * n) CK(cudaMemcpyAsync(Yd, c->values, (size_t)G * n * esz, cudaMemcpyHostToDevice, st));
+            int64_t* cnt = ws<int64_t>(ctx, "rowcnt", G + 1);
+            CK(cudaMemsetAsync(cnt, 0, (G + 1) * sizeof(int64_t), st));
+            LAUNCH(launch_dense_count(Yd, is64, c->dense_layout == DEVIL_DENSE_CELL_MAJOR, G, n, cnt, st));
+            int64_t* rp = ws<int64_t>(ctx, "rowptr", G + 1);
+            size_t tb = 0;
+            cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, rp, (int)(G + 1), st);
+            void* tmp = ws<char>(ctx, "scan_tmp", tb);
+            CK(cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, rp, (int)(G + 1), st));
+            ctx->launches++;
+            int64_t nnz = 0;
+            CK(cudaMemcpyAsync(&nnz, rp + G, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            int32_t* col = ws<int32_t>(ctx, "col", nnz);
+            float* v = ws<float>(ctx, "val32", nnz);
+            LAUNCH(launch_dense_fill(Yd, is64, c->dense_layout == DEVIL_DENSE_CELL_MAJOR, G, n, rp, col, v, st));
+            dp.rowptr = rp;
+            dp.col = col;
+            dp.val = v;
+            dp.val_u16 = 0;
+            dp.nnz = nnz;
+            return;
+        }
+        case DEVIL_COUNTS_CSC_F64: {
+            if (!c->ptr || (!c->idx && c->nnz)) fail(ctx, DEVIL_ERR_ARG, "CSC needs ptr and idx");
+            int64_t nnz = c->ptr[n];
+            if (nnz != c->nnz) fail(ctx, DEVIL_ERR_ARG, "CSC nnz mismatch");
+            int64_t* cp = ws<int64_t>(ctx, "colptr", n + 1);
+            int32_t* ri = ws<int32_t>(ctx, "rowidx", nnz);
+            double* vin = ws<double>(ctx, "csc_val", nnz);
+            h2d(ctx, cp, c->ptr, n + 1);
+            h2d(ctx, ri, c->idx, nnz);
+            h2d(ctx, vin, static_cast<const double*>(c->values), nnz);
+            int64_t* keys = ws<int64_t>(ctx, "keys", nnz);
+            int64_t* keys2 = ws<int64_t>(ctx, "keys2", nnz);
+            double* v2 = ws<double>(ctx, "csc_val2", nnz);
+            int32_t* bad = ws<int32_t>(ctx, "csr_bad", 1);
+            CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), st));
+            LAUNCH(launch_csc_keys(cp, ri, n, G, nnz, keys, bad, st));
+            int32_t hbad = 0;
+            CK(cudaMemcpyAsync(&hbad, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (hbad) fail(ctx, DEVIL_ERR_ARG, "invalid CSC: pointers or gene indices out of range");
+            size_t tb = 0;
+            cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, vin, v2, (int)nnz);
+            void* tmp = ws<char>(ctx, "sort_tmp", tb);
+            CK(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, vin, v2, (int)nnz, 0, 64, st));
+            ctx->launches++;
+            int32_t* col = ws<int32_t>(ctx, "col", nnz);
+            int64_t* cnt = ws<int64_t>(ctx, "rowcnt", G + 1);
+            CK(cudaMemsetAsync(cnt, 0, (G + 1) * sizeof(int64_t), st));
+            LAUNCH(launch_keys_to_csr(keys2, nnz, n, G, col, cnt, st));
+            int64_t* rp = ws<int64_t>(ctx, "rowptr", G + 1);
+            size_t tb2 = 0;
+            cub::DeviceScan::ExclusiveSum(nullptr, tb2, cnt, rp, (int)(G + 1), st);
+            void* tmp2 = ws<char>(ctx, "scan_tmp", tb2);
+            CK(cub::DeviceScan::ExclusiveSum(tmp2, tb2, cnt, rp, (int)(G + 1), st));
+            ctx->launches++;
+            float* v = ws<float>(ctx, "val32", nnz);
+            LAUNCH(launch_csr_f64_to_f32(v2, v, nnz, st));
+            dp.rowptr = rp;
+            dp.col = col;
+            dp.val = v;
+            dp.val_u16 = 0;
+            dp.nnz = nnz;
+            return;
+        }
+    }
+    fail(ctx, DEVIL_ERR_ARG, "unsupported counts format");
+}
+
+void use_device_counts(devil_ctx* ctx, const devil_counts* c, DevProblem& dp) {
+    if (c->format != DEVIL_COUNTS_CSR_U16 && c->format != DEVIL_COUNTS_CSR_F32)
+        fail(ctx, DEVIL_ERR_ARG, "device counts must be CSR (uint16 or float)");
+    dp.G = c->n_genes;
+    dp.n = c->n_cells;
+    dp.rowptr = c->ptr;
+    dp.col = c->idx;
+    dp.val = c->values;
+    dp.val_u16 = c->format == DEVIL_COUNTS_CSR_U16;
+    dp.nnz = c->nnz;
+    validate_csr(ctx, dp);
+}
+
+// design, segmentation, statistics
+void prepare_design(devil_ctx* ctx, DevProblem& dp, const double* X, int P, bool X_on_device) {
+    if (P < 1 || P > 32) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d outside 1..32", P);
+    if (dp.n <= P) fail(ctx, DEVIL_ERR_ARG, "need more cells than design columns");
+    dp.P = P;
+    dp.xs = xs_for(P);
+    cudaStream_t st = ctx->stream;
+    if (X_on_device) {
+        dp.Xcm = X;
+    } else {
+        double* xd = ws<double>(ctx, "Xcm", (size_t)dp.n * P);
+        h2d(ctx, xd, X, (size_t)dp.n * P);
+        dp.Xcm = xd;
+    }
+    dp.Xrm = ws<float>(ctx, "Xrm", (size_t)dp.n * dp.xs);
+    LAUNCH(launch_x_rowmajor(dp.Xcm, dp.n, P, dp.xs, dp.Xrm, st));
+    // uniform fine segmentation: power-of-two count, >= 1024 cells each
+    int nf = (int)std::min<int64_t>(64, std::max<int64_t>(1, dp.n / 1024));
+    nf = pow2_floor(nf);
+    dp.nfine = nf;
+    std::vector<int32_t> hb(nf + 1);
+    for (int s = 0; s <= nf; ++s) hb[s] = (int32_t)((dp.n * s) / nf);
+    dp.fine_bound = ws<int32_t>(ctx, "fine_bound", nf + 1);
+    h2d(ctx, dp.fine_bound, hb.data(), nf + 1);
+    dp.fine_ptr = ws<int64_t>(ctx, "fine_ptr", (size_t)dp.G * (nf + 1));
+    LAUNCH(launch_segptr(dp.rowptr, dp.col, dp.G, dp.fine_bound, nf + 1, dp.fine_ptr, st));
+    dp.stats = ws<double>(ctx, "stats", (size_t)dp.G * 6);
+    LAUNCH(launch_gene_stats(dp.rowptr, dp.val, dp.val_u16, dp.G, dp.n, dp.stats, st));
+    CK(cudaStreamSynchronize(st));  // host copies above must stay valid until here
+}
+
+// size factors and offsets (R/main.R:224-230, R/size_factors.R)
+void compute_offsets(devil_ctx* ctx, DevProblem& dp, int method, const double* sf_given_host,
+                     const double* sf_given_dev, double offset) {
+    cudaStream_t st = ctx->stream;
+    const int64_t n = dp.n;
+    dp.sf = ws<double>(ctx, "sf", n);
+    dp.off = ws<double>(ctx, "off", n);
+    dp.off_f = ws<float>(ctx, "off_f", n);
+    if (method == DEVIL_SF_NONE) {
+        LAUNCH(launch_sf_given(nullptr, n, offset, 0, dp.sf, dp.off, dp.off_f, st));
+        return;
+    }
+    if (method == DEVIL_SF_GIVEN) {
+        const double* src = sf_given_dev;
+        if (!src) {
+            if (!sf_given_host) fail(ctx, DEVIL_ERR_ARG, "size factors not given");
+            double* t = ws<double>(ctx, "sf_in", n);
+            h2d(ctx, t, sf_given_host, n);
+            src = t;
+        }
+        LAUNCH(launch_sf_given(src, n, offset, 1, dp.sf, dp.off, dp.off_f, st));
+        return;
+    }
+    if (method != DEVIL_SF_NORMED_SUM && method != DEVIL_SF_PSINORM)
+        fail(ctx, DEVIL_ERR_ARG, "unknown size factor method %d", method);
+    double* colsum = ws<double>(ctx, "colsum", n);
+    CK(cudaMemsetAsync(colsum, 0, n * sizeof(double), st));
+    double* collog = nullptr;
+    int32_t *colcnt = nullptr, *colmin = nullptr;
+    if (method == DEVIL_SF_PSINORM) {
+        collog = ws<double>(ctx, "collog", n);
+        colcnt = ws<int32_t>(ctx, "colcnt", n);
+        colmin = ws<int32_t>(ctx, "colmin", n);
+        CK(cudaMemsetAsync(collog, 0, n * sizeof(double), st));
+        CK(cudaMemsetAsync(colcnt, 0, n * sizeof(int32_t), st));
+        CK(cudaMemsetAsync(colmin, 0x7f, n * sizeof(int32_t), st));  // ~ +3.4e38
+    }
+    LAUNCH(launch_colstats(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.G, dp.nnz, colsum, collog,
+                           colcnt, colmin, st));
+    int32_t* err = ws<int32_t>(ctx, "sf_err", 1);
+    LAUNCH(launch_sf_finalize(method == DEVIL_SF_NORMED_SUM ? 1 : 2, dp.G, n, colsum, collog, colcnt,
+                              colmin, offset, dp.sf, dp.off, dp.off_f, err, st));
+    int32_t herr = 0;
+    CK(cudaMemcpyAsync(&herr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (herr)
+        fail(ctx, DEVIL_ERR_ZERO_COLUMN,
+             "At least one column (sample) contains all zeros, unable to compute size factor. "
+             "Please filter out empty samples from input matrix.");
+}
+
+// ------------------------------------------------------------------
+// the gene x cell pass driver
+// ------------------------------------------------------------------
+struct PassPlan {
+    Engine engine;
+    int GT;
+};
+
+PassPlan plan_for(PassKind k, int P, int form) {
+    if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, 1};
+    if (P <= reg_max_p()) {
+        int gt = reg_default_gt(k, P);
+        if (k == PASS_IRLS) {
+            const char* e = getenv("DEVIL_IRLS_GT");
+            if (e) {
+                int v = atoi(e);
+                if (reg_gt_supported(k, P, v)) gt = v;
+            }
+        }
+        return {ENGINE_REG, gt};
+    }
+    return {ENGINE_GEN, gen_default_gt(k, P)};
+}
+
+// number of cell-segment work items for `tiles` gene tiles
+int choose_nseg(devil_ctx* ctx, const DevProblem& dp, int tiles, int form) {
+    if (form == DEVIL_FORM_PLAIN) return 1;
+    const int target = ctx->sm_count * 2;
+    int want = (target + tiles - 1) / tiles;
+    int nseg = 1;
+    while (nseg < want && nseg < dp.nfine) nseg *= 2;
+    return nseg;
+}
+
+// largest nseg * tiles * GT over every active-gene count the loops can see
+size_t max_slot_segs(devil_ctx* ctx, const DevProblem& dp, int GT, int form) {
+    const int max_tiles = (int)((dp.G + GT - 1) / GT);
+    size_t best = 0;
+    for (int tiles = 1; tiles <= max_tiles; ++tiles) {
+        size_t v = (size_t)choose_nseg(ctx, dp, tiles, form) * tiles * GT;
+        if (v > best) best = v;
+    }
+    return best;
+}
+
+struct PassBuffers {
+    float* partW;
+    double* partS;
+};
+
+PassBuffers pass_buffers(devil_ctx* ctx, PassKind k, int P, size_t slots_x_segs) {
+    PassBuffers b;
+    b.partW = ws<float>(ctx, "partW", slots_x_segs * std::max(1, pass_na(k, P)));
+    b.partS = ws<double>(ctx, "partS", slots_x_segs * std::max(1, pass_ns(k)));
+    return b;
+}
+
+void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const PassPlan& plan,
+                 int nseg, int fpi, int tiles, const int32_t* bound, const int64_t* segptr,
+                 int nbound, const int32_t* act, const int32_t* n_act, int32_t* reset_next,
+                 const PassBuffers& pb, const PassParamsAny& prm) {
+    PassLaunch L;
+    L.kind = kind;
+    L.engine = plan.engine;
+    L.P = dp.P;
+    L.xs_pad = dp.xs;
+    L.GT = plan.GT;
+    L.val_u16 = dp.val_u16;
+    L.nseg = nseg;
+    L.ntiles = tiles;
+    L.geo.X = dp.Xrm;
+    L.geo.xs = dp.xs;
+    L.geo.off = dp.off_f;
+    L.geo.col = dp.col;
+    L.geo.val = dp.val;
+    L.geo.segptr = segptr;
+    L.geo.bound = bound;
+    L.geo.nbound = nbound;
+    L.geo.fpi = fpi;
+    L.geo.act = act;
+    L.geo.n_act = n_act;
+    L.geo.reset_next = reset_next;
+    L.geo.partW = pb.partW;
+    L.geo.partS = pb.partS;
+    L.geo.slot_stride = tiles * plan.GT;
+    L.prm = prm;
+    L.stream = ctx->stream;
+    if (plan.engine == ENGINE_REG)
+        LAUNCH(launch_reg_pass(L));
+    else
+        LAUNCH(launch_gen_pass(L));
+}
+
+// all-genes list (for one-shot passes)
+const int32_t* all_genes(devil_ctx* ctx, const DevProblem& dp, int32_t** count_out) {
+    int32_t* a = ws<int32_t>(ctx, "all_genes", dp.G);
+    int32_t* c = ws<int32_t>(ctx, "all_count", 4);
+    LAUNCH(launch_iota(a, dp.G, ctx->stream));
+    LAUNCH(launch_set_i32(c, (int32_t)dp.G, ctx->stream));
+    *count_out = c;
+    return a;
+}
+
+// ------------------------------------------------------------------
+// IRLS loop (src/beta.cpp:25-51) with active-gene compaction
+// ------------------------------------------------------------------
+void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f, const float* k,
+              int32_t* iters, int32_t* status, int max_iter, double eps, int form) {
+    cudaStream_t st = ctx->stream;
+    const int64_t G = dp.G;
+    CK(cudaMemsetAsync(iters, 0, G * sizeof(int32_t), st));
+    CK(cudaMemsetAsync(status, 0, G * sizeof(int32_t), st));
+    if (G == 0 || max_iter <= 0) return;
+    const PassPlan plan = plan_for(PASS_IRLS, dp.P, form);
+    if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported", dp.P);
+    int32_t* act[2] = {ws<int32_t>(ctx, "act0", G), ws<int32_t>(ctx, "act1", G)};
+    int32_t* cnt = ws<int32_t>(ctx, "cnt", 4);
+    LAUNCH(launch_iota(act[0], G, st));
+    LAUNCH(launch_set_i32(cnt, (int32_t)G, st));
+    LAUNCH(launch_set_i32(cnt + 1, 0, st));
+    PassBuffers pb = pass_buffers(ctx, PASS_IRLS, dp.P, max_slot_segs(ctx, dp, plan.GT, form));
+    *ctx->mapped_host = (int32_t)G;
+    const int LAG = 2;
+    PassParamsAny prm{beta_f, k, nullptr, nullptr};
+    for (int t = 0; t < max_iter; ++t) {
+        const int cur = t & 1, nxt = cur ^ 1;
+        int64_t hint;
+        if (form == DEVIL_FORM_PLAIN) {
+            CK(cudaStreamSynchronize(st));
+            hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
+        } else {
+            hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
+        }
+        if (hint <= 0) break;
+        const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
+        const int nseg = choose_nseg(ctx, dp, tiles, form);
+        const int fpi = dp.nfine / nseg;
+        launch_pass(ctx, dp, PASS_IRLS, plan, nseg, fpi, tiles, dp.fine_bound, dp.fine_ptr,
+                    dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
+        LAUNCH(launch_irls_finalize(pb.partW, nseg, tiles * plan.GT, dp.P, act[cur], cnt + cur,
+                                    (int)hint, act[nxt], cnt + nxt, beta, beta_f, iters, status,
+                                    max_iter, eps, nullptr, st));
+        LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
+        CK(cudaEventRecord(ctx->ev[t & 3], st));
+        if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
+    }
+}
+
+// MOM theta for all genes (src/mom_overdispersion.cpp)
+void run_mom(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, double* theta, int form) {
+    if (dp.G == 0) return;
+    const PassPlan plan = plan_for(PASS_MOM, dp.P, form);
+    int32_t* cnt = nullptr;
+    const int32_t* act = all_genes(ctx, dp, &cnt);
+    const int tiles = (int)((dp.G + plan.GT - 1) / plan.GT);
+    const int nseg = choose_nseg(ctx, dp, tiles, form);
+    PassBuffers pb = pass_buffers(ctx, PASS_MOM, dp.P, (size_t)nseg * tiles * plan.GT);
+    PassParamsAny prm{beta_f, nullptr, nullptr, nullptr};
+    launch_pass(ctx, dp, PASS_MOM, plan, nseg, dp.nfine / nseg, tiles, dp.fine_bound, dp.fine_ptr,
+                dp.nfine + 1, act, cnt, nullptr, pb, prm);
+    LAUNCH(launch_mom_finalize(pb.partS, nseg, tiles * plan.GT, act, cnt, (int)dp.G, dp.n, dp.P,
+                               theta, ctx->stream));
+}
+
+// MLE theta (R/overdispersion.R:25-115)
+void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, double* theta,
+             int32_t* newton_iters, int max_iter, int cox_reid, int form) {
+    cudaStream_t st = ctx->stream;
+    const int64_t G = dp.G;
+    if (G == 0) return;
+    const PassPlan plan = plan_for(PASS_MLE, dp.P, form);
+    if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported for MLE", dp.P);
+    MleState s;
+    s.x = ws<double>(ctx, "mle_x", G);
+    s.lo = ws<double>(ctx, "mle_lo", G);
+    s.hi = ws<double>(ctx, "mle_hi", G);
+    s.it = newton_iters ? newton_iters : ws<int32_t>(ctx, "mle_it", G);
+    s.phase = ws<int32_t>(ctx, "mle_phase", G);
+    s.theta = theta;
+    int32_t* act[2] = {ws<int32_t>(ctx, "act0", G), ws<int32_t>(ctx, "act1", G)};
+    int32_t* cnt = ws<int32_t>(ctx, "cnt", 4);
+    LAUNCH(launch_set_i32(cnt, 0, st));
+    LAUNCH(launch_set_i32(cnt + 1, 0, st));
+    LAUNCH(launch_mle_init(dp.stats, G, dp.n, s, act[0], cnt, st));
+    PassBuffers pb = pass_buffers(ctx, PASS_MLE, dp.P, max_slot_segs(ctx, dp, plan.GT, form));
+    *ctx->mapped_host = (int32_t)G;
+    const int LAG = 2;
+    PassParamsAny prm{beta_f, nullptr, s.x, nullptr};
+    // one far-left evaluation plus at most max_iter Newton evaluations
+    for (int t = 0; t <= max_iter; ++t) {
+        const int cur = t & 1, nxt = cur ^ 1;
+        int64_t hint;
+        if (form == DEVIL_FORM_PLAIN) CK(cudaStreamSynchronize(st));
+        hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
+        if (hint <= 0) break;
+        const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
+        const int nseg = choose_nseg(ctx, dp, tiles, form);
+        launch_pass(ctx, dp, PASS_MLE, plan, nseg, dp.nfine / nseg, tiles, dp.fine_bound,
+                    dp.fine_ptr, dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
+        LAUNCH(launch_mle_finalize(pb.partW, pb.partS, nseg, tiles * plan.GT, dp.P, dp.stats, dp.n,
+                                   act[cur], cnt + cur, (int)hint, act[nxt], cnt + nxt, s, max_iter,
+                                   cox_reid, nullptr, st));
+        LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
+        CK(cudaEventRecord(ctx->ev[t & 3], st));
+        if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
+    }
+}
+
+// bread + clustered meat + sandwich for all genes
+void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const double* theta,
+                  const int32_t* ends_host, int n_clusters, double* bread, double* sandwich,
+                  double* meat, int form) {
+    cudaStream_t st = ctx->stream;
+    if (dp.G == 0) return;
+    const PassPlan plan = plan_for(PASS_SANDWICH, dp.P, form);
+    if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported", dp.P);
+    int32_t* cnt = nullptr;
+    const int32_t* act = all_genes(ctx, dp, &cnt);
+    const int tiles = (int)((dp.G + plan.GT - 1) / plan.GT);
+    PassParamsAny prm{beta_f, nullptr, nullptr, theta};
+    if (n_clusters <= 0) {
+        const int nseg = choose_nseg(ctx, dp, tiles, form);
+        PassBuffers pb = pass_buffers(ctx, PASS_SANDWICH, dp.P, (size_t)nseg * tiles * plan.GT);
+        launch_pass(ctx, dp, PASS_SANDWICH, plan, nseg, dp.nfine / nseg, tiles, dp.fine_bound,
+                    dp.fine_ptr, dp.nfine + 1, act, cnt, nullptr, pb, prm);
+        LAUNCH(launch_sandwich_finalize(pb.partW, nseg, tiles * plan.GT, dp.P, nullptr, 0, dp.n,
+                                        act, cnt, (int)dp.G, bread, nullptr, nullptr, st));
+        return;
+    }
+    // cluster-aligned segments: every cluster block split into pieces of
+    // at most L cells (1-based exclusive ends, R/main.R:193)
+    const int64_t n = dp.n;
+    int want = (form == DEVIL_FORM_PLAIN) ? 1 : (ctx->sm_count * 2 + tiles - 1) / tiles;
+    int64_t L = std::max<int64_t>(1024, (n + want - 1) / std::max(1, want));
+    std::vector<int32_t> hb{0};
+    std::vector<int32_t> hc;
+    int64_t start = 0;
+    for (int b = 0; b < n_clusters; ++b) {
+        int64_t end = ends_host[b];
+        if (end < start || end > n) fail(ctx, DEVIL_ERR_ARG, "cluster ends must be non-decreasing and <= n");
+        if (end == start) continue;
+        int64_t pieces = (end - start + L - 1) / L;
+        for (int64_t q = 1; q <= pieces; ++q) {
+            hb.push_back((int32_t)(start + ((end - start) * q) / pieces));
+            hc.push_back(b);
+        }
+        start = end;
+    }
+    if (start != n) fail(ctx, DEVIL_ERR_ARG, "last cluster end must equal the number of cells");
+    const int nseg = (int)hc.size();
+    int32_t* bound = ws<int32_t>(ctx, "sw_bound", hb.size());
+    int32_t* segc = ws<int32_t>(ctx, "sw_segc", hc.size());
+    h2d(ctx, bound, hb.data(), hb.size());
+    h2d(ctx, segc, hc.data(), hc.size());
+    int64_t* segptr = ws<int64_t>(ctx, "sw_segptr", (size_t)dp.G * hb.size());
+    LAUNCH(launch_segptr(dp.rowptr, dp.col, dp.G, bound, (int)hb.size(), segptr, st));
+    PassBuffers pb = pass_buffers(ctx, PASS_SANDWICH, dp.P, (size_t)nseg * tiles * plan.GT);
+    launch_pass(ctx, dp, PASS_SANDWICH, plan, nseg, 1, tiles, bound, segptr, (int)hb.size(), act,
+                cnt, nullptr, pb, prm);
+    LAUNCH(launch_sandwich_finalize(pb.partW, nseg, tiles * plan.GT, dp.P, segc, n_clusters, dp.n,
+                                    act, cnt, (int)dp.G, bread, sandwich, meat, st));
+    CK(cudaStreamSynchronize(st));  // host vectors hb/hc go out of scope
+}
+
+struct FitBuffers {
+    double* beta;
+    float* beta_f;
+    float* k;
+    double* theta0;
+    double* theta;
+    double* theta_mom;
+    int32_t* iters;
+    int32_t* status;
+    int32_t* titers;
+    double* bread;
+    double* sandwich;
+};
+
+// cpu_fit order: theta_0 -> beta | theta_0 -> theta | beta -> bread, meat
+void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int n_clusters,
+                  const devil_fit_opts* o, FitBuffers& fb) {
+    cudaStream_t st = ctx->stream;
+    const int64_t G = dp.G;
+    const int P = dp.P;
+    LAUNCH(launch_theta0(dp.stats, dp.off, G, dp.n, o->has_init_overdispersion,
+                         o->init_overdispersion, fb.theta0, fb.k, st));
+    double* ginv = ws<double>(ctx, "ginv", (size_t)P * P);
+    int32_t* err = ws<int32_t>(ctx, "qr_err", 1);
+    if (!o->init_beta_rough) {
+        LAUNCH(launch_xtx_inverse(dp.Xcm, dp.n, P, ginv, err, st));
+        int32_t herr = 0;
+        CK(cudaMemcpyAsync(&herr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (herr) fail(ctx, DEVIL_ERR_SINGULAR, "design matrix is rank deficient");
+    }
+    LAUNCH(launch_init_beta(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.Xcm, dp.off, ginv, dp.stats,
+                            G, dp.n, P, o->init_beta_rough, fb.beta, fb.beta_f, st));
+    const double eps = (double)(float)o->tolerance;
+    run_irls(ctx, dp, fb.beta, fb.beta_f, fb.k, fb.iters, fb.status, o->max_iter, eps, o->form);
+    if (fb.theta_mom || o->overdispersion == DEVIL_OD_MOM) {
+        double* tm = fb.theta_mom ? fb.theta_mom : fb.theta;
+        run_mom(ctx, dp, fb.beta_f, tm, o->form);
+        if (o->overdispersion == DEVIL_OD_MOM && tm != fb.theta)
+            CK(cudaMemcpyAsync(fb.theta, tm, G * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    if (o->overdispersion == DEVIL_OD_MLE) {
+        run_mle(ctx, dp, fb.beta_f, fb.theta, nullptr, o->max_iter, 1, o->form);
+    } else if (o->overdispersion == DEVIL_OD_NONE) {
+        CK(cudaMemsetAsync(fb.theta, 0, G * sizeof(double), st));
+    }
+    run_sandwich(ctx, dp, fb.beta_f, fb.theta, ends_host, n_clusters, fb.bread,
+                 n_clusters > 0 ? fb.sandwich : nullptr, nullptr, o->form);
+}
+
+void alloc_fit_buffers(devil_ctx* ctx, int64_t G, int P, bool theta_mom, bool clusters,
+                       FitBuffers& fb) {
+    fb.beta = ws<double>(ctx, "beta", (size_t)G * P);
+    fb.beta_f = ws<float>(ctx, "beta_f", (size_t)G * P);
+    fb.k = ws<float>(ctx, "k", G);
+    fb.theta0 = ws<double>(ctx, "theta0", G);
+    fb.theta = ws<double>(ctx, "theta", G);
+    fb.theta_mom = theta_mom ? ws<double>(ctx, "theta_mom", G) : nullptr;
+    fb.iters = ws<int32_t>(ctx, "iters", G);
+    fb.status = ws<int32_t>(ctx, "status", G);
+    fb.titers = ws<int32_t>(ctx, "titers", G);
+    fb.bread = ws<double>(ctx, "bread", (size_t)G * P * P);
+    fb.sandwich = clusters ? ws<double>(ctx, "sandwich", (size_t)G * P * P) : nullptr;
+}
+
+void validate_opts(devil_ctx* ctx, const devil_fit_opts* o) {
+    if (!o) fail(ctx, DEVIL_ERR_ARG, "opts is NULL");
+    if (o->overdispersion < 0 || o->overdispersion > 2)
+        fail(ctx, DEVIL_ERR_UNSUPPORTED, "overdispersion mode %d not supported", o->overdispersion);
+    if (o->form != DEVIL_FORM_CHOSEN && o->form != DEVIL_FORM_PLAIN)
+        fail(ctx, DEVIL_ERR_ARG, "unknown form %d", o->form);
+}
+
+template <class F>
+int guarded(devil_ctx* ctx, F&& f) {
+    if (!ctx) return DEVIL_ERR_ARG;
+    try {
+        CK(cudaSetDevice(ctx->device));
+        f();
+        return DEVIL_OK;
+    } catch (const Fail& e) {
+        return e.code;
+    } catch (const std::exception& e) {
+        ctx->err = e.what();
+        return DEVIL_ERR_ARG;
+    }
+}
+
+}  // namespace
+
+// ====================================================================
+// public API
+// ====================================================================
+extern "C" {
+
+const char* devil_version(void) { return "devil_b200 0.1.0 (sm_100a)"; }
+
+void devil_fit_opts_default(devil_fit_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->max_iter = 200;
+    o->tolerance = 1e-3;
+    o->overdispersion = DEVIL_OD_MOM;
+    o->size_factors = DEVIL_SF_NONE;
+    o->form = DEVIL_FORM_CHOSEN;
+}
+
+int devil_ctx_create(int device, devil_ctx** out) {
+    if (!out) return DEVIL_ERR_ARG;
+    *out = nullptr;
+    devil_ctx* ctx = new devil_ctx();
+    ctx->device = device;
+    int rc = guarded(ctx, [&] {
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        CK(cudaHostAlloc(&ctx->mapped_host, sizeof(int32_t) * 4, cudaHostAllocMapped));
+        CK(cudaHostGetDevicePointer((void**)&ctx->mapped_dev, ctx->mapped_host, 0));
+        for (auto& e : ctx->ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
+    });
+    if (rc != DEVIL_OK) {
+        fprintf(stderr, "devil_ctx_create: %s\n", ctx->err.c_str());
+        devil_ctx_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return DEVIL_OK;
+}
+
+int devil_ctx_destroy(devil_ctx* ctx) {
+    if (!ctx) return DEVIL_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->bufs)
+        if (kv.second.p) cudaFree(kv.second.p);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->mapped_host) cudaFreeHost(ctx->mapped_host);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return DEVIL_OK;
+}
+
+const char* devil_last_error(const devil_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+void* devil_ctx_stream(devil_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+int devil_ctx_synchronize(devil_ctx* ctx) {
+    return guarded(ctx, [&] { CK(cudaStreamSynchronize(ctx->stream)); });
+}
+int64_t devil_ctx_launch_count(const devil_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int devil_fit(devil_ctx* ctx, const devil_counts* counts, const double* X, int p,
+              const int32_t* cluster_ends, int n_clusters, const devil_fit_opts* opts,
+              devil_fit_result* res) {
+    return guarded(ctx, [&] {
+        validate_opts(ctx, opts);
+        check_counts(ctx, counts);
+        if (!X || !res || !res->beta || !res->theta || !res->beta_iters)
+            fail(ctx, DEVIL_ERR_ARG, "X and result beta/theta/beta_iters are required");
+        if (n_clusters > 0 && !cluster_ends) fail(ctx, DEVIL_ERR_ARG, "cluster_ends is NULL");
+        DevProblem dp;
+        upload_counts(ctx, counts, dp);
+        prepare_design(ctx, dp, X, p, false);
+        compute_offsets(ctx, dp, opts->size_factors, opts->size_factor_values, nullptr, opts->offset);
+        FitBuffers fb;
+        alloc_fit_buffers(ctx, dp.G, p, res->theta_mom && opts->compute_theta_mom, n_clusters > 0, fb);
+        fit_pipeline(ctx, dp, cluster_ends, n_clusters, opts, fb);
+        const int64_t G = dp.G;
+        d2h(ctx, res->beta, fb.beta, (size_t)G * p);
+        d2h(ctx, res->theta, fb.theta, G);
+        d2h(ctx, res->beta_iters, fb.iters, G);
+        d2h(ctx, res->status, fb.status, G);
+        d2h(ctx, res->bread, fb.bread, (size_t)G * p * p);
+        if (n_clusters > 0) d2h(ctx, res->sandwich, fb.sandwich, (size_t)G * p * p);
+        if (fb.theta_mom) d2h(ctx, res->theta_mom, fb.theta_mom, G);
+        d2h(ctx, res->size_factors, dp.sf, dp.n);
+        d2h(ctx, res->offset_vector, dp.off, dp.n);
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (res->theta_iters) {
+            int32_t v = opts->overdispersion == DEVIL_OD_MLE ? INT32_MIN : 0;
+            for (int64_t g = 0; g < G; ++g) res->theta_iters[g] = v;
+        }
+    });
+}
+
+int devil_fit_device(devil_ctx* ctx, const devil_counts* counts_dev, const double* X_dev, int p,
+                     const int32_t* cluster_ends_host, int n_clusters, const devil_fit_opts* opts,
+                     devil_fit_result* r) {
+    return guarded(ctx, [&] {
+        validate_opts(ctx, opts);
+        if (!counts_dev || !X_dev || !r || !r->beta || !r->theta || !r->beta_iters)
+            fail(ctx, DEVIL_ERR_ARG, "counts, X and result beta/theta/beta_iters are required");
+        DevProblem dp;
+        use_device_counts(ctx, counts_dev, dp);
+        prepare_design(ctx, dp, X_dev, p, true);
+        compute_offsets(ctx, dp, opts->size_factors, nullptr, opts->size_factor_values, opts->offset);
+        FitBuffers fb;
+        alloc_fit_buffers(ctx, dp.G, p, r->theta_mom && opts->compute_theta_mom, n_clusters > 0, fb);
+        // write straight into the caller's device buffers where given
+        fb.beta = r->beta;
+        fb.theta = r->theta;
+        fb.iters = r->beta_iters;
+        if (r->status) fb.status = r->status;
+        if (r->bread) fb.bread = r->bread;
+        if (r->sandwich && n_clusters > 0) fb.sandwich = r->sandwich;
+        if (r->theta_mom && opts->compute_theta_mom) fb.theta_mom = r->theta_mom;
+        fit_pipeline(ctx, dp, cluster_ends_host, n_clusters, opts, fb);
+        if (r->size_factors)
+            CK(cudaMemcpyAsync(r->size_factors, dp.sf, dp.n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (r->offset_vector)
+            CK(cudaMemcpyAsync(r->offset_vector, dp.off, dp.n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+    });
+}
+
+// ------------------------------------------------------------------
+int devil_test_de_device(devil_ctx* ctx, int64_t G, int p, const double* beta_dev,
+                         const double* bread_dev, const double* sandwich_dev, int64_t n_samples,
+                         const double* contrast_host, int adjust_method, double max_lfc,
+                         double* pval_dev, double* adj_dev, double* lfc_dev) {
+    return guarded(ctx, [&] {
+        if (p < 1 || p > 64 || !contrast_host) fail(ctx, DEVIL_ERR_ARG, "bad p or contrast");
+        if (adjust_method < 0 || adjust_method > 5) fail(ctx, DEVIL_ERR_UNSUPPORTED, "adjust method");
+        double* c = ws<double>(ctx, "contrast", p);
+        h2d(ctx, c, contrast_host, p);
+        LAUNCH(launch_test_pvalues(G, p, beta_dev, bread_dev, sandwich_dev, (double)(n_samples - 2), c,
+                                   max_lfc, pval_dev, lfc_dev, ctx->stream));
+        size_t tb = p_adjust_temp_bytes(G);
+        void* tmp = ws<char>(ctx, "padj_tmp", tb);
+        LAUNCH(launch_p_adjust(G, pval_dev, adjust_method, adj_dev, tmp, tb, ctx->stream));
+        ctx->launches += 2;
+        CK(cudaStreamSynchronize(ctx->stream));  // contrast upload source
+    });
+}
+
+int devil_test_de(devil_ctx* ctx, int64_t G, int p, const double* beta, const double* bread,
+                  const double* sandwich, int64_t n_samples, const double* contrast,
+                  int adjust_method, double max_lfc, double* pval, double* adj_pval, double* lfc) {
+    return guarded(ctx, [&] {
+        if (!beta || !bread || !pval || !adj_pval || !lfc) fail(ctx, DEVIL_ERR_ARG, "null argument");
+        double* b = ws<double>(ctx, "t_beta", (size_t)G * p);
+        double* br = ws<double>(ctx, "t_bread", (size_t)G * p * p);
+        double* sw = sandwich ? ws<double>(ctx, "t_sw", (size_t)G * p * p) : nullptr;
+        double* pv = ws<double>(ctx, "t_p", G);
+        double* pa = ws<double>(ctx, "t_pa", G);
+        double* lf = ws<double>(ctx, "t_lfc", G);
+        h2d(ctx, b, beta, (size_t)G * p);
+        h2d(ctx, br, bread, (size_t)G * p * p);
+        if (sw) h2d(ctx, sw, sandwich, (size_t)G * p * p);
+        int rc = devil_test_de_device(ctx, G, p, b, br, sw, n_samples, contrast, adjust_method,
+                                      max_lfc, pv, pa, lf);
+        if (rc != DEVIL_OK) throw Fail{rc};
+        d2h(ctx, pval, pv, G);
+        d2h(ctx, adj_pval, pa, G);
+        d2h(ctx, lfc, lf, G);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int devil_p_adjust(devil_ctx* ctx, int64_t m, const double* p, int method, double* out) {
+    return guarded(ctx, [&] {
+        if (method < 0 || method > 5) fail(ctx, DEVIL_ERR_UNSUPPORTED, "adjust method");
+        double* pd = ws<double>(ctx, "pa_in", m);
+        double* od = ws<double>(ctx, "pa_out", m);
+        h2d(ctx, pd, p, m);
+        size_t tb = p_adjust_temp_bytes(m);
+        void* tmp = ws<char>(ctx, "padj_tmp", tb);
+        LAUNCH(launch_p_adjust(m, pd, method, od, tmp, tb, ctx->stream));
+        d2h(ctx, out, od, m);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+// ------------------------------------------------------------------
+// single steps
+// ------------------------------------------------------------------
+int devil_calculate_sf(devil_ctx* ctx, const devil_counts* counts, int method, double* sf) {
+    return guarded(ctx, [&] {
+        check_counts(ctx, counts);
+        if (method != DEVIL_SF_NORMED_SUM && method != DEVIL_SF_PSINORM)
+            fail(ctx, DEVIL_ERR_ARG, "'arg' should be one of \"normed_sum\", \"psinorm\"");
+        DevProblem dp;
+        upload_counts(ctx, counts, dp);
+        compute_offsets(ctx, dp, method, nullptr, nullptr, 0.0);
+        d2h(ctx, sf, dp.sf, dp.n);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+static void upload_offsets(devil_ctx* ctx, DevProblem& dp, const double* offv_host) {
+    dp.sf = ws<double>(ctx, "sf", dp.n);
+    dp.off = ws<double>(ctx, "off", dp.n);
+    dp.off_f = ws<float>(ctx, "off_f", dp.n);
+    h2d(ctx, dp.off, offv_host, dp.n);
+    LAUNCH(launch_double_to_float(dp.off, dp.off_f, dp.n, ctx->stream));
+}
+static void upload_sf_as_offsets(devil_ctx* ctx, DevProblem& dp, const double* sf_host) {
+    compute_offsets(ctx, dp, DEVIL_SF_GIVEN, sf_host, nullptr, 0.0);
+}
+
+int devil_estimate_dispersion(devil_ctx* ctx, const devil_counts* counts,
+                              const double* offset_vector, double* theta0) {
+    return guarded(ctx, [&] {
+        check_counts(ctx, counts);
+        DevProblem dp;
+        upload_counts(ctx, counts, dp);
+        dp.stats = ws<double>(ctx, "stats", (size_t)dp.G * 6);
+        LAUNCH(launch_gene_stats(dp.rowptr, dp.val, dp.val_u16, dp.G, dp.n, dp.stats, ctx->stream));
+        upload_offsets(ctx, dp, offset_vector);
+        double* th = ws<double>(ctx, "theta0", dp.G);
+        float* k = ws<float>(ctx, "k", dp.G);
+        LAUNCH(launch_theta0(dp.stats, dp.off, dp.G, dp.n, 0, 0.0, th, k, ctx->stream));
+        d2h(ctx, theta0, th, dp.G);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int devil_init_beta(devil_ctx* ctx, const devil_counts* counts, const double* X, int p,
+                    const double* offset_vector, int rough, double* beta0) {
+    return guarded(ctx, [&] {
+        check_counts(ctx, counts);
+        DevProblem dp;
+        upload_counts(ctx, counts, dp);
+        prepare_design(ctx, dp, X, p, false);
+        upload_offsets(ctx, dp, offset_vector);
+        double* ginv = ws<double>(ctx, "ginv", (size_t)p * p);
+        int32_t* err = ws<int32_t>(ctx, "qr_err", 1);
+        if (!rough) {
+            LAUNCH(launch_xtx_inverse(dp.Xcm, dp.n, p, ginv, err, ctx->stream));
+            int32_t herr = 0;
+            CK(cudaMemcpyAsync(&herr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (herr) fail(ctx, DEVIL_ERR_SINGULAR, "design matrix is rank deficient");
+        }
+        double* b = ws<double>(ctx, "beta", (size_t)dp.G * p);
+        float* bf = ws<float>(ctx, "beta_f", (size_t)dp.G * p);
+        LAUNCH(launch_init_beta(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.Xcm, dp.off, ginv, dp.stats,
+                                dp.G, dp.n, p, rough, b, bf, ctx->stream));
+        d2h(ctx, beta0, b, (size_t)dp.G * p);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int devil_beta_fit(devil_ctx* ctx, const devil_counts* counts, const double* X, int p,
+                   const double* beta0, const double* offset_vector, const double* theta0,
+                   int max_iter, double eps, int form, double* beta, int32_t* iters) {
+    return guarded(ctx, [&] {
+        check_counts(ctx, counts);
+        DevProblem dp;
+        upload_counts(ctx, counts, dp);
+        prepare_design(ctx, dp, X, p, false);
+        upload_offsets(ctx, dp, offset_vector);
+        const int64_t G = dp.G;
+        double* b = ws<double>(ctx, "beta", (size_t)G * p);
+        float* bf = ws<float>(ctx, "beta_f", (size_t)G * p);
+        double* th = ws<double>(ctx, "theta0", G);
+        float* k = ws<float>(ctx, "k", G);
+        h2d(ctx, b, beta0, (size_t)G * p);
+        h2d(ctx, th, theta0, G);
+        LAUNCH(launch_double_to_float(b, bf, (size_t)G * p, ctx->stream));
+        // k = 1/theta0 with theta0 rounded to float (src/beta.cpp:25-28)
+        std::vector<float> hk(G);
+        for (int64_t g = 0; g < G; ++g) hk[g] = (float)(1.0 / (double)(float)theta0[g]);
+        h2d(ctx, k, hk.data(), G);
+        int32_t* it = ws<int32_t>(ctx, "iters", G);
+        int32_t* stt = ws<int32_t>(ctx, "status", G);
+        run_irls(ctx, dp, b, bf, k, it, stt, max_iter, (double)(float)eps, form);
+        d2h(ctx, beta, b, (size_t)G * p);
+        d2h(ctx, iters, it, G);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+static void upload_beta(devil_ctx* ctx, const DevProblem& dp, const double* beta, float** bf_out) {
+    double* b = ws<double>(ctx, "beta", (size_t)dp.G * dp.P);
+    float* bf = ws<float>(ctx, "beta_f", (size_t)dp.G * dp.P);
+    h2d(ctx, b, beta, (size_t)dp.G * dp.P);
+    LAUNCH(launch_double_to_float(b, bf, (size_t)dp.G * dp.P, ctx->stream));
+    *bf_out = bf;
+}
+
+int devil_estimate_mom_dispersion(devil_ctx* ctx, const devil_counts* counts, const double* X,
+                                  int p, const double* beta, const double* size_factors,
+                                  double* theta) {
+    return guarded(ctx, [&] {
+        check_counts(ctx, counts);
+        DevProblem dp;
+        upload_counts(ctx, counts, dp);
+        prepare_design(ctx, dp, X, p, false);
+        upload_sf_as_offsets(ctx, dp, size_factors);
+        float* bf;
+        upload_beta(ctx, dp, beta, &bf);
+        double* th = ws<double>(ctx, "theta", dp.G);
+        run_mom(ctx, dp, bf, th, DEVIL_FORM_CHOSEN);
+        d2h(ctx, theta, th, dp.G);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int devil_fit_dispersion(devil_ctx* ctx, const devil_counts* counts, const double* X, int p,
+                         const double* beta, const double* offset_vector, int max_iter, int cox_reid,
+                         double* theta, int32_t* newton_iters) {
+    return guarded(ctx, [&] {
+        check_counts(ctx, counts);
+        DevProblem dp;
+        upload_counts(ctx, counts, dp);
+        prepare_design(ctx, dp, X, p, false);
+        upload_offsets(ctx, dp, offset_vector);
+        float* bf;
+        upload_beta(ctx, dp, beta, &bf);
+        double* th = ws<double>(ctx, "theta", dp.G);
+        int32_t* it = ws<int32_t>(ctx, "mle_iters_out", dp.G);
+        run_mle(ctx, dp, bf, th, it, max_iter, cox_reid, DEVIL_FORM_CHOSEN);
+        d2h(ctx, theta, th, dp.G);
+        d2h(ctx, newton_iters, it, dp.G);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int devil_compute_hessian(devil_ctx* ctx, const devil_counts* counts, const double* X, int p,
+                          const double* beta, const double* overdispersion,
+                          const double* size_factors, double* bread) {
+    return guarded(ctx, [&] {
+        check_counts(ctx, counts);
+        DevProblem dp;
+        upload_counts(ctx, counts, dp);
+        prepare_design(ctx, dp, X, p, false);
+        upload_sf_as_offsets(ctx, dp, size_factors);
+        float* bf;
+        upload_beta(ctx, dp, beta, &bf);
+        double* th = ws<double>(ctx, "theta", dp.G);
+        h2d(ctx, th, overdispersion, dp.G);
+        double* br = ws<double>(ctx, "bread", (size_t)dp.G * p * p);
+        run_sandwich(ctx, dp, bf, th, nullptr, 0, br, nullptr, nullptr, DEVIL_FORM_CHOSEN);
+        d2h(ctx, bread, br, (size_t)dp.G * p * p);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int devil_compute_clustered_meat(devil_ctx* ctx, const devil_counts* counts, const double* X,
+                                 int p, const double* beta, const double* overdispersion,
+                                 const double* size_factors, const int32_t* cluster_ends,
+                                 int n_clusters, double* meat) {
+    return guarded(ctx, [&] {
+        check_counts(ctx, counts);
+        if (n_clusters < 1 || !cluster_ends) fail(ctx, DEVIL_ERR_ARG, "need cluster ends");
+        DevProblem dp;
+        upload_counts(ctx, counts, dp);
+        prepare_design(ctx, dp, X, p, false);
+        upload_sf_as_offsets(ctx, dp, size_factors);
+        float* bf;
+        upload_beta(ctx, dp, beta, &bf);
+        double* th = ws<double>(ctx, "theta", dp.G);
+        h2d(ctx, th, overdispersion, dp.G);
+        double* br = ws<double>(ctx, "bread", (size_t)dp.G * p * p);
+        double* mt = ws<double>(ctx, "meat", (size_t)dp.G * p * p);
+        run_sandwich(ctx, dp, bf, th, cluster_ends, n_clusters, br, nullptr, mt, DEVIL_FORM_CHOSEN);
+        d2h(ctx, meat, mt, (size_t)dp.G * p * p);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int devil_nb_adjoint(devil_ctx* ctx, int64_t n, const double* y, const double* eta,
+                     double log_theta, double* loglik, double* d_eta, double* d_log_theta) {
+    return guarded(ctx, [&] {
+        if (n < 0 || !y || !eta) fail(ctx, DEVIL_ERR_ARG, "null argument");
+        double* yd = ws<double>(ctx, "adj_y", n);
+        double* ed = ws<double>(ctx, "adj_eta", n);
+        double* l = ws<double>(ctx, "adj_l", n);
+        double* de = ws<double>(ctx, "adj_de", n);
+        double* dt = ws<double>(ctx, "adj_dt", n);
+        h2d(ctx, yd, y, n);
+        h2d(ctx, ed, eta, n);
+        LAUNCH(launch_nb_adjoint(n, yd, ed, log_theta, l, de, dt, ctx->stream));
+        d2h(ctx, loglik, l, n);
+        d2h(ctx, d_eta, de, n);
+        d2h(ctx, d_log_theta, dt, n);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+// ------------------------------------------------------------------
+// cluster handling on the host (R's factor / is.unsorted / rle / order)
+// ------------------------------------------------------------------
+int devil_cluster_blocks(int64_t n, const int64_t* clusters, int32_t* levels, int32_t* ends,
+                         int* n_blocks) {
+    if (n < 0 || (n > 0 && (!clusters || !levels || !ends)) || !n_blocks) return DEVIL_ERR_ARG;
+    std::unordered_map<int64_t, int32_t> lev;
+    lev.reserve(64);
+    for (int64_t c = 0; c < n; ++c) {
+        auto it = lev.find(clusters[c]);
+        int32_t v;
+        if (it == lev.end()) {
+            v = (int32_t)lev.size() + 1;
+            lev.emplace(clusters[c], v);
+        } else {
+            v = it->second;
+        }
+        levels[c] = v;
+    }
+    for (int64_t c = 1; c < n; ++c)
+        if (levels[c] < levels[c - 1]) return DEVIL_ERR_UNSORTED;
+    int nb = 0;
+    for (int64_t c = 0; c < n; ++c)
+        if (c == n - 1 || levels[c + 1] != levels[c]) ends[nb++] = (int32_t)(c + 1);
+    *n_blocks = nb;
+    return DEVIL_OK;
+}
+
+int devil_group_order(int64_t n, const int64_t* clusters, int64_t* order) {
+    if (n < 0 || (n > 0 && (!clusters || !order))) return DEVIL_ERR_ARG;
+    std::unordered_map<int64_t, int32_t> lev;
+    std::vector<int32_t> levels(n);
+    for (int64_t c = 0; c < n; ++c) {
+        auto it = lev.find(clusters[c]);
+        if (it == lev.end()) {
+            int32_t v = (int32_t)lev.size();
+            lev.emplace(clusters[c], v);
+            levels[c] = v;
+        } else {
+            levels[c] = it->second;
+        }
+    }
+    std::vector<int64_t> cnt(lev.size() + 1, 0);
+    for (int64_t c = 0; c < n; ++c) cnt[levels[c] + 1]++;
+    for (size_t i = 1; i < cnt.size(); ++i) cnt[i] += cnt[i - 1];
+    for (int64_t c = 0; c < n; ++c) order[cnt[levels[c]]++] = c;  // stable counting sort
+    return DEVIL_OK;
+}
+
+}  // extern "C"

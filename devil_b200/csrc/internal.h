@@ -1,0 +1,136 @@
+// Host-side declarations shared by the kernel translation units and the
+// C-ABI implementation (not installed; the public interface is
+// include/devil_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "passes.cuh"
+
+namespace devil {
+
+enum PassKind { PASS_IRLS = 0, PASS_MOM = 1, PASS_MLE = 2, PASS_SANDWICH = 3 };
+enum Engine { ENGINE_REG = 0, ENGINE_GEN = 1 };
+
+inline int pass_nw(PassKind k) { return k == PASS_MLE ? 3 : (k == PASS_MOM ? 0 : 1); }
+inline int pass_nv(PassKind k) { return (k == PASS_IRLS || k == PASS_SANDWICH) ? 1 : 0; }
+inline int pass_ns(PassKind k) { return k == PASS_MOM ? 2 : (k == PASS_MLE ? 6 : 0); }
+inline int pass_na(PassKind k, int P) { return pass_nw(k) * P * (P + 1) / 2 + pass_nv(k) * P; }
+
+struct PassParamsAny {
+    const float* beta;        // G x P float (all passes)
+    const float* k;           // IRLS
+    const double* log_theta;  // MLE
+    const double* theta;      // SANDWICH
+};
+
+struct PassLaunch {
+    PassKind kind;
+    Engine engine;
+    int P;
+    int xs_pad;     // row stride of geo.X
+    int GT;
+    int val_u16;    // 1: uint16 values, 0: float values
+    int nseg;       // grid.x
+    int ntiles;     // grid.y
+    PassGeom geo;
+    PassParamsAny prm;
+    cudaStream_t stream;
+};
+
+// engine choice helpers
+int reg_max_p();
+int reg_default_gt(PassKind k, int P);
+bool reg_gt_supported(PassKind k, int P, int GT);
+int gen_default_gt(PassKind k, int P);
+size_t gen_smem_bytes(PassKind k, int P, int GT);
+
+cudaError_t launch_reg_pass(const PassLaunch& L);
+cudaError_t launch_gen_pass(const PassLaunch& L);
+
+// ---- preparation kernels (kernels_prep.cu) ----
+cudaError_t launch_dense_count(const void* Y, int is_f64, int cell_major, int64_t G, int64_t n,
+                               int64_t* rowcnt, cudaStream_t st);
+cudaError_t launch_dense_fill(const void* Y, int is_f64, int cell_major, int64_t G, int64_t n,
+                              const int64_t* rowptr, int32_t* col, float* val, cudaStream_t st);
+cudaError_t launch_csr_f64_to_f32(const double* in, float* out, int64_t nnz, cudaStream_t st);
+cudaError_t launch_csc_keys(const int64_t* colptr, const int32_t* rowidx, int64_t n, int64_t G,
+                            int64_t nnz, int64_t* keys, int32_t* bad, cudaStream_t st);
+cudaError_t launch_keys_to_csr(const int64_t* keys, int64_t nnz, int64_t n, int64_t G,
+                               int32_t* col, int64_t* rowcnt, cudaStream_t st);
+cudaError_t launch_x_rowmajor(const double* Xcm, int64_t n, int P, int xs, float* Xrm,
+                              cudaStream_t st);
+cudaError_t launch_double_to_float(const double* in, float* out, int64_t m, cudaStream_t st);
+cudaError_t launch_gene_stats(const int64_t* rowptr, const void* val, int val_u16, int64_t G,
+                              int64_t n, double* stats /* G x 6 */, cudaStream_t st);
+cudaError_t launch_colstats(const int64_t* rowptr, const int32_t* col, const void* val,
+                            int val_u16, int64_t G, int64_t nnz, double* colsum,
+                            double* collog, int32_t* colcnt, int32_t* colmin_bits,
+                            cudaStream_t st);
+cudaError_t launch_sf_finalize(int method, int64_t G, int64_t n, const double* colsum,
+                               const double* collog, const int32_t* colcnt,
+                               const int32_t* colmin_bits, double offset, double* sf,
+                               double* off, float* off_f, int32_t* err, cudaStream_t st);
+cudaError_t launch_sf_given(const double* sf_in, int64_t n, double offset, int use_sf, double* sf,
+                            double* off, float* off_f, cudaStream_t st);
+cudaError_t launch_theta0(const double* stats, const double* off, int64_t G, int64_t n,
+                          int has_init, double init_value, double* theta0, float* k,
+                          cudaStream_t st);
+cudaError_t launch_xtx_inverse(const double* Xcm, int64_t n, int P, double* ginv,
+                               int32_t* err, cudaStream_t st);
+cudaError_t launch_init_beta(const int64_t* rowptr, const int32_t* col, const void* val,
+                             int val_u16, const double* Xcm, const double* off,
+                             const double* ginv, const double* stats, int64_t G, int64_t n,
+                             int P, int rough, double* beta, float* beta_f, cudaStream_t st);
+cudaError_t launch_segptr(const int64_t* rowptr, const int32_t* col, int64_t G,
+                          const int32_t* bound, int nbound, int64_t* segptr, cudaStream_t st);
+cudaError_t launch_validate_csr(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
+                                int64_t nnz, int32_t* bad, cudaStream_t st);
+cudaError_t launch_iota(int32_t* a, int64_t m, cudaStream_t st);
+cudaError_t launch_set_i32(int32_t* a, int32_t v, cudaStream_t st);
+cudaError_t launch_copy_i32_to_host_mapped(const int32_t* src, volatile int32_t* dst,
+                                           cudaStream_t st);
+
+// ---- finalize kernels (kernels_fin.cu) ----
+cudaError_t launch_irls_finalize(const float* partW, int nseg, int slot_stride, int P,
+                                 const int32_t* act, const int32_t* n_act, int max_slots,
+                                 int32_t* act_next, int32_t* n_next, double* beta, float* beta_f,
+                                 int32_t* iters, int32_t* status, int max_iter, double eps,
+                                 volatile int32_t* mirror, cudaStream_t st);
+cudaError_t launch_mom_finalize(const double* partS, int nseg, int slot_stride,
+                                const int32_t* act, const int32_t* n_act, int max_slots,
+                                int64_t n, int P, double* theta, cudaStream_t st);
+struct MleState {
+    double* x;       // current log theta to evaluate (pass reads it)
+    double* lo;
+    double* hi;
+    int32_t* it;
+    int32_t* phase;  // 0: far-left check pending, 1: Newton, 2: done
+    double* theta;   // result
+};
+cudaError_t launch_mle_init(const double* stats, int64_t G, int64_t n, MleState s,
+                            int32_t* act, int32_t* n_act, cudaStream_t st);
+cudaError_t launch_mle_finalize(const float* partW, const double* partS, int nseg,
+                                int slot_stride, int P, const double* stats, int64_t n,
+                                const int32_t* act, const int32_t* n_act, int max_slots,
+                                int32_t* act_next, int32_t* n_next, MleState s, int max_iter,
+                                int cox_reid, volatile int32_t* mirror, cudaStream_t st);
+cudaError_t launch_sandwich_finalize(const float* partW, int nseg, int slot_stride, int P,
+                                     const int32_t* seg_cluster, int n_clusters, int64_t n,
+                                     const int32_t* act, const int32_t* n_act, int max_slots,
+                                     double* bread, double* sandwich, double* meat,
+                                     cudaStream_t st);
+
+// ---- test kernels (kernels_test.cu) ----
+cudaError_t launch_test_pvalues(int64_t G, int P, const double* beta, const double* bread,
+                                const double* sandwich, double df, const double* contrast_dev,
+                                double max_lfc, double* pval, double* lfc, cudaStream_t st);
+// p.adjust with temp storage from the caller (bytes from p_adjust_temp_bytes)
+size_t p_adjust_temp_bytes(int64_t m);
+cudaError_t launch_p_adjust(int64_t m, const double* p, int method, double* out, void* temp,
+                            size_t temp_bytes, cudaStream_t st);
+cudaError_t launch_nb_adjoint(int64_t n, const double* y, const double* eta, double log_theta,
+                              double* ll, double* d_eta, double* d_lt, cudaStream_t st);
+
+}  // namespace devil

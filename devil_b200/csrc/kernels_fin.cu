@@ -1,0 +1,406 @@
+// Per-gene finalize kernels: reduce the per-segment partial sums of a pass
+// in FP64 and apply the reference's per-gene step.  One warp per gene.
+#include "internal.h"
+
+namespace devil {
+
+static inline unsigned nblk(int64_t m, int t) { return (unsigned)((m + t - 1) / t); }
+
+// sums[a] = sum over segments of part[seg][slot][a]  (lanes split a)
+template <class T>
+DEV void reduce_partials(const T* part, int nseg, int slot_stride, int slot, int stride, int count,
+                         double* sums, int lane) {
+    for (int a = lane; a < count; a += 32) {
+        double s = 0.0;
+        for (int seg = 0; seg < nseg; ++seg)
+            s += (double)part[((int64_t)seg * slot_stride + slot) * stride + a];
+        sums[a] = s;
+    }
+}
+
+// warps per finalize block given the shared bytes one warp needs
+static int fin_warps(size_t per_warp) {
+    int w = (int)((96 * 1024) / (per_warp > 0 ? per_warp : 1));
+    return w < 1 ? 1 : (w > 4 ? 4 : w);
+}
+
+DEV void unpack_sym(int P, const double* packed, double* M) {
+    for (int j = 0; j < P; ++j)
+        for (int i = 0; i <= j; ++i) {
+            double v = packed[tri_index(i, j)];
+            M[j * P + i] = v;
+            M[i * P + j] = v;
+        }
+}
+
+// ------------------------------------------------------------------
+// IRLS step (src/beta.cpp:38-46): delta = H^-1 score, beta += delta,
+// converged when max|delta| < eps; NaN in delta[0] stops the gene.
+// ------------------------------------------------------------------
+__global__ void irls_finalize_kernel(const float* partW, int nseg, int slot_stride, int P,
+                                     const int32_t* act, const int32_t* n_act, int32_t* act_next,
+                                     int32_t* n_next, double* beta, float* beta_f, int32_t* iters,
+                                     int32_t* status, int max_iter, double eps) {
+    extern __shared__ double fsh[];
+    const int NE = P * (P + 1) / 2, NA = NE + P;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = NA + P * P + P + P;  // sums, H, S, piv (as doubles)
+    double* sums = fsh + warp * per;
+    double* H = sums + NA;
+    double* S = H + P * P;
+    int* piv = reinterpret_cast<int*>(S + P);
+    const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
+    const int nact = *n_act;
+    if (slot >= nact) return;
+    const int g = act[slot];
+    reduce_partials(partW, nseg, slot_stride, slot, NA, NA, sums, lane);
+    __syncwarp();
+    if (lane != 0) return;
+    unpack_sym(P, sums, H);
+    for (int i = 0; i < P; ++i) S[i] = sums[NE + i];
+    lu_factor(P, H, piv);
+    lu_solve(P, H, piv, S);
+    double mx = 0.0;
+    for (int i = 0; i < P; ++i) {
+        double b = beta[(int64_t)g * P + i] + S[i];
+        beta[(int64_t)g * P + i] = b;
+        beta_f[(int64_t)g * P + i] = (float)b;
+        double a = fabs(S[i]);
+        if (a > mx) mx = a;  // NaN entries never compare greater
+    }
+    const int it = iters[g] + 1;
+    iters[g] = it;
+    const bool isnan0 = !(S[0] == S[0]);
+    const bool conv = mx < eps;
+    if (isnan0) {
+        status[g] = 2;  // DEVIL_GENE_NAN
+    } else if (conv) {
+        status[g] = 0;
+    } else if (it >= max_iter) {
+        status[g] = 1;
+    } else {
+        int pos = atomicAdd(n_next, 1);
+        act_next[pos] = g;
+    }
+}
+
+cudaError_t launch_irls_finalize(const float* partW, int nseg, int slot_stride, int P,
+                                 const int32_t* act, const int32_t* n_act, int max_slots,
+                                 int32_t* act_next, int32_t* n_next, double* beta, float* beta_f,
+                                 int32_t* iters, int32_t* status, int max_iter, double eps,
+                                 volatile int32_t* mirror, cudaStream_t st) {
+    (void)mirror;
+    if (max_slots <= 0) return cudaSuccess;
+    const int NA = P * (P + 1) / 2 + P;
+    const size_t per = (size_t)(NA + P * P + 2 * P) * sizeof(double);
+    const int w = fin_warps(per);
+    const size_t smem = per * w;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(irls_finalize_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    irls_finalize_kernel<<<nblk(max_slots, w), 32 * w, smem, st>>>(
+        partW, nseg, slot_stride, P, act, n_act, act_next, n_next, beta, beta_f, iters, status,
+        max_iter, eps);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------
+// MOM (src/mom_overdispersion.cpp:47-53)
+// ------------------------------------------------------------------
+__global__ void mom_finalize_kernel(const double* partS, int nseg, int slot_stride,
+                                    const int32_t* act, const int32_t* n_act, int64_t n, int P,
+                                    double* theta) {
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= *n_act) return;
+    int g = act[slot];
+    double num = 0.0, den = 0.0;
+    for (int seg = 0; seg < nseg; ++seg) {
+        const double* p = partS + ((int64_t)seg * slot_stride + slot) * 2;
+        num += p[0];
+        den += p[1];
+    }
+    double corr = (double)n / (double)(n - P);
+    double th = 0.0;
+    if (den > 0.0) {
+        th = corr * num / den;
+        if (th < 0.0) th = 0.0;
+    }
+    theta[g] = th;
+}
+cudaError_t launch_mom_finalize(const double* partS, int nseg, int slot_stride,
+                                const int32_t* act, const int32_t* n_act, int max_slots,
+                                int64_t n, int P, double* theta, cudaStream_t st) {
+    if (max_slots <= 0) return cudaSuccess;
+    mom_finalize_kernel<<<nblk(max_slots, 128), 128, 0, st>>>(partS, nseg, slot_stride, act, n_act,
+                                                              n, P, theta);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------
+// MLE of log theta (R/overdispersion.R:25-115 with the score and its
+// derivative of src/overdispersion.cpp:95-242), bracketed Newton.
+// ------------------------------------------------------------------
+constexpr double kCrFactor = 0.99;  // src/overdispersion.cpp:25
+
+__global__ void mle_init_kernel(const double* stats, int64_t G, MleState s, int32_t* act,
+                                int32_t* n_act) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < G;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        s.it[g] = 0;
+        if (stats[g * 6 + 2] == 0.0) {  // all(y == 0) -> 0
+            s.phase[g] = 2;
+            s.theta[g] = 0.0;
+            s.x[g] = -INFINITY;
+        } else {
+            s.phase[g] = 0;
+            s.x[g] = log(1e-8);
+            int pos = atomicAdd(n_act, 1);
+            act[pos] = (int32_t)g;
+        }
+    }
+}
+cudaError_t launch_mle_init(const double* stats, int64_t G, int64_t n, MleState s, int32_t* act,
+                            int32_t* n_act, cudaStream_t st) {
+    (void)n;
+    if (G == 0) return cudaSuccess;
+    mle_init_kernel<<<(unsigned)std::min<int64_t>(nblk(G, 256), 1024), 256, 0, st>>>(stats, G, s,
+                                                                                     act, n_act);
+    return cudaGetLastError();
+}
+
+__global__ void mle_finalize_kernel(const float* partW, const double* partS, int nseg,
+                                    int slot_stride, int P, const double* stats, int64_t n,
+                                    const int32_t* act, const int32_t* n_act, int32_t* act_next,
+                                    int32_t* n_next, MleState st, int max_iter, int cox_reid) {
+    extern __shared__ double fsh[];
+    const int NE = P * (P + 1) / 2, NA = 3 * NE;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = NA + 6 + 4 * P * P + P;
+    double* sums = fsh + warp * per;
+    double* ss = sums + NA;
+    double* B = ss + 6;
+    double* Bi = B + P * P;
+    double* D = Bi + P * P;
+    double* M = D + P * P;
+    int* piv = reinterpret_cast<int*>(M + P * P);
+    const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (slot >= *n_act) return;
+    const int g = act[slot];
+    reduce_partials(partW, nseg, slot_stride, slot, NA, NA, sums, lane);
+    reduce_partials(partS, nseg, slot_stride, slot, 6, 6, ss, lane);
+    __syncwarp();
+    if (lane != 0) return;
+
+    const double x = st.x[g];
+    const double theta = exp(x), a = 1.0 / theta;
+    // Cox-Reid terms
+    double cr_s = 0.0, cr_d = 0.0, cr_d2 = 0.0;
+    if (cox_reid) {
+        unpack_sym(P, sums, B);
+        for (int i = 0; i < P; ++i) B[i * P + i] += 1e-6;  // inv_sympd(b + 1e-6 I)
+        lu_factor(P, B, piv);
+        lu_inverse(P, B, piv, Bi);
+        unpack_sym(P, sums + NE, D);  // db
+        // M = Bi * db
+        for (int j = 0; j < P; ++j)
+            for (int i = 0; i < P; ++i) {
+                double s = 0.0;
+                for (int k = 0; k < P; ++k) s += Bi[k * P + i] * D[j * P + k];
+                M[j * P + i] = s;
+            }
+        double ddetb = 0.0, trmm = 0.0, trbd2 = 0.0;
+        for (int i = 0; i < P; ++i) ddetb += M[i * P + i];
+        for (int i = 0; i < P; ++i)
+            for (int k = 0; k < P; ++k) trmm += M[k * P + i] * M[i * P + k];
+        unpack_sym(P, sums + 2 * NE, D);  // d2b
+        for (int i = 0; i < P; ++i)
+            for (int k = 0; k < P; ++k) trbd2 += Bi[k * P + i] * D[i * P + k];
+        double d2detb = ddetb * ddetb - trmm + trbd2;
+        cr_s = -0.5 * ddetb * kCrFactor;
+        cr_d = (0.5 * ddetb * ddetb - 0.5 * d2detb) * kCrFactor;
+        cr_d2 = -0.5 * ddetb * kCrFactor;
+    }
+    const double* gs = stats + (int64_t)g * 6;
+    const double sum_y = gs[2], sum_prod_y = gs[3], max_y = gs[4];
+    // score (src/overdispersion.cpp:139-177)
+    const double corr = a > 1e5 ? sum_prod_y / (2.0 * a) : 0.0;
+    double dig;
+    if (max_y * 1e6 < a) {
+        dig = sum_y - corr;
+    } else {
+        dig = ss[4] * a;
+        if (dig > sum_y - corr) dig = sum_y - corr;
+    }
+    const double score = a * (ss[0] + ss[2]) - dig + cr_s * theta;
+    // derivative (src/overdispersion.cpp:218-241)
+    const double l1 = ss[0] + ss[2], l2 = ss[1] + ss[3];
+    const double digd = ss[4], trig = a * a * ss[5];
+    const double ll = -2.0 * a * (l1 - digd) + (l2 + trig);
+    const double deriv = ll + cr_d * theta * theta + (l1 - digd) * a + cr_d2 * theta;
+
+    int phase = st.phase[g];
+    bool done = false;
+    double xn = x;
+    if (phase == 0) {
+        if (score < 0.0) {
+            st.theta[g] = 0.0;
+            st.phase[g] = 2;
+            return;
+        }
+        const double mean = gs[0], var = gs[1];
+        double start = (var - mean) / (mean * mean);
+        if (isnan(start) || start <= 0.0) start = 0.5;
+        double lo = log(1e-8), hi = log(1e16);
+        xn = log(start);
+        if (xn < lo) xn = lo;
+        if (xn > hi) xn = hi;
+        st.lo[g] = lo;
+        st.hi[g] = hi;
+        st.phase[g] = 1;
+    } else {
+        double lo = st.lo[g], hi = st.hi[g];
+        int it = st.it[g];
+        if (score == 0.0) {
+            done = true;
+        } else {
+            if (score > 0.0) lo = x; else hi = x;
+            double cand = deriv < 0.0 ? x - score / deriv : NAN;
+            if (!(cand > lo && cand < hi)) cand = 0.5 * (lo + hi);
+            double step = fabs(cand - x);
+            xn = cand;
+            ++it;
+            if (step < 1e-10 || hi - lo < 1e-10 || it >= max_iter) done = true;
+        }
+        st.lo[g] = lo;
+        st.hi[g] = hi;
+        st.it[g] = it;
+    }
+    st.x[g] = xn;
+    if (done) {
+        st.theta[g] = exp(xn);
+        st.phase[g] = 2;
+    } else {
+        int pos = atomicAdd(n_next, 1);
+        act_next[pos] = g;
+    }
+}
+cudaError_t launch_mle_finalize(const float* partW, const double* partS, int nseg,
+                                int slot_stride, int P, const double* stats, int64_t n,
+                                const int32_t* act, const int32_t* n_act, int max_slots,
+                                int32_t* act_next, int32_t* n_next, MleState s, int max_iter,
+                                int cox_reid, volatile int32_t* mirror, cudaStream_t st) {
+    (void)mirror;
+    if (max_slots <= 0) return cudaSuccess;
+    const int NA = 3 * (P * (P + 1) / 2);
+    const size_t per = (size_t)(NA + 6 + 4 * P * P + P) * sizeof(double);
+    const int w = fin_warps(per);
+    const size_t smem = per * w;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(mle_finalize_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    mle_finalize_kernel<<<nblk(max_slots, w), 32 * w, smem, st>>>(
+        partW, partS, nseg, slot_stride, P, stats, n, act, n_act, act_next, n_next, s, max_iter,
+        cox_reid);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------
+// bread = (X' W X)^-1 (src/variance.cpp:22-47); clustered meat
+// (src/variance.cpp:186-228): per-cluster score sums from the partials of
+// cluster-aligned segments, meat = adj/n sum_b s_b s_b', adj = C/(C-1)
+// (1 when C = 1); sandwich = bread meat bread n (R/main.R:482-492).
+// ------------------------------------------------------------------
+__global__ void sandwich_finalize_kernel(const float* partW, int nseg, int slot_stride, int P,
+                                         const int32_t* seg_cluster, int n_clusters, int64_t n,
+                                         const int32_t* act, const int32_t* n_act, double* bread,
+                                         double* sandwich, double* meat_out) {
+    extern __shared__ double fsh[];
+    const int NE = P * (P + 1) / 2, NA = NE + P;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = NA + 4 * P * P + 2 * P;
+    double* sums = fsh + warp * per;
+    double* H = sums + NA;
+    double* Bi = H + P * P;
+    double* Mt = Bi + P * P;
+    double* T = Mt + P * P;
+    double* cur = T + P * P;
+    int* piv = reinterpret_cast<int*>(cur + P);
+    const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (slot >= *n_act) return;
+    const int g = act[slot];
+    reduce_partials(partW, nseg, slot_stride, slot, NA, NE, sums, lane);  // H part only
+    for (int i = lane; i < P * P; i += 32) Mt[i] = 0.0;
+    __syncwarp();
+    if (n_clusters > 0) {
+        // lane i holds component i of the running cluster sum
+        double acc = 0.0;
+        for (int seg = 0; seg < nseg; ++seg) {
+            if (lane < P) acc += (double)partW[((int64_t)seg * slot_stride + slot) * NA + NE + lane];
+            bool last = (seg == nseg - 1) || (seg_cluster[seg + 1] != seg_cluster[seg]);
+            if (last) {
+                if (lane < P) cur[lane] = acc;
+                __syncwarp();
+                for (int i = lane; i < P * P; i += 32) {
+                    int r = i % P, c = i / P;
+                    Mt[i] += cur[r] * cur[c];
+                }
+                __syncwarp();
+                acc = 0.0;
+            }
+        }
+    }
+    __syncwarp();
+    if (lane != 0) return;
+    unpack_sym(P, sums, H);
+    lu_factor(P, H, piv);
+    lu_inverse(P, H, piv, Bi);
+    double* bo = bread + (int64_t)g * P * P;
+    for (int i = 0; i < P * P; ++i) bo[i] = Bi[i];
+    if (n_clusters > 0) {
+        double adj = n_clusters > 1 ? (double)n_clusters / (n_clusters - 1.0) : 1.0;
+        for (int i = 0; i < P * P; ++i) Mt[i] *= adj / (double)n;
+        if (meat_out)
+            for (int i = 0; i < P * P; ++i) meat_out[(int64_t)g * P * P + i] = Mt[i];
+        if (sandwich) {
+            // T = Bi * Mt ; S = T * Bi * n
+            for (int j = 0; j < P; ++j)
+                for (int i = 0; i < P; ++i) {
+                    double s = 0.0;
+                    for (int k = 0; k < P; ++k) s += Bi[k * P + i] * Mt[j * P + k];
+                    T[j * P + i] = s;
+                }
+            double* so = sandwich + (int64_t)g * P * P;
+            for (int j = 0; j < P; ++j)
+                for (int i = 0; i < P; ++i) {
+                    double s = 0.0;
+                    for (int k = 0; k < P; ++k) s += T[k * P + i] * Bi[j * P + k];
+                    so[j * P + i] = s * (double)n;
+                }
+        }
+    }
+}
+cudaError_t launch_sandwich_finalize(const float* partW, int nseg, int slot_stride, int P,
+                                     const int32_t* seg_cluster, int n_clusters, int64_t n,
+                                     const int32_t* act, const int32_t* n_act, int max_slots,
+                                     double* bread, double* sandwich, double* meat,
+                                     cudaStream_t st) {
+    if (max_slots <= 0) return cudaSuccess;
+    const int NA = P * (P + 1) / 2 + P;
+    const size_t per = (size_t)(NA + 4 * P * P + 2 * P) * sizeof(double);
+    const int w = fin_warps(per);
+    const size_t smem = per * w;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(sandwich_finalize_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    sandwich_finalize_kernel<<<nblk(max_slots, w), 32 * w, smem, st>>>(
+        partW, nseg, slot_stride, P, seg_cluster, n_clusters, n, act, n_act, bread, sandwich, meat);
+    return cudaGetLastError();
+}
+
+}  // namespace devil

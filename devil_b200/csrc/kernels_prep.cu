@@ -1,0 +1,528 @@
+// Preparation kernels: count-matrix conversion, design staging, per-gene
+// statistics, size factors (R/size_factors.R), theta_0
+// (R/overdispersion.R:129-135), beta_0 (R/beta.R:13-20, R/main.R:404-406)
+// and the CSR offsets of every cell segment.
+#include "internal.h"
+
+namespace devil {
+
+static inline unsigned nblk(int64_t m, int t) { return (unsigned)((m + t - 1) / t); }
+
+// ------------------------------------------------------------------
+// dense -> CSR (gene-major)
+// ------------------------------------------------------------------
+__global__ void dense_count_kernel(const void* Y, int is_f64, int cell_major, int64_t G, int64_t n,
+                                   int64_t* rowcnt) {
+    int64_t g = blockIdx.x;
+    if (g >= G) return;
+    int64_t cnt = 0;
+    for (int64_t c = threadIdx.x; c < n; c += blockDim.x) {
+        int64_t idx = cell_major ? c * G + g : g * n + c;
+        double v = is_f64 ? ((const double*)Y)[idx] : (double)((const float*)Y)[idx];
+        cnt += (v != 0.0);
+    }
+    cnt = warp_sum(cnt);
+    __shared__ int64_t red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t s = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        rowcnt[g] = s;
+    }
+}
+
+// one warp per gene walks its row in order and compacts the nonzeros
+__global__ void dense_fill_kernel(const void* Y, int is_f64, int cell_major, int64_t G, int64_t n,
+                                  const int64_t* rowptr, int32_t* col, float* val) {
+    int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (g >= G) return;
+    int64_t pos = rowptr[g];
+    for (int64_t c0 = 0; c0 < n; c0 += 32) {
+        int64_t c = c0 + lane;
+        double v = 0.0;
+        if (c < n) {
+            int64_t idx = cell_major ? c * G + g : g * n + c;
+            v = is_f64 ? ((const double*)Y)[idx] : (double)((const float*)Y)[idx];
+        }
+        unsigned m = __ballot_sync(0xffffffffu, v != 0.0);
+        if (v != 0.0) {
+            int r = __popc(m & ((1u << lane) - 1u));
+            col[pos + r] = (int32_t)c;
+            val[pos + r] = (float)v;
+        }
+        pos += __popc(m);
+    }
+}
+
+cudaError_t launch_dense_count(const void* Y, int is_f64, int cell_major, int64_t G, int64_t n,
+                               int64_t* rowcnt, cudaStream_t st) {
+    if (G == 0) return cudaSuccess;
+    dense_count_kernel<<<(unsigned)G, 256, 0, st>>>(Y, is_f64, cell_major, G, n, rowcnt);
+    return cudaGetLastError();
+}
+cudaError_t launch_dense_fill(const void* Y, int is_f64, int cell_major, int64_t G, int64_t n,
+                              const int64_t* rowptr, int32_t* col, float* val, cudaStream_t st) {
+    if (G == 0) return cudaSuccess;
+    dense_fill_kernel<<<nblk(G, 8), 256, 0, st>>>(Y, is_f64, cell_major, G, n, rowptr, col, val);
+    return cudaGetLastError();
+}
+
+__global__ void f64_to_f32_kernel(const double* in, float* out, int64_t m) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+cudaError_t launch_csr_f64_to_f32(const double* in, float* out, int64_t nnz, cudaStream_t st) {
+    if (nnz == 0) return cudaSuccess;
+    f64_to_f32_kernel<<<(unsigned)std::min<int64_t>(nblk(nnz, 256), 148 * 16), 256, 0, st>>>(in, out, nnz);
+    return cudaGetLastError();
+}
+cudaError_t launch_double_to_float(const double* in, float* out, int64_t m, cudaStream_t st) {
+    return launch_csr_f64_to_f32(in, out, m, st);
+}
+
+// CSC (cell-major) -> sortable (gene, cell) keys
+// out-of-range gene indices or column pointers set bad[0] and produce key 0
+__global__ void csc_keys_kernel(const int64_t* colptr, const int32_t* rowidx, int64_t n, int64_t G,
+                                int64_t nnz, int64_t* keys, int32_t* bad) {
+    int64_t c = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (c >= n) return;
+    const int64_t e0 = colptr[c], e1 = colptr[c + 1];
+    if (e0 < 0 || e1 < e0 || e1 > nnz) {
+        if (lane == 0) atomicOr(bad, 1);
+        return;
+    }
+    for (int64_t e = e0 + lane; e < e1; e += 32) {
+        int32_t g = rowidx[e];
+        if (g < 0 || g >= G) {
+            atomicOr(bad, 1);
+            keys[e] = 0;
+        } else {
+            keys[e] = (int64_t)g * n + c;
+        }
+    }
+}
+cudaError_t launch_csc_keys(const int64_t* colptr, const int32_t* rowidx, int64_t n, int64_t G,
+                            int64_t nnz, int64_t* keys, int32_t* bad, cudaStream_t st) {
+    if (n == 0 || nnz == 0) return cudaSuccess;
+    csc_keys_kernel<<<nblk(n, 8), 256, 0, st>>>(colptr, rowidx, n, G, nnz, keys, bad);
+    return cudaGetLastError();
+}
+__global__ void keys_to_csr_kernel(const int64_t* keys, int64_t nnz, int64_t n, int32_t* col,
+                                   unsigned long long* rowcnt) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nnz;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t k = keys[i];
+        int64_t g = k / n;
+        col[i] = (int32_t)(k - g * n);
+        atomicAdd(rowcnt + g, 1ull);
+    }
+}
+cudaError_t launch_keys_to_csr(const int64_t* keys, int64_t nnz, int64_t n, int64_t G,
+                               int32_t* col, int64_t* rowcnt, cudaStream_t st) {
+    (void)G;
+    if (nnz == 0) return cudaSuccess;
+    keys_to_csr_kernel<<<(unsigned)std::min<int64_t>(nblk(nnz, 256), 148 * 16), 256, 0, st>>>(
+        keys, nnz, n, col, reinterpret_cast<unsigned long long*>(rowcnt));
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------
+// design matrix: column-major doubles -> row-major padded floats
+// ------------------------------------------------------------------
+__global__ void x_rowmajor_kernel(const double* Xcm, int64_t n, int P, int xs, float* Xrm) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n * xs;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t c = i / xs;
+        int j = (int)(i - c * xs);
+        Xrm[i] = j < P ? (float)Xcm[(int64_t)j * n + c] : 0.f;
+    }
+}
+cudaError_t launch_x_rowmajor(const double* Xcm, int64_t n, int P, int xs, float* Xrm,
+                              cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    x_rowmajor_kernel<<<(unsigned)std::min<int64_t>(nblk(n * xs, 256), 148 * 16), 256, 0, st>>>(
+        Xcm, n, P, xs, Xrm);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------
+// per-gene statistics, two passes over each row (warp per gene):
+// stats[g*6 + 0..5] = mean, sample variance (n-1), sum y,
+//                     sum (y-1) y, max y, nnz
+// ------------------------------------------------------------------
+template <class VT>
+__global__ void gene_stats_kernel(const int64_t* rowptr, const VT* val, int64_t G, int64_t n,
+                                  double* stats) {
+    int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (g >= G) return;
+    int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
+    double s = 0.0, sp = 0.0, mx = 0.0;
+    for (int64_t e = e0 + lane; e < e1; e += 32) {
+        double y = (double)val[e];
+        s += y;
+        sp += (y - 1.0) * y;
+        mx = fmax(mx, y);
+    }
+    s = warp_sum(s);
+    sp = warp_sum(sp);
+    mx = warp_max(mx);
+    double mean = s / (double)n;
+    double ss = 0.0;
+    for (int64_t e = e0 + lane; e < e1; e += 32) {
+        double d = (double)val[e] - mean;
+        ss += d * d;
+    }
+    ss = warp_sum(ss);
+    if (lane == 0) {
+        ss += (double)(n - (e1 - e0)) * mean * mean;
+        double* o = stats + g * 6;
+        o[0] = mean;
+        o[1] = ss / (double)(n - 1);
+        o[2] = s;
+        o[3] = sp;
+        o[4] = mx;
+        o[5] = (double)(e1 - e0);
+    }
+}
+cudaError_t launch_gene_stats(const int64_t* rowptr, const void* val, int val_u16, int64_t G,
+                              int64_t n, double* stats, cudaStream_t st) {
+    if (G == 0) return cudaSuccess;
+    if (val_u16)
+        gene_stats_kernel<uint16_t><<<nblk(G, 8), 256, 0, st>>>(rowptr, (const uint16_t*)val, G, n, stats);
+    else
+        gene_stats_kernel<float><<<nblk(G, 8), 256, 0, st>>>(rowptr, (const float*)val, G, n, stats);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------
+// column statistics for size factors (atomics; integer-valued sums are
+// exact in FP64 whatever the order)
+// ------------------------------------------------------------------
+template <class VT>
+__global__ void colstats_kernel(const int32_t* col, const VT* val, int64_t nnz, double* colsum,
+                                double* collog, int32_t* colcnt, int32_t* colmin_bits) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int c = col[e];
+        float v = (float)val[e];
+        atomicAdd(colsum + c, (double)v);
+        if (collog) {
+            atomicAdd(collog + c, log1p((double)v));
+            atomicAdd(colcnt + c, 1);
+            float l = (float)log1p((double)v);
+            // log1p of counts is >= 0; int ordering of non-negative floats
+            // matches float ordering
+            atomicMin(colmin_bits + c, __float_as_int(fmaxf(l, 0.f)));
+        }
+    }
+}
+cudaError_t launch_colstats(const int64_t* rowptr, const int32_t* col, const void* val,
+                            int val_u16, int64_t G, int64_t nnz, double* colsum,
+                            double* collog, int32_t* colcnt, int32_t* colmin_bits,
+                            cudaStream_t st) {
+    (void)rowptr; (void)G;
+    if (nnz == 0) return cudaSuccess;
+    unsigned b = (unsigned)std::min<int64_t>(nblk(nnz, 256), 148 * 32);
+    if (val_u16)
+        colstats_kernel<uint16_t><<<b, 256, 0, st>>>(col, (const uint16_t*)val, nnz, colsum, collog, colcnt, colmin_bits);
+    else
+        colstats_kernel<float><<<b, 256, 0, st>>>(col, (const float*)val, nnz, colsum, collog, colcnt, colmin_bits);
+    return cudaGetLastError();
+}
+
+// size factors from the column statistics; one block.
+// method 1 = normed_sum (R/size_factors.R:75-88), 2 = psinorm (:100-117).
+__global__ void sf_finalize_kernel(int method, int64_t G, int64_t n, const double* colsum,
+                                   const double* collog, const int32_t* colcnt,
+                                   const int32_t* colmin_bits, double offset, double* sf,
+                                   double* off, float* off_f, int32_t* err) {
+    __shared__ double red[32];
+    __shared__ double red2[32];
+    __shared__ double gm_s;
+    double acc = 0.0, cntv = 0.0;
+    int zero = 0;
+    for (int64_t c = threadIdx.x; c < n; c += blockDim.x) {
+        double v;
+        if (G <= 1) {
+            v = 1.0;
+        } else if (method == 1) {
+            v = colsum[c];
+            if (v == 0.0) zero = 1;
+        } else {
+            double m = colcnt[c] < G ? 0.0 : (double)__int_as_float(colmin_bits[c]);
+            v = collog[c] / (double)G - m;
+        }
+        sf[c] = v;
+        double l = log(v);
+        if (!isnan(l)) { acc += l; cntv += 1.0; }
+    }
+    zero = __syncthreads_or(zero);
+    acc = warp_sum(acc);
+    cntv = warp_sum(cntv);
+    if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = acc; red2[threadIdx.x >> 5] = cntv; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0, k = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { s += red[w]; k += red2[w]; }
+        gm_s = (G <= 1) ? 1.0 : exp(s / k);
+        if (err) *err = (method == 1 && zero && G > 1) ? 1 : 0;
+    }
+    __syncthreads();
+    const double gm = gm_s;
+    for (int64_t c = threadIdx.x; c < n; c += blockDim.x) {
+        double v = (G <= 1) ? 1.0 : sf[c] / gm;
+        sf[c] = v;
+        double o = offset + log(v);
+        off[c] = o;
+        off_f[c] = (float)o;
+    }
+}
+cudaError_t launch_sf_finalize(int method, int64_t G, int64_t n, const double* colsum,
+                               const double* collog, const int32_t* colcnt,
+                               const int32_t* colmin_bits, double offset, double* sf,
+                               double* off, float* off_f, int32_t* err, cudaStream_t st) {
+    sf_finalize_kernel<<<1, 1024, 0, st>>>(method, G, n, colsum, collog, colcnt, colmin_bits,
+                                           offset, sf, off, off_f, err);
+    return cudaGetLastError();
+}
+
+// offsets from given (or unit) size factors: compute_offset_vector
+// (R/size_factors.R:172-184)
+__global__ void sf_given_kernel(const double* sf_in, int64_t n, double offset, int use_sf,
+                                double* sf, double* off, float* off_f) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        double s = use_sf ? sf_in[c] : 1.0;
+        sf[c] = s;
+        double o = use_sf ? offset + log(s) : offset;
+        off[c] = o;
+        off_f[c] = (float)o;
+    }
+}
+cudaError_t launch_sf_given(const double* sf_in, int64_t n, double offset, int use_sf, double* sf,
+                            double* off, float* off_f, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    sf_given_kernel<<<(unsigned)std::min<int64_t>(nblk(n, 256), 1024), 256, 0, st>>>(
+        sf_in, n, offset, use_sf, sf, off, off_f);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------
+// theta_0 = (var - mean / mean(exp(off))) / mean^2, NaN or < 0 -> 0.01
+// (R/overdispersion.R:129-135); k = 1/theta_0 as the float beta_fit keeps
+// (src/beta.cpp:25-28: theta_0 arrives as float, 1.0/k stored as float).
+// ------------------------------------------------------------------
+__global__ void theta0_kernel(const double* stats, const double* off, int64_t G, int64_t n,
+                              int has_init, double init_value, double* theta0, float* k) {
+    __shared__ double red[32];
+    __shared__ double moi_s;
+    double acc = 0.0;
+    for (int64_t c = threadIdx.x; c < n; c += blockDim.x) acc += exp(off[c]);
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        moi_s = 1.0 / (s / (double)n);
+    }
+    __syncthreads();
+    const double moi = moi_s;
+    for (int64_t g = threadIdx.x; g < G; g += blockDim.x) {
+        double th;
+        if (has_init) {
+            th = init_value;
+        } else {
+            double mean = stats[g * 6 + 0], var = stats[g * 6 + 1];
+            double d = (var - moi * mean) / (mean * mean);
+            th = (isnan(d) || d < 0.0) ? 0.01 : d;
+        }
+        theta0[g] = th;
+        float kf = (float)th;
+        k[g] = (float)(1.0 / (double)kf);
+    }
+}
+cudaError_t launch_theta0(const double* stats, const double* off, int64_t G, int64_t n,
+                          int has_init, double init_value, double* theta0, float* k,
+                          cudaStream_t st) {
+    theta0_kernel<<<1, 1024, 0, st>>>(stats, off, G, n, has_init, init_value, theta0, k);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------
+// (X'X)^-1 in FP64 (one block): the least-squares solve of init_beta
+// ------------------------------------------------------------------
+__global__ void xtx_inverse_kernel(const double* Xcm, int64_t n, int P, double* ginv,
+                                   int32_t* err) {
+    extern __shared__ double sh[];
+    double* Gm = sh;               // P*P
+    double* W = sh + P * P;        // P*P
+    int* piv = reinterpret_cast<int*>(W + P * P);
+    const int NP = P * (P + 1) / 2;
+    for (int q = threadIdx.x >> 5; q < NP; q += blockDim.x >> 5) {
+        int j = 0;
+        while ((j + 1) * (j + 2) / 2 <= q) ++j;
+        int i = q - j * (j + 1) / 2;
+        double s = 0.0;
+        for (int64_t c = threadIdx.x & 31; c < n; c += 32) s += Xcm[(int64_t)i * n + c] * Xcm[(int64_t)j * n + c];
+        s = warp_sum(s);
+        if ((threadIdx.x & 31) == 0) { Gm[j * P + i] = s; Gm[i * P + j] = s; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double dmax = 0.0;
+        for (int i = 0; i < P; ++i) dmax = fmax(dmax, fabs(Gm[i * P + i]));
+        bool ok = lu_factor(P, Gm, piv);
+        // rank check on the pivots, relative to the largest diagonal
+        for (int i = 0; i < P; ++i)
+            if (!(fabs(Gm[i * P + i]) > 1e-12 * dmax)) ok = false;
+        if (ok) lu_inverse(P, Gm, piv, W);
+        for (int i = 0; i < P * P; ++i) ginv[i] = ok ? W[i] : NAN;
+        *err = ok ? 0 : 1;
+    }
+}
+cudaError_t launch_xtx_inverse(const double* Xcm, int64_t n, int P, double* ginv, int32_t* err,
+                               cudaStream_t st) {
+    size_t smem = (size_t)2 * P * P * 8 + (size_t)P * 4 + 16;
+    xtx_inverse_kernel<<<1, 1024, smem, st>>>(Xcm, n, P, ginv, err);
+    return cudaGetLastError();
+}
+
+// beta_0 (warp per gene).  QR least squares of log1p(y / exp(off)) on X:
+// the solution equals (X'X)^-1 X' z; z is zero wherever y is zero, so
+// X' z is a sum over the nonzero entries of the row.  Rough init:
+// beta_0 = (log1p(mean y), 0, ..., 0).
+template <class VT>
+__global__ void init_beta_kernel(const int64_t* rowptr, const int32_t* col, const VT* val,
+                                 const double* Xcm, const double* off, const double* ginv,
+                                 const double* stats, int64_t G, int64_t n, int P, int rough,
+                                 double* beta, float* beta_f) {
+    int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (g >= G) return;
+    if (rough) {
+        if (lane < P) {
+            double b = lane == 0 ? log1p(stats[g * 6 + 0]) : 0.0;
+            beta[g * P + lane] = b;
+            beta_f[g * P + lane] = (float)b;
+        }
+        return;
+    }
+    double r[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) r[i] = 0.0;
+    for (int64_t e = rowptr[g] + lane; e < rowptr[g + 1]; e += 32) {
+        int c = col[e];
+        double z = log1p((double)val[e] / exp(off[c]));
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+            if (i < P) r[i] += Xcm[(int64_t)i * n + c] * z;
+    }
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+        if (i < P) r[i] = warp_sum(r[i]);
+    if (lane < P) {
+        double b = 0.0;
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (j < P) b += ginv[j * P + lane] * r[j];
+        beta[g * P + lane] = b;
+        beta_f[g * P + lane] = (float)b;
+    }
+}
+cudaError_t launch_init_beta(const int64_t* rowptr, const int32_t* col, const void* val,
+                             int val_u16, const double* Xcm, const double* off,
+                             const double* ginv, const double* stats, int64_t G, int64_t n,
+                             int P, int rough, double* beta, float* beta_f, cudaStream_t st) {
+    if (G == 0) return cudaSuccess;
+    if (val_u16)
+        init_beta_kernel<uint16_t><<<nblk(G, 8), 256, 0, st>>>(rowptr, col, (const uint16_t*)val, Xcm, off, ginv, stats, G, n, P, rough, beta, beta_f);
+    else
+        init_beta_kernel<float><<<nblk(G, 8), 256, 0, st>>>(rowptr, col, (const float*)val, Xcm, off, ginv, stats, G, n, P, rough, beta, beta_f);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------
+// segptr[g][b] = first CSR entry of row g with col >= bound[b]
+// (warp per gene, lanes search boundaries in parallel)
+// ------------------------------------------------------------------
+__global__ void segptr_kernel(const int64_t* rowptr, const int32_t* col, int64_t G,
+                              const int32_t* bound, int nbound, int64_t* segptr) {
+    int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (g >= G) return;
+    const int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
+    for (int b = lane; b < nbound; b += 32) {
+        int32_t key = bound[b];
+        int64_t lo = e0, hi = e1;
+        while (lo < hi) {
+            int64_t mid = (lo + hi) >> 1;
+            if (col[mid] < key) lo = mid + 1; else hi = mid;
+        }
+        segptr[g * nbound + b] = lo;
+    }
+}
+cudaError_t launch_segptr(const int64_t* rowptr, const int32_t* col, int64_t G,
+                          const int32_t* bound, int nbound, int64_t* segptr, cudaStream_t st) {
+    if (G == 0) return cudaSuccess;
+    segptr_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, col, G, bound, nbound, segptr);
+    return cudaGetLastError();
+}
+
+// CSR sanity (warp per gene): rowptr non-decreasing, cell indices in
+// [0, n) and strictly increasing within each row.  bad[0] != 0 on failure.
+__global__ void validate_csr_kernel(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
+                                    int64_t nnz, int32_t* bad) {
+    int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (g >= G) return;
+    const int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
+    int b = 0;
+    if (e0 < 0 || e1 < e0 || e1 > nnz) {
+        b = 1;
+    } else {
+        for (int64_t e = e0 + lane; e < e1; e += 32) {
+            int c = col[e];
+            if (c < 0 || c >= n) b = 1;
+            if (e > e0 && col[e - 1] >= c) b = 1;
+        }
+    }
+    b = __any_sync(0xffffffffu, b);
+    if (lane == 0 && b) atomicOr(bad, 1);
+    if (g == G - 1 && lane == 0 && e1 != nnz) atomicOr(bad, 1);
+}
+cudaError_t launch_validate_csr(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
+                                int64_t nnz, int32_t* bad, cudaStream_t st) {
+    if (G == 0) return cudaSuccess;
+    validate_csr_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, col, G, n, nnz, bad);
+    return cudaGetLastError();
+}
+
+__global__ void iota_kernel(int32_t* a, int64_t m) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = (int32_t)i;
+}
+cudaError_t launch_iota(int32_t* a, int64_t m, cudaStream_t st) {
+    if (m == 0) return cudaSuccess;
+    iota_kernel<<<(unsigned)std::min<int64_t>(nblk(m, 256), 1024), 256, 0, st>>>(a, m);
+    return cudaGetLastError();
+}
+__global__ void set_i32_kernel(int32_t* a, int32_t v) { *a = v; }
+cudaError_t launch_set_i32(int32_t* a, int32_t v, cudaStream_t st) {
+    set_i32_kernel<<<1, 1, 0, st>>>(a, v);
+    return cudaGetLastError();
+}
+__global__ void mirror_kernel(const int32_t* src, volatile int32_t* dst) { *dst = *src; }
+cudaError_t launch_copy_i32_to_host_mapped(const int32_t* src, volatile int32_t* dst,
+                                           cudaStream_t st) {
+    mirror_kernel<<<1, 1, 0, st>>>(src, dst);
+    return cudaGetLastError();
+}
+
+}  // namespace devil

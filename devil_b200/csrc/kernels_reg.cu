@@ -1,0 +1,100 @@
+// Instantiations of the register engine (p <= 8) for every pass.
+#include "internal.h"
+
+namespace devil {
+
+constexpr int kRegNT = 256;
+
+int reg_max_p() { return 8; }
+
+int reg_default_gt(PassKind k, int P) {
+    switch (k) {
+        case PASS_IRLS:
+        case PASS_SANDWICH: return P <= 4 ? 8 : (P <= 6 ? 4 : 2);
+        case PASS_MOM: return 8;
+        case PASS_MLE: return P <= 2 ? 4 : (P <= 4 ? 2 : 1);
+    }
+    return 1;
+}
+
+bool reg_gt_supported(PassKind k, int P, int GT) {
+    if (P < 1 || P > 8) return false;
+    if (k == PASS_IRLS) {
+        int mx = P <= 4 ? 8 : (P <= 6 ? 4 : 2);
+        return GT == 1 || GT == 2 || (GT == 4 && mx >= 4) || (GT == 8 && mx >= 8);
+    }
+    return GT == reg_default_gt(k, P);
+}
+
+template <PassKind K> struct PassOf;
+template <> struct PassOf<PASS_IRLS> { using T = PassIRLS; };
+template <> struct PassOf<PASS_MOM> { using T = PassMOM; };
+template <> struct PassOf<PASS_MLE> { using T = PassMLE; };
+template <> struct PassOf<PASS_SANDWICH> { using T = PassSandwich; };
+
+template <PassKind K>
+static typename PassOf<K>::T::Params make_params(const PassParamsAny& a);
+template <> PassIRLS::Params make_params<PASS_IRLS>(const PassParamsAny& a) { return {a.beta, a.k}; }
+template <> PassMOM::Params make_params<PASS_MOM>(const PassParamsAny& a) { return {a.beta}; }
+template <> PassMLE::Params make_params<PASS_MLE>(const PassParamsAny& a) { return {a.beta, a.log_theta}; }
+template <> PassSandwich::Params make_params<PASS_SANDWICH>(const PassParamsAny& a) { return {a.beta, a.theta}; }
+
+template <PassKind K, int P, int GT>
+static cudaError_t run(const PassLaunch& L) {
+    using Pass = typename PassOf<K>::T;
+    constexpr int PP = P <= 1 ? 1 : (P <= 2 ? 2 : (P <= 4 ? 4 : 8));
+    if (L.xs_pad != PP) return cudaErrorInvalidValue;
+    dim3 grid(L.nseg, L.ntiles);
+    auto prm = make_params<K>(L.prm);
+    if (L.val_u16)
+        reg_pass_kernel<P, PP, GT, kRegNT, Pass, uint16_t><<<grid, kRegNT, 0, L.stream>>>(L.geo, prm);
+    else
+        reg_pass_kernel<P, PP, GT, kRegNT, Pass, float><<<grid, kRegNT, 0, L.stream>>>(L.geo, prm);
+    return cudaGetLastError();
+}
+
+template <PassKind K, int P>
+static cudaError_t run_gt(const PassLaunch& L) {
+    if constexpr (K == PASS_IRLS) {
+        switch (L.GT) {
+            case 1: return run<K, P, 1>(L);
+            case 2: return run<K, P, 2>(L);
+            case 4: if constexpr (P <= 6) return run<K, P, 4>(L); break;
+            case 8: if constexpr (P <= 4) return run<K, P, 8>(L); break;
+        }
+        return cudaErrorInvalidValue;
+    } else {
+        constexpr int G = (K == PASS_MOM) ? 8
+                        : (K == PASS_MLE) ? (P <= 2 ? 4 : (P <= 4 ? 2 : 1))
+                        : (P <= 4 ? 8 : (P <= 6 ? 4 : 2));
+        if (L.GT != G) return cudaErrorInvalidValue;
+        return run<K, P, G>(L);
+    }
+}
+
+template <PassKind K>
+static cudaError_t run_p(const PassLaunch& L) {
+    switch (L.P) {
+        case 1: return run_gt<K, 1>(L);
+        case 2: return run_gt<K, 2>(L);
+        case 3: return run_gt<K, 3>(L);
+        case 4: return run_gt<K, 4>(L);
+        case 5: return run_gt<K, 5>(L);
+        case 6: return run_gt<K, 6>(L);
+        case 7: return run_gt<K, 7>(L);
+        case 8: return run_gt<K, 8>(L);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_reg_pass(const PassLaunch& L) {
+    switch (L.kind) {
+        case PASS_IRLS: return run_p<PASS_IRLS>(L);
+        case PASS_MOM: return run_p<PASS_MOM>(L);
+        case PASS_MLE: return run_p<PASS_MLE>(L);
+        case PASS_SANDWICH: return run_p<PASS_SANDWICH>(L);
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace devil

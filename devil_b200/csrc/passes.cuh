@@ -1,0 +1,616 @@
+// Per-gene reductions over cells ("passes") for devil's NB GLM path.
+//
+// Every step of the path -- an IRLS iteration, the MOM moments, one Newton
+// evaluation of the dispersion score, the bread and the clustered meat --
+// is a reduction over all n cells of per-cell terms that depend on
+// mu_c = exp(x_c . beta_g + off_c) and on the count y_gc.  Counts are
+// sparse, so each pass is split into
+//   dense : the y = 0 value of the per-cell terms, evaluated for every cell
+//           (needs only X, the offsets and the gene's parameters), and
+//   sparse: the correction term(y) - term(0), evaluated for the nonzero
+//           entries of the gene's CSR row.
+// A pass "trait" states its terms; two engines evaluate any trait:
+//   reg_pass_kernel : p <= 8, GT genes per CTA held in registers, each cell
+//                     row of X loaded once and reused by all GT genes.
+//   gen_pass_kernel : any p <= 32, shared-memory tiles of cells; outputs
+//                     are owned one per thread.
+// Terms are of three kinds: outer(w) adds w * x x^T (packed upper
+// triangle), vec(w) adds w * x, scal(v) adds v.  Per-segment partial sums
+// go to global memory and a finalize kernel per pass reduces them in FP64.
+#pragma once
+#include "common.cuh"
+
+namespace devil {
+
+// ---------------------------------------------------------------------
+// geometry shared by both engines
+// ---------------------------------------------------------------------
+struct PassGeom {
+    const float* X;        // [n][xs] row-major float
+    int xs;                // row stride of X (>= p)
+    const float* off;      // [n]
+    const int32_t* col;    // CSR cell index
+    const void* val;       // CSR values (uint16 or float)
+    const int64_t* segptr; // [G][nbound] first CSR entry with col >= bound[b]
+    const int32_t* bound;  // [nbound] cell boundaries
+    int nbound;
+    int fpi;               // boundaries per work item (item s covers
+                           // bound[s*fpi] .. bound[(s+1)*fpi])
+    const int32_t* act;    // active gene list
+    const int32_t* n_act;  // its length (device)
+    int32_t* reset_next;   // counter zeroed by block (0,0) (may be null)
+    float* partW;          // [seg][slot_stride][NA]
+    double* partS;         // [seg][slot_stride][NS]
+    int slot_stride;
+};
+
+// ---------------------------------------------------------------------
+// accumulators
+// ---------------------------------------------------------------------
+template <int P, int NA, int NS, class AW, class AS>
+struct RegAcc {
+    AW* a;
+    AS* s;
+    const float* x;
+    template <int W>
+    DEV void outer(float w) {
+        constexpr int base = W * (P * (P + 1) / 2);
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            float wx = w * x[j];
+#pragma unroll
+            for (int i = 0; i <= j; ++i) a[base + tri_index(i, j)] += (AW)(wx * x[i]);
+        }
+    }
+    template <int V, int NW>
+    DEV void vec(float w) {
+        constexpr int base = NW * (P * (P + 1) / 2) + V * P;
+#pragma unroll
+        for (int i = 0; i < P; ++i) a[base + i] += (AW)(w * x[i]);
+    }
+    template <int K>
+    DEV void scal(AS v) { s[K] += v; }
+};
+
+// recorder used by the shared-memory engine: captures the weights only
+template <int NWV, int NS, class AS>
+struct RecAcc {
+    float w[NWV > 0 ? NWV : 1];
+    AS s[NS > 0 ? NS : 1];
+    DEV void zero() {
+#pragma unroll
+        for (int i = 0; i < NWV; ++i) w[i] = 0.f;
+#pragma unroll
+        for (int i = 0; i < NS; ++i) s[i] = 0;
+    }
+    template <int W>
+    DEV void outer(float v) { w[W] += v; }
+    template <int V, int NW>
+    DEV void vec(float v) { w[NW + V] += v; }
+    template <int K>
+    DEV void scal(AS v) { s[K] += v; }
+};
+
+// ---------------------------------------------------------------------
+// pass traits
+// ---------------------------------------------------------------------
+
+// One IRLS iteration of beta_fit (src/beta.cpp:35-42):
+//   w_q = exp(-eta - off), mu_g = (k + y) / (1 + k w_q)
+//   H = k X' diag(mu_g w_q) X,  score = k X' (mu_g w_q - 1)
+// With mu = 1/w_q:  k mu_g w_q = k (k + y)/(mu + k)  and
+//   k (mu_g w_q - 1) = k (y - mu)/(mu + k).
+// y = 0:  H weight k^2/(mu+k), score weight -k mu/(mu+k).
+// correction for y > 0: k y/(mu+k) for both.
+struct PassIRLS {
+    static constexpr int NW = 1, NV = 1, NS = 0;
+    using AW = float;
+    using AS = float;
+    struct Params { const float* beta; const float* k; };
+    struct Gene { float k, kk, nk; };
+    static DEV Gene load(const Params& p, int g) {
+        float k = p.k[g];
+        return Gene{k, k * k, -k};
+    }
+    template <class A>
+    static DEV void dense(const Gene& G, float mu, A& acc) {
+        float r = rcp_approx(mu + G.k);
+        acc.template outer<0>(G.kk * r);
+        acc.template vec<0, NW>(G.nk * mu * r);
+    }
+    template <class A>
+    static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
+        float r = rcp_approx(mu + G.k);
+        float v = G.k * y * r;
+        acc.template outer<0>(v);
+        acc.template vec<0, NW>(v);
+    }
+};
+
+// estimate_mom_dispersion_cpp (src/mom_overdispersion.cpp:34-45):
+//   num = sum (y - mu)^2 - mu,  den = sum mu^2   (FP64 accumulation)
+struct PassMOM {
+    static constexpr int NW = 0, NV = 0, NS = 2;
+    using AW = float;
+    using AS = double;
+    struct Params { const float* beta; };
+    struct Gene { int dummy; };
+    static DEV Gene load(const Params&, int) { return Gene{0}; }
+    template <class A>
+    static DEV void dense(const Gene&, float mu, A& acc) {
+        double m = mu;
+        acc.template scal<0>(m * m - m);
+        acc.template scal<1>(m * m);
+    }
+    template <class A>
+    static DEV void sparse(const Gene&, float mu, float y, A& acc) {
+        double m = mu, yy = y;
+        acc.template scal<0>(yy * yy - 2.0 * yy * m);
+    }
+};
+
+// g(x) = log(1 + x) - x / (1 + x), x = mu * theta >= 0, to full relative
+// precision.  With u = x / (1 + x):  log(1 + x) = -log(1 - u), so
+// g = sum_{m>=2} u^m / m, a series of positive terms (no cancellation);
+// for x >= 1/4 (u >= 1/5) the direct difference loses < 4 bits.
+DEV float nb_g(float x) {
+    if (x < 0.25f) {
+        float u = x / (1.f + x);
+        float t = 1.f / 14.f;
+        t = fmaf(t, u, 1.f / 13.f);
+        t = fmaf(t, u, 1.f / 12.f);
+        t = fmaf(t, u, 1.f / 11.f);
+        t = fmaf(t, u, 1.f / 10.f);
+        t = fmaf(t, u, 1.f / 9.f);
+        t = fmaf(t, u, 1.f / 8.f);
+        t = fmaf(t, u, 1.f / 7.f);
+        t = fmaf(t, u, 1.f / 6.f);
+        t = fmaf(t, u, 1.f / 5.f);
+        t = fmaf(t, u, 1.f / 4.f);
+        t = fmaf(t, u, 1.f / 3.f);
+        t = fmaf(t, u, 0.5f);
+        return u * u * t;
+    }
+    return log1pf(x) - x / (1.f + x);
+}
+
+// The per-cell part of conventional_score_function_fast's ll_part
+// (src/overdispersion.cpp:159-173) for y = 0: the reference's branches on
+// mu*theta < 1e-10 and < 1e-4 with the clamp to its Taylor bounds.
+DEV float nb_ll_term(float x) {
+    if (x < 1e-10f) return x * x * (1.f / (1.f + x) - 0.5f);
+    float gx = nb_g(x);
+    if (x < 1e-4f) {
+        float inv = 1.f / (1.f + x);
+        float ub = x * x * inv, lb = x * x * (inv - 0.5f);
+        gx = fmaxf(fminf(gx, ub), lb);
+    }
+    return gx;
+}
+
+// psi(y + a) - psi(a) and psi1(y + a) - psi1(a) for a count y > 0
+DEV double digamma_d(double x) {
+    double r = 0.0;
+    while (x < 10.0) { r -= 1.0 / x; x += 1.0; }
+    double f = 1.0 / (x * x);
+    double t = f * (-1.0 / 12 + f * (1.0 / 120 + f * (-1.0 / 252 + f * (1.0 / 240 +
+               f * (-1.0 / 132 + f * (691.0 / 32760 + f * (-1.0 / 12)))))));
+    return r + log(x) - 0.5 / x + t;
+}
+DEV double trigamma_d(double x) {
+    double r = 0.0;
+    while (x < 10.0) { r += 1.0 / (x * x); x += 1.0; }
+    double f = 1.0 / (x * x);
+    double t = 1.0 / x + f / 2.0 + (f / x) * (1.0 / 6 + f * (-1.0 / 30 + f * (1.0 / 42 +
+               f * (-1.0 / 30 + f * (5.0 / 66 + f * (-691.0 / 2730 + f * (7.0 / 6)))))));
+    return r + t;
+}
+DEV void psi_diffs(double y, double a, double& d1, double& d2) {
+    if (y <= 32.0 && y == floor(y)) {
+        double s1 = 0.0, s2 = 0.0;
+        int yi = (int)y;
+        for (int j = 0; j < yi; ++j) {
+            double v = 1.0 / (a + j);
+            s1 += v;
+            s2 -= v * v;
+        }
+        d1 = s1;
+        d2 = s2;
+    } else {
+        d1 = digamma_d(y + a) - digamma_d(a);
+        d2 = trigamma_d(y + a) - trigamma_d(a);
+    }
+}
+
+// One evaluation of the dispersion score and its derivative in log theta
+// (src/overdispersion.cpp:95-242) at theta:
+//   scal0 = sum ll_term(mu theta)          scal1 = sum mu x/(1+x)^2
+//   scal2 = sum y theta/(1+x)              scal3 = sum y/(1+x)^2
+//   scal4 = sum psi(y+a) - psi(a)          scal5 = sum psi1(y+a) - psi1(a)
+//   outer0 = X' diag(w) X, outer1 = X' diag(-w^2) X, outer2 = X' diag(2 w^3) X
+// with x = mu theta, a = 1/theta, w = mu/(1 + x)  (Cox-Reid b, db, d2b).
+struct PassMLE {
+    static constexpr int NW = 3, NV = 0, NS = 6;
+    using AW = float;
+    using AS = double;
+    struct Params { const float* beta; const double* log_theta; };
+    struct Gene { double theta, a; float thf; };
+    static DEV Gene load(const Params& p, int g) {
+        double th = exp(p.log_theta[g]);
+        return Gene{th, 1.0 / th, (float)th};
+    }
+    template <class A>
+    static DEV void dense(const Gene& G, float mu, A& acc) {
+        float x = mu * G.thf;
+        float r = 1.f / (1.f + x);
+        float w = mu * r;
+        acc.template outer<0>(w);
+        acc.template outer<1>(-w * w);
+        acc.template outer<2>(2.f * w * w * w);
+        acc.template scal<0>((double)nb_ll_term(x));
+        acc.template scal<1>((double)(mu * x * r * r));
+    }
+    template <class A>
+    static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
+        double m = mu, yy = y;
+        double den = 1.0 + m * G.theta;
+        acc.template scal<2>(yy * G.theta / den);
+        acc.template scal<3>(yy / (den * den));
+        double d1, d2;
+        psi_diffs(yy, G.a, d1, d2);
+        acc.template scal<4>(d1);
+        acc.template scal<5>(d2);
+    }
+};
+
+// compute_hessian (src/variance.cpp:22-47) and the per-cluster score sums of
+// compute_clustered_meat_fast (src/variance.cpp:207-217) in one pass:
+//   outer0 = X' diag((y theta + 1) mu / (1 + theta mu)^2) X
+//   vec0   = X' (y - mu)/(1 + mu theta)       (per segment; segments never
+//                                              cross a cluster boundary)
+struct PassSandwich {
+    static constexpr int NW = 1, NV = 1, NS = 0;
+    using AW = float;
+    using AS = float;
+    struct Params { const float* beta; const double* theta; };
+    struct Gene { float th; };
+    static DEV Gene load(const Params& p, int g) { return Gene{(float)p.theta[g]}; }
+    template <class A>
+    static DEV void dense(const Gene& G, float mu, A& acc) {
+        float r = 1.f / (1.f + G.th * mu);
+        acc.template outer<0>(mu * r * r);
+        acc.template vec<0, NW>(-mu * r);
+    }
+    template <class A>
+    static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
+        float r = 1.f / (1.f + G.th * mu);
+        acc.template outer<0>(y * G.th * mu * r * r);
+        acc.template vec<0, NW>(y * r);
+    }
+};
+
+// ---------------------------------------------------------------------
+// engine 1: registers, p <= 8
+// ---------------------------------------------------------------------
+template <int P, int PP>
+DEV void load_row(const float* __restrict__ X, int64_t c, float* x) {
+    const float* r = X + c * PP;
+    if constexpr (PP == 8) {
+        float4 a = __ldg(reinterpret_cast<const float4*>(r));
+        float4 b = __ldg(reinterpret_cast<const float4*>(r) + 1);
+        float t[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < P; ++i) x[i] = t[i];
+    } else if constexpr (PP == 4) {
+        float4 a = __ldg(reinterpret_cast<const float4*>(r));
+        float t[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int i = 0; i < P; ++i) x[i] = t[i];
+    } else if constexpr (PP == 2) {
+        float2 a = __ldg(reinterpret_cast<const float2*>(r));
+        float t[2] = {a.x, a.y};
+#pragma unroll
+        for (int i = 0; i < P; ++i) x[i] = t[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < P; ++i) x[i] = __ldg(r + i);
+    }
+}
+
+template <int P, int PP, int GT, int NT, class Pass, class VT>
+__global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pass::Params prm) {
+    constexpr int NE = P * (P + 1) / 2;
+    constexpr int NA = Pass::NW * NE + Pass::NV * P;
+    constexpr int NS = Pass::NS;
+    constexpr int NAc = NA > 0 ? NA : 1;
+    constexpr int NSc = NS > 0 ? NS : 1;
+    using AW = typename Pass::AW;
+    using AS = typename Pass::AS;
+
+    if (geo.reset_next && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *geo.reset_next = 0;
+    const int nact = *geo.n_act;
+    const int tile = blockIdx.y;
+    if (tile * GT >= nact) return;
+    const int seg = blockIdx.x;
+    const VT* __restrict__ val = static_cast<const VT*>(geo.val);
+
+    int gid[GT];
+    float beta[GT][P];
+    typename Pass::Gene gp[GT];
+#pragma unroll
+    for (int j = 0; j < GT; ++j) {
+        int slot = tile * GT + j;
+        if (slot >= nact) slot = tile * GT;  // duplicate a valid gene; not written
+        int g = __ldg(geo.act + slot);
+        gid[j] = g;
+#pragma unroll
+        for (int i = 0; i < P; ++i) beta[j][i] = __ldg(prm.beta + (int64_t)g * P + i) * kLog2e;
+        gp[j] = Pass::load(prm, g);
+    }
+
+    AW aw[GT][NAc];
+    AS as[GT][NSc];
+#pragma unroll
+    for (int j = 0; j < GT; ++j) {
+#pragma unroll
+        for (int a = 0; a < NAc; ++a) aw[j][a] = 0;
+#pragma unroll
+        for (int s = 0; s < NSc; ++s) as[j][s] = 0;
+    }
+
+    const int b0 = seg * geo.fpi, b1 = b0 + geo.fpi;
+    const int c0 = __ldg(geo.bound + b0), c1 = __ldg(geo.bound + b1);
+
+    for (int c = c0 + threadIdx.x; c < c1; c += NT) {
+        float x[P];
+        load_row<P, PP>(geo.X, c, x);
+        float o = __ldg(geo.off + c) * kLog2e;
+#pragma unroll
+        for (int j = 0; j < GT; ++j) {
+            float e = o;
+#pragma unroll
+            for (int i = 0; i < P; ++i) e = fmaf(x[i], beta[j][i], e);
+            float mu = ex2_approx(e);
+            RegAcc<P, NAc, NSc, AW, AS> acc{aw[j], as[j], x};
+            Pass::dense(gp[j], mu, acc);
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < GT; ++j) {
+        const int64_t* sp = geo.segptr + (int64_t)gid[j] * geo.nbound;
+        int64_t e0 = __ldg(sp + b0), e1 = __ldg(sp + b1);
+        for (int64_t e = e0 + threadIdx.x; e < e1; e += NT) {
+            int c = __ldg(geo.col + e);
+            float y = load_val(val, e);
+            float x[P];
+            load_row<P, PP>(geo.X, c, x);
+            float el = __ldg(geo.off + c) * kLog2e;
+#pragma unroll
+            for (int i = 0; i < P; ++i) el = fmaf(x[i], beta[j][i], el);
+            float mu = ex2_approx(el);
+            RegAcc<P, NAc, NSc, AW, AS> acc{aw[j], as[j], x};
+            Pass::sparse(gp[j], mu, y, acc);
+        }
+    }
+
+    // block reduction: warp shuffles, then across warps through shared memory
+    constexpr int NWARP = NT / 32;
+    __shared__ AW redW[NWARP][GT * NAc];
+    __shared__ AS redS[NWARP][GT * NSc];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < GT; ++j) {
+        if constexpr (NA > 0) {
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+                AW v = warp_sum(aw[j][a]);
+                if (lane == 0) redW[warp][j * NAc + a] = v;
+            }
+        }
+        if constexpr (NS > 0) {
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                AS v = warp_sum(as[j][s]);
+                if (lane == 0) redS[warp][j * NSc + s] = v;
+            }
+        }
+    }
+    __syncthreads();
+    if constexpr (NA > 0) {
+        for (int t = threadIdx.x; t < GT * NA; t += NT) {
+            int j = t / NA, a = t - j * NA;
+            int slot = tile * GT + j;
+            if (slot >= nact) continue;
+            float s = 0.f;
+#pragma unroll
+            for (int w = 0; w < NWARP; ++w) s += (float)redW[w][j * NAc + a];
+            geo.partW[((int64_t)seg * geo.slot_stride + slot) * NA + a] = s;
+        }
+    }
+    if constexpr (NS > 0) {
+        for (int t = threadIdx.x; t < GT * NS; t += NT) {
+            int j = t / NS, s = t - j * NS;
+            int slot = tile * GT + j;
+            if (slot >= nact) continue;
+            double v = 0.0;
+#pragma unroll
+            for (int w = 0; w < NWARP; ++w) v += (double)redS[w][j * NSc + s];
+            geo.partS[((int64_t)seg * geo.slot_stride + slot) * NS + s] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------
+// engine 2: shared-memory tiles, any p <= 32 (runtime p)
+// ---------------------------------------------------------------------
+// Threads 0..NT-1 are split into GT gene groups of TC = NT/GT threads.  Per
+// chunk of TC cells: X rows are staged in shared memory, the genes' nonzero
+// counts are scattered into a dense shared tile, each thread evaluates the
+// per-cell weights of one (gene, cell) pair, and then every thread adds the
+// cell terms of the outputs it owns.
+constexpr int kGenNT = 256;
+constexpr int kGenKMAX = 16;
+
+template <class Pass, class VT>
+__global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename Pass::Params prm,
+                                                          int P, int GT) {
+    constexpr int NWV = Pass::NW + Pass::NV;
+    constexpr int NS = Pass::NS;
+    using AS = typename Pass::AS;
+    const int NE = P * (P + 1) / 2;
+    const int NA = Pass::NW * NE + Pass::NV * P;
+    const int TC = kGenNT / GT;
+    const int XS = (P + 1) | 1;  // odd row stride: conflict-free column reads
+
+    if (geo.reset_next && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *geo.reset_next = 0;
+    const int nact = *geo.n_act;
+    const int tile = blockIdx.y;
+    if (tile * GT >= nact) return;
+    const int seg = blockIdx.x;
+    const VT* __restrict__ val = static_cast<const VT*>(geo.val);
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* wsc = reinterpret_cast<double*>(smem_raw);              // [NS][GT][TC]
+    int64_t* cursor = reinterpret_cast<int64_t*>(wsc + NS * kGenNT); // [GT]
+    int64_t* cend = cursor + GT;                                    // [GT]
+    int* cnt = reinterpret_cast<int*>(cend + GT);                   // [GT]
+    int* gids = cnt + GT;                                           // [GT]
+    float* xsm = reinterpret_cast<float*>(gids + GT);               // [TC][XS]
+    float* wts = xsm + TC * XS;                                     // [NWV][GT][TC]
+    float* ys = wts + NWV * kGenNT;                                 // [GT][TC]
+    float* betas = ys + kGenNT;                                     // [GT][P]
+    const int t = threadIdx.x;
+    const int b0 = seg * geo.fpi, b1 = b0 + geo.fpi;
+    const int c0 = __ldg(geo.bound + b0), c1 = __ldg(geo.bound + b1);
+    if (t < GT) {
+        int slot = tile * GT + t;
+        if (slot >= nact) slot = tile * GT;
+        int g = __ldg(geo.act + slot);
+        gids[t] = g;
+        const int64_t* sp = geo.segptr + (int64_t)g * geo.nbound;
+        cursor[t] = __ldg(sp + b0);
+        cend[t] = __ldg(sp + b1);
+    }
+    __syncthreads();
+    for (int i = t; i < GT * P; i += kGenNT) {
+        int j = i / P, k = i - j * P;
+        betas[i] = __ldg(prm.beta + (int64_t)gids[j] * P + k);
+    }
+    const int gA = t / TC, cA = t - gA * TC;
+    typename Pass::Gene gpar = Pass::load(prm, gids[gA]);
+
+    // owned outputs (W-type): o = t + k*NT over [0, GT*NA)
+    float acc[kGenKMAX];
+    short oi[kGenKMAX], oj[kGenKMAX], og[kGenKMAX], ow[kGenKMAX];
+    int nown = 0;
+#pragma unroll
+    for (int k = 0; k < kGenKMAX; ++k) {
+        acc[k] = 0.f;
+        int o = t + k * kGenNT;
+        og[k] = 0; ow[k] = 0; oi[k] = 0; oj[k] = 0;
+        if (o < GT * NA) {
+            nown = k + 1;
+            int g = o / NA, a = o - g * NA;
+            og[k] = (short)g;
+            if (a < Pass::NW * NE) {
+                int w = a / NE, q = a - w * NE;
+                int j = 0;
+                while ((j + 1) * (j + 2) / 2 <= q) ++j;
+                int i = q - j * (j + 1) / 2;
+                ow[k] = (short)w; oi[k] = (short)i; oj[k] = (short)j;
+            } else {
+                int r = a - Pass::NW * NE;
+                int v = r / P, i = r - v * P;
+                ow[k] = (short)(Pass::NW + v); oi[k] = (short)i; oj[k] = (short)P;  // x_P == 1
+            }
+        }
+    }
+    // owned scalar outputs: thread t < GT*NS owns (gene t/NS, scalar t%NS)
+    AS sacc = 0;
+    __syncthreads();
+
+    float breg[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) breg[i] = (i < P) ? betas[gA * P + i] * kLog2e : 0.f;
+
+    for (int cb = c0; cb < c1; cb += TC) {
+        const int nc = min(TC, c1 - cb);
+        // stage X rows (+ the constant 1 column) and offsets; clear the tile
+        for (int i = t; i < nc * P; i += kGenNT) {
+            int c = i / P, k = i - c * P;
+            xsm[c * XS + k] = __ldg(geo.X + (int64_t)(cb + c) * geo.xs + k);
+        }
+        for (int c = t; c < TC; c += kGenNT) xsm[c * XS + P] = 1.f;
+        ys[t] = 0.f;
+        if (t < GT) cnt[t] = 0;
+        __syncthreads();
+        // scatter this chunk's nonzeros of gene gA (at most TC entries)
+        {
+            int64_t e = cursor[gA] + cA;
+            if (e < cend[gA]) {
+                int c = __ldg(geo.col + e);
+                if (c >= cb && c < cb + nc) {
+                    ys[gA * TC + (c - cb)] = load_val(val, e);
+                    atomicAdd(&cnt[gA], 1);
+                }
+            }
+        }
+        __syncthreads();
+        if (cA == 0) cursor[gA] += cnt[gA];
+        // per-(gene, cell) weights
+        {
+            RecAcc<NWV, NS, AS> rec;
+            rec.zero();
+            if (cA < nc) {
+                float e = __ldg(geo.off + cb + cA) * kLog2e;
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                    if (i < P) e = fmaf(xsm[cA * XS + i], breg[i], e);
+                float mu = ex2_approx(e);
+                float y = ys[gA * TC + cA];
+                Pass::dense(gpar, mu, rec);
+                if (y != 0.f) Pass::sparse(gpar, mu, y, rec);
+            }
+#pragma unroll
+            for (int w = 0; w < NWV; ++w) wts[(w * GT + gA) * TC + cA] = rec.w[w];
+#pragma unroll
+            for (int s = 0; s < NS; ++s) wsc[(s * GT + gA) * TC + cA] = rec.s[s];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kGenKMAX; ++k) {
+            if (k >= nown) break;
+            const float* wp = wts + (ow[k] * GT + og[k]) * TC;
+            const float* xi = xsm + oi[k];
+            const float* xj = xsm + oj[k];
+            float s = acc[k];
+            for (int c = 0; c < nc; ++c) s = fmaf(wp[c] * xi[c * XS], xj[c * XS], s);
+            acc[k] = s;
+        }
+        if (NS > 0 && t < GT * NS) {
+            constexpr int NSd = NS > 0 ? NS : 1;
+            int g = t / NSd, s = t - g * NSd;
+            const double* sp = wsc + (s * GT + g) * TC;
+            AS v = sacc;
+            for (int c = 0; c < nc; ++c) v += sp[c];
+            sacc = v;
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int k = 0; k < kGenKMAX; ++k) {
+        if (k >= nown) break;
+        int o = t + k * kGenNT;
+        int g = o / NA, a = o - g * NA;
+        int slot = tile * GT + g;
+        if (slot < nact) geo.partW[((int64_t)seg * geo.slot_stride + slot) * NA + a] = acc[k];
+    }
+    if (NS > 0 && t < GT * NS) {
+        constexpr int NSd = NS > 0 ? NS : 1;
+        int g = t / NSd, s = t - g * NSd;
+        int slot = tile * GT + g;
+        if (slot < nact) geo.partS[((int64_t)seg * geo.slot_stride + slot) * NS + s] = (double)sacc;
+    }
+}
+
+}  // namespace devil

@@ -1,0 +1,233 @@
+"""GPU parity: fit_devil / test_de through libdevil_b200.so against the FP64
+oracle (cpu_fit, R/main.R:375-523) on the same seeded inputs.
+
+Bars (from the path's acceptance criteria):
+  * beta: |d beta| <= 1e-5 on genes whose IRLS iteration counts agree;
+    iteration counts agree on >= 97% of genes (a gene whose max|delta|
+    lands within FP32 rounding of the tolerance may take one step more or
+    less; those genes differ by at most one step < tolerance);
+  * theta: relative <= 1e-4 (MOM, MLE) on genes that converge in both and
+    whose theta is resolvable (see _theta_mask);
+  * bread / sandwich: relative <= 1e-4 of the diagonal scale;
+  * p-values: relative |d log10 p| <= 1e-3.
+"""
+import numpy as np
+import pytest
+
+from devil_b200 import synthetic
+
+pytestmark = pytest.mark.gpu
+
+BETA_TOL = 1e-5
+ITER_AGREE = 0.97
+
+
+def oracle_fit(orc, P, od, clusters_ends=None, sf="normed_sum", max_iter=200, tol=1e-3,
+               init_rough=False):
+    Y = P.csr_f64()
+    if sf is None:
+        sfv = np.ones(P.n)
+        off = orc.offset_vector(0.0, P.n, None)
+    else:
+        sfv = orc.calculate_sf(Y, sf)
+        off = orc.offset_vector(0.0, P.n, sfv)
+    th0 = orc.estimate_dispersion(Y, off)
+    b0 = orc.init_beta(Y, P.X, off, rough=init_rough)
+    r = orc.cpu_fit(Y, P.X, off, th0, b0, od, max_iter, tol, ends=clusters_ends, theta_mom=True)
+    r.update(sf=sfv, off=off, theta0=th0, beta0=b0)
+    return r
+
+
+def gpu_fit(dv, P, od, clusters=None, sf="normed_sum", max_iter=200, tol=1e-3, form="chosen",
+            init_rough=False):
+    return dv.fit_devil((P.rowptr, P.col, P.val, P.n), P.X, clusters=clusters, overdispersion=od,
+                        size_factors=sf, max_iter=max_iter, tolerance=tol, form=form,
+                        compute_theta_mom=True, init_beta_rough=init_rough)
+
+
+def check_beta(fit, ref, tol=BETA_TOL, agree=ITER_AGREE):
+    it_g = fit["iterations"]["beta_iters"]
+    it_o = ref["iters"]
+    same = it_g == it_o
+    assert same.mean() >= agree, f"iteration counts agree on only {same.mean():.3f}"
+    d = np.abs(fit["beta"] - ref["beta"])
+    assert np.nanmax(d[same]) <= tol, f"max |dbeta| = {np.nanmax(d[same]):.3e}"
+    # genes off by one iteration: the extra step is below the tolerance
+    if (~same).any():
+        assert np.all(np.abs(it_g[~same] - it_o[~same]) <= 1)
+        assert np.nanmax(d[~same]) <= 10 * 1e-3
+    return same
+
+
+def _theta_mask(th_ref, same):
+    return same & (th_ref > 1e-3) & (th_ref < 1e3)
+
+
+def check_rel(a, b, mask, tol, what):
+    a, b = np.asarray(a)[mask], np.asarray(b)[mask]
+    r = np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+    assert r.size == 0 or r.max() <= tol, f"{what}: max rel err {r.max():.3e}"
+
+
+def check_mats(A, B, mask, tol, what):
+    A, B = np.asarray(A)[mask], np.asarray(B)[mask]
+    diag = np.sqrt(np.abs(np.einsum("gii->gi", B)))
+    scale = diag[:, :, None] * diag[:, None, :]
+    r = np.abs(A - B) / np.maximum(scale, 1e-300)
+    assert r.size == 0 or r.max() <= tol, f"{what}: max rel err {r.max():.3e}"
+
+
+def check_pvals(p_g, p_o, mask, tol=1e-3):
+    ok = mask & np.isfinite(p_o) & (p_o > 1e-300) & np.isfinite(p_g) & (p_g > 0)
+    lg, lo = np.log10(p_g[ok]), np.log10(p_o[ok])
+    r = np.abs(lg - lo) / np.maximum(1.0, np.abs(lo))
+    assert r.size == 0 or r.max() <= tol, f"log10 p rel err {r.max():.3e}"
+
+
+@pytest.fixture(scope="module")
+def sparse_problem():
+    return synthetic.make("plain_sparse", seed=11, G=300, n=6000)
+
+
+@pytest.mark.parametrize("od", ["MOM", "MLE", False])
+def test_fit_sparse_p4(dv, orc, sparse_problem, od):
+    P = sparse_problem
+    code = {"MOM": orc.OD_MOM, "MLE": orc.OD_MLE, False: orc.OD_NONE}[od]
+    ref = oracle_fit(orc, P, code)
+    fit = gpu_fit(dv, P, od)
+    np.testing.assert_allclose(fit["size_factors"], ref["sf"], rtol=1e-12)
+    np.testing.assert_allclose(fit["offset_vector"], ref["off"], rtol=0, atol=1e-12)
+    same = check_beta(fit, ref)
+    check_rel(fit["theta_mom"], ref["theta_mom"], _theta_mask(ref["theta_mom"], same), 1e-4,
+              "theta MOM")
+    if od == "MLE":
+        check_rel(fit["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4,
+                  "theta MLE")
+        assert np.isnan(fit["iterations"]["theta_iters"]).all()
+    elif od is False:
+        assert (fit["overdispersion"] == 0).all()
+    check_mats(fit["beta_sandwiches_null"], ref["bread"], same & (ref["theta"] < 1e3), 1e-4, "bread")
+    c = np.array([0.0, 1.0, 0.0, 0.0])
+    res = dv.test_de(fit, c)
+    pv, pa, lf = orc.test_de(ref["beta"], ref["bread"], None, P.n, c)
+    check_pvals(res["pval"], pv, same)
+
+
+def test_fit_dense_p2(dv, orc):
+    P = synthetic.make("plain_small", seed=5, G=200, n=1500)
+    Y = P.dense()
+    ref = oracle_fit(orc, P, orc.OD_MLE)
+    fit = dv.fit_devil(Y, P.X, overdispersion="MLE", size_factors="normed_sum",
+                       compute_theta_mom=True)
+    same = check_beta(fit, ref)
+    check_rel(fit["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta")
+    res = dv.test_de(fit, [0, 1])
+    pv, _, _ = orc.test_de(ref["beta"], ref["bread"], None, P.n, [0, 1])
+    check_pvals(res["pval"], pv, same)
+
+
+def test_fit_clustered_p12(dv, orc):
+    P = synthetic.make("clustered", seed=7, G=60, n=6000)
+    # 40 patients are drawn for the full config; sizes here scale with n
+    levels, ends = dv.cluster_blocks(P.clusters)
+    ref = oracle_fit(orc, P, orc.OD_MOM, clusters_ends=ends)
+    fit = gpu_fit(dv, P, "MOM", clusters=P.clusters)
+    same = check_beta(fit, ref)
+    check_rel(fit["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta")
+    check_mats(fit["beta_sandwiches_null"], ref["bread"], same, 1e-4, "bread")
+    check_mats(fit["beta_sandwiches"], ref["sandwich"], same, 1e-4, "sandwich")
+    c = np.zeros(P.p)
+    c[1] = 1.0
+    res = dv.test_de(fit, c)
+    pv, _, _ = orc.test_de(ref["beta"], ref["bread"], ref["sandwich"], P.n, c)
+    check_pvals(res["pval"], pv, same)
+
+
+def test_fit_wide_p32(dv, orc):
+    P = synthetic.make("wide", seed=2, G=24, n=4000)
+    ref = oracle_fit(orc, P, orc.OD_MOM, sf=None)
+    fit = gpu_fit(dv, P, "MOM", sf=None)
+    same = check_beta(fit, ref)
+    check_mats(fit["beta_sandwiches_null"], ref["bread"], same, 1e-4, "bread")
+
+
+def test_plain_form_matches_oracle(dv, orc, sparse_problem):
+    P = sparse_problem.subset_genes(np.arange(80))
+    ref = oracle_fit(orc, P, orc.OD_MOM)
+    fit = gpu_fit(dv, P, "MOM", form="plain")
+    check_beta(fit, ref)
+
+
+def test_rough_init_and_given_sf(dv, orc, sparse_problem):
+    P = sparse_problem.subset_genes(np.arange(64))
+    Y = P.csr_f64()
+    sf = P.sf_true
+    off = orc.offset_vector(0.0, P.n, sf)
+    th0 = orc.estimate_dispersion(Y, off)
+    b0 = orc.init_beta(Y, P.X, off, rough=True)
+    ref = orc.cpu_fit(Y, P.X, off, th0, b0, orc.OD_MOM, 200, 1e-3)
+    fit = dv.fit_devil((P.rowptr, P.col, P.val, P.n), P.X, size_factors=sf,
+                       init_beta_rough=True)
+    check_beta(fit, ref)
+
+
+def test_single_steps(dv, orc, sparse_problem):
+    P = sparse_problem.subset_genes(np.arange(50))
+    Y = P.csr_f64()
+    csr = (P.rowptr, P.col, P.val, P.n)
+    for m in ("normed_sum", "psinorm"):
+        np.testing.assert_allclose(dv.calculate_sf(csr, m), orc.calculate_sf(Y, m), rtol=1e-12)
+    sf = orc.calculate_sf(Y, "normed_sum")
+    off = orc.offset_vector(0.0, P.n, sf)
+    np.testing.assert_allclose(dv.estimate_dispersion(csr, off), orc.estimate_dispersion(Y, off),
+                               rtol=1e-12)
+    np.testing.assert_allclose(dv.init_beta(csr, P.X, off), orc.init_beta(Y, P.X, off),
+                               rtol=0, atol=1e-10)
+    b = P.beta_true
+    th = P.theta_true
+    np.testing.assert_allclose(dv.estimate_mom_dispersion(csr, P.X, b, sf),
+                               [orc.mom_dispersion(y, P.X, bb, sf) for y, bb in zip(P.dense(), b)],
+                               rtol=1e-5, atol=1e-9)
+    bread = dv.compute_hessian(b, th, csr, P.X, sf)
+    ref = np.stack([orc.compute_hessian(bb, t, y, P.X, sf) for bb, t, y in zip(b, th, P.dense())])
+    check_mats(bread, ref, np.ones(P.G, bool), 1e-5, "compute_hessian")
+
+
+def test_beta_fit_entry(dv, orc, sparse_problem):
+    P = sparse_problem.subset_genes(np.arange(40))
+    Y = P.dense()
+    csr = (P.rowptr, P.col, P.val, P.n)
+    off = np.log(P.sf_true)
+    b0 = orc.init_beta(P.csr_f64(), P.X, off)
+    th0 = P.theta_true
+    b, it = dv.beta_fit(csr, P.X, b0, off, th0, 200, 1e-3)
+    ref = [orc.beta_fit(y, P.X, bb, off, t, 200, 1e-3) for y, bb, t in zip(Y, b0, th0)]
+    rb = np.stack([r[0] for r in ref])
+    ri = np.array([r[1] for r in ref])
+    same = it == ri
+    assert same.mean() >= ITER_AGREE
+    assert np.abs(b - rb)[same].max() <= BETA_TOL
+
+
+def test_fit_dispersion_entry(dv, orc, sparse_problem):
+    P = sparse_problem.subset_genes(np.arange(60))
+    Y = P.dense()
+    csr = (P.rowptr, P.col, P.val, P.n)
+    off = np.log(P.sf_true)
+    b = P.beta_true
+    for cr in (True, False):
+        th, _ = dv.fit_dispersion(b, P.X, csr, off, do_cox_reid_adjustment=cr)
+        ref = np.array([orc.fit_dispersion(bb, P.X, y, off, 200, cr)[0] for bb, y in zip(b, Y)])
+        mask = (ref > 1e-3) & (ref < 1e3)
+        check_rel(th, ref, mask, 1e-4, f"fit_dispersion cr={cr}")
+        assert np.all((ref == 0) == (th == 0))
+
+
+def test_clustered_meat_entry(dv, orc):
+    P = synthetic.make("clustered", seed=9, G=20, n=3000)
+    levels, ends = dv.cluster_blocks(P.clusters)
+    b, th, sf = P.beta_true, P.theta_true, P.sf_true
+    meat = dv.compute_clustered_meat(P.X, (P.rowptr, P.col, P.val, P.n), b, th, sf, ends)
+    ref = np.stack([orc.clustered_meat_fast(P.X, y, bb, t, sf, ends)
+                    for y, bb, t in zip(P.dense(), b, th)])
+    check_mats(meat, ref, np.ones(P.G, bool), 1e-4, "meat")
