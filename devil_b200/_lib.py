@@ -33,7 +33,8 @@ EXPORTS = (
     "devil_calculate_sf", "devil_estimate_dispersion", "devil_init_beta", "devil_beta_fit",
     "devil_estimate_mom_dispersion", "devil_fit_dispersion", "devil_compute_hessian",
     "devil_compute_clustered_meat", "devil_nb_adjoint", "devil_cluster_blocks",
-    "devil_group_order",
+    "devil_group_order", "devil_ctx_set_profiling", "devil_ctx_profile",
+    "devil_p_adjust_device",
 )
 
 
@@ -99,6 +100,7 @@ def load():
         L.devil_test_de.argtypes = [vp, i64, i, vp, vp, vp, i64, vp, i, dbl, vp, vp, vp]
         L.devil_test_de_device.argtypes = L.devil_test_de.argtypes
         L.devil_p_adjust.argtypes = [vp, i64, vp, i, vp]
+        L.devil_p_adjust_device.argtypes = [vp, i64, vp, i, vp]
         L.devil_calculate_sf.argtypes = [vp, C.POINTER(Counts), i, vp]
         L.devil_estimate_dispersion.argtypes = [vp, C.POINTER(Counts), vp, vp]
         L.devil_init_beta.argtypes = [vp, C.POINTER(Counts), vp, i, vp, i, vp]
@@ -111,6 +113,8 @@ def load():
         L.devil_nb_adjoint.argtypes = [vp, i64, vp, vp, dbl, vp, vp, vp]
         L.devil_cluster_blocks.argtypes = [i64, vp, vp, vp, C.POINTER(C.c_int)]
         L.devil_group_order.argtypes = [i64, vp, vp]
+        L.devil_ctx_set_profiling.argtypes = [vp, i]
+        L.devil_ctx_profile.argtypes = [vp, i, C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]
         _lib = L
     return _lib
 
@@ -139,6 +143,17 @@ class Context:
     @property
     def stream(self) -> int:
         return int(load().devil_ctx_stream(self.h) or 0)
+
+    def set_profiling(self, enable: bool):
+        self.check(load().devil_ctx_set_profiling(self.h, int(bool(enable))))
+
+    def profile(self, kind: int):
+        """(launches, total ms, algorithmic bytes) of pass kind 0 IRLS, 1 MOM,
+        2 MLE, 3 bread/meat since profiling was enabled."""
+        n, ms, b = C.c_int64(0), C.c_double(0), C.c_double(0)
+        self.check(load().devil_ctx_profile(self.h, int(kind), C.byref(n), C.byref(ms),
+                                            C.byref(b)))
+        return n.value, ms.value, b.value
 
     def synchronize(self):
         self.check(load().devil_ctx_synchronize(self.h))

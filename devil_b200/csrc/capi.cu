@@ -35,6 +35,15 @@ struct devil_ctx {
     int32_t* mapped_dev = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int sm_count = 148;
+    // profiling: CUDA events around every pass launch, per pass kind
+    int profiling = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    struct Rec { int kind; size_t e0, e1; };
+    std::vector<Rec> recs;
+    int64_t prof_launches[4] = {0, 0, 0, 0};
+    double prof_ms[4] = {0, 0, 0, 0};
+    double prof_bytes[4] = {0, 0, 0, 0};
 };
 
 namespace {
@@ -93,6 +102,34 @@ T* ws(devil_ctx* ctx, const std::string& name, size_t count) {
     return static_cast<T*>(b.p);
 }
 
+size_t prof_event(devil_ctx* ctx) {
+    if (ctx->ev_used == ctx->ev_pool.size()) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        ctx->ev_pool.push_back(e);
+    }
+    size_t i = ctx->ev_used++;
+    CK(cudaEventRecord(ctx->ev_pool[i], ctx->stream));
+    return i;
+}
+
+// fold recorded event pairs into the per-kind totals (synchronizes)
+void prof_collect(devil_ctx* ctx) {
+    if (!ctx->profiling || ctx->recs.empty()) {
+        ctx->ev_used = 0;
+        return;
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (auto& r : ctx->recs) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->ev_pool[r.e0], ctx->ev_pool[r.e1]));
+        ctx->prof_ms[r.kind] += ms;
+        ctx->prof_launches[r.kind] += 1;
+    }
+    ctx->recs.clear();
+    ctx->ev_used = 0;
+}
+
 template <class T>
 void h2d(devil_ctx* ctx, T* dst, const T* src, size_t count) {
     if (count) CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
@@ -122,6 +159,7 @@ struct DevProblem {
     int64_t nnz = 0;
     const double* Xcm = nullptr;
     float* Xrm = nullptr;
+    double* Xdrm = nullptr;  // row-major FP64 copy for the FP64 passes
     double* sf = nullptr;
     double* off = nullptr;
     float* off_f = nullptr;
@@ -299,6 +337,8 @@ void prepare_design(devil_ctx* ctx, DevProblem& dp, const double* X, int P, bool
     }
     dp.Xrm = ws<float>(ctx, "Xrm", (size_t)dp.n * dp.xs);
     LAUNCH(launch_x_rowmajor(dp.Xcm, dp.n, P, dp.xs, dp.Xrm, st));
+    dp.Xdrm = ws<double>(ctx, "Xdrm", (size_t)dp.n * dp.xs);
+    LAUNCH(launch_x_rowmajor_d(dp.Xcm, dp.n, P, dp.xs, dp.Xdrm, st));
     // uniform fine segmentation: power-of-two count, >= 1024 cells each
     int nf = (int)std::min<int64_t>(64, std::max<int64_t>(1, dp.n / 1024));
     nf = pow2_floor(nf);
@@ -411,13 +451,15 @@ size_t max_slot_segs(devil_ctx* ctx, const DevProblem& dp, int GT, int form) {
 }
 
 struct PassBuffers {
-    float* partW;
+    void* partW;     // Pass::AW partial sums (float, or double for the sandwich)
     double* partS;
+    float* partWf() const { return static_cast<float*>(partW); }
+    double* partWd() const { return static_cast<double*>(partW); }
 };
 
 PassBuffers pass_buffers(devil_ctx* ctx, PassKind k, int P, size_t slots_x_segs) {
     PassBuffers b;
-    b.partW = ws<float>(ctx, "partW", slots_x_segs * std::max(1, pass_na(k, P)));
+    b.partW = ws<double>(ctx, "partW", slots_x_segs * std::max(1, pass_na(k, P)));
     b.partS = ws<double>(ctx, "partS", slots_x_segs * std::max(1, pass_ns(k)));
     return b;
 }
@@ -438,6 +480,8 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
     L.geo.X = dp.Xrm;
     L.geo.xs = dp.xs;
     L.geo.off = dp.off_f;
+    L.geo.Xd = dp.Xdrm;
+    L.geo.offd = dp.off;
     L.geo.col = dp.col;
     L.geo.val = dp.val;
     L.geo.segptr = segptr;
@@ -452,10 +496,35 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
     L.geo.slot_stride = tiles * plan.GT;
     L.prm = prm;
     L.stream = ctx->stream;
+    size_t e0 = ctx->profiling ? prof_event(ctx) : 0;
     if (plan.engine == ENGINE_REG)
         LAUNCH(launch_reg_pass(L));
     else
         LAUNCH(launch_gen_pass(L));
+    if (ctx->profiling) {
+        size_t e1 = prof_event(ctx);
+        ctx->recs.push_back({(int)kind, e0, e1});
+        if (ctx->ev_used > 4096) prof_collect(ctx);
+    }
+}
+
+// algorithmic bytes of the passes one gene took part in: its CSR entries
+// (uint16 value + int32 cell index, or float + int32), its beta / gene
+// parameters, its partial sums; plus the design and offsets once per launch
+void prof_add_bytes(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const int32_t* passes,
+                    int64_t launches) {
+    if (!ctx->profiling) return;
+    int64_t* acc = ws<int64_t>(ctx, "prof_acc", 2);
+    CK(cudaMemsetAsync(acc, 0, 2 * sizeof(int64_t), ctx->stream));
+    LAUNCH(launch_pass_volume(dp.rowptr, passes, dp.G, acc, ctx->stream));
+    int64_t h[2] = {0, 0};
+    CK(cudaMemcpyAsync(h, acc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double ebytes = dp.val_u16 ? 6.0 : 8.0;
+    const int na = pass_na(kind, dp.P), ns = pass_ns(kind);
+    const double per_gene = 4.0 * dp.P + 8.0 + 4.0 * na + 8.0 * ns + 16.0;
+    ctx->prof_bytes[kind] += ebytes * (double)h[0] + per_gene * (double)h[1] +
+                             (double)launches * (double)dp.n * 4.0 * (dp.xs + 1);
 }
 
 // all-genes list (for one-shot passes)
@@ -488,7 +557,8 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
     PassBuffers pb = pass_buffers(ctx, PASS_IRLS, dp.P, max_slot_segs(ctx, dp, plan.GT, form));
     *ctx->mapped_host = (int32_t)G;
     const int LAG = 2;
-    PassParamsAny prm{beta_f, k, nullptr, nullptr};
+    PassParamsAny prm{beta_f, beta, k, nullptr, nullptr};
+    int64_t launched = 0;
     for (int t = 0; t < max_iter; ++t) {
         const int cur = t & 1, nxt = cur ^ 1;
         int64_t hint;
@@ -504,17 +574,23 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
         const int fpi = dp.nfine / nseg;
         launch_pass(ctx, dp, PASS_IRLS, plan, nseg, fpi, tiles, dp.fine_bound, dp.fine_ptr,
                     dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
-        LAUNCH(launch_irls_finalize(pb.partW, nseg, tiles * plan.GT, dp.P, act[cur], cnt + cur,
+        ++launched;
+        LAUNCH(launch_irls_finalize(pb.partWf(), nseg, tiles * plan.GT, dp.P, act[cur], cnt + cur,
                                     (int)hint, act[nxt], cnt + nxt, beta, beta_f, iters, status,
                                     max_iter, eps, nullptr, st));
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
     }
+    if (ctx->profiling) {
+        prof_collect(ctx);
+        prof_add_bytes(ctx, dp, PASS_IRLS, iters, launched);
+    }
 }
 
 // MOM theta for all genes (src/mom_overdispersion.cpp)
-void run_mom(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, double* theta, int form) {
+void run_mom(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const double* beta_d,
+             double* theta, int form) {
     if (dp.G == 0) return;
     const PassPlan plan = plan_for(PASS_MOM, dp.P, form);
     int32_t* cnt = nullptr;
@@ -522,11 +598,17 @@ void run_mom(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, double* 
     const int tiles = (int)((dp.G + plan.GT - 1) / plan.GT);
     const int nseg = choose_nseg(ctx, dp, tiles, form);
     PassBuffers pb = pass_buffers(ctx, PASS_MOM, dp.P, (size_t)nseg * tiles * plan.GT);
-    PassParamsAny prm{beta_f, nullptr, nullptr, nullptr};
+    PassParamsAny prm{beta_f, beta_d, nullptr, nullptr, nullptr};
     launch_pass(ctx, dp, PASS_MOM, plan, nseg, dp.nfine / nseg, tiles, dp.fine_bound, dp.fine_ptr,
                 dp.nfine + 1, act, cnt, nullptr, pb, prm);
     LAUNCH(launch_mom_finalize(pb.partS, nseg, tiles * plan.GT, act, cnt, (int)dp.G, dp.n, dp.P,
                                theta, ctx->stream));
+    if (ctx->profiling) {
+        prof_collect(ctx);
+        int32_t* ones = ws<int32_t>(ctx, "prof_ones", dp.G);
+        LAUNCH(launch_fill_i32(ones, 1, dp.G, ctx->stream));
+        prof_add_bytes(ctx, dp, PASS_MOM, ones, 1);
+    }
 }
 
 // MLE theta (R/overdispersion.R:25-115)
@@ -552,7 +634,8 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, double* 
     PassBuffers pb = pass_buffers(ctx, PASS_MLE, dp.P, max_slot_segs(ctx, dp, plan.GT, form));
     *ctx->mapped_host = (int32_t)G;
     const int LAG = 2;
-    PassParamsAny prm{beta_f, nullptr, s.x, nullptr};
+    PassParamsAny prm{beta_f, nullptr, nullptr, s.x, nullptr};
+    int64_t launched = 0;
     // one far-left evaluation plus at most max_iter Newton evaluations
     for (int t = 0; t <= max_iter; ++t) {
         const int cur = t & 1, nxt = cur ^ 1;
@@ -564,17 +647,26 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, double* 
         const int nseg = choose_nseg(ctx, dp, tiles, form);
         launch_pass(ctx, dp, PASS_MLE, plan, nseg, dp.nfine / nseg, tiles, dp.fine_bound,
                     dp.fine_ptr, dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
-        LAUNCH(launch_mle_finalize(pb.partW, pb.partS, nseg, tiles * plan.GT, dp.P, dp.stats, dp.n,
+        ++launched;
+        LAUNCH(launch_mle_finalize(pb.partWf(), pb.partS, nseg, tiles * plan.GT, dp.P, dp.stats, dp.n,
                                    act[cur], cnt + cur, (int)hint, act[nxt], cnt + nxt, s, max_iter,
                                    cox_reid, nullptr, st));
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
     }
+    if (ctx->profiling) {
+        prof_collect(ctx);
+        // genes take part in phase-0 plus one pass per Newton step
+        int32_t* np1 = ws<int32_t>(ctx, "prof_mle_passes", G);
+        LAUNCH(launch_mle_passes(s.it, s.phase, dp.stats, G, np1, st));
+        prof_add_bytes(ctx, dp, PASS_MLE, np1, launched);
+    }
 }
 
 // bread + clustered meat + sandwich for all genes
-void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const double* theta,
+void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const double* beta_d,
+                  const double* theta,
                   const int32_t* ends_host, int n_clusters, double* bread, double* sandwich,
                   double* meat, int form) {
     cudaStream_t st = ctx->stream;
@@ -584,14 +676,20 @@ void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, con
     int32_t* cnt = nullptr;
     const int32_t* act = all_genes(ctx, dp, &cnt);
     const int tiles = (int)((dp.G + plan.GT - 1) / plan.GT);
-    PassParamsAny prm{beta_f, nullptr, nullptr, theta};
+    PassParamsAny prm{beta_f, beta_d, nullptr, nullptr, theta};
     if (n_clusters <= 0) {
         const int nseg = choose_nseg(ctx, dp, tiles, form);
         PassBuffers pb = pass_buffers(ctx, PASS_SANDWICH, dp.P, (size_t)nseg * tiles * plan.GT);
         launch_pass(ctx, dp, PASS_SANDWICH, plan, nseg, dp.nfine / nseg, tiles, dp.fine_bound,
                     dp.fine_ptr, dp.nfine + 1, act, cnt, nullptr, pb, prm);
-        LAUNCH(launch_sandwich_finalize(pb.partW, nseg, tiles * plan.GT, dp.P, nullptr, 0, dp.n,
+        LAUNCH(launch_sandwich_finalize(pb.partWd(), nseg, tiles * plan.GT, dp.P, nullptr, 0, dp.n,
                                         act, cnt, (int)dp.G, bread, nullptr, nullptr, st));
+        if (ctx->profiling) {
+            prof_collect(ctx);
+            int32_t* ones = ws<int32_t>(ctx, "prof_ones", dp.G);
+            LAUNCH(launch_fill_i32(ones, 1, dp.G, st));
+            prof_add_bytes(ctx, dp, PASS_SANDWICH, ones, 1);
+        }
         return;
     }
     // cluster-aligned segments: every cluster block split into pieces of
@@ -624,9 +722,15 @@ void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, con
     PassBuffers pb = pass_buffers(ctx, PASS_SANDWICH, dp.P, (size_t)nseg * tiles * plan.GT);
     launch_pass(ctx, dp, PASS_SANDWICH, plan, nseg, 1, tiles, bound, segptr, (int)hb.size(), act,
                 cnt, nullptr, pb, prm);
-    LAUNCH(launch_sandwich_finalize(pb.partW, nseg, tiles * plan.GT, dp.P, segc, n_clusters, dp.n,
+    LAUNCH(launch_sandwich_finalize(pb.partWd(), nseg, tiles * plan.GT, dp.P, segc, n_clusters, dp.n,
                                     act, cnt, (int)dp.G, bread, sandwich, meat, st));
     CK(cudaStreamSynchronize(st));  // host vectors hb/hc go out of scope
+    if (ctx->profiling) {
+        prof_collect(ctx);
+        int32_t* ones = ws<int32_t>(ctx, "prof_ones", dp.G);
+        LAUNCH(launch_fill_i32(ones, 1, dp.G, st));
+        prof_add_bytes(ctx, dp, PASS_SANDWICH, ones, 1);
+    }
 }
 
 struct FitBuffers {
@@ -666,7 +770,7 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     run_irls(ctx, dp, fb.beta, fb.beta_f, fb.k, fb.iters, fb.status, o->max_iter, eps, o->form);
     if (fb.theta_mom || o->overdispersion == DEVIL_OD_MOM) {
         double* tm = fb.theta_mom ? fb.theta_mom : fb.theta;
-        run_mom(ctx, dp, fb.beta_f, tm, o->form);
+        run_mom(ctx, dp, fb.beta_f, fb.beta, tm, o->form);
         if (o->overdispersion == DEVIL_OD_MOM && tm != fb.theta)
             CK(cudaMemcpyAsync(fb.theta, tm, G * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
@@ -675,7 +779,7 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     } else if (o->overdispersion == DEVIL_OD_NONE) {
         CK(cudaMemsetAsync(fb.theta, 0, G * sizeof(double), st));
     }
-    run_sandwich(ctx, dp, fb.beta_f, fb.theta, ends_host, n_clusters, fb.bread,
+    run_sandwich(ctx, dp, fb.beta_f, fb.beta, fb.theta, ends_host, n_clusters, fb.bread,
                  n_clusters > 0 ? fb.sandwich : nullptr, nullptr, o->form);
 }
 
@@ -766,6 +870,7 @@ int devil_ctx_destroy(devil_ctx* ctx) {
         if (kv.second.p) cudaFree(kv.second.p);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->mapped_host) cudaFreeHost(ctx->mapped_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -778,6 +883,29 @@ int devil_ctx_synchronize(devil_ctx* ctx) {
     return guarded(ctx, [&] { CK(cudaStreamSynchronize(ctx->stream)); });
 }
 int64_t devil_ctx_launch_count(const devil_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int devil_ctx_set_profiling(devil_ctx* ctx, int enable) {
+    return guarded(ctx, [&] {
+        prof_collect(ctx);
+        ctx->profiling = enable ? 1 : 0;
+        for (int k = 0; k < 4; ++k) {
+            ctx->prof_launches[k] = 0;
+            ctx->prof_ms[k] = 0.0;
+            ctx->prof_bytes[k] = 0.0;
+        }
+    });
+}
+
+int devil_ctx_profile(devil_ctx* ctx, int pass_kind, int64_t* launches, double* ms,
+                      double* alg_bytes) {
+    return guarded(ctx, [&] {
+        if (pass_kind < 0 || pass_kind > 3) fail(ctx, DEVIL_ERR_ARG, "pass kind 0..3");
+        prof_collect(ctx);
+        if (launches) *launches = ctx->prof_launches[pass_kind];
+        if (ms) *ms = ctx->prof_ms[pass_kind];
+        if (alg_bytes) *alg_bytes = ctx->prof_bytes[pass_kind];
+    });
+}
 
 int devil_fit(devil_ctx* ctx, const devil_counts* counts, const double* X, int p,
               const int32_t* cluster_ends, int n_clusters, const devil_fit_opts* opts,
@@ -900,6 +1028,16 @@ int devil_p_adjust(devil_ctx* ctx, int64_t m, const double* p, int method, doubl
     });
 }
 
+int devil_p_adjust_device(devil_ctx* ctx, int64_t m, const double* p_dev, int method,
+                          double* out_dev) {
+    return guarded(ctx, [&] {
+        if (method < 0 || method > 5) fail(ctx, DEVIL_ERR_UNSUPPORTED, "adjust method");
+        size_t tb = p_adjust_temp_bytes(m);
+        void* tmp = ws<char>(ctx, "padj_tmp", tb);
+        LAUNCH(launch_p_adjust(m, p_dev, method, out_dev, tmp, tb, ctx->stream));
+    });
+}
+
 // ------------------------------------------------------------------
 // single steps
 // ------------------------------------------------------------------
@@ -1000,12 +1138,14 @@ int devil_beta_fit(devil_ctx* ctx, const devil_counts* counts, const double* X, 
     });
 }
 
-static void upload_beta(devil_ctx* ctx, const DevProblem& dp, const double* beta, float** bf_out) {
+static void upload_beta(devil_ctx* ctx, const DevProblem& dp, const double* beta, float** bf_out,
+                        double** bd_out) {
     double* b = ws<double>(ctx, "beta", (size_t)dp.G * dp.P);
     float* bf = ws<float>(ctx, "beta_f", (size_t)dp.G * dp.P);
     h2d(ctx, b, beta, (size_t)dp.G * dp.P);
     LAUNCH(launch_double_to_float(b, bf, (size_t)dp.G * dp.P, ctx->stream));
     *bf_out = bf;
+    *bd_out = b;
 }
 
 int devil_estimate_mom_dispersion(devil_ctx* ctx, const devil_counts* counts, const double* X,
@@ -1018,9 +1158,10 @@ int devil_estimate_mom_dispersion(devil_ctx* ctx, const devil_counts* counts, co
         prepare_design(ctx, dp, X, p, false);
         upload_sf_as_offsets(ctx, dp, size_factors);
         float* bf;
-        upload_beta(ctx, dp, beta, &bf);
+        double* bd;
+        upload_beta(ctx, dp, beta, &bf, &bd);
         double* th = ws<double>(ctx, "theta", dp.G);
-        run_mom(ctx, dp, bf, th, DEVIL_FORM_CHOSEN);
+        run_mom(ctx, dp, bf, bd, th, DEVIL_FORM_CHOSEN);
         d2h(ctx, theta, th, dp.G);
         CK(cudaStreamSynchronize(ctx->stream));
     });
@@ -1036,7 +1177,8 @@ int devil_fit_dispersion(devil_ctx* ctx, const devil_counts* counts, const doubl
         prepare_design(ctx, dp, X, p, false);
         upload_offsets(ctx, dp, offset_vector);
         float* bf;
-        upload_beta(ctx, dp, beta, &bf);
+        double* bd;
+        upload_beta(ctx, dp, beta, &bf, &bd);
         double* th = ws<double>(ctx, "theta", dp.G);
         int32_t* it = ws<int32_t>(ctx, "mle_iters_out", dp.G);
         run_mle(ctx, dp, bf, th, it, max_iter, cox_reid, DEVIL_FORM_CHOSEN);
@@ -1056,11 +1198,12 @@ int devil_compute_hessian(devil_ctx* ctx, const devil_counts* counts, const doub
         prepare_design(ctx, dp, X, p, false);
         upload_sf_as_offsets(ctx, dp, size_factors);
         float* bf;
-        upload_beta(ctx, dp, beta, &bf);
+        double* bd;
+        upload_beta(ctx, dp, beta, &bf, &bd);
         double* th = ws<double>(ctx, "theta", dp.G);
         h2d(ctx, th, overdispersion, dp.G);
         double* br = ws<double>(ctx, "bread", (size_t)dp.G * p * p);
-        run_sandwich(ctx, dp, bf, th, nullptr, 0, br, nullptr, nullptr, DEVIL_FORM_CHOSEN);
+        run_sandwich(ctx, dp, bf, bd, th, nullptr, 0, br, nullptr, nullptr, DEVIL_FORM_CHOSEN);
         d2h(ctx, bread, br, (size_t)dp.G * p * p);
         CK(cudaStreamSynchronize(ctx->stream));
     });
@@ -1078,12 +1221,13 @@ int devil_compute_clustered_meat(devil_ctx* ctx, const devil_counts* counts, con
         prepare_design(ctx, dp, X, p, false);
         upload_sf_as_offsets(ctx, dp, size_factors);
         float* bf;
-        upload_beta(ctx, dp, beta, &bf);
+        double* bd;
+        upload_beta(ctx, dp, beta, &bf, &bd);
         double* th = ws<double>(ctx, "theta", dp.G);
         h2d(ctx, th, overdispersion, dp.G);
         double* br = ws<double>(ctx, "bread", (size_t)dp.G * p * p);
         double* mt = ws<double>(ctx, "meat", (size_t)dp.G * p * p);
-        run_sandwich(ctx, dp, bf, th, cluster_ends, n_clusters, br, nullptr, mt, DEVIL_FORM_CHOSEN);
+        run_sandwich(ctx, dp, bf, bd, th, cluster_ends, n_clusters, br, nullptr, mt, DEVIL_FORM_CHOSEN);
         d2h(ctx, meat, mt, (size_t)dp.G * p * p);
         CK(cudaStreamSynchronize(ctx->stream));
     });

@@ -19,7 +19,8 @@ inline int pass_ns(PassKind k) { return k == PASS_MOM ? 2 : (k == PASS_MLE ? 6 :
 inline int pass_na(PassKind k, int P) { return pass_nw(k) * P * (P + 1) / 2 + pass_nv(k) * P; }
 
 struct PassParamsAny {
-    const float* beta;        // G x P float (all passes)
+    const float* beta;        // G x P float (FP32 passes)
+    const double* beta_d;     // G x P double (FP64 passes)
     const float* k;           // IRLS
     const double* log_theta;  // MLE
     const double* theta;      // SANDWICH
@@ -61,6 +62,8 @@ cudaError_t launch_keys_to_csr(const int64_t* keys, int64_t nnz, int64_t n, int6
                                int32_t* col, int64_t* rowcnt, cudaStream_t st);
 cudaError_t launch_x_rowmajor(const double* Xcm, int64_t n, int P, int xs, float* Xrm,
                               cudaStream_t st);
+cudaError_t launch_x_rowmajor_d(const double* Xcm, int64_t n, int P, int xs, double* Xrm,
+                                cudaStream_t st);
 cudaError_t launch_double_to_float(const double* in, float* out, int64_t m, cudaStream_t st);
 cudaError_t launch_gene_stats(const int64_t* rowptr, const void* val, int val_u16, int64_t G,
                               int64_t n, double* stats /* G x 6 */, cudaStream_t st);
@@ -88,6 +91,11 @@ cudaError_t launch_segptr(const int64_t* rowptr, const int32_t* col, int64_t G,
 cudaError_t launch_validate_csr(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
                                 int64_t nnz, int32_t* bad, cudaStream_t st);
 cudaError_t launch_iota(int32_t* a, int64_t m, cudaStream_t st);
+cudaError_t launch_pass_volume(const int64_t* rowptr, const int32_t* passes, int64_t G,
+                               int64_t* acc, cudaStream_t st);
+cudaError_t launch_fill_i32(int32_t* a, int32_t v, int64_t m, cudaStream_t st);
+cudaError_t launch_mle_passes(const int32_t* it, const int32_t* phase, const double* stats,
+                              int64_t G, int32_t* out, cudaStream_t st);
 cudaError_t launch_set_i32(int32_t* a, int32_t v, cudaStream_t st);
 cudaError_t launch_copy_i32_to_host_mapped(const int32_t* src, volatile int32_t* dst,
                                            cudaStream_t st);
@@ -116,7 +124,7 @@ cudaError_t launch_mle_finalize(const float* partW, const double* partS, int nse
                                 const int32_t* act, const int32_t* n_act, int max_slots,
                                 int32_t* act_next, int32_t* n_next, MleState s, int max_iter,
                                 int cox_reid, volatile int32_t* mirror, cudaStream_t st);
-cudaError_t launch_sandwich_finalize(const float* partW, int nseg, int slot_stride, int P,
+cudaError_t launch_sandwich_finalize(const double* partW, int nseg, int slot_stride, int P,
                                      const int32_t* seg_cluster, int n_clusters, int64_t n,
                                      const int32_t* act, const int32_t* n_act, int max_slots,
                                      double* bread, double* sandwich, double* meat,

@@ -262,7 +262,11 @@ __global__ void mle_finalize_kernel(const float* partW, const double* partS, int
     } else {
         double lo = st.lo[g], hi = st.hi[g];
         int it = st.it[g];
-        if (score == 0.0) {
+        // The per-cell terms are FP32 (summed in FP64): the score is resolved
+        // to about 1e-6 of the size of its two opposing parts.  A score inside
+        // that band is zero to working precision.
+        const double resolution = 1e-6 * (fabs(a * (ss[0] + ss[2])) + fabs(dig));
+        if (score == 0.0 || fabs(score) <= resolution) {
             done = true;
         } else {
             if (score > 0.0) lo = x; else hi = x;
@@ -314,7 +318,7 @@ cudaError_t launch_mle_finalize(const float* partW, const double* partS, int nse
 // cluster-aligned segments, meat = adj/n sum_b s_b s_b', adj = C/(C-1)
 // (1 when C = 1); sandwich = bread meat bread n (R/main.R:482-492).
 // ------------------------------------------------------------------
-__global__ void sandwich_finalize_kernel(const float* partW, int nseg, int slot_stride, int P,
+__global__ void sandwich_finalize_kernel(const double* partW, int nseg, int slot_stride, int P,
                                          const int32_t* seg_cluster, int n_clusters, int64_t n,
                                          const int32_t* act, const int32_t* n_act, double* bread,
                                          double* sandwich, double* meat_out) {
@@ -339,7 +343,7 @@ __global__ void sandwich_finalize_kernel(const float* partW, int nseg, int slot_
         // lane i holds component i of the running cluster sum
         double acc = 0.0;
         for (int seg = 0; seg < nseg; ++seg) {
-            if (lane < P) acc += (double)partW[((int64_t)seg * slot_stride + slot) * NA + NE + lane];
+            if (lane < P) acc += partW[((int64_t)seg * slot_stride + slot) * NA + NE + lane];
             bool last = (seg == nseg - 1) || (seg_cluster[seg + 1] != seg_cluster[seg]);
             if (last) {
                 if (lane < P) cur[lane] = acc;
@@ -383,7 +387,7 @@ __global__ void sandwich_finalize_kernel(const float* partW, int nseg, int slot_
         }
     }
 }
-cudaError_t launch_sandwich_finalize(const float* partW, int nseg, int slot_stride, int P,
+cudaError_t launch_sandwich_finalize(const double* partW, int nseg, int slot_stride, int P,
                                      const int32_t* seg_cluster, int n_clusters, int64_t n,
                                      const int32_t* act, const int32_t* n_act, int max_slots,
                                      double* bread, double* sandwich, double* meat,

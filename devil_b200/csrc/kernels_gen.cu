@@ -26,10 +26,10 @@ size_t gen_smem_bytes(PassKind k, int P, int GT) {
 
 template <class Pass>
 static typename Pass::Params params_of(const PassParamsAny& a);
-template <> PassIRLS::Params params_of<PassIRLS>(const PassParamsAny& a) { return {a.beta, a.k}; }
-template <> PassMOM::Params params_of<PassMOM>(const PassParamsAny& a) { return {a.beta}; }
-template <> PassMLE::Params params_of<PassMLE>(const PassParamsAny& a) { return {a.beta, a.log_theta}; }
-template <> PassSandwich::Params params_of<PassSandwich>(const PassParamsAny& a) { return {a.beta, a.theta}; }
+template <> PassIRLS::Params params_of<PassIRLS>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.k}; }
+template <> PassMOM::Params params_of<PassMOM>(const PassParamsAny& a) { return {a.beta, a.beta_d}; }
+template <> PassMLE::Params params_of<PassMLE>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.log_theta}; }
+template <> PassSandwich::Params params_of<PassSandwich>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.theta}; }
 
 template <class Pass>
 static cudaError_t run(const PassLaunch& L) {

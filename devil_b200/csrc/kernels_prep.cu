@@ -149,6 +149,22 @@ cudaError_t launch_x_rowmajor(const double* Xcm, int64_t n, int P, int xs, float
     return cudaGetLastError();
 }
 
+__global__ void x_rowmajor_d_kernel(const double* Xcm, int64_t n, int P, int xs, double* Xrm) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n * xs;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t c = i / xs;
+        int j = (int)(i - c * xs);
+        Xrm[i] = j < P ? Xcm[(int64_t)j * n + c] : 0.0;
+    }
+}
+cudaError_t launch_x_rowmajor_d(const double* Xcm, int64_t n, int P, int xs, double* Xrm,
+                                cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    x_rowmajor_d_kernel<<<(unsigned)std::min<int64_t>(nblk(n * xs, 256), 148 * 16), 256, 0, st>>>(
+        Xcm, n, P, xs, Xrm);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------
 // per-gene statistics, two passes over each row (warp per gene):
 // stats[g*6 + 0..5] = mean, sample variance (n-1), sum y,
@@ -500,6 +516,55 @@ cudaError_t launch_validate_csr(const int64_t* rowptr, const int32_t* col, int64
                                 int64_t nnz, int32_t* bad, cudaStream_t st) {
     if (G == 0) return cudaSuccess;
     validate_csr_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, col, G, n, nnz, bad);
+    return cudaGetLastError();
+}
+
+// acc[0] += sum_g passes[g] * nnz_g, acc[1] += sum_g passes[g]
+__global__ void pass_volume_kernel(const int64_t* rowptr, const int32_t* passes, int64_t G,
+                                   long long* acc) {
+    long long v = 0, w = 0;
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < G;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        long long k = passes[g];
+        v += k * (long long)(rowptr[g + 1] - rowptr[g]);
+        w += k;
+    }
+    v = warp_sum(v);
+    w = warp_sum(w);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(reinterpret_cast<unsigned long long*>(acc), (unsigned long long)v);
+        atomicAdd(reinterpret_cast<unsigned long long*>(acc + 1), (unsigned long long)w);
+    }
+}
+cudaError_t launch_pass_volume(const int64_t* rowptr, const int32_t* passes, int64_t G,
+                               int64_t* acc, cudaStream_t st) {
+    if (G == 0) return cudaSuccess;
+    pass_volume_kernel<<<(unsigned)std::min<int64_t>(nblk(G, 256), 256), 256, 0, st>>>(
+        rowptr, passes, G, reinterpret_cast<long long*>(acc));
+    return cudaGetLastError();
+}
+__global__ void fill_i32_kernel(int32_t* a, int32_t v, int64_t m) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+         i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = v;
+}
+cudaError_t launch_fill_i32(int32_t* a, int32_t v, int64_t m, cudaStream_t st) {
+    if (m == 0) return cudaSuccess;
+    fill_i32_kernel<<<(unsigned)std::min<int64_t>(nblk(m, 256), 1024), 256, 0, st>>>(a, v, m);
+    return cudaGetLastError();
+}
+// MLE passes per gene: 0 for all-zero genes, else the far-left evaluation
+// plus the Newton evaluations
+__global__ void mle_passes_kernel(const int32_t* it, const int32_t* phase, const double* stats,
+                                  int64_t G, int32_t* out) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < G;
+         g += (int64_t)gridDim.x * blockDim.x)
+        out[g] = stats[g * 6 + 2] == 0.0 ? 0 : 1 + it[g];
+}
+cudaError_t launch_mle_passes(const int32_t* it, const int32_t* phase, const double* stats,
+                              int64_t G, int32_t* out, cudaStream_t st) {
+    if (G == 0) return cudaSuccess;
+    mle_passes_kernel<<<(unsigned)std::min<int64_t>(nblk(G, 256), 1024), 256, 0, st>>>(it, phase, stats, G, out);
     return cudaGetLastError();
 }
 

@@ -9,8 +9,8 @@ int reg_max_p() { return 8; }
 
 int reg_default_gt(PassKind k, int P) {
     switch (k) {
-        case PASS_IRLS:
-        case PASS_SANDWICH: return P <= 4 ? 8 : (P <= 6 ? 4 : 2);
+        case PASS_IRLS: return P <= 4 ? 8 : (P <= 6 ? 4 : 2);
+        case PASS_SANDWICH: return P <= 2 ? 8 : (P <= 4 ? 4 : (P <= 6 ? 2 : 1));
         case PASS_MOM: return 8;
         case PASS_MLE: return P <= 2 ? 4 : (P <= 4 ? 2 : 1);
     }
@@ -34,10 +34,10 @@ template <> struct PassOf<PASS_SANDWICH> { using T = PassSandwich; };
 
 template <PassKind K>
 static typename PassOf<K>::T::Params make_params(const PassParamsAny& a);
-template <> PassIRLS::Params make_params<PASS_IRLS>(const PassParamsAny& a) { return {a.beta, a.k}; }
-template <> PassMOM::Params make_params<PASS_MOM>(const PassParamsAny& a) { return {a.beta}; }
-template <> PassMLE::Params make_params<PASS_MLE>(const PassParamsAny& a) { return {a.beta, a.log_theta}; }
-template <> PassSandwich::Params make_params<PASS_SANDWICH>(const PassParamsAny& a) { return {a.beta, a.theta}; }
+template <> PassIRLS::Params make_params<PASS_IRLS>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.k}; }
+template <> PassMOM::Params make_params<PASS_MOM>(const PassParamsAny& a) { return {a.beta, a.beta_d}; }
+template <> PassMLE::Params make_params<PASS_MLE>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.log_theta}; }
+template <> PassSandwich::Params make_params<PASS_SANDWICH>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.theta}; }
 
 template <PassKind K, int P, int GT>
 static cudaError_t run(const PassLaunch& L) {
@@ -66,7 +66,7 @@ static cudaError_t run_gt(const PassLaunch& L) {
     } else {
         constexpr int G = (K == PASS_MOM) ? 8
                         : (K == PASS_MLE) ? (P <= 2 ? 4 : (P <= 4 ? 2 : 1))
-                        : (P <= 4 ? 8 : (P <= 6 ? 4 : 2));
+                        : (P <= 2 ? 8 : (P <= 4 ? 4 : (P <= 6 ? 2 : 1)));
         if (L.GT != G) return cudaErrorInvalidValue;
         return run<K, P, G>(L);
     }

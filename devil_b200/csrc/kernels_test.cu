@@ -35,11 +35,29 @@ DEV double betacf_d(double a, double b, double x) {
     return h;
 }
 
+// lgamma(a + b) - lgamma(a) for a >= 100 from the Stirling series of
+// ln G(z) = (z - 1/2) ln z - z + ln(2 pi)/2 + 1/(12 z) - 1/(360 z^3) + ...,
+// the leading terms differenced analytically (df up to 1e6 keeps full
+// relative precision).
+DEV double lgamma_diff_large(double a, double b) {
+    double z = a + b;
+    double d = (a - 0.5) * log1p(b / a) + b * log(z) - b;
+    d += (1.0 / 12.0) * (1.0 / z - 1.0 / a);
+    d -= (1.0 / 360.0) * (1.0 / (z * z * z) - 1.0 / (a * a * a));
+    d += (1.0 / 1260.0) * (1.0 / (z * z * z * z * z) - 1.0 / (a * a * a * a * a));
+    return d;
+}
+DEV double log_beta_d(double a, double b) {
+    if (a >= 100.0 && b < a) return lgamma(b) - lgamma_diff_large(a, b);
+    if (b >= 100.0 && a < b) return lgamma(a) - lgamma_diff_large(b, a);
+    return lgamma(a) + lgamma(b) - lgamma(a + b);
+}
+
 // I_x(a, b) with both x and 1 - x supplied (no cancellation in either)
 DEV double ibeta_d(double a, double b, double x, double omx) {
     if (x <= 0.0) return 0.0;
     if (omx <= 0.0) return 1.0;
-    double lbeta = lgamma(a) + lgamma(b) - lgamma(a + b);
+    double lbeta = log_beta_d(a, b);
     double lfront = (x > 0.5) ? a * log1p(-omx) + b * log(omx) : a * log(x) + b * log1p(-x);
     lfront -= lbeta;
     if (x < (a + 1.0) / (a + b + 2.0)) return exp(lfront) * betacf_d(a, b, x) / a;

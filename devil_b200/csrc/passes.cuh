@@ -29,6 +29,8 @@ struct PassGeom {
     const float* X;        // [n][xs] row-major float
     int xs;                // row stride of X (>= p)
     const float* off;      // [n]
+    const double* Xd;      // [n][xs] row-major double (FP64 passes)
+    const double* offd;    // [n] (FP64 passes)
     const int32_t* col;    // CSR cell index
     const void* val;       // CSR values (uint16 or float)
     const int64_t* segptr; // [G][nbound] first CSR entry with col >= bound[b]
@@ -39,7 +41,7 @@ struct PassGeom {
     const int32_t* act;    // active gene list
     const int32_t* n_act;  // its length (device)
     int32_t* reset_next;   // counter zeroed by block (0,0) (may be null)
-    float* partW;          // [seg][slot_stride][NA]
+    void* partW;           // [seg][slot_stride][NA] of Pass::AW
     double* partS;         // [seg][slot_stride][NS]
     int slot_stride;
 };
@@ -47,23 +49,23 @@ struct PassGeom {
 // ---------------------------------------------------------------------
 // accumulators
 // ---------------------------------------------------------------------
-template <int P, int NA, int NS, class AW, class AS>
+template <int P, int NA, int NS, class AW, class AS, class R>
 struct RegAcc {
     AW* a;
     AS* s;
-    const float* x;
+    const R* x;
     template <int W>
-    DEV void outer(float w) {
+    DEV void outer(R w) {
         constexpr int base = W * (P * (P + 1) / 2);
 #pragma unroll
         for (int j = 0; j < P; ++j) {
-            float wx = w * x[j];
+            R wx = w * x[j];
 #pragma unroll
             for (int i = 0; i <= j; ++i) a[base + tri_index(i, j)] += (AW)(wx * x[i]);
         }
     }
     template <int V, int NW>
-    DEV void vec(float w) {
+    DEV void vec(R w) {
         constexpr int base = NW * (P * (P + 1) / 2) + V * P;
 #pragma unroll
         for (int i = 0; i < P; ++i) a[base + i] += (AW)(w * x[i]);
@@ -73,20 +75,20 @@ struct RegAcc {
 };
 
 // recorder used by the shared-memory engine: captures the weights only
-template <int NWV, int NS, class AS>
+template <int NWV, int NS, class AS, class R>
 struct RecAcc {
-    float w[NWV > 0 ? NWV : 1];
+    R w[NWV > 0 ? NWV : 1];
     AS s[NS > 0 ? NS : 1];
     DEV void zero() {
 #pragma unroll
-        for (int i = 0; i < NWV; ++i) w[i] = 0.f;
+        for (int i = 0; i < NWV; ++i) w[i] = 0;
 #pragma unroll
         for (int i = 0; i < NS; ++i) s[i] = 0;
     }
     template <int W>
-    DEV void outer(float v) { w[W] += v; }
+    DEV void outer(R v) { w[W] += v; }
     template <int V, int NW>
-    DEV void vec(float v) { w[NW + V] += v; }
+    DEV void vec(R v) { w[NW + V] += v; }
     template <int K>
     DEV void scal(AS v) { s[K] += v; }
 };
@@ -104,21 +106,22 @@ struct RecAcc {
 // correction for y > 0: k y/(mu+k) for both.
 struct PassIRLS {
     static constexpr int NW = 1, NV = 1, NS = 0;
+    static constexpr bool F64 = false;
     using AW = float;
     using AS = float;
-    struct Params { const float* beta; const float* k; };
+    struct Params { const float* beta; const double* beta_d; const float* k; };
     struct Gene { float k, kk, nk; };
     static DEV Gene load(const Params& p, int g) {
         float k = p.k[g];
         return Gene{k, k * k, -k};
     }
-    template <class A>
+    template <class R, class A>
     static DEV void dense(const Gene& G, float mu, A& acc) {
         float r = rcp_approx(mu + G.k);
         acc.template outer<0>(G.kk * r);
         acc.template vec<0, NW>(G.nk * mu * r);
     }
-    template <class A>
+    template <class R, class A>
     static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
         float r = rcp_approx(mu + G.k);
         float v = G.k * y * r;
@@ -128,22 +131,24 @@ struct PassIRLS {
 };
 
 // estimate_mom_dispersion_cpp (src/mom_overdispersion.cpp:34-45):
-//   num = sum (y - mu)^2 - mu,  den = sum mu^2   (FP64 accumulation)
+//   num = sum (y - mu)^2 - mu,  den = sum mu^2
+// One pass, evaluated in FP64 per cell (num cancels for near-Poisson genes).
 struct PassMOM {
     static constexpr int NW = 0, NV = 0, NS = 2;
+    static constexpr bool F64 = true;
     using AW = float;
     using AS = double;
-    struct Params { const float* beta; };
+    struct Params { const float* beta; const double* beta_d; };
     struct Gene { int dummy; };
     static DEV Gene load(const Params&, int) { return Gene{0}; }
-    template <class A>
-    static DEV void dense(const Gene&, float mu, A& acc) {
+    template <class R, class A>
+    static DEV void dense(const Gene&, R mu, A& acc) {
         double m = mu;
         acc.template scal<0>(m * m - m);
         acc.template scal<1>(m * m);
     }
-    template <class A>
-    static DEV void sparse(const Gene&, float mu, float y, A& acc) {
+    template <class R, class A>
+    static DEV void sparse(const Gene&, R mu, float y, A& acc) {
         double m = mu, yy = y;
         acc.template scal<0>(yy * yy - 2.0 * yy * m);
     }
@@ -231,15 +236,16 @@ DEV void psi_diffs(double y, double a, double& d1, double& d2) {
 // with x = mu theta, a = 1/theta, w = mu/(1 + x)  (Cox-Reid b, db, d2b).
 struct PassMLE {
     static constexpr int NW = 3, NV = 0, NS = 6;
+    static constexpr bool F64 = false;
     using AW = float;
     using AS = double;
-    struct Params { const float* beta; const double* log_theta; };
+    struct Params { const float* beta; const double* beta_d; const double* log_theta; };
     struct Gene { double theta, a; float thf; };
     static DEV Gene load(const Params& p, int g) {
         double th = exp(p.log_theta[g]);
         return Gene{th, 1.0 / th, (float)th};
     }
-    template <class A>
+    template <class R, class A>
     static DEV void dense(const Gene& G, float mu, A& acc) {
         float x = mu * G.thf;
         float r = 1.f / (1.f + x);
@@ -250,7 +256,7 @@ struct PassMLE {
         acc.template scal<0>((double)nb_ll_term(x));
         acc.template scal<1>((double)(mu * x * r * r));
     }
-    template <class A>
+    template <class R, class A>
     static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
         double m = mu, yy = y;
         double den = 1.0 + m * G.theta;
@@ -268,24 +274,27 @@ struct PassMLE {
 //   outer0 = X' diag((y theta + 1) mu / (1 + theta mu)^2) X
 //   vec0   = X' (y - mu)/(1 + mu theta)       (per segment; segments never
 //                                              cross a cluster boundary)
+// One pass, evaluated in FP64 per cell with FP64 sums: the bread is an
+// inverse, so cond(H) multiplies every relative error of H.
 struct PassSandwich {
     static constexpr int NW = 1, NV = 1, NS = 0;
-    using AW = float;
+    static constexpr bool F64 = true;
+    using AW = double;
     using AS = float;
-    struct Params { const float* beta; const double* theta; };
-    struct Gene { float th; };
-    static DEV Gene load(const Params& p, int g) { return Gene{(float)p.theta[g]}; }
-    template <class A>
-    static DEV void dense(const Gene& G, float mu, A& acc) {
-        float r = 1.f / (1.f + G.th * mu);
+    struct Params { const float* beta; const double* beta_d; const double* theta; };
+    struct Gene { double th; };
+    static DEV Gene load(const Params& p, int g) { return Gene{p.theta[g]}; }
+    template <class R, class A>
+    static DEV void dense(const Gene& G, R mu, A& acc) {
+        R r = (R)1 / ((R)1 + (R)G.th * mu);
         acc.template outer<0>(mu * r * r);
         acc.template vec<0, NW>(-mu * r);
     }
-    template <class A>
-    static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
-        float r = 1.f / (1.f + G.th * mu);
-        acc.template outer<0>(y * G.th * mu * r * r);
-        acc.template vec<0, NW>(y * r);
+    template <class R, class A>
+    static DEV void sparse(const Gene& G, R mu, float y, A& acc) {
+        R r = (R)1 / ((R)1 + (R)G.th * mu);
+        acc.template outer<0>((R)y * (R)G.th * mu * r * r);
+        acc.template vec<0, NW>((R)y * r);
     }
 };
 
@@ -334,8 +343,10 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
     const int seg = blockIdx.x;
     const VT* __restrict__ val = static_cast<const VT*>(geo.val);
 
+    constexpr bool F64 = Pass::F64;
     int gid[GT];
-    float beta[GT][P];
+    float beta[GT][P];                 // FP32 passes: log2(e)-scaled
+    double betad[GT][F64 ? P : 1];     // FP64 passes
     typename Pass::Gene gp[GT];
 #pragma unroll
     for (int j = 0; j < GT; ++j) {
@@ -343,8 +354,13 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
         if (slot >= nact) slot = tile * GT;  // duplicate a valid gene; not written
         int g = __ldg(geo.act + slot);
         gid[j] = g;
+        if constexpr (F64) {
 #pragma unroll
-        for (int i = 0; i < P; ++i) beta[j][i] = __ldg(prm.beta + (int64_t)g * P + i) * kLog2e;
+            for (int i = 0; i < P; ++i) betad[j][i] = __ldg(prm.beta_d + (int64_t)g * P + i);
+        } else {
+#pragma unroll
+            for (int i = 0; i < P; ++i) beta[j][i] = __ldg(prm.beta + (int64_t)g * P + i) * kLog2e;
+        }
         gp[j] = Pass::load(prm, g);
     }
 
@@ -362,17 +378,33 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
     const int c0 = __ldg(geo.bound + b0), c1 = __ldg(geo.bound + b1);
 
     for (int c = c0 + threadIdx.x; c < c1; c += NT) {
-        float x[P];
-        load_row<P, PP>(geo.X, c, x);
-        float o = __ldg(geo.off + c) * kLog2e;
+        if constexpr (F64) {
+            double x[P];
 #pragma unroll
-        for (int j = 0; j < GT; ++j) {
-            float e = o;
+            for (int i = 0; i < P; ++i) x[i] = __ldg(geo.Xd + (int64_t)c * PP + i);
+            const double o = __ldg(geo.offd + c);
 #pragma unroll
-            for (int i = 0; i < P; ++i) e = fmaf(x[i], beta[j][i], e);
-            float mu = ex2_approx(e);
-            RegAcc<P, NAc, NSc, AW, AS> acc{aw[j], as[j], x};
-            Pass::dense(gp[j], mu, acc);
+            for (int j = 0; j < GT; ++j) {
+                double e = o;
+#pragma unroll
+                for (int i = 0; i < P; ++i) e = fma(x[i], betad[j][i], e);
+                double mu = exp(e);
+                RegAcc<P, NAc, NSc, AW, AS, double> acc{aw[j], as[j], x};
+                Pass::template dense<double>(gp[j], mu, acc);
+            }
+        } else {
+            float x[P];
+            load_row<P, PP>(geo.X, c, x);
+            float o = __ldg(geo.off + c) * kLog2e;
+#pragma unroll
+            for (int j = 0; j < GT; ++j) {
+                float e = o;
+#pragma unroll
+                for (int i = 0; i < P; ++i) e = fmaf(x[i], beta[j][i], e);
+                float mu = ex2_approx(e);
+                RegAcc<P, NAc, NSc, AW, AS, float> acc{aw[j], as[j], x};
+                Pass::template dense<float>(gp[j], mu, acc);
+            }
         }
     }
 #pragma unroll
@@ -382,14 +414,26 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
         for (int64_t e = e0 + threadIdx.x; e < e1; e += NT) {
             int c = __ldg(geo.col + e);
             float y = load_val(val, e);
-            float x[P];
-            load_row<P, PP>(geo.X, c, x);
-            float el = __ldg(geo.off + c) * kLog2e;
+            if constexpr (F64) {
+                double x[P];
 #pragma unroll
-            for (int i = 0; i < P; ++i) el = fmaf(x[i], beta[j][i], el);
-            float mu = ex2_approx(el);
-            RegAcc<P, NAc, NSc, AW, AS> acc{aw[j], as[j], x};
-            Pass::sparse(gp[j], mu, y, acc);
+                for (int i = 0; i < P; ++i) x[i] = __ldg(geo.Xd + (int64_t)c * PP + i);
+                double el = __ldg(geo.offd + c);
+#pragma unroll
+                for (int i = 0; i < P; ++i) el = fma(x[i], betad[j][i], el);
+                double mu = exp(el);
+                RegAcc<P, NAc, NSc, AW, AS, double> acc{aw[j], as[j], x};
+                Pass::template sparse<double>(gp[j], mu, y, acc);
+            } else {
+                float x[P];
+                load_row<P, PP>(geo.X, c, x);
+                float el = __ldg(geo.off + c) * kLog2e;
+#pragma unroll
+                for (int i = 0; i < P; ++i) el = fmaf(x[i], beta[j][i], el);
+                float mu = ex2_approx(el);
+                RegAcc<P, NAc, NSc, AW, AS, float> acc{aw[j], as[j], x};
+                Pass::template sparse<float>(gp[j], mu, y, acc);
+            }
         }
     }
 
@@ -421,10 +465,10 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
             int j = t / NA, a = t - j * NA;
             int slot = tile * GT + j;
             if (slot >= nact) continue;
-            float s = 0.f;
+            AW s = 0;
 #pragma unroll
-            for (int w = 0; w < NWARP; ++w) s += (float)redW[w][j * NAc + a];
-            geo.partW[((int64_t)seg * geo.slot_stride + slot) * NA + a] = s;
+            for (int w = 0; w < NWARP; ++w) s += redW[w][j * NAc + a];
+            static_cast<AW*>(geo.partW)[((int64_t)seg * geo.slot_stride + slot) * NA + a] = s;
         }
     }
     if constexpr (NS > 0) {
@@ -499,13 +543,14 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
     const int gA = t / TC, cA = t - gA * TC;
     typename Pass::Gene gpar = Pass::load(prm, gids[gA]);
 
-    // owned outputs (W-type): o = t + k*NT over [0, GT*NA)
-    float acc[kGenKMAX];
+    // owned outputs (W-type): o = t + k*NT over [0, GT*NA); per-chunk FP32
+    // sums are folded into FP64 accumulators
+    double acc[kGenKMAX];
     short oi[kGenKMAX], oj[kGenKMAX], og[kGenKMAX], ow[kGenKMAX];
     int nown = 0;
 #pragma unroll
     for (int k = 0; k < kGenKMAX; ++k) {
-        acc[k] = 0.f;
+        acc[k] = 0;
         int o = t + k * kGenNT;
         og[k] = 0; ow[k] = 0; oi[k] = 0; oj[k] = 0;
         if (o < GT * NA) {
@@ -529,9 +574,11 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
     AS sacc = 0;
     __syncthreads();
 
+    constexpr bool F64 = Pass::F64;
     float breg[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) breg[i] = (i < P) ? betas[gA * P + i] * kLog2e : 0.f;
+    const double* bd = prm.beta_d + (int64_t)gids[gA] * P;
 
     for (int cb = c0; cb < c1; cb += TC) {
         const int nc = min(TC, c1 - cb);
@@ -558,8 +605,24 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
         __syncthreads();
         if (cA == 0) cursor[gA] += cnt[gA];
         // per-(gene, cell) weights
-        {
-            RecAcc<NWV, NS, AS> rec;
+        if constexpr (F64) {
+            RecAcc<NWV, NS, AS, double> rec;
+            rec.zero();
+            if (cA < nc) {
+                const int64_t c = cb + cA;
+                double e = __ldg(geo.offd + c);
+                for (int i = 0; i < P; ++i) e = fma(__ldg(geo.Xd + c * geo.xs + i), __ldg(bd + i), e);
+                double mu = exp(e);
+                float y = ys[gA * TC + cA];
+                Pass::template dense<double>(gpar, mu, rec);
+                if (y != 0.f) Pass::template sparse<double>(gpar, mu, y, rec);
+            }
+#pragma unroll
+            for (int w = 0; w < NWV; ++w) wts[(w * GT + gA) * TC + cA] = (float)rec.w[w];
+#pragma unroll
+            for (int s = 0; s < NS; ++s) wsc[(s * GT + gA) * TC + cA] = rec.s[s];
+        } else {
+            RecAcc<NWV, NS, AS, float> rec;
             rec.zero();
             if (cA < nc) {
                 float e = __ldg(geo.off + cb + cA) * kLog2e;
@@ -568,8 +631,8 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
                     if (i < P) e = fmaf(xsm[cA * XS + i], breg[i], e);
                 float mu = ex2_approx(e);
                 float y = ys[gA * TC + cA];
-                Pass::dense(gpar, mu, rec);
-                if (y != 0.f) Pass::sparse(gpar, mu, y, rec);
+                Pass::template dense<float>(gpar, mu, rec);
+                if (y != 0.f) Pass::template sparse<float>(gpar, mu, y, rec);
             }
 #pragma unroll
             for (int w = 0; w < NWV; ++w) wts[(w * GT + gA) * TC + cA] = rec.w[w];
@@ -583,9 +646,9 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
             const float* wp = wts + (ow[k] * GT + og[k]) * TC;
             const float* xi = xsm + oi[k];
             const float* xj = xsm + oj[k];
-            float s = acc[k];
+            float s = 0.f;
             for (int c = 0; c < nc; ++c) s = fmaf(wp[c] * xi[c * XS], xj[c * XS], s);
-            acc[k] = s;
+            acc[k] += (double)s;
         }
         if (NS > 0 && t < GT * NS) {
             constexpr int NSd = NS > 0 ? NS : 1;
@@ -603,7 +666,9 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
         int o = t + k * kGenNT;
         int g = o / NA, a = o - g * NA;
         int slot = tile * GT + g;
-        if (slot < nact) geo.partW[((int64_t)seg * geo.slot_stride + slot) * NA + a] = acc[k];
+        if (slot < nact)
+            static_cast<typename Pass::AW*>(geo.partW)[((int64_t)seg * geo.slot_stride + slot) * NA + a] =
+                (typename Pass::AW)acc[k];
     }
     if (NS > 0 && t < GT * NS) {
         constexpr int NSd = NS > 0 ? NS : 1;

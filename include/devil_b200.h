@@ -127,6 +127,15 @@ DEVIL_API int  devil_ctx_synchronize(devil_ctx *ctx);
 /* kernel launches issued by this context since creation (for accounting) */
 DEVIL_API int64_t devil_ctx_launch_count(const devil_ctx *ctx);
 
+/* Profiling (no counterpart in the reference, whose only timing is wall
+ * clock prints in src/beta.cpp:89-124): when enabled, every per-gene cell
+ * pass launch is bracketed by CUDA events on the context stream and its
+ * algorithmic bytes are accounted from the per-gene pass counts.
+ * pass_kind: 0 IRLS, 1 MOM, 2 MLE, 3 bread/meat.  Enabling resets. */
+DEVIL_API int devil_ctx_set_profiling(devil_ctx *ctx, int enable);
+DEVIL_API int devil_ctx_profile(devil_ctx *ctx, int pass_kind, int64_t *launches, double *ms,
+                                double *alg_bytes);
+
 /* ---- full pipeline --------------------------------------------------- */
 /* fit_devil(x, design_matrix, clusters, overdispersion, init_overdispersion,
  *           init_beta_rough, offset, size_factors, max_iter, tolerance)
@@ -166,8 +175,11 @@ DEVIL_API int devil_test_de_device(devil_ctx *ctx, int64_t n_genes, int p, const
                          const double *contrast_host, int adjust_method, double max_lfc,
                          double *pval_dev, double *adj_pval_dev, double *lfc_dev);
 
-/* stats::p.adjust on the device (NaN = NA, excluded from n) */
+/* stats::p.adjust (called at R/test.R:127) on the device (NaN = NA,
+ * excluded from n) */
 DEVIL_API int devil_p_adjust(devil_ctx *ctx, int64_t m, const double *p, int method, double *out);
+DEVIL_API int devil_p_adjust_device(devil_ctx *ctx, int64_t m, const double *p_dev, int method,
+                                    double *out_dev);
 
 /* ---- single steps (each mirrors one reference function) -------------- */
 /* calculate_sf / normed_sum_sf / psinorm_sf (R/size_factors.R:37-117) */

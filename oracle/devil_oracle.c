@@ -114,13 +114,33 @@ static double betacf(double a, double b, double x)
     return h;
 }
 
+/* lgamma(a + b) - lgamma(a) for a >= 100, from the Stirling series
+ * ln G(z) = (z - 1/2) ln z - z + ln(2 pi)/2 + 1/(12 z) - 1/(360 z^3) + ...
+ * with the leading terms differenced analytically (no cancellation). */
+static double lgamma_diff_large(double a, double b)
+{
+    double z = a + b;
+    double d = (a - 0.5) * log1p(b / a) + b * log(z) - b;
+    d += (1.0 / 12.0) * (1.0 / z - 1.0 / a);
+    d -= (1.0 / 360.0) * (1.0 / (z * z * z) - 1.0 / (a * a * a));
+    d += (1.0 / 1260.0) * (1.0 / (z * z * z * z * z) - 1.0 / (a * a * a * a * a));
+    return d;
+}
+
+static double log_beta(double a, double b)
+{
+    if (a >= 100.0 && b < a) return lgamma(b) - lgamma_diff_large(a, b);
+    if (b >= 100.0 && a < b) return lgamma(a) - lgamma_diff_large(b, a);
+    return lgamma(a) + lgamma(b) - lgamma(a + b);
+}
+
 /* regularised incomplete beta I_x(a,b) with x and (1-x) both supplied so
  * that neither is formed by cancellation. */
 static double ibeta(double a, double b, double x, double omx)
 {
     if (x <= 0.0) return 0.0;
     if (omx <= 0.0) return 1.0;
-    double lbeta = lgamma(a) + lgamma(b) - lgamma(a + b);
+    double lbeta = log_beta(a, b);
     double lfront = a * log(x) + b * log1p(-x);
     if (x > 0.5) lfront = a * log1p(-omx) + b * log(omx);
     lfront -= lbeta;

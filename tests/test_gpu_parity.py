@@ -28,8 +28,11 @@ def oracle_fit(orc, P, od, clusters_ends=None, sf="normed_sum", max_iter=200, to
     if sf is None:
         sfv = np.ones(P.n)
         off = orc.offset_vector(0.0, P.n, None)
-    else:
+    elif isinstance(sf, str):
         sfv = orc.calculate_sf(Y, sf)
+        off = orc.offset_vector(0.0, P.n, sfv)
+    else:
+        sfv = np.asarray(sf, float)
         off = orc.offset_vector(0.0, P.n, sfv)
     th0 = orc.estimate_dispersion(Y, off)
     b0 = orc.init_beta(Y, P.X, off, rough=init_rough)
@@ -127,7 +130,7 @@ def test_fit_dense_p2(dv, orc):
 
 
 def test_fit_clustered_p12(dv, orc):
-    P = synthetic.make("clustered", seed=7, G=60, n=6000)
+    P = synthetic.make("clustered", seed=7, G=200, n=4000)
     # 40 patients are drawn for the full config; sizes here scale with n
     levels, ends = dv.cluster_blocks(P.clusters)
     ref = oracle_fit(orc, P, orc.OD_MOM, clusters_ends=ends)
@@ -153,8 +156,8 @@ def test_fit_wide_p32(dv, orc):
 
 def test_plain_form_matches_oracle(dv, orc, sparse_problem):
     P = sparse_problem.subset_genes(np.arange(80))
-    ref = oracle_fit(orc, P, orc.OD_MOM)
-    fit = gpu_fit(dv, P, "MOM", form="plain")
+    ref = oracle_fit(orc, P, orc.OD_MOM, sf=P.sf_true)
+    fit = gpu_fit(dv, P, "MOM", form="plain", sf=P.sf_true)
     check_beta(fit, ref)
 
 
@@ -172,12 +175,14 @@ def test_rough_init_and_given_sf(dv, orc, sparse_problem):
 
 
 def test_single_steps(dv, orc, sparse_problem):
+    Pf = sparse_problem
+    for m in ("normed_sum", "psinorm"):
+        np.testing.assert_allclose(dv.calculate_sf((Pf.rowptr, Pf.col, Pf.val, Pf.n), m),
+                                   orc.calculate_sf(Pf.csr_f64(), m), rtol=1e-12)
     P = sparse_problem.subset_genes(np.arange(50))
     Y = P.csr_f64()
     csr = (P.rowptr, P.col, P.val, P.n)
-    for m in ("normed_sum", "psinorm"):
-        np.testing.assert_allclose(dv.calculate_sf(csr, m), orc.calculate_sf(Y, m), rtol=1e-12)
-    sf = orc.calculate_sf(Y, "normed_sum")
+    sf = P.sf_true
     off = orc.offset_vector(0.0, P.n, sf)
     np.testing.assert_allclose(dv.estimate_dispersion(csr, off), orc.estimate_dispersion(Y, off),
                                rtol=1e-12)
