@@ -577,7 +577,7 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
         ++launched;
         LAUNCH(launch_irls_finalize(pb.partWf(), nseg, tiles * plan.GT, dp.P, act[cur], cnt + cur,
                                     (int)hint, act[nxt], cnt + nxt, beta, beta_f, iters, status,
-                                    max_iter, eps, nullptr, st));
+                                    max_iter, eps, k, st));
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
@@ -626,6 +626,8 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, double* 
     s.it = newton_iters ? newton_iters : ws<int32_t>(ctx, "mle_it", G);
     s.phase = ws<int32_t>(ctx, "mle_phase", G);
     s.theta = theta;
+    s.dx = ws<double>(ctx, "mle_dx", G);
+    s.dxold = ws<double>(ctx, "mle_dxold", G);
     int32_t* act[2] = {ws<int32_t>(ctx, "act0", G), ws<int32_t>(ctx, "act1", G)};
     int32_t* cnt = ws<int32_t>(ctx, "cnt", 4);
     LAUNCH(launch_set_i32(cnt, 0, st));

@@ -105,7 +105,7 @@ cudaError_t launch_irls_finalize(const float* partW, int nseg, int slot_stride, 
                                  const int32_t* act, const int32_t* n_act, int max_slots,
                                  int32_t* act_next, int32_t* n_next, double* beta, float* beta_f,
                                  int32_t* iters, int32_t* status, int max_iter, double eps,
-                                 volatile int32_t* mirror, cudaStream_t st);
+                                 const float* k, cudaStream_t st);
 cudaError_t launch_mom_finalize(const double* partS, int nseg, int slot_stride,
                                 const int32_t* act, const int32_t* n_act, int max_slots,
                                 int64_t n, int P, double* theta, cudaStream_t st);
@@ -116,6 +116,8 @@ struct MleState {
     int32_t* it;
     int32_t* phase;  // 0: far-left check pending, 1: Newton, 2: done
     double* theta;   // result
+    double* dx;      // last step and the one before (bisection safeguard)
+    double* dxold;
 };
 cudaError_t launch_mle_init(const double* stats, int64_t G, int64_t n, MleState s,
                             int32_t* act, int32_t* n_act, cudaStream_t st);

@@ -40,7 +40,7 @@ DEV void unpack_sym(int P, const double* packed, double* M) {
 __global__ void irls_finalize_kernel(const float* partW, int nseg, int slot_stride, int P,
                                      const int32_t* act, const int32_t* n_act, int32_t* act_next,
                                      int32_t* n_next, double* beta, float* beta_f, int32_t* iters,
-                                     int32_t* status, int max_iter, double eps) {
+                                     int32_t* status, int max_iter, double eps, const float* kf) {
     extern __shared__ double fsh[];
     const int NE = P * (P + 1) / 2, NA = NE + P;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -56,8 +56,11 @@ __global__ void irls_finalize_kernel(const float* partW, int nseg, int slot_stri
     reduce_partials(partW, nseg, slot_stride, slot, NA, NA, sums, lane);
     __syncwarp();
     if (lane != 0) return;
+    // the pass accumulates H / k^2 and -score / k (see PassIRLS)
+    const double k = (double)kf[g];
     unpack_sym(P, sums, H);
-    for (int i = 0; i < P; ++i) S[i] = sums[NE + i];
+    for (int i = 0; i < P * P; ++i) H[i] *= k * k;
+    for (int i = 0; i < P; ++i) S[i] = -k * sums[NE + i];
     lu_factor(P, H, piv);
     lu_solve(P, H, piv, S);
     double mx = 0.0;
@@ -88,8 +91,7 @@ cudaError_t launch_irls_finalize(const float* partW, int nseg, int slot_stride, 
                                  const int32_t* act, const int32_t* n_act, int max_slots,
                                  int32_t* act_next, int32_t* n_next, double* beta, float* beta_f,
                                  int32_t* iters, int32_t* status, int max_iter, double eps,
-                                 volatile int32_t* mirror, cudaStream_t st) {
-    (void)mirror;
+                                 const float* k, cudaStream_t st) {
     if (max_slots <= 0) return cudaSuccess;
     const int NA = P * (P + 1) / 2 + P;
     const size_t per = (size_t)(NA + P * P + 2 * P) * sizeof(double);
@@ -102,7 +104,7 @@ cudaError_t launch_irls_finalize(const float* partW, int nseg, int slot_stride, 
     }
     irls_finalize_kernel<<<nblk(max_slots, w), 32 * w, smem, st>>>(
         partW, nseg, slot_stride, P, act, n_act, act_next, n_next, beta, beta_f, iters, status,
-        max_iter, eps);
+        max_iter, eps, k);
     return cudaGetLastError();
 }
 
@@ -258,27 +260,36 @@ __global__ void mle_finalize_kernel(const float* partW, const double* partS, int
         if (xn > hi) xn = hi;
         st.lo[g] = lo;
         st.hi[g] = hi;
+        st.dx[g] = hi - lo;
+        st.dxold[g] = hi - lo;
         st.phase[g] = 1;
     } else {
         double lo = st.lo[g], hi = st.hi[g];
+        double dx = st.dx[g], dxold = st.dxold[g];
         int it = st.it[g];
-        // The per-cell terms are FP32 (summed in FP64): the score is resolved
-        // to about 1e-6 of the size of its two opposing parts.  A score inside
-        // that band is zero to working precision.
-        const double resolution = 1e-6 * (fabs(a * (ss[0] + ss[2])) + fabs(dig));
-        if (score == 0.0 || fabs(score) <= resolution) {
+        if (score == 0.0) {
             done = true;
         } else {
             if (score > 0.0) lo = x; else hi = x;
+            // Newton inside the bracket; bisect when the step leaves it or
+            // fails to halve the step before last
             double cand = deriv < 0.0 ? x - score / deriv : NAN;
-            if (!(cand > lo && cand < hi)) cand = 0.5 * (lo + hi);
-            double step = fabs(cand - x);
+            if (!(cand > lo && cand < hi) || fabs(cand - x) > 0.5 * fabs(dxold)) {
+                dxold = dx;
+                dx = 0.5 * (hi - lo);
+                cand = lo + dx;
+            } else {
+                dxold = dx;
+                dx = fabs(cand - x);
+            }
             xn = cand;
             ++it;
-            if (step < 1e-10 || hi - lo < 1e-10 || it >= max_iter) done = true;
+            if (dx < 1e-10 || hi - lo < 1e-10 || it >= max_iter) done = true;
         }
         st.lo[g] = lo;
         st.hi[g] = hi;
+        st.dx[g] = dx;
+        st.dxold[g] = dxold;
         st.it[g] = it;
     }
     st.x[g] = xn;

@@ -49,20 +49,20 @@ struct PassGeom {
 // ---------------------------------------------------------------------
 // accumulators
 // ---------------------------------------------------------------------
+// zz holds the cell's products x_i x_j (packed upper triangle), computed
+// once per cell and shared by the gene tile.
 template <int P, int NA, int NS, class AW, class AS, class R>
 struct RegAcc {
     AW* a;
     AS* s;
     const R* x;
+    const R* zz;
     template <int W>
     DEV void outer(R w) {
-        constexpr int base = W * (P * (P + 1) / 2);
+        constexpr int NE = P * (P + 1) / 2;
+        constexpr int base = W * NE;
 #pragma unroll
-        for (int j = 0; j < P; ++j) {
-            R wx = w * x[j];
-#pragma unroll
-            for (int i = 0; i <= j; ++i) a[base + tri_index(i, j)] += (AW)(wx * x[i]);
-        }
+        for (int q = 0; q < NE; ++q) a[base + q] += (AW)(w * zz[q]);
     }
     template <int V, int NW>
     DEV void vec(R w) {
@@ -100,33 +100,35 @@ struct RecAcc {
 // One IRLS iteration of beta_fit (src/beta.cpp:35-42):
 //   w_q = exp(-eta - off), mu_g = (k + y) / (1 + k w_q)
 //   H = k X' diag(mu_g w_q) X,  score = k X' (mu_g w_q - 1)
-// With mu = 1/w_q:  k mu_g w_q = k (k + y)/(mu + k)  and
-//   k (mu_g w_q - 1) = k (y - mu)/(mu + k).
-// y = 0:  H weight k^2/(mu+k), score weight -k mu/(mu+k).
-// correction for y > 0: k y/(mu+k) for both.
+// With mu = 1/w_q and r = 1/(mu + k):  k mu_g w_q = k (k + y) r  and
+//   k (mu_g w_q - 1) = k (y - mu) r.  The pass accumulates
+//   outer0 = sum r x x' + sum_{y>0} (y/k) r x x'      (H = k^2 outer0)
+//   vec0   = sum mu r x - sum_{y>0} y r x            (score = -k vec0)
+// so a zero cell costs one reciprocal, one product and the FMAs; the
+// constant factors are applied in FP64 by the finalize.
 struct PassIRLS {
     static constexpr int NW = 1, NV = 1, NS = 0;
     static constexpr bool F64 = false;
     using AW = float;
     using AS = float;
     struct Params { const float* beta; const double* beta_d; const float* k; };
-    struct Gene { float k, kk, nk; };
+    struct Gene { float k, rk; };
     static DEV Gene load(const Params& p, int g) {
         float k = p.k[g];
-        return Gene{k, k * k, -k};
+        return Gene{k, 1.f / k};
     }
     template <class R, class A>
     static DEV void dense(const Gene& G, float mu, A& acc) {
         float r = rcp_approx(mu + G.k);
-        acc.template outer<0>(G.kk * r);
-        acc.template vec<0, NW>(G.nk * mu * r);
+        acc.template outer<0>(r);
+        acc.template vec<0, NW>(mu * r);
     }
     template <class R, class A>
     static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
         float r = rcp_approx(mu + G.k);
-        float v = G.k * y * r;
-        acc.template outer<0>(v);
-        acc.template vec<0, NW>(v);
+        float yr = y * r;
+        acc.template outer<0>(yr * G.rk);
+        acc.template vec<0, NW>(-yr);
     }
 };
 
@@ -377,32 +379,59 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
     const int b0 = seg * geo.fpi, b1 = b0 + geo.fpi;
     const int c0 = __ldg(geo.bound + b0), c1 = __ldg(geo.bound + b1);
 
-    for (int c = c0 + threadIdx.x; c < c1; c += NT) {
-        if constexpr (F64) {
+    if constexpr (F64) {
+        for (int c = c0 + threadIdx.x; c < c1; c += NT) {
             double x[P];
 #pragma unroll
             for (int i = 0; i < P; ++i) x[i] = __ldg(geo.Xd + (int64_t)c * PP + i);
             const double o = __ldg(geo.offd + c);
+            double zz[P * (P + 1) / 2];
+#pragma unroll
+            for (int jj = 0; jj < P; ++jj)
+#pragma unroll
+                for (int ii = 0; ii <= jj; ++ii) zz[tri_index(ii, jj)] = x[ii] * x[jj];
 #pragma unroll
             for (int j = 0; j < GT; ++j) {
                 double e = o;
 #pragma unroll
                 for (int i = 0; i < P; ++i) e = fma(x[i], betad[j][i], e);
                 double mu = exp(e);
-                RegAcc<P, NAc, NSc, AW, AS, double> acc{aw[j], as[j], x};
+                RegAcc<P, NAc, NSc, AW, AS, double> acc{aw[j], as[j], x, zz};
                 Pass::template dense<double>(gp[j], mu, acc);
             }
-        } else {
+        }
+    } else {
+        // software pipeline: the next cell's row is in flight while the gene
+        // tile works on the current one
+        int c = c0 + threadIdx.x;
+        float xn[P];
+        float on = 0.f;
+        if (c < c1) {
+            load_row<P, PP>(geo.X, c, xn);
+            on = __ldg(geo.off + c);
+        }
+        for (; c < c1; c += NT) {
             float x[P];
-            load_row<P, PP>(geo.X, c, x);
-            float o = __ldg(geo.off + c) * kLog2e;
+#pragma unroll
+            for (int i = 0; i < P; ++i) x[i] = xn[i];
+            const float o = on * kLog2e;
+            const int cn = c + NT;
+            if (cn < c1) {
+                load_row<P, PP>(geo.X, cn, xn);
+                on = __ldg(geo.off + cn);
+            }
+            float zz[P * (P + 1) / 2];
+#pragma unroll
+            for (int jj = 0; jj < P; ++jj)
+#pragma unroll
+                for (int ii = 0; ii <= jj; ++ii) zz[tri_index(ii, jj)] = x[ii] * x[jj];
 #pragma unroll
             for (int j = 0; j < GT; ++j) {
                 float e = o;
 #pragma unroll
                 for (int i = 0; i < P; ++i) e = fmaf(x[i], beta[j][i], e);
                 float mu = ex2_approx(e);
-                RegAcc<P, NAc, NSc, AW, AS, float> acc{aw[j], as[j], x};
+                RegAcc<P, NAc, NSc, AW, AS, float> acc{aw[j], as[j], x, zz};
                 Pass::template dense<float>(gp[j], mu, acc);
             }
         }
@@ -410,10 +439,19 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
 #pragma unroll
     for (int j = 0; j < GT; ++j) {
         const int64_t* sp = geo.segptr + (int64_t)gid[j] * geo.nbound;
-        int64_t e0 = __ldg(sp + b0), e1 = __ldg(sp + b1);
-        for (int64_t e = e0 + threadIdx.x; e < e1; e += NT) {
-            int c = __ldg(geo.col + e);
-            float y = load_val(val, e);
+        const int64_t e0 = __ldg(sp + b0), e1 = __ldg(sp + b1);
+        // two-stage pipeline: indices two entries ahead, rows one ahead
+        int64_t e = e0 + threadIdx.x;
+        int cA = 0, cB = 0;
+        float yA = 0.f, yB = 0.f;
+        if (e < e1) { cA = __ldg(geo.col + e); yA = load_val(val, e); }
+        if (e + NT < e1) { cB = __ldg(geo.col + e + NT); yB = load_val(val, e + NT); }
+        for (; e < e1; e += NT) {
+            const int c = cA;
+            const float y = yA;
+            cA = cB;
+            yA = yB;
+            if (e + 2 * NT < e1) { cB = __ldg(geo.col + e + 2 * NT); yB = load_val(val, e + 2 * NT); }
             if constexpr (F64) {
                 double x[P];
 #pragma unroll
@@ -422,7 +460,12 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
 #pragma unroll
                 for (int i = 0; i < P; ++i) el = fma(x[i], betad[j][i], el);
                 double mu = exp(el);
-                RegAcc<P, NAc, NSc, AW, AS, double> acc{aw[j], as[j], x};
+                double zz[P * (P + 1) / 2];
+#pragma unroll
+                for (int jj = 0; jj < P; ++jj)
+#pragma unroll
+                    for (int ii = 0; ii <= jj; ++ii) zz[tri_index(ii, jj)] = x[ii] * x[jj];
+                RegAcc<P, NAc, NSc, AW, AS, double> acc{aw[j], as[j], x, zz};
                 Pass::template sparse<double>(gp[j], mu, y, acc);
             } else {
                 float x[P];
@@ -431,7 +474,12 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
 #pragma unroll
                 for (int i = 0; i < P; ++i) el = fmaf(x[i], beta[j][i], el);
                 float mu = ex2_approx(el);
-                RegAcc<P, NAc, NSc, AW, AS, float> acc{aw[j], as[j], x};
+                float zz[P * (P + 1) / 2];
+#pragma unroll
+                for (int jj = 0; jj < P; ++jj)
+#pragma unroll
+                    for (int ii = 0; ii <= jj; ++ii) zz[tri_index(ii, jj)] = x[ii] * x[jj];
+                RegAcc<P, NAc, NSc, AW, AS, float> acc{aw[j], as[j], x, zz};
                 Pass::template sparse<float>(gp[j], mu, y, acc);
             }
         }

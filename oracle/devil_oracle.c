@@ -703,11 +703,11 @@ double orc_fit_dispersion(int64_t n, int p, const double *y, const double *X, co
 
     double lo = log(1e-8);
     if (orc_nb_score(&d, lo, cr) < 0.0) { free(mu); return 0.0; }
-    double hi = log(1e16), lo_b = log(1e-16);
-    (void)lo_b;
+    double hi = log(1e16);
     double x = log(start);
     if (x < lo) x = lo;
     if (x > hi) x = hi;
+    double dx = hi - lo, dxold = hi - lo;
     int it = 0;
     for (; it < max_iter; it++) {
         double s = orc_nb_score(&d, x, cr);
@@ -715,10 +715,18 @@ double orc_fit_dispersion(int64_t n, int p, const double *y, const double *X, co
         if (s > 0.0) lo = x; else hi = x;
         double dd = orc_nb_deriv_score(&d, x, cr);
         double xn = (dd < 0.0) ? x - s / dd : NAN;
-        if (!(xn > lo && xn < hi)) xn = 0.5 * (lo + hi);
-        double step = fabs(xn - x);
+        /* Newton inside the bracket; bisect when the step leaves it or fails
+         * to halve the step before last (safeguarded Newton, "rtsafe") */
+        if (!(xn > lo && xn < hi) || fabs(xn - x) > 0.5 * fabs(dxold)) {
+            dxold = dx;
+            dx = 0.5 * (hi - lo);
+            xn = lo + dx;
+        } else {
+            dxold = dx;
+            dx = fabs(xn - x);
+        }
         x = xn;
-        if (step < 1e-10 || hi - lo < 1e-10) { it++; break; }
+        if (dx < 1e-10 || hi - lo < 1e-10) { it++; break; }
     }
     *iters = it;
     free(mu);
