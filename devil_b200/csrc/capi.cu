@@ -612,7 +612,8 @@ void run_mom(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
 }
 
 // MLE theta (R/overdispersion.R:25-115)
-void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, double* theta,
+void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const double* beta_d,
+             double* theta,
              int32_t* newton_iters, int max_iter, int cox_reid, int form) {
     cudaStream_t st = ctx->stream;
     const int64_t G = dp.G;
@@ -636,7 +637,7 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, double* 
     PassBuffers pb = pass_buffers(ctx, PASS_MLE, dp.P, max_slot_segs(ctx, dp, plan.GT, form));
     *ctx->mapped_host = (int32_t)G;
     const int LAG = 2;
-    PassParamsAny prm{beta_f, nullptr, nullptr, s.x, nullptr};
+    PassParamsAny prm{beta_f, beta_d, nullptr, s.x, nullptr};
     int64_t launched = 0;
     // one far-left evaluation plus at most max_iter Newton evaluations
     for (int t = 0; t <= max_iter; ++t) {
@@ -777,7 +778,7 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
             CK(cudaMemcpyAsync(fb.theta, tm, G * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     if (o->overdispersion == DEVIL_OD_MLE) {
-        run_mle(ctx, dp, fb.beta_f, fb.theta, nullptr, o->max_iter, 1, o->form);
+        run_mle(ctx, dp, fb.beta_f, fb.beta, fb.theta, nullptr, o->max_iter, 1, o->form);
     } else if (o->overdispersion == DEVIL_OD_NONE) {
         CK(cudaMemsetAsync(fb.theta, 0, G * sizeof(double), st));
     }
@@ -1183,7 +1184,7 @@ int devil_fit_dispersion(devil_ctx* ctx, const devil_counts* counts, const doubl
         upload_beta(ctx, dp, beta, &bf, &bd);
         double* th = ws<double>(ctx, "theta", dp.G);
         int32_t* it = ws<int32_t>(ctx, "mle_iters_out", dp.G);
-        run_mle(ctx, dp, bf, th, it, max_iter, cox_reid, DEVIL_FORM_CHOSEN);
+        run_mle(ctx, dp, bf, bd, th, it, max_iter, cox_reid, DEVIL_FORM_CHOSEN);
         d2h(ctx, theta, th, dp.G);
         d2h(ctx, newton_iters, it, dp.G);
         CK(cudaStreamSynchronize(ctx->stream));

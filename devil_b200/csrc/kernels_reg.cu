@@ -9,7 +9,7 @@ int reg_max_p() { return 8; }
 
 int reg_default_gt(PassKind k, int P) {
     switch (k) {
-        case PASS_IRLS: return P <= 4 ? 8 : (P <= 6 ? 4 : 2);
+        case PASS_IRLS: return P <= 6 ? 4 : 2;
         case PASS_SANDWICH: return P <= 2 ? 8 : (P <= 4 ? 4 : (P <= 6 ? 2 : 1));
         case PASS_MOM: return 8;
         case PASS_MLE: return P <= 2 ? 4 : (P <= 4 ? 2 : 1);

@@ -109,6 +109,7 @@ struct RecAcc {
 struct PassIRLS {
     static constexpr int NW = 1, NV = 1, NS = 0;
     static constexpr bool F64 = false;
+    static constexpr bool TABLES = false;
     using AW = float;
     using AS = float;
     struct Params { const float* beta; const double* beta_d; const float* k; };
@@ -138,6 +139,7 @@ struct PassIRLS {
 struct PassMOM {
     static constexpr int NW = 0, NV = 0, NS = 2;
     static constexpr bool F64 = true;
+    static constexpr bool TABLES = false;
     using AW = float;
     using AS = double;
     struct Params { const float* beta; const double* beta_d; };
@@ -212,20 +214,58 @@ DEV double trigamma_d(double x) {
                f * (-1.0 / 30 + f * (5.0 / 66 + f * (-691.0 / 2730 + f * (7.0 / 6)))))));
     return r + t;
 }
-DEV void psi_diffs(double y, double a, double& d1, double& d2) {
-    if (y <= 32.0 && y == floor(y)) {
-        double s1 = 0.0, s2 = 0.0;
-        int yi = (int)y;
-        for (int j = 0; j < yi; ++j) {
-            double v = 1.0 / (a + j);
-            s1 += v;
-            s2 -= v * v;
+
+// Per-gene tables of psi(v + a) - psi(a) and psi1(v + a) - psi1(a) for
+// v = 0..kPsiTab-1, from psi(x + 1) = psi(x) + 1/x (prefix sums of 1/(a+j)
+// and -1/(a+j)^2).  Counts are integers, so most nonzeros read a table
+// entry; larger counts evaluate the asymptotic series.  This plays the role
+// of the reference's count table (make_table_if_small,
+// src/overdispersion.cpp:32-46): the digamma work no longer scales with
+// the nonzeros.
+constexpr int kPsiTab = 64;
+struct PsiTable {
+    const double* d1;  // [kPsiTab]
+    const double* d2;  // [kPsiTab]
+    double pa, ta;     // psi(a), psi1(a) for counts beyond the table
+};
+// build tables for GTn genes with parameter a[j] using all threads of the
+// block (one thread per (gene, v)); tab layout [gene][2][kPsiTab]
+DEV void build_psi_tables(int GTn, const double* a, double* tab, double* scratch) {
+    // scratch: [GTn][kPsiTab] terms; inclusive scan by one warp per gene
+    for (int i = threadIdx.x; i < GTn * kPsiTab; i += blockDim.x) {
+        int j = i / kPsiTab, v = i - j * kPsiTab;
+        double t = (v == 0) ? 0.0 : 1.0 / (a[j] + (v - 1));
+        scratch[i] = t;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int j = warp; j < GTn; j += nw) {
+        double c1 = 0.0, c2 = 0.0;
+        for (int base = 0; base < kPsiTab; base += 32) {
+            double t = scratch[j * kPsiTab + base + lane];
+            double s1 = t, s2 = -t * t;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                double u1 = __shfl_up_sync(0xffffffffu, s1, o);
+                double u2 = __shfl_up_sync(0xffffffffu, s2, o);
+                if (lane >= o) { s1 += u1; s2 += u2; }
+            }
+            tab[(j * 2 + 0) * kPsiTab + base + lane] = c1 + s1;
+            tab[(j * 2 + 1) * kPsiTab + base + lane] = c2 + s2;
+            c1 += __shfl_sync(0xffffffffu, s1, 31);
+            c2 += __shfl_sync(0xffffffffu, s2, 31);
         }
-        d1 = s1;
-        d2 = s2;
+    }
+    __syncthreads();
+}
+DEV void psi_diffs_tab(double y, double a, const PsiTable& T, double& d1, double& d2) {
+    if (y < (double)kPsiTab && y == floor(y)) {
+        int v = (int)y;
+        d1 = T.d1[v];
+        d2 = T.d2[v];
     } else {
-        d1 = digamma_d(y + a) - digamma_d(a);
-        d2 = trigamma_d(y + a) - trigamma_d(a);
+        d1 = digamma_d(y + a) - T.pa;
+        d2 = trigamma_d(y + a) - T.ta;
     }
 }
 
@@ -239,13 +279,14 @@ DEV void psi_diffs(double y, double a, double& d1, double& d2) {
 struct PassMLE {
     static constexpr int NW = 3, NV = 0, NS = 6;
     static constexpr bool F64 = false;
+    static constexpr bool TABLES = true;
     using AW = float;
     using AS = double;
     struct Params { const float* beta; const double* beta_d; const double* log_theta; };
-    struct Gene { double theta, a; float thf; };
+    struct Gene { double theta, a; float thf; PsiTable tab; };
     static DEV Gene load(const Params& p, int g) {
         double th = exp(p.log_theta[g]);
-        return Gene{th, 1.0 / th, (float)th};
+        return Gene{th, 1.0 / th, (float)th, PsiTable{nullptr, nullptr, 0.0, 0.0}};
     }
     template <class R, class A>
     static DEV void dense(const Gene& G, float mu, A& acc) {
@@ -261,11 +302,11 @@ struct PassMLE {
     template <class R, class A>
     static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
         double m = mu, yy = y;
-        double den = 1.0 + m * G.theta;
-        acc.template scal<2>(yy * G.theta / den);
-        acc.template scal<3>(yy / (den * den));
+        double r = 1.0 / (1.0 + m * G.theta);
+        acc.template scal<2>(yy * G.theta * r);
+        acc.template scal<3>(yy * r * r);
         double d1, d2;
-        psi_diffs(yy, G.a, d1, d2);
+        psi_diffs_tab(yy, G.a, G.tab, d1, d2);
         acc.template scal<4>(d1);
         acc.template scal<5>(d2);
     }
@@ -281,6 +322,7 @@ struct PassMLE {
 struct PassSandwich {
     static constexpr int NW = 1, NV = 1, NS = 0;
     static constexpr bool F64 = true;
+    static constexpr bool TABLES = false;
     using AW = double;
     using AS = float;
     struct Params { const float* beta; const double* beta_d; const double* theta; };
@@ -364,6 +406,25 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
             for (int i = 0; i < P; ++i) beta[j][i] = __ldg(prm.beta + (int64_t)g * P + i) * kLog2e;
         }
         gp[j] = Pass::load(prm, g);
+    }
+    if constexpr (Pass::TABLES) {
+        __shared__ double psitab[GT * 2 * kPsiTab];
+        __shared__ double psiscr[GT * kPsiTab];
+        __shared__ double psia[GT];
+        if (threadIdx.x < GT) {
+#pragma unroll
+            for (int j = 0; j < GT; ++j)
+                if (j == (int)threadIdx.x) psia[j] = gp[j].a;
+        }
+        __syncthreads();
+        build_psi_tables(GT, psia, psitab, psiscr);
+#pragma unroll
+        for (int j = 0; j < GT; ++j) {
+            gp[j].tab.d1 = psitab + (j * 2 + 0) * kPsiTab;
+            gp[j].tab.d2 = psitab + (j * 2 + 1) * kPsiTab;
+            gp[j].tab.pa = digamma_d(gp[j].a);
+            gp[j].tab.ta = trigamma_d(gp[j].a);
+        }
     }
 
     AW aw[GT][NAc];
@@ -590,6 +651,18 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
     }
     const int gA = t / TC, cA = t - gA * TC;
     typename Pass::Gene gpar = Pass::load(prm, gids[gA]);
+    if constexpr (Pass::TABLES) {
+        __shared__ double psitab[8 * 2 * kPsiTab];
+        __shared__ double psiscr[8 * kPsiTab];
+        __shared__ double psia[8];
+        if (cA == 0) psia[gA] = gpar.a;
+        __syncthreads();
+        build_psi_tables(GT, psia, psitab, psiscr);
+        gpar.tab.d1 = psitab + (gA * 2 + 0) * kPsiTab;
+        gpar.tab.d2 = psitab + (gA * 2 + 1) * kPsiTab;
+        gpar.tab.pa = digamma_d(gpar.a);
+        gpar.tab.ta = trigamma_d(gpar.a);
+    }
 
     // owned outputs (W-type): o = t + k*NT over [0, GT*NA); per-chunk FP32
     // sums are folded into FP64 accumulators
@@ -623,9 +696,6 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
     __syncthreads();
 
     constexpr bool F64 = Pass::F64;
-    float breg[32];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) breg[i] = (i < P) ? betas[gA * P + i] * kLog2e : 0.f;
     const double* bd = prm.beta_d + (int64_t)gids[gA] * P;
 
     for (int cb = c0; cb < c1; cb += TC) {
@@ -673,11 +743,12 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
             RecAcc<NWV, NS, AS, float> rec;
             rec.zero();
             if (cA < nc) {
-                float e = __ldg(geo.off + cb + cA) * kLog2e;
-#pragma unroll
-                for (int i = 0; i < 32; ++i)
-                    if (i < P) e = fmaf(xsm[cA * XS + i], breg[i], e);
-                float mu = ex2_approx(e);
+                // eta in FP64 (a sum of terms that may be large and cancel)
+                const int64_t c = cb + cA;
+                double ed = __ldg(geo.offd + c);
+                for (int i = 0; i < P; ++i)
+                    ed = fma(__ldg(geo.Xd + c * geo.xs + i), __ldg(bd + i), ed);
+                float mu = ex2_approx((float)(ed * 1.4426950408889634));
                 float y = ys[gA * TC + cA];
                 Pass::template dense<float>(gpar, mu, rec);
                 if (y != 0.f) Pass::template sparse<float>(gpar, mu, y, rec);
