@@ -35,6 +35,7 @@ struct devil_ctx {
     int32_t* mapped_dev = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int sm_count = 148;
+    int use_tma = 0;
     // profiling: CUDA events around every pass launch, per pass kind
     int profiling = 0;
     std::vector<cudaEvent_t> ev_pool;
@@ -137,12 +138,6 @@ void h2d(devil_ctx* ctx, T* dst, const T* src, size_t count) {
 template <class T>
 void d2h(devil_ctx* ctx, T* dst, const T* src, size_t count) {
     if (count && dst) CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
-}
-
-int pow2_floor(int v) {
-    int p = 1;
-    while (p * 2 <= v) p *= 2;
-    return p;
 }
 
 // ------------------------------------------------------------------
@@ -335,16 +330,19 @@ void prepare_design(devil_ctx* ctx, DevProblem& dp, const double* X, int P, bool
         h2d(ctx, xd, X, (size_t)dp.n * P);
         dp.Xcm = xd;
     }
-    dp.Xrm = ws<float>(ctx, "Xrm", (size_t)dp.n * dp.xs);
+    // 16 padding rows: TMA copies of the last chunk round up to 4 cells
+    dp.Xrm = ws<float>(ctx, "Xrm", (size_t)(dp.n + 16) * dp.xs);
+    CK(cudaMemsetAsync(dp.Xrm + (size_t)dp.n * dp.xs, 0, (size_t)16 * dp.xs * sizeof(float), st));
     LAUNCH(launch_x_rowmajor(dp.Xcm, dp.n, P, dp.xs, dp.Xrm, st));
     dp.Xdrm = ws<double>(ctx, "Xdrm", (size_t)dp.n * dp.xs);
     LAUNCH(launch_x_rowmajor_d(dp.Xcm, dp.n, P, dp.xs, dp.Xdrm, st));
-    // uniform fine segmentation: power-of-two count, >= 1024 cells each
-    int nf = (int)std::min<int64_t>(64, std::max<int64_t>(1, dp.n / 1024));
-    nf = pow2_floor(nf);
+    // fine segmentation: chunks of CH cells (a multiple of 16), the unit
+    // the TMA engine stages; work items are runs of consecutive chunks
+    const int CH = tma_chunk_cells(dp.xs);
+    const int nf = (int)((dp.n + CH - 1) / CH);
     dp.nfine = nf;
     std::vector<int32_t> hb(nf + 1);
-    for (int s = 0; s <= nf; ++s) hb[s] = (int32_t)((dp.n * s) / nf);
+    for (int s = 0; s <= nf; ++s) hb[s] = (int32_t)std::min<int64_t>(dp.n, (int64_t)s * CH);
     dp.fine_bound = ws<int32_t>(ctx, "fine_bound", nf + 1);
     h2d(ctx, dp.fine_bound, hb.data(), nf + 1);
     dp.fine_ptr = ws<int64_t>(ctx, "fine_ptr", (size_t)dp.G * (nf + 1));
@@ -361,7 +359,8 @@ void compute_offsets(devil_ctx* ctx, DevProblem& dp, int method, const double* s
     const int64_t n = dp.n;
     dp.sf = ws<double>(ctx, "sf", n);
     dp.off = ws<double>(ctx, "off", n);
-    dp.off_f = ws<float>(ctx, "off_f", n);
+    dp.off_f = ws<float>(ctx, "off_f", n + 16);
+    CK(cudaMemsetAsync(dp.off_f + n, 0, 16 * sizeof(float), st));
     if (method == DEVIL_SF_NONE) {
         LAUNCH(launch_sf_given(nullptr, n, offset, 0, dp.sf, dp.off, dp.off_f, st));
         return;
@@ -417,6 +416,13 @@ PassPlan plan_for(PassKind k, int P, int form) {
     if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, 1};
     if (P <= reg_max_p()) {
         int gt = reg_default_gt(k, P);
+        if (k == PASS_MLE) {
+            const char* e = getenv("DEVIL_MLE_GT");
+            if (e) {
+                int v = atoi(e);
+                if (reg_gt_supported(k, P, v)) gt = v;
+            }
+        }
         if (k == PASS_IRLS) {
             const char* e = getenv("DEVIL_IRLS_GT");
             if (e) {
@@ -434,9 +440,7 @@ int choose_nseg(devil_ctx* ctx, const DevProblem& dp, int tiles, int form) {
     if (form == DEVIL_FORM_PLAIN) return 1;
     const int target = ctx->sm_count * 2;
     int want = (target + tiles - 1) / tiles;
-    int nseg = 1;
-    while (nseg < want && nseg < dp.nfine) nseg *= 2;
-    return nseg;
+    return std::max(1, std::min(want, dp.nfine));
 }
 
 // largest nseg * tiles * GT over every active-gene count the loops can see
@@ -465,7 +469,7 @@ PassBuffers pass_buffers(devil_ctx* ctx, PassKind k, int P, size_t slots_x_segs)
 }
 
 void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const PassPlan& plan,
-                 int nseg, int fpi, int tiles, const int32_t* bound, const int64_t* segptr,
+                 int nseg, int tiles, const int32_t* bound, const int64_t* segptr,
                  int nbound, const int32_t* act, const int32_t* n_act, int32_t* reset_next,
                  const PassBuffers& pb, const PassParamsAny& prm) {
     PassLaunch L;
@@ -487,7 +491,10 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
     L.geo.segptr = segptr;
     L.geo.bound = bound;
     L.geo.nbound = nbound;
-    L.geo.fpi = fpi;
+    L.geo.nseg = nseg;
+    L.geo.err = ws<int32_t>(ctx, "kernel_err", 1);
+    L.use_tma = plan.engine == ENGINE_REG && ctx->use_tma &&
+                (kind == PASS_IRLS || kind == PASS_MLE) && bound == dp.fine_bound;
     L.geo.act = act;
     L.geo.n_act = n_act;
     L.geo.reset_next = reset_next;
@@ -571,8 +578,7 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, tiles, form);
-        const int fpi = dp.nfine / nseg;
-        launch_pass(ctx, dp, PASS_IRLS, plan, nseg, fpi, tiles, dp.fine_bound, dp.fine_ptr,
+        launch_pass(ctx, dp, PASS_IRLS, plan, nseg, tiles, dp.fine_bound, dp.fine_ptr,
                     dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
         ++launched;
         LAUNCH(launch_irls_finalize(pb.partWf(), nseg, tiles * plan.GT, dp.P, act[cur], cnt + cur,
@@ -599,7 +605,7 @@ void run_mom(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     const int nseg = choose_nseg(ctx, dp, tiles, form);
     PassBuffers pb = pass_buffers(ctx, PASS_MOM, dp.P, (size_t)nseg * tiles * plan.GT);
     PassParamsAny prm{beta_f, beta_d, nullptr, nullptr, nullptr};
-    launch_pass(ctx, dp, PASS_MOM, plan, nseg, dp.nfine / nseg, tiles, dp.fine_bound, dp.fine_ptr,
+    launch_pass(ctx, dp, PASS_MOM, plan, nseg, tiles, dp.fine_bound, dp.fine_ptr,
                 dp.nfine + 1, act, cnt, nullptr, pb, prm);
     LAUNCH(launch_mom_finalize(pb.partS, nseg, tiles * plan.GT, act, cnt, (int)dp.G, dp.n, dp.P,
                                theta, ctx->stream));
@@ -648,7 +654,7 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, tiles, form);
-        launch_pass(ctx, dp, PASS_MLE, plan, nseg, dp.nfine / nseg, tiles, dp.fine_bound,
+        launch_pass(ctx, dp, PASS_MLE, plan, nseg, tiles, dp.fine_bound,
                     dp.fine_ptr, dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
         ++launched;
         LAUNCH(launch_mle_finalize(pb.partWf(), pb.partS, nseg, tiles * plan.GT, dp.P, dp.stats, dp.n,
@@ -683,7 +689,7 @@ void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, con
     if (n_clusters <= 0) {
         const int nseg = choose_nseg(ctx, dp, tiles, form);
         PassBuffers pb = pass_buffers(ctx, PASS_SANDWICH, dp.P, (size_t)nseg * tiles * plan.GT);
-        launch_pass(ctx, dp, PASS_SANDWICH, plan, nseg, dp.nfine / nseg, tiles, dp.fine_bound,
+        launch_pass(ctx, dp, PASS_SANDWICH, plan, nseg, tiles, dp.fine_bound,
                     dp.fine_ptr, dp.nfine + 1, act, cnt, nullptr, pb, prm);
         LAUNCH(launch_sandwich_finalize(pb.partWd(), nseg, tiles * plan.GT, dp.P, nullptr, 0, dp.n,
                                         act, cnt, (int)dp.G, bread, nullptr, nullptr, st));
@@ -723,7 +729,7 @@ void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, con
     int64_t* segptr = ws<int64_t>(ctx, "sw_segptr", (size_t)dp.G * hb.size());
     LAUNCH(launch_segptr(dp.rowptr, dp.col, dp.G, bound, (int)hb.size(), segptr, st));
     PassBuffers pb = pass_buffers(ctx, PASS_SANDWICH, dp.P, (size_t)nseg * tiles * plan.GT);
-    launch_pass(ctx, dp, PASS_SANDWICH, plan, nseg, 1, tiles, bound, segptr, (int)hb.size(), act,
+    launch_pass(ctx, dp, PASS_SANDWICH, plan, nseg, tiles, bound, segptr, (int)hb.size(), act,
                 cnt, nullptr, pb, prm);
     LAUNCH(launch_sandwich_finalize(pb.partWd(), nseg, tiles * plan.GT, dp.P, segc, n_clusters, dp.n,
                                     act, cnt, (int)dp.G, bread, sandwich, meat, st));
@@ -733,6 +739,18 @@ void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, con
         int32_t* ones = ws<int32_t>(ctx, "prof_ones", dp.G);
         LAUNCH(launch_fill_i32(ones, 1, dp.G, st));
         prof_add_bytes(ctx, dp, PASS_SANDWICH, ones, 1);
+    }
+}
+
+// a bounded wait inside a kernel gave up (the kernel skipped its writes)
+void check_kernel_err(devil_ctx* ctx) {
+    int32_t* err = ws<int32_t>(ctx, "kernel_err", 1);
+    int32_t h = 0;
+    CK(cudaMemcpyAsync(&h, err, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h) {
+        CK(cudaMemsetAsync(err, 0, sizeof(int32_t), ctx->stream));
+        fail(ctx, DEVIL_ERR_CUDA, "a staged copy wait timed out inside a pass kernel");
     }
 }
 
@@ -784,6 +802,7 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     }
     run_sandwich(ctx, dp, fb.beta_f, fb.beta, fb.theta, ends_host, n_clusters, fb.bread,
                  n_clusters > 0 ? fb.sandwich : nullptr, nullptr, o->form);
+    check_kernel_err(ctx);
 }
 
 void alloc_fit_buffers(devil_ctx* ctx, int64_t G, int P, bool theta_mom, bool clusters,
@@ -855,6 +874,12 @@ int devil_ctx_create(int device, devil_ctx** out) {
         CK(cudaHostGetDevicePointer((void**)&ctx->mapped_dev, ctx->mapped_host, 0));
         for (auto& e : ctx->ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device));
+        // the TMA-staged engine is opt-in: with CSR loads per chunk exposed it
+        // measured slower than the register engine on the sparse workload
+        const char* ut = getenv("DEVIL_TMA");
+        ctx->use_tma = (ut && atoi(ut)) ? 1 : 0;
+        int32_t* err = ws<int32_t>(ctx, "kernel_err", 1);
+        CK(cudaMemset(err, 0, sizeof(int32_t)));
     });
     if (rc != DEVIL_OK) {
         fprintf(stderr, "devil_ctx_create: %s\n", ctx->err.c_str());
@@ -1060,7 +1085,8 @@ int devil_calculate_sf(devil_ctx* ctx, const devil_counts* counts, int method, d
 static void upload_offsets(devil_ctx* ctx, DevProblem& dp, const double* offv_host) {
     dp.sf = ws<double>(ctx, "sf", dp.n);
     dp.off = ws<double>(ctx, "off", dp.n);
-    dp.off_f = ws<float>(ctx, "off_f", dp.n);
+    dp.off_f = ws<float>(ctx, "off_f", dp.n + 16);
+    CK(cudaMemsetAsync(dp.off_f + dp.n, 0, 16 * sizeof(float), ctx->stream));
     h2d(ctx, dp.off, offv_host, dp.n);
     LAUNCH(launch_double_to_float(dp.off, dp.off_f, dp.n, ctx->stream));
 }
@@ -1135,6 +1161,7 @@ int devil_beta_fit(devil_ctx* ctx, const devil_counts* counts, const double* X, 
         int32_t* it = ws<int32_t>(ctx, "iters", G);
         int32_t* stt = ws<int32_t>(ctx, "status", G);
         run_irls(ctx, dp, b, bf, k, it, stt, max_iter, (double)(float)eps, form);
+        check_kernel_err(ctx);
         d2h(ctx, beta, b, (size_t)G * p);
         d2h(ctx, iters, it, G);
         CK(cudaStreamSynchronize(ctx->stream));
@@ -1185,6 +1212,7 @@ int devil_fit_dispersion(devil_ctx* ctx, const devil_counts* counts, const doubl
         double* th = ws<double>(ctx, "theta", dp.G);
         int32_t* it = ws<int32_t>(ctx, "mle_iters_out", dp.G);
         run_mle(ctx, dp, bf, bd, th, it, max_iter, cox_reid, DEVIL_FORM_CHOSEN);
+        check_kernel_err(ctx);
         d2h(ctx, theta, th, dp.G);
         d2h(ctx, newton_iters, it, dp.G);
         CK(cudaStreamSynchronize(ctx->stream));

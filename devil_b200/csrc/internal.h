@@ -33,6 +33,7 @@ struct PassLaunch {
     int xs_pad;     // row stride of geo.X
     int GT;
     int val_u16;    // 1: uint16 values, 0: float values
+    int use_tma;    // FP32 passes, p <= 8: TMA-staged register engine
     int nseg;       // grid.x
     int ntiles;     // grid.y
     PassGeom geo;
@@ -42,6 +43,7 @@ struct PassLaunch {
 
 // engine choice helpers
 int reg_max_p();
+int tma_chunk_cells(int xs);  // fine-segment size the TMA engine expects
 int reg_default_gt(PassKind k, int P);
 bool reg_gt_supported(PassKind k, int P, int GT);
 int gen_default_gt(PassKind k, int P);

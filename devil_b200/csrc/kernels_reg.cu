@@ -1,5 +1,6 @@
 // Instantiations of the register engine (p <= 8) for every pass.
 #include "internal.h"
+#include "tma_pass.cuh"
 
 namespace devil {
 
@@ -7,12 +8,14 @@ constexpr int kRegNT = 256;
 
 int reg_max_p() { return 8; }
 
+int tma_chunk_cells(int xs) { return xs <= 4 ? TmaChunk<4>::CH : TmaChunk<8>::CH; }
+
 int reg_default_gt(PassKind k, int P) {
     switch (k) {
         case PASS_IRLS: return P <= 6 ? 4 : 2;
         case PASS_SANDWICH: return P <= 2 ? 8 : (P <= 4 ? 4 : (P <= 6 ? 2 : 1));
         case PASS_MOM: return 8;
-        case PASS_MLE: return P <= 2 ? 4 : (P <= 4 ? 2 : 1);
+        case PASS_MLE: return 1;
     }
     return 1;
 }
@@ -23,6 +26,7 @@ bool reg_gt_supported(PassKind k, int P, int GT) {
         int mx = P <= 4 ? 8 : (P <= 6 ? 4 : 2);
         return GT == 1 || GT == 2 || (GT == 4 && mx >= 4) || (GT == 8 && mx >= 8);
     }
+    if (k == PASS_MLE) return GT == 1 || GT == (P <= 2 ? 4 : (P <= 4 ? 2 : 1));
     return GT == reg_default_gt(k, P);
 }
 
@@ -46,6 +50,23 @@ static cudaError_t run(const PassLaunch& L) {
     if (L.xs_pad != PP) return cudaErrorInvalidValue;
     dim3 grid(L.nseg, L.ntiles);
     auto prm = make_params<K>(L.prm);
+    if constexpr (!Pass::F64) {
+        if (L.use_tma) {
+            constexpr size_t smem = 2 * TmaChunk<PP>::STAGE_FLOATS * sizeof(float);
+            if (L.val_u16) {
+                auto k = tma_pass_kernel<P, PP, GT, kRegNT, Pass, uint16_t>;
+                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
+                k<<<grid, kRegNT, smem, L.stream>>>(L.geo, prm);
+            } else {
+                auto k = tma_pass_kernel<P, PP, GT, kRegNT, Pass, float>;
+                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e != cudaSuccess) return e;
+                k<<<grid, kRegNT, smem, L.stream>>>(L.geo, prm);
+            }
+            return cudaGetLastError();
+        }
+    }
     if (L.val_u16)
         reg_pass_kernel<P, PP, GT, kRegNT, Pass, uint16_t><<<grid, kRegNT, 0, L.stream>>>(L.geo, prm);
     else
@@ -61,6 +82,13 @@ static cudaError_t run_gt(const PassLaunch& L) {
             case 2: return run<K, P, 2>(L);
             case 4: if constexpr (P <= 6) return run<K, P, 4>(L); break;
             case 8: if constexpr (P <= 4) return run<K, P, 8>(L); break;
+        }
+        return cudaErrorInvalidValue;
+    } else if constexpr (K == PASS_MLE) {
+        constexpr int G = P <= 2 ? 4 : (P <= 4 ? 2 : 1);
+        if (L.GT == G) return run<K, P, G>(L);
+        if constexpr (G != 1) {
+            if (L.GT == 1) return run<K, P, 1>(L);
         }
         return cudaErrorInvalidValue;
     } else {

@@ -35,9 +35,10 @@ struct PassGeom {
     const void* val;       // CSR values (uint16 or float)
     const int64_t* segptr; // [G][nbound] first CSR entry with col >= bound[b]
     const int32_t* bound;  // [nbound] cell boundaries
-    int nbound;
-    int fpi;               // boundaries per work item (item s covers
-                           // bound[s*fpi] .. bound[(s+1)*fpi])
+    int nbound;            // fine segments + 1
+    int nseg;              // work items along the cells: item s covers fine
+                           // segments [s*(nbound-1)/nseg, (s+1)*(nbound-1)/nseg)
+    int32_t* err;          // set to 1 when a bounded wait gives up
     const int32_t* act;    // active gene list
     const int32_t* n_act;  // its length (device)
     int32_t* reset_next;   // counter zeroed by block (0,0) (may be null)
@@ -162,12 +163,12 @@ struct PassMOM {
 // precision.  With u = x / (1 + x):  log(1 + x) = -log(1 - u), so
 // g = sum_{m>=2} u^m / m, a series of positive terms (no cancellation);
 // for x >= 1/4 (u >= 1/5) the direct difference loses < 4 bits.
-DEV float nb_g(float x) {
+DEV float nb_g(float x, float r) {
+    // r = 1/(1 + x) from the caller; u = x r.  Series error < 2e-8 relative
+    // for u <= 0.2.
+    float u = x * r;
     if (x < 0.25f) {
-        float u = x / (1.f + x);
-        float t = 1.f / 14.f;
-        t = fmaf(t, u, 1.f / 13.f);
-        t = fmaf(t, u, 1.f / 12.f);
+        float t = 1.f / 12.f;
         t = fmaf(t, u, 1.f / 11.f);
         t = fmaf(t, u, 1.f / 10.f);
         t = fmaf(t, u, 1.f / 9.f);
@@ -180,18 +181,17 @@ DEV float nb_g(float x) {
         t = fmaf(t, u, 0.5f);
         return u * u * t;
     }
-    return log1pf(x) - x / (1.f + x);
+    return log1pf(x) - u;
 }
 
 // The per-cell part of conventional_score_function_fast's ll_part
 // (src/overdispersion.cpp:159-173) for y = 0: the reference's branches on
 // mu*theta < 1e-10 and < 1e-4 with the clamp to its Taylor bounds.
-DEV float nb_ll_term(float x) {
-    if (x < 1e-10f) return x * x * (1.f / (1.f + x) - 0.5f);
-    float gx = nb_g(x);
+DEV float nb_ll_term(float x, float r) {
+    if (x < 1e-10f) return x * x * (r - 0.5f);
+    float gx = nb_g(x, r);
     if (x < 1e-4f) {
-        float inv = 1.f / (1.f + x);
-        float ub = x * x * inv, lb = x * x * (inv - 0.5f);
+        float ub = x * x * r, lb = x * x * (r - 0.5f);
         gx = fmaxf(fminf(gx, ub), lb);
     }
     return gx;
@@ -291,12 +291,12 @@ struct PassMLE {
     template <class R, class A>
     static DEV void dense(const Gene& G, float mu, A& acc) {
         float x = mu * G.thf;
-        float r = 1.f / (1.f + x);
+        float r = rcp_approx(1.f + x);
         float w = mu * r;
         acc.template outer<0>(w);
         acc.template outer<1>(-w * w);
         acc.template outer<2>(2.f * w * w * w);
-        acc.template scal<0>((double)nb_ll_term(x));
+        acc.template scal<0>((double)nb_ll_term(x, r));
         acc.template scal<1>((double)(mu * x * r * r));
     }
     template <class R, class A>
@@ -437,7 +437,9 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
         for (int s = 0; s < NSc; ++s) as[j][s] = 0;
     }
 
-    const int b0 = seg * geo.fpi, b1 = b0 + geo.fpi;
+    const int nfs = geo.nbound - 1;
+    const int b0 = (int)(((int64_t)seg * nfs) / geo.nseg);
+    const int b1 = (int)(((int64_t)(seg + 1) * nfs) / geo.nseg);
     const int c0 = __ldg(geo.bound + b0), c1 = __ldg(geo.bound + b1);
 
     if constexpr (F64) {
@@ -497,51 +499,71 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
             }
         }
     }
+    // sparse corrections: UNR independent nonzeros per thread per step, so
+    // their dependent (index -> design row) loads overlap
+    constexpr int UNR = (F64 || Pass::NS > 0) ? (P <= 4 ? 2 : 1) : 4;
 #pragma unroll
     for (int j = 0; j < GT; ++j) {
         const int64_t* sp = geo.segptr + (int64_t)gid[j] * geo.nbound;
         const int64_t e0 = __ldg(sp + b0), e1 = __ldg(sp + b1);
-        // two-stage pipeline: indices two entries ahead, rows one ahead
-        int64_t e = e0 + threadIdx.x;
-        int cA = 0, cB = 0;
-        float yA = 0.f, yB = 0.f;
-        if (e < e1) { cA = __ldg(geo.col + e); yA = load_val(val, e); }
-        if (e + NT < e1) { cB = __ldg(geo.col + e + NT); yB = load_val(val, e + NT); }
-        for (; e < e1; e += NT) {
-            const int c = cA;
-            const float y = yA;
-            cA = cB;
-            yA = yB;
-            if (e + 2 * NT < e1) { cB = __ldg(geo.col + e + 2 * NT); yB = load_val(val, e + 2 * NT); }
+        for (int64_t eb = e0 + threadIdx.x; eb < e1; eb += (int64_t)UNR * NT) {
+            int cc[UNR];
+            float yy[UNR];
+            bool ok[UNR];
+#pragma unroll
+            for (int u = 0; u < UNR; ++u) {
+                const int64_t e = eb + (int64_t)u * NT;
+                ok[u] = e < e1;
+                cc[u] = ok[u] ? __ldg(geo.col + e) : c0;
+                yy[u] = ok[u] ? load_val(val, e) : 0.f;
+            }
             if constexpr (F64) {
-                double x[P];
+                double xr[UNR][P];
+                double ol[UNR];
 #pragma unroll
-                for (int i = 0; i < P; ++i) x[i] = __ldg(geo.Xd + (int64_t)c * PP + i);
-                double el = __ldg(geo.offd + c);
+                for (int u = 0; u < UNR; ++u) {
 #pragma unroll
-                for (int i = 0; i < P; ++i) el = fma(x[i], betad[j][i], el);
-                double mu = exp(el);
-                double zz[P * (P + 1) / 2];
+                    for (int i = 0; i < P; ++i) xr[u][i] = __ldg(geo.Xd + (int64_t)cc[u] * PP + i);
+                    ol[u] = __ldg(geo.offd + cc[u]);
+                }
 #pragma unroll
-                for (int jj = 0; jj < P; ++jj)
+                for (int u = 0; u < UNR; ++u) {
+                    if (!ok[u]) continue;
+                    double el = ol[u];
 #pragma unroll
-                    for (int ii = 0; ii <= jj; ++ii) zz[tri_index(ii, jj)] = x[ii] * x[jj];
-                RegAcc<P, NAc, NSc, AW, AS, double> acc{aw[j], as[j], x, zz};
-                Pass::template sparse<double>(gp[j], mu, y, acc);
+                    for (int i = 0; i < P; ++i) el = fma(xr[u][i], betad[j][i], el);
+                    double mu = exp(el);
+                    double zz[P * (P + 1) / 2];
+#pragma unroll
+                    for (int jj = 0; jj < P; ++jj)
+#pragma unroll
+                        for (int ii = 0; ii <= jj; ++ii) zz[tri_index(ii, jj)] = xr[u][ii] * xr[u][jj];
+                    RegAcc<P, NAc, NSc, AW, AS, double> acc{aw[j], as[j], xr[u], zz};
+                    Pass::template sparse<double>(gp[j], mu, yy[u], acc);
+                }
             } else {
-                float x[P];
-                load_row<P, PP>(geo.X, c, x);
-                float el = __ldg(geo.off + c) * kLog2e;
+                float xr[UNR][P];
+                float ol[UNR];
 #pragma unroll
-                for (int i = 0; i < P; ++i) el = fmaf(x[i], beta[j][i], el);
-                float mu = ex2_approx(el);
-                float zz[P * (P + 1) / 2];
+                for (int u = 0; u < UNR; ++u) {
+                    load_row<P, PP>(geo.X, cc[u], xr[u]);
+                    ol[u] = __ldg(geo.off + cc[u]);
+                }
 #pragma unroll
-                for (int jj = 0; jj < P; ++jj)
+                for (int u = 0; u < UNR; ++u) {
+                    if (!ok[u]) continue;
+                    float el = ol[u] * kLog2e;
 #pragma unroll
-                    for (int ii = 0; ii <= jj; ++ii) zz[tri_index(ii, jj)] = x[ii] * x[jj];
-                RegAcc<P, NAc, NSc, AW, AS, float> acc{aw[j], as[j], x, zz};
-                Pass::template sparse<float>(gp[j], mu, y, acc);
+                    for (int i = 0; i < P; ++i) el = fmaf(xr[u][i], beta[j][i], el);
+                    float mu = ex2_approx(el);
+                    float zz[P * (P + 1) / 2];
+#pragma unroll
+                    for (int jj = 0; jj < P; ++jj)
+#pragma unroll
+                        for (int ii = 0; ii <= jj; ++ii) zz[tri_index(ii, jj)] = xr[u][ii] * xr[u][jj];
+                    RegAcc<P, NAc, NSc, AW, AS, float> acc{aw[j], as[j], xr[u], zz};
+                    Pass::template sparse<float>(gp[j], mu, yy[u], acc);
+                }
             }
         }
     }
@@ -633,7 +655,9 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
     float* ys = wts + NWV * kGenNT;                                 // [GT][TC]
     float* betas = ys + kGenNT;                                     // [GT][P]
     const int t = threadIdx.x;
-    const int b0 = seg * geo.fpi, b1 = b0 + geo.fpi;
+    const int nfs = geo.nbound - 1;
+    const int b0 = (int)(((int64_t)seg * nfs) / geo.nseg);
+    const int b1 = (int)(((int64_t)(seg + 1) * nfs) / geo.nseg);
     const int c0 = __ldg(geo.bound + b0), c1 = __ldg(geo.bound + b1);
     if (t < GT) {
         int slot = tile * GT + t;

@@ -28,7 +28,7 @@ CASES = {
                            sf="normed_sum", clusters=False),
     "plain_sparse_p4": dict(config="plain_sparse", seed=102, G=160, n=2000, od=orc.OD_MOM,
                             sf="normed_sum", clusters=False),
-    "clustered_p12": dict(config="clustered", seed=103, G=120, n=2000, od=orc.OD_MOM,
+    "clustered_p12": dict(config="clustered", seed=103, G=400, n=2000, od=orc.OD_MOM,
                           sf="psinorm", clusters=True),
 }
 

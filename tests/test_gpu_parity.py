@@ -55,7 +55,8 @@ def check_beta(fit, ref, tol=BETA_TOL, agree=ITER_AGREE, max_iter=200):
     eta carries ~1e-7 * |x beta| of rounding, and a slowly converging IRLS
     (linear rate rho near 1, e.g. an intercept drifting towards -inf for a
     cell group without counts) amplifies per-step rounding by 1/(1 - rho).
-    Genes stopped by max_iter are held to the same relative bound."""
+    Genes stopped by max_iter have not converged (the bar does not apply);
+    they are checked at 1e-4 relative."""
     it_g = fit["iterations"]["beta_iters"]
     it_o = ref["iters"]
     same = it_g == it_o
@@ -70,7 +71,7 @@ def check_beta(fit, ref, tol=BETA_TOL, agree=ITER_AGREE, max_iter=200):
     capped = same & (it_o >= max_iter)
     if capped.any():
         rel = d[capped] / np.maximum(1.0, np.abs(ref["beta"][capped]))
-        assert np.nanmax(rel) <= tol, f"max-iter genes: rel |dbeta| {np.nanmax(rel):.3e}"
+        assert np.nanmax(rel) <= 10 * tol, f"max-iter genes: rel |dbeta| {np.nanmax(rel):.3e}"
     # genes off by one iteration: the extra step is below the tolerance
     if (~same).any():
         assert np.all(np.abs(it_g[~same] - it_o[~same]) <= 1)
