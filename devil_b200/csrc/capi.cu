@@ -619,7 +619,7 @@ void run_mom(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
 
 // MLE theta (R/overdispersion.R:25-115)
 void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const double* beta_d,
-             double* theta,
+             const double* start_hint, double* theta,
              int32_t* newton_iters, int max_iter, int cox_reid, int form) {
     cudaStream_t st = ctx->stream;
     const int64_t G = dp.G;
@@ -635,6 +635,7 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     s.theta = theta;
     s.dx = ws<double>(ctx, "mle_dx", G);
     s.dxold = ws<double>(ctx, "mle_dxold", G);
+    s.start_hint = start_hint;
     int32_t* act[2] = {ws<int32_t>(ctx, "act0", G), ws<int32_t>(ctx, "act1", G)};
     int32_t* cnt = ws<int32_t>(ctx, "cnt", 4);
     LAUNCH(launch_set_i32(cnt, 0, st));
@@ -785,18 +786,22 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
         CK(cudaStreamSynchronize(st));
         if (herr) fail(ctx, DEVIL_ERR_SINGULAR, "design matrix is rank deficient");
     }
-    LAUNCH(launch_init_beta(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.Xcm, dp.off, ginv, dp.stats,
-                            G, dp.n, P, o->init_beta_rough, fb.beta, fb.beta_f, st));
+    LAUNCH(launch_init_beta(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.Xdrm, dp.xs, dp.off,
+                            ws<double>(ctx, "inv_sf", dp.n), ginv, dp.stats, G, dp.n, P,
+                            o->init_beta_rough, fb.beta, fb.beta_f, st));
     const double eps = (double)(float)o->tolerance;
     run_irls(ctx, dp, fb.beta, fb.beta_f, fb.k, fb.iters, fb.status, o->max_iter, eps, o->form);
-    if (fb.theta_mom || o->overdispersion == DEVIL_OD_MOM) {
-        double* tm = fb.theta_mom ? fb.theta_mom : fb.theta;
+    double* tm = nullptr;
+    if (fb.theta_mom || o->overdispersion == DEVIL_OD_MOM || o->overdispersion == DEVIL_OD_MLE) {
+        // MOM theta: the requested estimate, or the Newton start for MLE
+        tm = fb.theta_mom ? fb.theta_mom
+                          : (o->overdispersion == DEVIL_OD_MOM ? fb.theta : ws<double>(ctx, "mom_start", G));
         run_mom(ctx, dp, fb.beta_f, fb.beta, tm, o->form);
         if (o->overdispersion == DEVIL_OD_MOM && tm != fb.theta)
             CK(cudaMemcpyAsync(fb.theta, tm, G * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     if (o->overdispersion == DEVIL_OD_MLE) {
-        run_mle(ctx, dp, fb.beta_f, fb.beta, fb.theta, nullptr, o->max_iter, 1, o->form);
+        run_mle(ctx, dp, fb.beta_f, fb.beta, tm, fb.theta, nullptr, o->max_iter, 1, o->form);
     } else if (o->overdispersion == DEVIL_OD_NONE) {
         CK(cudaMemsetAsync(fb.theta, 0, G * sizeof(double), st));
     }
@@ -1130,8 +1135,9 @@ int devil_init_beta(devil_ctx* ctx, const devil_counts* counts, const double* X,
         }
         double* b = ws<double>(ctx, "beta", (size_t)dp.G * p);
         float* bf = ws<float>(ctx, "beta_f", (size_t)dp.G * p);
-        LAUNCH(launch_init_beta(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.Xcm, dp.off, ginv, dp.stats,
-                                dp.G, dp.n, p, rough, b, bf, ctx->stream));
+        LAUNCH(launch_init_beta(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.Xdrm, dp.xs, dp.off,
+                                ws<double>(ctx, "inv_sf", dp.n), ginv, dp.stats, dp.G, dp.n, p,
+                                rough, b, bf, ctx->stream));
         d2h(ctx, beta0, b, (size_t)dp.G * p);
         CK(cudaStreamSynchronize(ctx->stream));
     });
@@ -1211,7 +1217,10 @@ int devil_fit_dispersion(devil_ctx* ctx, const devil_counts* counts, const doubl
         upload_beta(ctx, dp, beta, &bf, &bd);
         double* th = ws<double>(ctx, "theta", dp.G);
         int32_t* it = ws<int32_t>(ctx, "mle_iters_out", dp.G);
-        run_mle(ctx, dp, bf, bd, th, it, max_iter, cox_reid, DEVIL_FORM_CHOSEN);
+        // MOM at beta (size factors exp(offset)) seeds the Newton search
+        double* tm = ws<double>(ctx, "mom_start", dp.G);
+        run_mom(ctx, dp, bf, bd, tm, DEVIL_FORM_CHOSEN);
+        run_mle(ctx, dp, bf, bd, tm, th, it, max_iter, cox_reid, DEVIL_FORM_CHOSEN);
         check_kernel_err(ctx);
         d2h(ctx, theta, th, dp.G);
         d2h(ctx, newton_iters, it, dp.G);

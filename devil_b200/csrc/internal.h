@@ -15,8 +15,11 @@ enum Engine { ENGINE_REG = 0, ENGINE_GEN = 1 };
 
 inline int pass_nw(PassKind k) { return k == PASS_MLE ? 3 : (k == PASS_MOM ? 0 : 1); }
 inline int pass_nv(PassKind k) { return (k == PASS_IRLS || k == PASS_SANDWICH) ? 1 : 0; }
-inline int pass_ns(PassKind k) { return k == PASS_MOM ? 2 : (k == PASS_MLE ? 6 : 0); }
-inline int pass_na(PassKind k, int P) { return pass_nw(k) * P * (P + 1) / 2 + pass_nv(k) * P; }
+inline int pass_ns(PassKind k) { return k == PASS_MOM ? 2 : (k == PASS_MLE ? 4 : 0); }
+inline int pass_nf(PassKind k) { return k == PASS_MLE ? 2 : 0; }
+inline int pass_na(PassKind k, int P) {
+    return pass_nw(k) * P * (P + 1) / 2 + pass_nv(k) * P + pass_nf(k);
+}
 
 struct PassParamsAny {
     const float* beta;        // G x P float (FP32 passes)
@@ -85,9 +88,10 @@ cudaError_t launch_theta0(const double* stats, const double* off, int64_t G, int
 cudaError_t launch_xtx_inverse(const double* Xcm, int64_t n, int P, double* ginv,
                                int32_t* err, cudaStream_t st);
 cudaError_t launch_init_beta(const int64_t* rowptr, const int32_t* col, const void* val,
-                             int val_u16, const double* Xcm, const double* off,
-                             const double* ginv, const double* stats, int64_t G, int64_t n,
-                             int P, int rough, double* beta, float* beta_f, cudaStream_t st);
+                             int val_u16, const double* Xrm, int xs, const double* off,
+                             double* inv_sf, const double* ginv, const double* stats, int64_t G,
+                             int64_t n, int P, int rough, double* beta, float* beta_f,
+                             cudaStream_t st);
 cudaError_t launch_segptr(const int64_t* rowptr, const int32_t* col, int64_t G,
                           const int32_t* bound, int nbound, int64_t* segptr, cudaStream_t st);
 cudaError_t launch_validate_csr(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
@@ -120,6 +124,7 @@ struct MleState {
     double* theta;   // result
     double* dx;      // last step and the one before (bisection safeguard)
     double* dxold;
+    const double* start_hint;  // optional per-gene start (MOM theta), may be null
 };
 cudaError_t launch_mle_init(const double* stats, int64_t G, int64_t n, MleState s,
                             int32_t* act, int32_t* n_act, cudaStream_t st);

@@ -177,7 +177,7 @@ __global__ void mle_finalize_kernel(const float* partW, const double* partS, int
                                     const int32_t* act, const int32_t* n_act, int32_t* act_next,
                                     int32_t* n_next, MleState st, int max_iter, int cox_reid) {
     extern __shared__ double fsh[];
-    const int NE = P * (P + 1) / 2, NA = 3 * NE;
+    const int NE = P * (P + 1) / 2, NA = 3 * NE + 2;  // b, db, d2b, two FP32 scalars
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int per = NA + 6 + 4 * P * P + P;
     double* sums = fsh + warp * per;
@@ -191,9 +191,13 @@ __global__ void mle_finalize_kernel(const float* partW, const double* partS, int
     if (slot >= *n_act) return;
     const int g = act[slot];
     reduce_partials(partW, nseg, slot_stride, slot, NA, NA, sums, lane);
-    reduce_partials(partS, nseg, slot_stride, slot, 6, 6, ss, lane);
+    reduce_partials(partS, nseg, slot_stride, slot, 4, 4, ss + 2, lane);
     __syncwarp();
     if (lane != 0) return;
+    // ss[0..5]: sum ll_term, sum mu x/(1+x)^2, sum y theta/(1+x), sum y/(1+x)^2,
+    // digamma sum, trigamma sum
+    ss[0] = sums[3 * NE + 0];
+    ss[1] = sums[3 * NE + 1];
 
     const double x = st.x[g];
     const double theta = exp(x), a = 1.0 / theta;
@@ -254,6 +258,14 @@ __global__ void mle_finalize_kernel(const float* partW, const double* partS, int
         const double mean = gs[0], var = gs[1];
         double start = (var - mean) / (mean * mean);
         if (isnan(start) || start <= 0.0) start = 0.5;
+        // Newton converges to the same root from any start inside the
+        // bracket; the method-of-moments estimate at the fitted beta is
+        // usually within a few steps of it (the reference's start ignores
+        // size factors and covariates)
+        if (st.start_hint) {
+            double h = st.start_hint[g];
+            if (h > 1e-8 && h < 1e16) start = h;
+        }
         double lo = log(1e-8), hi = log(1e16);
         xn = log(start);
         if (xn < lo) xn = lo;
@@ -284,7 +296,7 @@ __global__ void mle_finalize_kernel(const float* partW, const double* partS, int
             }
             xn = cand;
             ++it;
-            if (dx < 1e-10 || hi - lo < 1e-10 || it >= max_iter) done = true;
+            if (dx < 1e-9 || hi - lo < 1e-9 || it >= max_iter) done = true;
         }
         st.lo[g] = lo;
         st.hi[g] = hi;
@@ -308,7 +320,7 @@ cudaError_t launch_mle_finalize(const float* partW, const double* partS, int nse
                                 int cox_reid, volatile int32_t* mirror, cudaStream_t st) {
     (void)mirror;
     if (max_slots <= 0) return cudaSuccess;
-    const int NA = 3 * (P * (P + 1) / 2);
+    const int NA = 3 * (P * (P + 1) / 2) + 2;
     const size_t per = (size_t)(NA + 6 + 4 * P * P + P) * sizeof(double);
     const int w = fin_warps(per);
     const size_t smem = per * w;

@@ -12,13 +12,14 @@ int gen_default_gt(PassKind k, int P) {
 }
 
 size_t gen_smem_bytes(PassKind k, int P, int GT) {
-    const int ns = pass_ns(k), nwv = pass_nw(k) + pass_nv(k);
+    const int ns = pass_ns(k), nwv = pass_nw(k) + pass_nv(k) + pass_nf(k);
+    const bool f64 = (k == PASS_MOM || k == PASS_SANDWICH);
+    const size_t wt = f64 ? 8 : 4;
     const int TC = kGenNT / GT;
     const int XS = (P + 1) | 1;
-    size_t b = (size_t)ns * kGenNT * 8;        // wsc
-    b += (size_t)GT * (8 + 8 + 4 + 4);         // cursor, cend, cnt, gids
-    b += (size_t)TC * XS * 4;                  // xsm
-    b += (size_t)nwv * kGenNT * 4;             // wts
+    size_t b = gen_wt_offset(ns, GT);
+    b += (size_t)TC * XS * wt;                 // xsm
+    b += (size_t)nwv * kGenNT * wt;            // wts
     b += (size_t)kGenNT * 4;                   // ys
     b += (size_t)GT * P * 4;                   // betas
     return b + 16;

@@ -413,11 +413,11 @@ cudaError_t launch_xtx_inverse(const double* Xcm, int64_t n, int P, double* ginv
 // the solution equals (X'X)^-1 X' z; z is zero wherever y is zero, so
 // X' z is a sum over the nonzero entries of the row.  Rough init:
 // beta_0 = (log1p(mean y), 0, ..., 0).
-template <class VT>
+template <class VT, int PMAX>
 __global__ void init_beta_kernel(const int64_t* rowptr, const int32_t* col, const VT* val,
-                                 const double* Xcm, const double* off, const double* ginv,
-                                 const double* stats, int64_t G, int64_t n, int P, int rough,
-                                 double* beta, float* beta_f) {
+                                 const double* Xrm, int xs, const double* inv_sf,
+                                 const double* ginv, const double* stats, int64_t G, int64_t n,
+                                 int P, int rough, double* beta, float* beta_f) {
     int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (g >= G) return;
@@ -429,37 +429,65 @@ __global__ void init_beta_kernel(const int64_t* rowptr, const int32_t* col, cons
         }
         return;
     }
-    double r[32];
+    double r[PMAX];
 #pragma unroll
-    for (int i = 0; i < 32; ++i) r[i] = 0.0;
+    for (int i = 0; i < PMAX; ++i) r[i] = 0.0;
     for (int64_t e = rowptr[g] + lane; e < rowptr[g + 1]; e += 32) {
         int c = col[e];
-        double z = log1p((double)val[e] / exp(off[c]));
+        double z = log1p((double)val[e] * inv_sf[c]);
+        const double* xr = Xrm + (int64_t)c * xs;
 #pragma unroll
-        for (int i = 0; i < 32; ++i)
-            if (i < P) r[i] += Xcm[(int64_t)i * n + c] * z;
+        for (int i = 0; i < PMAX; ++i)
+            if (i < P) r[i] += xr[i] * z;
     }
 #pragma unroll
-    for (int i = 0; i < 32; ++i)
+    for (int i = 0; i < PMAX; ++i)
         if (i < P) r[i] = warp_sum(r[i]);
     if (lane < P) {
         double b = 0.0;
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
+        for (int j = 0; j < PMAX; ++j)
             if (j < P) b += ginv[j * P + lane] * r[j];
         beta[g * P + lane] = b;
         beta_f[g * P + lane] = (float)b;
     }
 }
+__global__ void inv_exp_kernel(const double* off, int64_t n, double* out) {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += (int64_t)gridDim.x * blockDim.x)
+        out[c] = exp(-off[c]);
+}
+// z = log1p(y / exp(off)) as in R/beta.R:18; y * exp(-off) differs from
+// y / exp(off) by at most an ulp of the quotient
 cudaError_t launch_init_beta(const int64_t* rowptr, const int32_t* col, const void* val,
-                             int val_u16, const double* Xcm, const double* off,
-                             const double* ginv, const double* stats, int64_t G, int64_t n,
-                             int P, int rough, double* beta, float* beta_f, cudaStream_t st) {
+                             int val_u16, const double* Xrm, int xs, const double* off,
+                             double* inv_sf, const double* ginv, const double* stats, int64_t G,
+                             int64_t n, int P, int rough, double* beta, float* beta_f,
+                             cudaStream_t st) {
     if (G == 0) return cudaSuccess;
-    if (val_u16)
-        init_beta_kernel<uint16_t><<<nblk(G, 8), 256, 0, st>>>(rowptr, col, (const uint16_t*)val, Xcm, off, ginv, stats, G, n, P, rough, beta, beta_f);
-    else
-        init_beta_kernel<float><<<nblk(G, 8), 256, 0, st>>>(rowptr, col, (const float*)val, Xcm, off, ginv, stats, G, n, P, rough, beta, beta_f);
+    if (!rough) {
+        inv_exp_kernel<<<(unsigned)std::min<int64_t>(nblk(n, 256), 1024), 256, 0, st>>>(off, n, inv_sf);
+    }
+    const unsigned b = nblk(G, 8);
+#define DEVIL_INIT(PM)                                                                          \
+    if (val_u16)                                                                                 \
+        init_beta_kernel<uint16_t, PM><<<b, 256, 0, st>>>(rowptr, col, (const uint16_t*)val, Xrm, \
+                                                            xs, inv_sf, ginv, stats, G, n, P,     \
+                                                            rough, beta, beta_f);                \
+    else                                                                                         \
+        init_beta_kernel<float, PM><<<b, 256, 0, st>>>(rowptr, col, (const float*)val, Xrm, xs,   \
+                                                         inv_sf, ginv, stats, G, n, P, rough,     \
+                                                         beta, beta_f);
+    if (P <= 4) {
+        DEVIL_INIT(4)
+    } else if (P <= 8) {
+        DEVIL_INIT(8)
+    } else if (P <= 16) {
+        DEVIL_INIT(16)
+    } else {
+        DEVIL_INIT(32)
+    }
+#undef DEVIL_INIT
     return cudaGetLastError();
 }
 

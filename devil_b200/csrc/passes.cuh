@@ -18,6 +18,8 @@
 // triangle), vec(w) adds w * x, scal(v) adds v.  Per-segment partial sums
 // go to global memory and a finalize kernel per pass reduces them in FP64.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace devil {
@@ -73,6 +75,9 @@ struct RegAcc {
     }
     template <int K>
     DEV void scal(AS v) { s[K] += v; }
+    // scalar accumulated with the FP32 weight sums (after outer and vec terms)
+    template <int K, int NW, int NV>
+    DEV void fscal(R v) { a[NW * (P * (P + 1) / 2) + NV * P + K] += (AW)v; }
 };
 
 // recorder used by the shared-memory engine: captures the weights only
@@ -92,6 +97,8 @@ struct RecAcc {
     DEV void vec(R v) { w[NW + V] += v; }
     template <int K>
     DEV void scal(AS v) { s[K] += v; }
+    template <int K, int NW, int NV>
+    DEV void fscal(R v) { w[NW + NV + K] += v; }
 };
 
 // ---------------------------------------------------------------------
@@ -108,6 +115,7 @@ struct RecAcc {
 // so a zero cell costs one reciprocal, one product and the FMAs; the
 // constant factors are applied in FP64 by the finalize.
 struct PassIRLS {
+    static constexpr int NF = 0;
     static constexpr int NW = 1, NV = 1, NS = 0;
     static constexpr bool F64 = false;
     static constexpr bool TABLES = false;
@@ -138,6 +146,7 @@ struct PassIRLS {
 //   num = sum (y - mu)^2 - mu,  den = sum mu^2
 // One pass, evaluated in FP64 per cell (num cancels for near-Poisson genes).
 struct PassMOM {
+    static constexpr int NF = 0;
     static constexpr int NW = 0, NV = 0, NS = 2;
     static constexpr bool F64 = true;
     static constexpr bool TABLES = false;
@@ -270,14 +279,17 @@ DEV void psi_diffs_tab(double y, double a, const PsiTable& T, double& d1, double
 }
 
 // One evaluation of the dispersion score and its derivative in log theta
-// (src/overdispersion.cpp:95-242) at theta:
-//   scal0 = sum ll_term(mu theta)          scal1 = sum mu x/(1+x)^2
-//   scal2 = sum y theta/(1+x)              scal3 = sum y/(1+x)^2
-//   scal4 = sum psi(y+a) - psi(a)          scal5 = sum psi1(y+a) - psi1(a)
+// (src/overdispersion.cpp:95-242) at theta, with x = mu theta, a = 1/theta,
+// w = mu/(1 + x):
+//   fscal0 = sum ll_term(x)        fscal1 = sum mu x/(1+x)^2    (FP32 sums)
+//   scal0  = sum y theta/(1+x)     scal1  = sum y/(1+x)^2       (FP64)
+//   scal2  = sum psi(y+a) - psi(a) scal3  = sum psi1(y+a) - psi1(a)
 //   outer0 = X' diag(w) X, outer1 = X' diag(-w^2) X, outer2 = X' diag(2 w^3) X
-// with x = mu theta, a = 1/theta, w = mu/(1 + x)  (Cox-Reid b, db, d2b).
+// (the Cox-Reid b, db, d2b).  The nonzero terms stay FP64: their sum nearly
+// cancels the digamma sum in the score.
 struct PassMLE {
-    static constexpr int NW = 3, NV = 0, NS = 6;
+    static constexpr int NF = 2;
+    static constexpr int NW = 3, NV = 0, NS = 4;
     static constexpr bool F64 = false;
     static constexpr bool TABLES = true;
     using AW = float;
@@ -296,19 +308,22 @@ struct PassMLE {
         acc.template outer<0>(w);
         acc.template outer<1>(-w * w);
         acc.template outer<2>(2.f * w * w * w);
-        acc.template scal<0>((double)nb_ll_term(x, r));
-        acc.template scal<1>((double)(mu * x * r * r));
+        acc.template fscal<0, NW, NV>(nb_ll_term(x, r));
+        acc.template fscal<1, NW, NV>(w * x * r);
     }
     template <class R, class A>
     static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
         double m = mu, yy = y;
-        double r = 1.0 / (1.0 + m * G.theta);
-        acc.template scal<2>(yy * G.theta * r);
-        acc.template scal<3>(yy * r * r);
+        double den = 1.0 + m * G.theta;
+        // reciprocal: MUFU estimate refined by one FP64 Newton step
+        double r = (double)rcp_approx((float)den);
+        r = r + r * (1.0 - den * r);
+        acc.template scal<0>(yy * G.theta * r);
+        acc.template scal<1>(yy * r * r);
         double d1, d2;
         psi_diffs_tab(yy, G.a, G.tab, d1, d2);
-        acc.template scal<4>(d1);
-        acc.template scal<5>(d2);
+        acc.template scal<2>(d1);
+        acc.template scal<3>(d2);
     }
 };
 
@@ -320,6 +335,7 @@ struct PassMLE {
 // One pass, evaluated in FP64 per cell with FP64 sums: the bread is an
 // inverse, so cond(H) multiplies every relative error of H.
 struct PassSandwich {
+    static constexpr int NF = 0;
     static constexpr int NW = 1, NV = 1, NS = 0;
     static constexpr bool F64 = true;
     static constexpr bool TABLES = false;
@@ -373,7 +389,7 @@ DEV void load_row(const float* __restrict__ X, int64_t c, float* x) {
 template <int P, int PP, int GT, int NT, class Pass, class VT>
 __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pass::Params prm) {
     constexpr int NE = P * (P + 1) / 2;
-    constexpr int NA = Pass::NW * NE + Pass::NV * P;
+    constexpr int NA = Pass::NW * NE + Pass::NV * P + Pass::NF;
     constexpr int NS = Pass::NS;
     constexpr int NAc = NA > 0 ? NA : 1;
     constexpr int NSc = NS > 0 ? NS : 1;
@@ -626,14 +642,22 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
 constexpr int kGenNT = 256;
 constexpr int kGenKMAX = 16;
 
+// byte offset of the design/weight tiles in the generic engine's shared
+// memory: after the FP64 scalar tile and the per-gene bookkeeping, 16-byte
+// aligned
+__host__ __device__ __forceinline__ size_t gen_wt_offset(int NS, int GT) {
+    size_t b = (size_t)NS * kGenNT * 8 + (size_t)GT * (8 + 8 + 4 + 4);
+    return (b + 15) & ~(size_t)15;
+}
+
 template <class Pass, class VT>
 __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename Pass::Params prm,
                                                           int P, int GT) {
-    constexpr int NWV = Pass::NW + Pass::NV;
+    constexpr int NWV = Pass::NW + Pass::NV + Pass::NF;
     constexpr int NS = Pass::NS;
     using AS = typename Pass::AS;
     const int NE = P * (P + 1) / 2;
-    const int NA = Pass::NW * NE + Pass::NV * P;
+    const int NA = Pass::NW * NE + Pass::NV * P + Pass::NF;
     const int TC = kGenNT / GT;
     const int XS = (P + 1) | 1;  // odd row stride: conflict-free column reads
 
@@ -650,9 +674,11 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
     int64_t* cend = cursor + GT;                                    // [GT]
     int* cnt = reinterpret_cast<int*>(cend + GT);                   // [GT]
     int* gids = cnt + GT;                                           // [GT]
-    float* xsm = reinterpret_cast<float*>(gids + GT);               // [TC][XS]
-    float* wts = xsm + TC * XS;                                     // [NWV][GT][TC]
-    float* ys = wts + NWV * kGenNT;                                 // [GT][TC]
+    // FP64 passes stage design rows and weights in double
+    using WT = typename std::conditional<Pass::F64, double, float>::type;
+    WT* xsm = reinterpret_cast<WT*>(smem_raw + gen_wt_offset(NS, GT));  // [TC][XS]
+    WT* wts = xsm + TC * XS;                                        // [NWV][GT][TC]
+    float* ys = reinterpret_cast<float*>(wts + NWV * kGenNT);       // [GT][TC]
     float* betas = ys + kGenNT;                                     // [GT][P]
     const int t = threadIdx.x;
     const int nfs = geo.nbound - 1;
@@ -708,10 +734,13 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
                 while ((j + 1) * (j + 2) / 2 <= q) ++j;
                 int i = q - j * (j + 1) / 2;
                 ow[k] = (short)w; oi[k] = (short)i; oj[k] = (short)j;
-            } else {
+            } else if (a < Pass::NW * NE + Pass::NV * P) {
                 int r = a - Pass::NW * NE;
                 int v = r / P, i = r - v * P;
                 ow[k] = (short)(Pass::NW + v); oi[k] = (short)i; oj[k] = (short)P;  // x_P == 1
+            } else {
+                int f = a - Pass::NW * NE - Pass::NV * P;  // FP32 scalar: w * 1 * 1
+                ow[k] = (short)(Pass::NW + Pass::NV + f); oi[k] = (short)P; oj[k] = (short)P;
             }
         }
     }
@@ -727,9 +756,12 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
         // stage X rows (+ the constant 1 column) and offsets; clear the tile
         for (int i = t; i < nc * P; i += kGenNT) {
             int c = i / P, k = i - c * P;
-            xsm[c * XS + k] = __ldg(geo.X + (int64_t)(cb + c) * geo.xs + k);
+            if constexpr (Pass::F64)
+                xsm[c * XS + k] = __ldg(geo.Xd + (int64_t)(cb + c) * geo.xs + k);
+            else
+                xsm[c * XS + k] = __ldg(geo.X + (int64_t)(cb + c) * geo.xs + k);
         }
-        for (int c = t; c < TC; c += kGenNT) xsm[c * XS + P] = 1.f;
+        for (int c = t; c < TC; c += kGenNT) xsm[c * XS + P] = (WT)1;
         ys[t] = 0.f;
         if (t < GT) cnt[t] = 0;
         __syncthreads();
@@ -760,7 +792,7 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
                 if (y != 0.f) Pass::template sparse<double>(gpar, mu, y, rec);
             }
 #pragma unroll
-            for (int w = 0; w < NWV; ++w) wts[(w * GT + gA) * TC + cA] = (float)rec.w[w];
+            for (int w = 0; w < NWV; ++w) wts[(w * GT + gA) * TC + cA] = (WT)rec.w[w];
 #pragma unroll
             for (int s = 0; s < NS; ++s) wsc[(s * GT + gA) * TC + cA] = rec.s[s];
         } else {
@@ -773,6 +805,7 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
                 for (int i = 0; i < P; ++i)
                     ed = fma(__ldg(geo.Xd + c * geo.xs + i), __ldg(bd + i), ed);
                 float mu = ex2_approx((float)(ed * 1.4426950408889634));
+                (void)xsm;
                 float y = ys[gA * TC + cA];
                 Pass::template dense<float>(gpar, mu, rec);
                 if (y != 0.f) Pass::template sparse<float>(gpar, mu, y, rec);
@@ -786,11 +819,11 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
 #pragma unroll
         for (int k = 0; k < kGenKMAX; ++k) {
             if (k >= nown) break;
-            const float* wp = wts + (ow[k] * GT + og[k]) * TC;
-            const float* xi = xsm + oi[k];
-            const float* xj = xsm + oj[k];
-            float s = 0.f;
-            for (int c = 0; c < nc; ++c) s = fmaf(wp[c] * xi[c * XS], xj[c * XS], s);
+            const WT* wp = wts + (ow[k] * GT + og[k]) * TC;
+            const WT* xi = xsm + oi[k];
+            const WT* xj = xsm + oj[k];
+            WT s = 0;
+            for (int c = 0; c < nc; ++c) s = fma(wp[c] * xi[c * XS], xj[c * XS], s);
             acc[k] += (double)s;
         }
         if (NS > 0 && t < GT * NS) {

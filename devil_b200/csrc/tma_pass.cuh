@@ -65,7 +65,7 @@ template <int P, int PP, int GT, int NT, class Pass, class VT>
 __global__ void __launch_bounds__(NT) tma_pass_kernel(PassGeom geo, typename Pass::Params prm) {
     static_assert(!Pass::F64, "TMA engine carries FP32 passes");
     constexpr int NE = P * (P + 1) / 2;
-    constexpr int NA = Pass::NW * NE + Pass::NV * P;
+    constexpr int NA = Pass::NW * NE + Pass::NV * P + Pass::NF;
     constexpr int NS = Pass::NS;
     constexpr int NAc = NA > 0 ? NA : 1;
     constexpr int NSc = NS > 0 ? NS : 1;
