@@ -287,7 +287,7 @@ def main():
     ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
     res = L.FitResult(ptr(out["beta"]), ptr(out["theta"]), ptr(out["iters"]), None,
                       ptr(out["bread"]), ptr(out["sw"]), ptr(out["theta_mom"]),
-                      ptr(out["status"]), ptr(out["sf"]), ptr(out["off"]))
+                      ptr(out["status"]), ptr(out["sf"]), ptr(out["off"]), None)
     contrast = np.zeros(p)
     contrast[1] = 1.0
     ends_np = None if ends is None else np.ascontiguousarray(ends, np.int32)
@@ -363,7 +363,7 @@ def main():
             ("padj", G, torch.float64), ("lfc", G, torch.float64)]}
         hres = L.FitResult(ptr(hb["beta"]), ptr(hb["theta"]), ptr(hb["iters"]), None,
                            ptr(hb["bread"]), None, ptr(hb["theta_mom"]), ptr(hb["status"]),
-                           ptr(hb["sf"]), ptr(hb["off"]))
+                           ptr(hb["sf"]), ptr(hb["off"]), None)
 
         def step_host():
             ctx.check(lib.devil_fit(ctx.h, C.byref(hc), ptr(h_X), p, None, 0, C.byref(opts),

@@ -62,7 +62,7 @@ class FitResult(C.Structure):
     _fields_ = [("beta", C.c_void_p), ("theta", C.c_void_p), ("beta_iters", C.c_void_p),
                 ("theta_iters", C.c_void_p), ("bread", C.c_void_p), ("sandwich", C.c_void_p),
                 ("theta_mom", C.c_void_p), ("status", C.c_void_p), ("size_factors", C.c_void_p),
-                ("offset_vector", C.c_void_p)]
+                ("offset_vector", C.c_void_p), ("meat", C.c_void_p)]
 
 
 _lib = None

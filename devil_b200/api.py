@@ -254,8 +254,9 @@ def fit_devil(x, design_matrix, clusters=None, overdispersion="MOM", init_overdi
     status = np.empty(G, np.int32)
     sfo = np.empty(n)
     offo = np.empty(n)
+    meat = np.empty((G, p, p)) if ends is not None else None
     res = L.FitResult(_ptr(beta), _ptr(theta), _ptr(iters), _ptr(titers), _ptr(bread), _ptr(sw),
-                      _ptr(tm), _ptr(status), _ptr(sfo), _ptr(offo))
+                      _ptr(tm), _ptr(status), _ptr(sfo), _ptr(offo), _ptr(meat))
     ctx = L.context(device)
     rc = L.load().devil_fit(ctx.h, counts.ref, _ptr(Xf), p, _ptr(ends),
                             0 if ends is None else len(ends), C.byref(opts), C.byref(res))
@@ -266,6 +267,7 @@ def fit_devil(x, design_matrix, clusters=None, overdispersion="MOM", init_overdi
     bread = np.ascontiguousarray(np.transpose(bread, (0, 2, 1)))
     if sw is not None:
         sw = np.ascontiguousarray(np.transpose(sw, (0, 2, 1)))
+        meat = np.ascontiguousarray(np.transpose(meat, (0, 2, 1)))
     th_it = titers.astype(np.float64)
     th_it[titers == L.NA_INT] = np.nan
     return dict(
@@ -281,6 +283,7 @@ def fit_devil(x, design_matrix, clusters=None, overdispersion="MOM", init_overdi
         input_parameters=dict(max_iter=max_iter, tolerance=tolerance),
         status=status,
         theta_mom=tm,
+        meat=meat,
     )
 
 

@@ -767,6 +767,7 @@ struct FitBuffers {
     int32_t* titers;
     double* bread;
     double* sandwich;
+    double* meat;
 };
 
 // cpu_fit order: theta_0 -> beta | theta_0 -> theta | beta -> bread, meat
@@ -806,7 +807,8 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
         CK(cudaMemsetAsync(fb.theta, 0, G * sizeof(double), st));
     }
     run_sandwich(ctx, dp, fb.beta_f, fb.beta, fb.theta, ends_host, n_clusters, fb.bread,
-                 n_clusters > 0 ? fb.sandwich : nullptr, nullptr, o->form);
+                 n_clusters > 0 ? fb.sandwich : nullptr, n_clusters > 0 ? fb.meat : nullptr,
+                 o->form);
     check_kernel_err(ctx);
 }
 
@@ -823,6 +825,7 @@ void alloc_fit_buffers(devil_ctx* ctx, int64_t G, int P, bool theta_mom, bool cl
     fb.titers = ws<int32_t>(ctx, "titers", G);
     fb.bread = ws<double>(ctx, "bread", (size_t)G * P * P);
     fb.sandwich = clusters ? ws<double>(ctx, "sandwich", (size_t)G * P * P) : nullptr;
+    fb.meat = clusters ? ws<double>(ctx, "meat_out", (size_t)G * P * P) : nullptr;
 }
 
 void validate_opts(devil_ctx* ctx, const devil_fit_opts* o) {
@@ -962,7 +965,10 @@ int devil_fit(devil_ctx* ctx, const devil_counts* counts, const double* X, int p
         d2h(ctx, res->beta_iters, fb.iters, G);
         d2h(ctx, res->status, fb.status, G);
         d2h(ctx, res->bread, fb.bread, (size_t)G * p * p);
-        if (n_clusters > 0) d2h(ctx, res->sandwich, fb.sandwich, (size_t)G * p * p);
+        if (n_clusters > 0) {
+            d2h(ctx, res->sandwich, fb.sandwich, (size_t)G * p * p);
+            d2h(ctx, res->meat, fb.meat, (size_t)G * p * p);
+        }
         if (fb.theta_mom) d2h(ctx, res->theta_mom, fb.theta_mom, G);
         d2h(ctx, res->size_factors, dp.sf, dp.n);
         d2h(ctx, res->offset_vector, dp.off, dp.n);
@@ -994,6 +1000,7 @@ int devil_fit_device(devil_ctx* ctx, const devil_counts* counts_dev, const doubl
         if (r->status) fb.status = r->status;
         if (r->bread) fb.bread = r->bread;
         if (r->sandwich && n_clusters > 0) fb.sandwich = r->sandwich;
+        if (r->meat && n_clusters > 0) fb.meat = r->meat;
         if (r->theta_mom && opts->compute_theta_mom) fb.theta_mom = r->theta_mom;
         fit_pipeline(ctx, dp, cluster_ends_host, n_clusters, opts, fb);
         if (r->size_factors)

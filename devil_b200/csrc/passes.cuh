@@ -101,6 +101,10 @@ struct RecAcc {
     DEV void fscal(R v) { w[NW + NV + K] += v; }
 };
 
+// reciprocal in the arithmetic of the pass: MUFU estimate in FP32, IEEE in FP64
+DEV float rcp_r(float x) { return rcp_approx(x); }
+DEV double rcp_r(double x) { return 1.0 / x; }
+
 // ---------------------------------------------------------------------
 // pass traits
 // ---------------------------------------------------------------------
@@ -128,16 +132,16 @@ struct PassIRLS {
         return Gene{k, 1.f / k};
     }
     template <class R, class A>
-    static DEV void dense(const Gene& G, float mu, A& acc) {
-        float r = rcp_approx(mu + G.k);
+    static DEV void dense(const Gene& G, R mu, A& acc) {
+        R r = rcp_r(mu + (R)G.k);
         acc.template outer<0>(r);
         acc.template vec<0, NW>(mu * r);
     }
     template <class R, class A>
-    static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
-        float r = rcp_approx(mu + G.k);
-        float yr = y * r;
-        acc.template outer<0>(yr * G.rk);
+    static DEV void sparse(const Gene& G, R mu, float y, A& acc) {
+        R r = rcp_r(mu + (R)G.k);
+        R yr = (R)y * r;
+        acc.template outer<0>(yr * (R)G.rk);  // rk scales H only, not the score
         acc.template vec<0, NW>(-yr);
     }
 };
@@ -193,15 +197,27 @@ DEV float nb_g(float x, float r) {
     return log1pf(x) - u;
 }
 
+DEV double nb_g(double x, double r) {
+    double u = x * r;
+    if (x < 0.25) {
+        double t = 0.0;
+        for (int m = 24; m >= 3; --m) t = fma(t, u, 1.0 / m);
+        t = fma(t, u, 0.5);
+        return u * u * t;
+    }
+    return log1p(x) - u;
+}
+
 // The per-cell part of conventional_score_function_fast's ll_part
 // (src/overdispersion.cpp:159-173) for y = 0: the reference's branches on
 // mu*theta < 1e-10 and < 1e-4 with the clamp to its Taylor bounds.
-DEV float nb_ll_term(float x, float r) {
-    if (x < 1e-10f) return x * x * (r - 0.5f);
-    float gx = nb_g(x, r);
-    if (x < 1e-4f) {
-        float ub = x * x * r, lb = x * x * (r - 0.5f);
-        gx = fmaxf(fminf(gx, ub), lb);
+template <class R>
+DEV R nb_ll_term(R x, R r) {
+    if (x < (R)1e-10) return x * x * (r - (R)0.5);
+    R gx = nb_g(x, r);
+    if (x < (R)1e-4) {
+        R ub = x * x * r, lb = x * x * (r - (R)0.5);
+        gx = fmax(fmin(gx, ub), lb);
     }
     return gx;
 }
@@ -301,18 +317,18 @@ struct PassMLE {
         return Gene{th, 1.0 / th, (float)th, PsiTable{nullptr, nullptr, 0.0, 0.0}};
     }
     template <class R, class A>
-    static DEV void dense(const Gene& G, float mu, A& acc) {
-        float x = mu * G.thf;
-        float r = rcp_approx(1.f + x);
-        float w = mu * r;
+    static DEV void dense(const Gene& G, R mu, A& acc) {
+        R x = mu * (sizeof(R) == 4 ? (R)G.thf : (R)G.theta);
+        R r = rcp_r((R)1 + x);
+        R w = mu * r;
         acc.template outer<0>(w);
         acc.template outer<1>(-w * w);
-        acc.template outer<2>(2.f * w * w * w);
-        acc.template fscal<0, NW, NV>(nb_ll_term(x, r));
+        acc.template outer<2>((R)2 * w * w * w);
+        acc.template fscal<0, NW, NV>(nb_ll_term<R>(x, r));
         acc.template fscal<1, NW, NV>(w * x * r);
     }
     template <class R, class A>
-    static DEV void sparse(const Gene& G, float mu, float y, A& acc) {
+    static DEV void sparse(const Gene& G, R mu, float y, A& acc) {
         double m = mu, yy = y;
         double den = 1.0 + m * G.theta;
         // reciprocal: MUFU estimate refined by one FP64 Newton step
@@ -748,7 +764,6 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
     AS sacc = 0;
     __syncthreads();
 
-    constexpr bool F64 = Pass::F64;
     const double* bd = prm.beta_d + (int64_t)gids[gA] * P;
 
     for (int cb = c0; cb < c1; cb += TC) {
@@ -779,7 +794,10 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
         __syncthreads();
         if (cA == 0) cursor[gA] += cnt[gA];
         // per-(gene, cell) weights
-        if constexpr (F64) {
+        {
+            // per-(gene, cell) weights in FP64 for every pass: this engine's
+            // cost is the outer-product phase, and FP64 here keeps the
+            // per-step error of slowly converging genes small
             RecAcc<NWV, NS, AS, double> rec;
             rec.zero();
             if (cA < nc) {
@@ -793,25 +811,6 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
             }
 #pragma unroll
             for (int w = 0; w < NWV; ++w) wts[(w * GT + gA) * TC + cA] = (WT)rec.w[w];
-#pragma unroll
-            for (int s = 0; s < NS; ++s) wsc[(s * GT + gA) * TC + cA] = rec.s[s];
-        } else {
-            RecAcc<NWV, NS, AS, float> rec;
-            rec.zero();
-            if (cA < nc) {
-                // eta in FP64 (a sum of terms that may be large and cancel)
-                const int64_t c = cb + cA;
-                double ed = __ldg(geo.offd + c);
-                for (int i = 0; i < P; ++i)
-                    ed = fma(__ldg(geo.Xd + c * geo.xs + i), __ldg(bd + i), ed);
-                float mu = ex2_approx((float)(ed * 1.4426950408889634));
-                (void)xsm;
-                float y = ys[gA * TC + cA];
-                Pass::template dense<float>(gpar, mu, rec);
-                if (y != 0.f) Pass::template sparse<float>(gpar, mu, y, rec);
-            }
-#pragma unroll
-            for (int w = 0; w < NWV; ++w) wts[(w * GT + gA) * TC + cA] = rec.w[w];
 #pragma unroll
             for (int s = 0; s < NS; ++s) wsc[(s * GT + gA) * TC + cA] = rec.s[s];
         }

@@ -113,6 +113,7 @@ typedef struct devil_fit_result {
     int32_t *status;        /* G  DEVIL_GENE_*             (optional)       */
     double  *size_factors;  /* n                           (optional)       */
     double  *offset_vector; /* n                           (optional)       */
+    double  *meat;          /* G x p x p, clusters only    (optional)       */
 } devil_fit_result;
 
 typedef struct devil_ctx devil_ctx;
