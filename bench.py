@@ -394,6 +394,11 @@ def main():
                "d2h_bytes_per_step": d2h, "ms_per_step": ems}
 
     # ---- roofline of the dominant kernel (IRLS cell pass) ----
+    engines = {name: ctx.engine(k) for k, name in enumerate(["irls", "mom", "mle", "bread_meat"])}
+    kernel = {"register": f"reg_pass_kernel<P={p},PassIRLS,uint16> (register tiles)",
+              "shared": f"gen_pass_kernel<PassIRLS,uint16> (shared-memory tiles, p={p})",
+              "groups": f"grp_pass_kernel<PassIRLS,uint16> (design groups, p={p})"}.get(
+                  engines["irls"], engines["irls"])
     n_l, t_ms, bytes_ = prof[0]
     peak, peak_kind = read_peaks()
     roof = None
@@ -401,12 +406,13 @@ def main():
         per_launch_s = t_ms / 1e3 / n_l
         alg_per_launch = bytes_ / n_l
         achieved = alg_per_launch / per_launch_s / 1e9
-        ratio = read_traffic_ratio()
+        # the committed DRAM/algorithmic ratio was measured on the register engine
+        ratio = read_traffic_ratio() if engines["irls"] == "register" else None
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4),
                 "traffic": None if ratio is None else round(ratio * alg_per_launch, 1),
                 "peak_source": f"{peak_kind} hbm_gbs",
-                "kernel": "reg_pass_kernel<P=4,GT=8,PassIRLS,uint16>",
+                "kernel": kernel,
                 "launches": n_l, "avg_launch_ms": round(t_ms / n_l, 4),
                 "alg_bytes_per_launch": round(alg_per_launch, 1),
                 "share_of_step": round(t_ms / args.steps / ms, 4)}
@@ -444,12 +450,15 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "genes/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        # per-cell arithmetic of the IRLS pass: FP32 in the register engine,
+        # FP64 in the shared-memory and design-group engines
+        "dtype": "f32" if engines["irls"] == "register" else "f64", "data": "synthetic",
         "config": dict(workload_desc(args.config, G, n, p, nnz), form=args.form,
                        l2="inputs exceed L2 (CSR of all genes, re-read every IRLS pass)",
                        parallelism=f"genes sharded over {world} rank(s), no exchange during "
                                    f"the fit; p-values all-gathered for BH",
-                       passes=passes,
+                       passes=passes, engines=engines,
                        converged_frac=float((out["status"] == 0).float().mean().item()),
                        mean_irls_iters=float(out["iters"].float().mean().item())),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,

@@ -33,7 +33,7 @@ EXPORTS = (
     "devil_calculate_sf", "devil_estimate_dispersion", "devil_init_beta", "devil_beta_fit",
     "devil_estimate_mom_dispersion", "devil_fit_dispersion", "devil_compute_hessian",
     "devil_compute_clustered_meat", "devil_nb_adjoint", "devil_cluster_blocks",
-    "devil_group_order", "devil_ctx_set_profiling", "devil_ctx_profile",
+    "devil_group_order", "devil_ctx_set_profiling", "devil_ctx_profile", "devil_ctx_engine",
     "devil_p_adjust_device",
 )
 
@@ -115,6 +115,8 @@ def load():
         L.devil_group_order.argtypes = [i64, vp, vp]
         L.devil_ctx_set_profiling.argtypes = [vp, i]
         L.devil_ctx_profile.argtypes = [vp, i, C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]
+        L.devil_ctx_engine.argtypes = [vp, i]
+        L.devil_ctx_engine.restype = i
         _lib = L
     return _lib
 
@@ -154,6 +156,12 @@ class Context:
         self.check(load().devil_ctx_profile(self.h, int(kind), C.byref(n), C.byref(ms),
                                             C.byref(b)))
         return n.value, ms.value, b.value
+
+    def engine(self, kind: int) -> str:
+        """Engine of the last launch of pass kind 0 IRLS, 1 MOM, 2 MLE,
+        3 bread/meat: "register", "shared", "groups" or "none"."""
+        e = load().devil_ctx_engine(self.h, int(kind))
+        return {0: "register", 1: "shared", 2: "groups"}.get(e, "none")
 
     def synchronize(self):
         self.check(load().devil_ctx_synchronize(self.h))

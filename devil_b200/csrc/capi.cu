@@ -36,6 +36,8 @@ struct devil_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int sm_count = 148;
     int use_tma = 0;
+    int use_groups = 1;
+    int debug = 0;  // DEVIL_DEBUG=1: engine choices on stderr
     // profiling: CUDA events around every pass launch, per pass kind
     int profiling = 0;
     std::vector<cudaEvent_t> ev_pool;
@@ -45,6 +47,9 @@ struct devil_ctx {
     int64_t prof_launches[4] = {0, 0, 0, 0};
     double prof_ms[4] = {0, 0, 0, 0};
     double prof_bytes[4] = {0, 0, 0, 0};
+    int last_engine[4] = {-1, -1, -1, -1};
+    // DEVIL_DEBUG: CUDA events at the phase boundaries of a fit
+    std::vector<std::pair<const char*, cudaEvent_t>> marks;
 };
 
 namespace {
@@ -131,6 +136,30 @@ void prof_collect(devil_ctx* ctx) {
     ctx->ev_used = 0;
 }
 
+// phase marks of a fit (DEVIL_DEBUG=1); dbg_report prints the gaps
+void dbg_mark(devil_ctx* ctx, const char* label) {
+    if (!ctx->debug) return;
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(e, ctx->stream));
+    ctx->marks.emplace_back(label, e);
+}
+void dbg_report(devil_ctx* ctx) {
+    if (!ctx->debug || ctx->marks.empty()) return;
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::string out = "devil_b200 phases (ms):";
+    for (size_t i = 1; i < ctx->marks.size(); ++i) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->marks[i - 1].second, ctx->marks[i].second));
+        char buf[96];
+        snprintf(buf, sizeof buf, " %s %.2f", ctx->marks[i].first, ms);
+        out += buf;
+    }
+    for (auto& m : ctx->marks) cudaEventDestroy(m.second);
+    ctx->marks.clear();
+    fprintf(stderr, "%s\n", out.c_str());
+}
+
 template <class T>
 void h2d(devil_ctx* ctx, T* dst, const T* src, size_t count) {
     if (count) CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
@@ -162,6 +191,19 @@ struct DevProblem {
     int nfine = 1;
     int32_t* fine_bound = nullptr;
     int64_t* fine_ptr = nullptr;
+    // design groups (kernels_grp.cu); active only for the chosen form
+    struct Groups {
+        bool active = false;
+        int U = 0, C = 1;
+        double* xg = nullptr;
+        double* E = nullptr;
+        int32_t* gcol = nullptr;
+        void* gval = nullptr;
+        int64_t* gptr = nullptr;
+        double* rs = nullptr;
+        double* rw = nullptr;
+        int32_t* rm = nullptr;
+    } grp;
 };
 
 int xs_for(int P) {
@@ -405,6 +447,178 @@ void compute_offsets(devil_ctx* ctx, DevProblem& dp, int method, const double* s
 }
 
 // ------------------------------------------------------------------
+// design groups: distinct design rows (x cluster) of the cells, their
+// Gauss rules and the CSR copy ordered by group (kernels_grp.cu).  Used
+// when the rows take at most kMaxGroups values and the rules are smaller
+// than the cells; otherwise, or when a rule fails its check, the passes
+// stay on the per-cell engines.
+// ------------------------------------------------------------------
+void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int n_clusters, int form) {
+    dp.grp = DevProblem::Groups{};
+    if (form != DEVIL_FORM_CHOSEN || !ctx->use_groups || dp.G == 0) return;
+    if (n_clusters > 1 && !ends_host) fail(ctx, DEVIL_ERR_ARG, "cluster_ends is NULL");
+    cudaStream_t st = ctx->stream;
+    const int64_t n = dp.n;
+    const int P = dp.P;
+    uint64_t* hk = ws<uint64_t>(ctx, "grp_hash", n);
+    uint64_t* hk2 = ws<uint64_t>(ctx, "grp_hash2", n);
+    int32_t* ix = ws<int32_t>(ctx, "grp_idx", n);
+    int32_t* ix2 = ws<int32_t>(ctx, "grp_idx2", n);
+    LAUNCH(launch_row_hash(dp.Xcm, n, P, hk, ix, st));
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, hk, hk2, ix, ix2, (int)n);
+    CK(cub::DeviceRadixSort::SortPairs(ws<char>(ctx, "grp_sort_tmp", tb), tb, hk, hk2, ix, ix2,
+                                       (int)n, 0, 64, st));
+    ctx->launches++;
+    int32_t* flag = ws<int32_t>(ctx, "grp_flag", n);
+    int32_t* incl = ws<int32_t>(ctx, "grp_incl", n);
+    int32_t* bad = ws<int32_t>(ctx, "grp_bad", 2);
+    CK(cudaMemsetAsync(bad, 0, 2 * sizeof(int32_t), st));
+    LAUNCH(launch_group_heads(dp.Xcm, n, P, hk2, ix2, flag, bad, st));
+    tb = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tb, flag, incl, (int)n);
+    CK(cub::DeviceScan::InclusiveSum(ws<char>(ctx, "grp_scan_tmp", tb), tb, flag, incl, (int)n, st));
+    ctx->launches++;
+    int32_t h[2] = {0, 0};
+    CK(cudaMemcpyAsync(h, incl + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h + 1, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const int U = h[0];
+    if (h[1] || U < 1 || U > kMaxGroups || (int64_t)U * kMinCellsPerGroup >= n) {
+        if (ctx->debug)
+            fprintf(stderr, "devil_b200: design not grouped (%d distinct rows%s)\n", U,
+                    h[1] ? ", hash collision" : "");
+        return;
+    }
+    dbg_mark(ctx, "g.rows");
+    const int C = (n_clusters > 1 && (int64_t)U * n_clusters <= kMaxFine) ? n_clusters : 1;
+    const int K = U * C;
+    int32_t* ucell = ws<int32_t>(ctx, "grp_ucell", n);
+    int32_t* head = ws<int32_t>(ctx, "grp_head", U);
+    LAUNCH(launch_group_assign(ix2, incl, flag, n, ucell, head, st));
+    double* xg = ws<double>(ctx, "grp_xg", (size_t)U * P);
+    LAUNCH(launch_group_rows(dp.Xcm, n, P, head, U, xg, st));
+    // fine keys u * C + cluster
+    int32_t* ends_d = ws<int32_t>(ctx, "grp_ends", std::max(1, C));
+    if (C > 1) {
+        for (int b = 0; b < C; ++b) {
+            const int64_t prev = b ? ends_host[b - 1] : 0;
+            if (ends_host[b] < prev || ends_host[b] > n)
+                fail(ctx, DEVIL_ERR_ARG, "cluster ends must be non-decreasing and <= n");
+        }
+        if (ends_host[C - 1] != n) fail(ctx, DEVIL_ERR_ARG, "last cluster end must equal the number of cells");
+        h2d(ctx, ends_d, ends_host, C);
+    }
+    int32_t* fkey = ws<int32_t>(ctx, "grp_fkey", n);
+    int32_t* cells = ix;  // reuse
+    LAUNCH(launch_fine_keys(ucell, ends_d, C, n, fkey, cells, st));
+    // cells by offset, then (stable) by group and by fine group: each
+    // group's cells sorted by offset, as the rules need
+    double* offs = ws<double>(ctx, "grp_offs", n);
+    int32_t* byoff = ws<int32_t>(ctx, "grp_byoff", n);
+    tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, dp.off, offs, cells, byoff, (int)n);
+    CK(cub::DeviceRadixSort::SortPairs(ws<char>(ctx, "grp_sort_tmp", tb), tb, dp.off, offs, cells,
+                                       byoff, (int)n, 0, 64, st));
+    ctx->launches++;
+    auto bits_for = [](int K) {
+        int b = 1;
+        while ((1 << b) < K) ++b;
+        return b;
+    };
+    int32_t* kin = ws<int32_t>(ctx, "grp_kin", n);
+    int32_t* kout = ws<int32_t>(ctx, "grp_kout", n);
+    int32_t* permC = ws<int32_t>(ctx, "grp_permC", n);
+    int64_t* gsC = ws<int64_t>(ctx, "grp_gsC", U + 1);
+    LAUNCH(launch_gather_keys(ucell, byoff, n, kin, st));
+    tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, byoff, permC, (int)n, 0, bits_for(U));
+    CK(cub::DeviceRadixSort::SortPairs(ws<char>(ctx, "grp_sort_tmp2", tb), tb, kin, kout, byoff, permC,
+                                       (int)n, 0, bits_for(U), st));
+    ctx->launches++;
+    LAUNCH(launch_group_starts(kout, n, U, gsC, st));
+    int32_t* permF = permC;
+    int64_t* gsF = gsC;
+    if (C > 1) {
+        permF = ws<int32_t>(ctx, "grp_permF", n);
+        gsF = ws<int64_t>(ctx, "grp_gsF", K + 1);
+        LAUNCH(launch_gather_keys(fkey, byoff, n, kin, st));
+        tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, byoff, permF, (int)n, 0, bits_for(K));
+        CK(cub::DeviceRadixSort::SortPairs(ws<char>(ctx, "grp_sort_tmp3", tb), tb, kin, kout, byoff,
+                                           permF, (int)n, 0, bits_for(K), st));
+        ctx->launches++;
+        LAUNCH(launch_group_starts(kout, n, K, gsF, st));
+    }
+    dbg_mark(ctx, "g.sort");
+    double* E = ws<double>(ctx, "grp_E", n);
+    LAUNCH(launch_exp(dp.off, n, E, st));
+    const int nrules = U + (C > 1 ? K : 0);
+    double* rs = ws<double>(ctx, "grp_rs", (size_t)nrules * kRuleCap);
+    double* rw = ws<double>(ctx, "grp_rw", (size_t)nrules * kRuleCap);
+    int32_t* rm = ws<int32_t>(ctx, "grp_rm", nrules);
+    double* scr = ws<double>(ctx, "grp_scr", (size_t)6 * n);
+    double* rerr = ws<double>(ctx, "grp_rerr", nrules);
+    LAUNCH(launch_group_rules(permC, gsC, permF, gsF, U, nrules, dp.off, n, scr, rs, rw, rm, rerr,
+                              bad + 1, st));
+    dbg_mark(ctx, "g.rules");
+    // CSR copy ordered by key within each gene
+    int32_t* gcol = ws<int32_t>(ctx, "grp_col", dp.nnz);
+    void* gval = dp.val_u16 ? (void*)ws<uint16_t>(ctx, "grp_val16", dp.nnz)
+                            : (void*)ws<float>(ctx, "grp_val32", dp.nnz);
+    int64_t* gptr = ws<int64_t>(ctx, "grp_ptr", (size_t)dp.G * (K + 1));
+    LAUNCH(launch_group_csr(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.G, fkey, K, gptr, gcol, gval, st));
+    dbg_mark(ctx, "g.csr");
+    CK(cudaMemcpyAsync(h + 1, bad + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (ctx->debug) {
+        std::vector<double> he(nrules);
+        std::vector<int32_t> hm(nrules);
+        CK(cudaMemcpy(he.data(), rerr, nrules * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hm.data(), rm, nrules * sizeof(int32_t), cudaMemcpyDeviceToHost));
+        double we = 0.0;
+        int mm = 0;
+        for (int i = 0; i < nrules; ++i) {
+            we = std::max(we, he[i]);
+            mm = std::max(mm, (int)hm[i]);
+        }
+        fprintf(stderr, "devil_b200: %d design groups x %d clusters, %d rules (max %d nodes, "
+                        "worst check error %.3g)%s\n", U, C, nrules, mm, we,
+                h[1] ? ": check failed, per-cell engines" : "");
+    }
+    if (h[1]) return;  // a rule missed its accuracy check: per-cell engines
+    auto& g = dp.grp;
+    g.active = true;
+    g.U = U;
+    g.C = C;
+    g.xg = xg;
+    g.E = E;
+    g.gcol = gcol;
+    g.gval = gval;
+    g.gptr = gptr;
+    g.rs = rs;
+    g.rw = rw;
+    g.rm = rm;
+}
+
+GrpGeom grp_geom(const DevProblem& dp) {
+    const auto& gr = dp.grp;
+    GrpGeom gg{};
+    gg.P = dp.P;
+    gg.U = gr.U;
+    gg.C = gr.C;
+    gg.xg = gr.xg;
+    gg.E = gr.E;
+    gg.gcol = gr.gcol;
+    gg.gval = gr.gval;
+    gg.gptr = gr.gptr;
+    gg.rs = gr.rs;
+    gg.rw = gr.rw;
+    gg.rm = gr.rm;
+    return gg;
+}
+
+// ------------------------------------------------------------------
 // the gene x cell pass driver
 // ------------------------------------------------------------------
 struct PassPlan {
@@ -412,8 +626,10 @@ struct PassPlan {
     int GT;
 };
 
-PassPlan plan_for(PassKind k, int P, int form) {
+PassPlan plan_for(PassKind k, const DevProblem& dp, int form) {
+    const int P = dp.P;
     if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, 1};
+    if (dp.grp.active) return {ENGINE_GRP, 1};
     if (P <= reg_max_p()) {
         int gt = reg_default_gt(k, P);
         if (k == PASS_MLE) {
@@ -436,28 +652,28 @@ PassPlan plan_for(PassKind k, int P, int form) {
 }
 
 // number of cell-segment work items for `tiles` gene tiles
-int choose_nseg(devil_ctx* ctx, const DevProblem& dp, int tiles, int form) {
-    if (form == DEVIL_FORM_PLAIN) return 1;
+int choose_nseg(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, int tiles, int form) {
+    if (form == DEVIL_FORM_PLAIN || plan.engine == ENGINE_GRP) return 1;
     const int target = ctx->sm_count * 2;
     int want = (target + tiles - 1) / tiles;
     return std::max(1, std::min(want, dp.nfine));
 }
 
 // largest nseg * tiles * GT over every active-gene count the loops can see
-size_t max_slot_segs(devil_ctx* ctx, const DevProblem& dp, int GT, int form) {
+size_t max_slot_segs(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, int form) {
+    const int GT = plan.GT;
     const int max_tiles = (int)((dp.G + GT - 1) / GT);
     size_t best = 0;
     for (int tiles = 1; tiles <= max_tiles; ++tiles) {
-        size_t v = (size_t)choose_nseg(ctx, dp, tiles, form) * tiles * GT;
+        size_t v = (size_t)choose_nseg(ctx, dp, plan, tiles, form) * tiles * GT;
         if (v > best) best = v;
     }
     return best;
 }
 
 struct PassBuffers {
-    void* partW;     // Pass::AW partial sums (float, or double for the sandwich)
+    void* partW;     // partial sums: Pass::AW from the register engine, double from the generic one
     double* partS;
-    float* partWf() const { return static_cast<float*>(partW); }
     double* partWd() const { return static_cast<double*>(partW); }
 };
 
@@ -471,7 +687,7 @@ PassBuffers pass_buffers(devil_ctx* ctx, PassKind k, int P, size_t slots_x_segs)
 void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const PassPlan& plan,
                  int nseg, int tiles, const int32_t* bound, const int64_t* segptr,
                  int nbound, const int32_t* act, const int32_t* n_act, int32_t* reset_next,
-                 const PassBuffers& pb, const PassParamsAny& prm) {
+                 const PassBuffers& pb, const PassParamsAny& prm, int fine = 0) {
     PassLaunch L;
     L.kind = kind;
     L.engine = plan.engine;
@@ -504,10 +720,22 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
     L.prm = prm;
     L.stream = ctx->stream;
     size_t e0 = ctx->profiling ? prof_event(ctx) : 0;
-    if (plan.engine == ENGINE_REG)
+    ctx->last_engine[kind] = (int)plan.engine;
+    if (plan.engine == ENGINE_GRP) {
+        GrpGeom gg = grp_geom(dp);
+        gg.fine = fine;
+        gg.act = act;
+        gg.n_act = n_act;
+        gg.reset_next = reset_next;
+        gg.partW = static_cast<double*>(pb.partW);
+        gg.partS = pb.partS;
+        gg.slot_stride = tiles;
+        LAUNCH(launch_grp_pass(kind, gg, prm, dp.val_u16, tiles, ctx->stream));
+    } else if (plan.engine == ENGINE_REG) {
         LAUNCH(launch_reg_pass(L));
-    else
+    } else {
         LAUNCH(launch_gen_pass(L));
+    }
     if (ctx->profiling) {
         size_t e1 = prof_event(ctx);
         ctx->recs.push_back({(int)kind, e0, e1});
@@ -519,7 +747,7 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
 // (uint16 value + int32 cell index, or float + int32), its beta / gene
 // parameters, its partial sums; plus the design and offsets once per launch
 void prof_add_bytes(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const int32_t* passes,
-                    int64_t launches) {
+                    int64_t launches, const PassPlan& plan) {
     if (!ctx->profiling) return;
     int64_t* acc = ws<int64_t>(ctx, "prof_acc", 2);
     CK(cudaMemsetAsync(acc, 0, 2 * sizeof(int64_t), ctx->stream));
@@ -530,8 +758,14 @@ void prof_add_bytes(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const i
     const double ebytes = dp.val_u16 ? 6.0 : 8.0;
     const int na = pass_na(kind, dp.P), ns = pass_ns(kind);
     const double per_gene = 4.0 * dp.P + 8.0 + 4.0 * na + 8.0 * ns + 16.0;
+    // per launch: the design and offsets, or the group rows, rules and exp(offset)
+    const double per_launch = plan.engine == ENGINE_GRP
+                                  ? (double)dp.grp.U * dp.P * 8.0 + (double)dp.n * 8.0 +
+                                        (double)(dp.grp.U * (dp.grp.C > 1 ? dp.grp.C + 1 : 1)) *
+                                            kRuleCap * 16.0
+                                  : (double)dp.n * 4.0 * (dp.xs + 1);
     ctx->prof_bytes[kind] += ebytes * (double)h[0] + per_gene * (double)h[1] +
-                             (double)launches * (double)dp.n * 4.0 * (dp.xs + 1);
+                             (double)launches * per_launch;
 }
 
 // all-genes list (for one-shot passes)
@@ -554,14 +788,16 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
     CK(cudaMemsetAsync(iters, 0, G * sizeof(int32_t), st));
     CK(cudaMemsetAsync(status, 0, G * sizeof(int32_t), st));
     if (G == 0 || max_iter <= 0) return;
-    const PassPlan plan = plan_for(PASS_IRLS, dp.P, form);
+    const PassPlan plan = plan_for(PASS_IRLS, dp, form);
     if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported", dp.P);
     int32_t* act[2] = {ws<int32_t>(ctx, "act0", G), ws<int32_t>(ctx, "act1", G)};
     int32_t* cnt = ws<int32_t>(ctx, "cnt", 4);
     LAUNCH(launch_iota(act[0], G, st));
     LAUNCH(launch_set_i32(cnt, (int32_t)G, st));
     LAUNCH(launch_set_i32(cnt + 1, 0, st));
-    PassBuffers pb = pass_buffers(ctx, PASS_IRLS, dp.P, max_slot_segs(ctx, dp, plan.GT, form));
+    PassBuffers pb = pass_buffers(ctx, PASS_IRLS, dp.P, max_slot_segs(ctx, dp, plan, form));
+    // copies of an earlier loop still in flight would overwrite the mirror
+    CK(cudaStreamSynchronize(st));
     *ctx->mapped_host = (int32_t)G;
     const int LAG = 2;
     PassParamsAny prm{beta_f, beta, k, nullptr, nullptr};
@@ -577,11 +813,11 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
         }
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
-        const int nseg = choose_nseg(ctx, dp, tiles, form);
+        const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
         launch_pass(ctx, dp, PASS_IRLS, plan, nseg, tiles, dp.fine_bound, dp.fine_ptr,
                     dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
         ++launched;
-        LAUNCH(launch_irls_finalize(pb.partWf(), nseg, tiles * plan.GT, dp.P, act[cur], cnt + cur,
+        LAUNCH(launch_irls_finalize(pb.partW, plan.engine != ENGINE_REG, nseg, tiles * plan.GT, dp.P, act[cur], cnt + cur,
                                     (int)hint, act[nxt], cnt + nxt, beta, beta_f, iters, status,
                                     max_iter, eps, k, st));
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
@@ -590,7 +826,7 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
     }
     if (ctx->profiling) {
         prof_collect(ctx);
-        prof_add_bytes(ctx, dp, PASS_IRLS, iters, launched);
+        prof_add_bytes(ctx, dp, PASS_IRLS, iters, launched, plan);
     }
 }
 
@@ -598,11 +834,11 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
 void run_mom(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const double* beta_d,
              double* theta, int form) {
     if (dp.G == 0) return;
-    const PassPlan plan = plan_for(PASS_MOM, dp.P, form);
+    const PassPlan plan = plan_for(PASS_MOM, dp, form);
     int32_t* cnt = nullptr;
     const int32_t* act = all_genes(ctx, dp, &cnt);
     const int tiles = (int)((dp.G + plan.GT - 1) / plan.GT);
-    const int nseg = choose_nseg(ctx, dp, tiles, form);
+    const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
     PassBuffers pb = pass_buffers(ctx, PASS_MOM, dp.P, (size_t)nseg * tiles * plan.GT);
     PassParamsAny prm{beta_f, beta_d, nullptr, nullptr, nullptr};
     launch_pass(ctx, dp, PASS_MOM, plan, nseg, tiles, dp.fine_bound, dp.fine_ptr,
@@ -613,7 +849,7 @@ void run_mom(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
         prof_collect(ctx);
         int32_t* ones = ws<int32_t>(ctx, "prof_ones", dp.G);
         LAUNCH(launch_fill_i32(ones, 1, dp.G, ctx->stream));
-        prof_add_bytes(ctx, dp, PASS_MOM, ones, 1);
+        prof_add_bytes(ctx, dp, PASS_MOM, ones, 1, plan);
     }
 }
 
@@ -624,7 +860,7 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     cudaStream_t st = ctx->stream;
     const int64_t G = dp.G;
     if (G == 0) return;
-    const PassPlan plan = plan_for(PASS_MLE, dp.P, form);
+    const PassPlan plan = plan_for(PASS_MLE, dp, form);
     if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported for MLE", dp.P);
     MleState s;
     s.x = ws<double>(ctx, "mle_x", G);
@@ -641,7 +877,9 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     LAUNCH(launch_set_i32(cnt, 0, st));
     LAUNCH(launch_set_i32(cnt + 1, 0, st));
     LAUNCH(launch_mle_init(dp.stats, G, dp.n, s, act[0], cnt, st));
-    PassBuffers pb = pass_buffers(ctx, PASS_MLE, dp.P, max_slot_segs(ctx, dp, plan.GT, form));
+    PassBuffers pb = pass_buffers(ctx, PASS_MLE, dp.P, max_slot_segs(ctx, dp, plan, form));
+    // copies of an earlier loop still in flight would overwrite the mirror
+    CK(cudaStreamSynchronize(st));
     *ctx->mapped_host = (int32_t)G;
     const int LAG = 2;
     PassParamsAny prm{beta_f, beta_d, nullptr, s.x, nullptr};
@@ -654,11 +892,11 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
         hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
-        const int nseg = choose_nseg(ctx, dp, tiles, form);
+        const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
         launch_pass(ctx, dp, PASS_MLE, plan, nseg, tiles, dp.fine_bound,
                     dp.fine_ptr, dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
         ++launched;
-        LAUNCH(launch_mle_finalize(pb.partWf(), pb.partS, nseg, tiles * plan.GT, dp.P, dp.stats, dp.n,
+        LAUNCH(launch_mle_finalize(pb.partW, plan.engine != ENGINE_REG, pb.partS, nseg, tiles * plan.GT, dp.P, dp.stats, dp.n,
                                    act[cur], cnt + cur, (int)hint, act[nxt], cnt + nxt, s, max_iter,
                                    cox_reid, nullptr, st));
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
@@ -670,7 +908,7 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
         // genes take part in phase-0 plus one pass per Newton step
         int32_t* np1 = ws<int32_t>(ctx, "prof_mle_passes", G);
         LAUNCH(launch_mle_passes(s.it, s.phase, dp.stats, G, np1, st));
-        prof_add_bytes(ctx, dp, PASS_MLE, np1, launched);
+        prof_add_bytes(ctx, dp, PASS_MLE, np1, launched, plan);
     }
 }
 
@@ -681,14 +919,45 @@ void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, con
                   double* meat, int form) {
     cudaStream_t st = ctx->stream;
     if (dp.G == 0) return;
-    const PassPlan plan = plan_for(PASS_SANDWICH, dp.P, form);
+    PassPlan plan = plan_for(PASS_SANDWICH, dp, form);
+    // the grouped sandwich needs the cells keyed by cluster too
+    if (plan.engine == ENGINE_GRP && n_clusters > 0 && dp.grp.C != n_clusters) {
+        DevProblem plain = dp;
+        plain.grp.active = false;
+        plan = plan_for(PASS_SANDWICH, plain, form);
+    }
     if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported", dp.P);
     int32_t* cnt = nullptr;
     const int32_t* act = all_genes(ctx, dp, &cnt);
     const int tiles = (int)((dp.G + plan.GT - 1) / plan.GT);
     PassParamsAny prm{beta_f, beta_d, nullptr, nullptr, theta};
+    if (plan.engine == ENGINE_GRP && n_clusters > 0) {
+        // one output segment per cluster (fine groups = (design row, cluster))
+        for (int b = 0; b < n_clusters; ++b) {
+            const int64_t prev = b ? ends_host[b - 1] : 0;
+            if (ends_host[b] < prev || ends_host[b] > dp.n)
+                fail(ctx, DEVIL_ERR_ARG, "cluster ends must be non-decreasing and <= n");
+        }
+        if (ends_host[n_clusters - 1] != dp.n)
+            fail(ctx, DEVIL_ERR_ARG, "last cluster end must equal the number of cells");
+        const int nseg = n_clusters;
+        int32_t* segc = ws<int32_t>(ctx, "sw_segc", nseg);
+        LAUNCH(launch_iota(segc, nseg, st));
+        PassBuffers pb = pass_buffers(ctx, PASS_SANDWICH, dp.P, (size_t)nseg * tiles);
+        launch_pass(ctx, dp, PASS_SANDWICH, plan, nseg, tiles, nullptr, nullptr, 0, act, cnt,
+                    nullptr, pb, prm, 1);
+        LAUNCH(launch_sandwich_finalize(pb.partWd(), nseg, tiles, dp.P, segc, n_clusters, dp.n, act,
+                                        cnt, (int)dp.G, bread, sandwich, meat, st));
+        if (ctx->profiling) {
+            prof_collect(ctx);
+            int32_t* ones = ws<int32_t>(ctx, "prof_ones", dp.G);
+            LAUNCH(launch_fill_i32(ones, 1, dp.G, st));
+            prof_add_bytes(ctx, dp, PASS_SANDWICH, ones, 1, plan);
+        }
+        return;
+    }
     if (n_clusters <= 0) {
-        const int nseg = choose_nseg(ctx, dp, tiles, form);
+        const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
         PassBuffers pb = pass_buffers(ctx, PASS_SANDWICH, dp.P, (size_t)nseg * tiles * plan.GT);
         launch_pass(ctx, dp, PASS_SANDWICH, plan, nseg, tiles, dp.fine_bound,
                     dp.fine_ptr, dp.nfine + 1, act, cnt, nullptr, pb, prm);
@@ -698,7 +967,7 @@ void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, con
             prof_collect(ctx);
             int32_t* ones = ws<int32_t>(ctx, "prof_ones", dp.G);
             LAUNCH(launch_fill_i32(ones, 1, dp.G, st));
-            prof_add_bytes(ctx, dp, PASS_SANDWICH, ones, 1);
+            prof_add_bytes(ctx, dp, PASS_SANDWICH, ones, 1, plan);
         }
         return;
     }
@@ -739,7 +1008,7 @@ void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, con
         prof_collect(ctx);
         int32_t* ones = ws<int32_t>(ctx, "prof_ones", dp.G);
         LAUNCH(launch_fill_i32(ones, 1, dp.G, st));
-        prof_add_bytes(ctx, dp, PASS_SANDWICH, ones, 1);
+        prof_add_bytes(ctx, dp, PASS_SANDWICH, ones, 1, plan);
     }
 }
 
@@ -776,6 +1045,7 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     cudaStream_t st = ctx->stream;
     const int64_t G = dp.G;
     const int P = dp.P;
+    dbg_mark(ctx, "groups");
     LAUNCH(launch_theta0(dp.stats, dp.off, G, dp.n, o->has_init_overdispersion,
                          o->init_overdispersion, fb.theta0, fb.k, st));
     double* ginv = ws<double>(ctx, "ginv", (size_t)P * P);
@@ -787,11 +1057,16 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
         CK(cudaStreamSynchronize(st));
         if (herr) fail(ctx, DEVIL_ERR_SINGULAR, "design matrix is rank deficient");
     }
-    LAUNCH(launch_init_beta(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.Xdrm, dp.xs, dp.off,
-                            ws<double>(ctx, "inv_sf", dp.n), ginv, dp.stats, G, dp.n, P,
-                            o->init_beta_rough, fb.beta, fb.beta_f, st));
+    if (dp.grp.active && !o->init_beta_rough)
+        LAUNCH(launch_grp_init_beta(grp_geom(dp), dp.val_u16, ginv, G, fb.beta, fb.beta_f, st));
+    else
+        LAUNCH(launch_init_beta(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.Xdrm, dp.xs, dp.off,
+                                ws<double>(ctx, "inv_sf", dp.n), ginv, dp.stats, G, dp.n, P,
+                                o->init_beta_rough, fb.beta, fb.beta_f, st));
     const double eps = (double)(float)o->tolerance;
+    dbg_mark(ctx, "init");
     run_irls(ctx, dp, fb.beta, fb.beta_f, fb.k, fb.iters, fb.status, o->max_iter, eps, o->form);
+    dbg_mark(ctx, "irls");
     double* tm = nullptr;
     if (fb.theta_mom || o->overdispersion == DEVIL_OD_MOM || o->overdispersion == DEVIL_OD_MLE) {
         // MOM theta: the requested estimate, or the Newton start for MLE
@@ -801,15 +1076,19 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
         if (o->overdispersion == DEVIL_OD_MOM && tm != fb.theta)
             CK(cudaMemcpyAsync(fb.theta, tm, G * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
+    dbg_mark(ctx, "mom");
     if (o->overdispersion == DEVIL_OD_MLE) {
         run_mle(ctx, dp, fb.beta_f, fb.beta, tm, fb.theta, nullptr, o->max_iter, 1, o->form);
     } else if (o->overdispersion == DEVIL_OD_NONE) {
         CK(cudaMemsetAsync(fb.theta, 0, G * sizeof(double), st));
     }
+    dbg_mark(ctx, "mle");
     run_sandwich(ctx, dp, fb.beta_f, fb.beta, fb.theta, ends_host, n_clusters, fb.bread,
                  n_clusters > 0 ? fb.sandwich : nullptr, n_clusters > 0 ? fb.meat : nullptr,
                  o->form);
+    dbg_mark(ctx, "sandwich");
     check_kernel_err(ctx);
+    dbg_report(ctx);
 }
 
 void alloc_fit_buffers(devil_ctx* ctx, int64_t G, int P, bool theta_mom, bool clusters,
@@ -844,9 +1123,13 @@ int guarded(devil_ctx* ctx, F&& f) {
         f();
         return DEVIL_OK;
     } catch (const Fail& e) {
+        // drain what the failed call queued before the next call reuses
+        // the context's workspace (the error message is kept)
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         return e.code;
     } catch (const std::exception& e) {
         ctx->err = e.what();
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         return DEVIL_ERR_ARG;
     }
 }
@@ -886,6 +1169,11 @@ int devil_ctx_create(int device, devil_ctx** out) {
         // measured slower than the register engine on the sparse workload
         const char* ut = getenv("DEVIL_TMA");
         ctx->use_tma = (ut && atoi(ut)) ? 1 : 0;
+        // the design-group engine is on unless DEVIL_GROUPS=0 (A/B timing)
+        const char* ug = getenv("DEVIL_GROUPS");
+        ctx->use_groups = (ug && !atoi(ug)) ? 0 : 1;
+        const char* dbg = getenv("DEVIL_DEBUG");
+        ctx->debug = (dbg && atoi(dbg)) ? 1 : 0;
         int32_t* err = ws<int32_t>(ctx, "kernel_err", 1);
         CK(cudaMemset(err, 0, sizeof(int32_t)));
     });
@@ -932,6 +1220,11 @@ int devil_ctx_set_profiling(devil_ctx* ctx, int enable) {
     });
 }
 
+int devil_ctx_engine(const devil_ctx* ctx, int pass_kind) {
+    if (!ctx || pass_kind < 0 || pass_kind > 3) return -1;
+    return ctx->last_engine[pass_kind];
+}
+
 int devil_ctx_profile(devil_ctx* ctx, int pass_kind, int64_t* launches, double* ms,
                       double* alg_bytes) {
     return guarded(ctx, [&] {
@@ -953,9 +1246,14 @@ int devil_fit(devil_ctx* ctx, const devil_counts* counts, const double* X, int p
             fail(ctx, DEVIL_ERR_ARG, "X and result beta/theta/beta_iters are required");
         if (n_clusters > 0 && !cluster_ends) fail(ctx, DEVIL_ERR_ARG, "cluster_ends is NULL");
         DevProblem dp;
+        dbg_mark(ctx, "start");
         upload_counts(ctx, counts, dp);
+        dbg_mark(ctx, "upload");
         prepare_design(ctx, dp, X, p, false);
+        dbg_mark(ctx, "design");
         compute_offsets(ctx, dp, opts->size_factors, opts->size_factor_values, nullptr, opts->offset);
+        dbg_mark(ctx, "offsets");
+        build_groups(ctx, dp, cluster_ends, n_clusters, opts->form);
         FitBuffers fb;
         alloc_fit_buffers(ctx, dp.G, p, res->theta_mom && opts->compute_theta_mom, n_clusters > 0, fb);
         fit_pipeline(ctx, dp, cluster_ends, n_clusters, opts, fb);
@@ -988,9 +1286,14 @@ int devil_fit_device(devil_ctx* ctx, const devil_counts* counts_dev, const doubl
         if (!counts_dev || !X_dev || !r || !r->beta || !r->theta || !r->beta_iters)
             fail(ctx, DEVIL_ERR_ARG, "counts, X and result beta/theta/beta_iters are required");
         DevProblem dp;
+        dbg_mark(ctx, "start");
         use_device_counts(ctx, counts_dev, dp);
+        dbg_mark(ctx, "validate");
         prepare_design(ctx, dp, X_dev, p, true);
+        dbg_mark(ctx, "design");
         compute_offsets(ctx, dp, opts->size_factors, nullptr, opts->size_factor_values, opts->offset);
+        dbg_mark(ctx, "offsets");
+        build_groups(ctx, dp, cluster_ends_host, n_clusters, opts->form);
         FitBuffers fb;
         alloc_fit_buffers(ctx, dp.G, p, r->theta_mom && opts->compute_theta_mom, n_clusters > 0, fb);
         // write straight into the caller's device buffers where given
@@ -1159,6 +1462,7 @@ int devil_beta_fit(devil_ctx* ctx, const devil_counts* counts, const double* X, 
         upload_counts(ctx, counts, dp);
         prepare_design(ctx, dp, X, p, false);
         upload_offsets(ctx, dp, offset_vector);
+        build_groups(ctx, dp, nullptr, 0, form);
         const int64_t G = dp.G;
         double* b = ws<double>(ctx, "beta", (size_t)G * p);
         float* bf = ws<float>(ctx, "beta_f", (size_t)G * p);
@@ -1200,6 +1504,7 @@ int devil_estimate_mom_dispersion(devil_ctx* ctx, const devil_counts* counts, co
         upload_counts(ctx, counts, dp);
         prepare_design(ctx, dp, X, p, false);
         upload_sf_as_offsets(ctx, dp, size_factors);
+        build_groups(ctx, dp, nullptr, 0, DEVIL_FORM_CHOSEN);
         float* bf;
         double* bd;
         upload_beta(ctx, dp, beta, &bf, &bd);
@@ -1219,6 +1524,7 @@ int devil_fit_dispersion(devil_ctx* ctx, const devil_counts* counts, const doubl
         upload_counts(ctx, counts, dp);
         prepare_design(ctx, dp, X, p, false);
         upload_offsets(ctx, dp, offset_vector);
+        build_groups(ctx, dp, nullptr, 0, DEVIL_FORM_CHOSEN);
         float* bf;
         double* bd;
         upload_beta(ctx, dp, beta, &bf, &bd);
@@ -1244,6 +1550,7 @@ int devil_compute_hessian(devil_ctx* ctx, const devil_counts* counts, const doub
         upload_counts(ctx, counts, dp);
         prepare_design(ctx, dp, X, p, false);
         upload_sf_as_offsets(ctx, dp, size_factors);
+        build_groups(ctx, dp, nullptr, 0, DEVIL_FORM_CHOSEN);
         float* bf;
         double* bd;
         upload_beta(ctx, dp, beta, &bf, &bd);
@@ -1267,6 +1574,7 @@ int devil_compute_clustered_meat(devil_ctx* ctx, const devil_counts* counts, con
         upload_counts(ctx, counts, dp);
         prepare_design(ctx, dp, X, p, false);
         upload_sf_as_offsets(ctx, dp, size_factors);
+        build_groups(ctx, dp, cluster_ends, n_clusters, DEVIL_FORM_CHOSEN);
         float* bf;
         double* bd;
         upload_beta(ctx, dp, beta, &bf, &bd);

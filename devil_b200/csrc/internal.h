@@ -11,7 +11,7 @@
 namespace devil {
 
 enum PassKind { PASS_IRLS = 0, PASS_MOM = 1, PASS_MLE = 2, PASS_SANDWICH = 3 };
-enum Engine { ENGINE_REG = 0, ENGINE_GEN = 1 };
+enum Engine { ENGINE_REG = 0, ENGINE_GEN = 1, ENGINE_GRP = 2 };
 
 inline int pass_nw(PassKind k) { return k == PASS_MLE ? 3 : (k == PASS_MOM ? 0 : 1); }
 inline int pass_nv(PassKind k) { return (k == PASS_IRLS || k == PASS_SANDWICH) ? 1 : 0; }
@@ -54,6 +54,59 @@ size_t gen_smem_bytes(PassKind k, int P, int GT);
 
 cudaError_t launch_reg_pass(const PassLaunch& L);
 cudaError_t launch_gen_pass(const PassLaunch& L);
+
+// ---- design-group engine (kernels_grp.cu) ----
+constexpr int kBinNodes = 10;         // Gauss nodes per offset bin
+constexpr double kBinWidth = 2.0;     // bin width in log size factor
+constexpr int kMaxBins = 32;          // bins per group (offsets spread over < 64)
+constexpr int kRuleCap = kMaxBins * kBinNodes;  // node capacity of one rule
+constexpr int kMaxGroups = 256;       // distinct design rows
+constexpr int kMaxFine = 4096;        // (design row, cluster) pairs
+constexpr int kMinCellsPerGroup = 32; // grouping pays when groups are larger
+struct GrpGeom {
+    int P, U, C;           // design columns, groups, clusters folded into the keys (1: none)
+    int fine;              // 1: groups are (row, cluster) pairs, one output segment per cluster
+    const double* xg;      // [U][P] distinct design rows
+    const double* E;       // [n] exp(offset)
+    const int32_t* gcol;   // CSR copy, entries ordered by key u * C + c within each gene
+    const void* gval;
+    const int64_t* gptr;   // [G][U*C + 1] absolute start of every key's entries
+    const double* rs;      // [rules][kRuleCap] node offsets; rules 0..U-1 coarse, U.. fine
+    const double* rw;      // [rules][kRuleCap] node weights
+    const int32_t* rm;     // [rules] node counts
+    const int32_t* act;
+    const int32_t* n_act;
+    int32_t* reset_next;
+    double* partW;         // FP64 partial sums, layout of the other engines
+    double* partS;
+    int slot_stride;
+};
+cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm, int val_u16,
+                            int max_slots, cudaStream_t st);
+cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* ginv, int64_t G,
+                                 double* beta, float* beta_f, cudaStream_t st);
+cudaError_t launch_row_hash(const double* X, int64_t n, int P, uint64_t* h, int32_t* idx,
+                            cudaStream_t st);
+cudaError_t launch_group_heads(const double* X, int64_t n, int P, const uint64_t* hs,
+                               const int32_t* is, int32_t* flag, int32_t* bad, cudaStream_t st);
+cudaError_t launch_group_assign(const int32_t* is, const int32_t* incl, const int32_t* flag,
+                                int64_t n, int32_t* ucell, int32_t* head, cudaStream_t st);
+cudaError_t launch_group_rows(const double* X, int64_t n, int P, const int32_t* head, int U,
+                              double* xg, cudaStream_t st);
+cudaError_t launch_fine_keys(const int32_t* ucell, const int32_t* ends, int C, int64_t n,
+                             int32_t* fkey, int32_t* cell, cudaStream_t st);
+cudaError_t launch_group_starts(const int32_t* ks, int64_t n, int K, int64_t* gstart,
+                                cudaStream_t st);
+cudaError_t launch_exp(const double* x, int64_t n, double* y, cudaStream_t st);
+cudaError_t launch_group_rules(const int32_t* permC, const int64_t* gsC, const int32_t* permF,
+                               const int64_t* gsF, int U, int nrules, const double* off, int64_t n,
+                               double* scr, double* rs, double* rw, int32_t* rm, double* rerr,
+                               int32_t* bad, cudaStream_t st);
+cudaError_t launch_gather_keys(const int32_t* keys, const int32_t* cells, int64_t n, int32_t* out,
+                               cudaStream_t st);
+cudaError_t launch_group_csr(const int64_t* rowptr, const int32_t* col, const void* val, int val_u16,
+                             int64_t G, const int32_t* fkey, int K, int64_t* gptr, int32_t* gcol,
+                             void* gval, cudaStream_t st);
 
 // ---- preparation kernels (kernels_prep.cu) ----
 cudaError_t launch_dense_count(const void* Y, int is_f64, int cell_major, int64_t G, int64_t n,
@@ -107,7 +160,8 @@ cudaError_t launch_copy_i32_to_host_mapped(const int32_t* src, volatile int32_t*
                                            cudaStream_t st);
 
 // ---- finalize kernels (kernels_fin.cu) ----
-cudaError_t launch_irls_finalize(const float* partW, int nseg, int slot_stride, int P,
+// wide: partial sums are FP64 (generic engine) instead of FP32
+cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slot_stride, int P,
                                  const int32_t* act, const int32_t* n_act, int max_slots,
                                  int32_t* act_next, int32_t* n_next, double* beta, float* beta_f,
                                  int32_t* iters, int32_t* status, int max_iter, double eps,
@@ -128,7 +182,7 @@ struct MleState {
 };
 cudaError_t launch_mle_init(const double* stats, int64_t G, int64_t n, MleState s,
                             int32_t* act, int32_t* n_act, cudaStream_t st);
-cudaError_t launch_mle_finalize(const float* partW, const double* partS, int nseg,
+cudaError_t launch_mle_finalize(const void* partW, bool wide, const double* partS, int nseg,
                                 int slot_stride, int P, const double* stats, int64_t n,
                                 const int32_t* act, const int32_t* n_act, int max_slots,
                                 int32_t* act_next, int32_t* n_next, MleState s, int max_iter,

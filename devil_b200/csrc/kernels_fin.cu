@@ -1,5 +1,7 @@
 // Per-gene finalize kernels: reduce the per-segment partial sums of a pass
 // in FP64 and apply the reference's per-gene step.  One warp per gene.
+#include <type_traits>
+
 #include "internal.h"
 
 namespace devil {
@@ -37,7 +39,8 @@ DEV void unpack_sym(int P, const double* packed, double* M) {
 // IRLS step (src/beta.cpp:38-46): delta = H^-1 score, beta += delta,
 // converged when max|delta| < eps; NaN in delta[0] stops the gene.
 // ------------------------------------------------------------------
-__global__ void irls_finalize_kernel(const float* partW, int nseg, int slot_stride, int P,
+template <class TW>
+__global__ void irls_finalize_kernel(const TW* partW, int nseg, int slot_stride, int P,
                                      const int32_t* act, const int32_t* n_act, int32_t* act_next,
                                      int32_t* n_next, double* beta, float* beta_f, int32_t* iters,
                                      int32_t* status, int max_iter, double eps, const float* kf) {
@@ -87,7 +90,7 @@ __global__ void irls_finalize_kernel(const float* partW, int nseg, int slot_stri
     }
 }
 
-cudaError_t launch_irls_finalize(const float* partW, int nseg, int slot_stride, int P,
+cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slot_stride, int P,
                                  const int32_t* act, const int32_t* n_act, int max_slots,
                                  int32_t* act_next, int32_t* n_next, double* beta, float* beta_f,
                                  int32_t* iters, int32_t* status, int max_iter, double eps,
@@ -97,15 +100,21 @@ cudaError_t launch_irls_finalize(const float* partW, int nseg, int slot_stride, 
     const size_t per = (size_t)(NA + P * P + 2 * P) * sizeof(double);
     const int w = fin_warps(per);
     const size_t smem = per * w;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(irls_finalize_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    irls_finalize_kernel<<<nblk(max_slots, w), 32 * w, smem, st>>>(
-        partW, nseg, slot_stride, P, act, n_act, act_next, n_next, beta, beta_f, iters, status,
-        max_iter, eps, k);
-    return cudaGetLastError();
+    auto go = [&](auto* pw) -> cudaError_t {
+        using TW = std::remove_const_t<std::remove_pointer_t<decltype(pw)>>;
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(irls_finalize_kernel<TW>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        irls_finalize_kernel<TW><<<nblk(max_slots, w), 32 * w, smem, st>>>(
+            pw, nseg, slot_stride, P, act, n_act, act_next, n_next, beta, beta_f, iters, status,
+            max_iter, eps, k);
+        return cudaGetLastError();
+    };
+    // the register engine leaves FP32 partial sums, the generic engine FP64
+    return wide ? go(static_cast<const double*>(partW)) : go(static_cast<const float*>(partW));
 }
 
 // ------------------------------------------------------------------
@@ -172,7 +181,8 @@ cudaError_t launch_mle_init(const double* stats, int64_t G, int64_t n, MleState 
     return cudaGetLastError();
 }
 
-__global__ void mle_finalize_kernel(const float* partW, const double* partS, int nseg,
+template <class TW>
+__global__ void mle_finalize_kernel(const TW* partW, const double* partS, int nseg,
                                     int slot_stride, int P, const double* stats, int64_t n,
                                     const int32_t* act, const int32_t* n_act, int32_t* act_next,
                                     int32_t* n_next, MleState st, int max_iter, int cox_reid) {
@@ -313,7 +323,7 @@ __global__ void mle_finalize_kernel(const float* partW, const double* partS, int
         act_next[pos] = g;
     }
 }
-cudaError_t launch_mle_finalize(const float* partW, const double* partS, int nseg,
+cudaError_t launch_mle_finalize(const void* partW, bool wide, const double* partS, int nseg,
                                 int slot_stride, int P, const double* stats, int64_t n,
                                 const int32_t* act, const int32_t* n_act, int max_slots,
                                 int32_t* act_next, int32_t* n_next, MleState s, int max_iter,
@@ -324,15 +334,20 @@ cudaError_t launch_mle_finalize(const float* partW, const double* partS, int nse
     const size_t per = (size_t)(NA + 6 + 4 * P * P + P) * sizeof(double);
     const int w = fin_warps(per);
     const size_t smem = per * w;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(mle_finalize_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    mle_finalize_kernel<<<nblk(max_slots, w), 32 * w, smem, st>>>(
-        partW, partS, nseg, slot_stride, P, stats, n, act, n_act, act_next, n_next, s, max_iter,
-        cox_reid);
-    return cudaGetLastError();
+    auto go = [&](auto* pw) -> cudaError_t {
+        using TW = std::remove_const_t<std::remove_pointer_t<decltype(pw)>>;
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(mle_finalize_kernel<TW>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        mle_finalize_kernel<TW><<<nblk(max_slots, w), 32 * w, smem, st>>>(
+            pw, partS, nseg, slot_stride, P, stats, n, act, n_act, act_next, n_next, s, max_iter,
+            cox_reid);
+        return cudaGetLastError();
+    };
+    return wide ? go(static_cast<const double*>(partW)) : go(static_cast<const float*>(partW));
 }
 
 // ------------------------------------------------------------------

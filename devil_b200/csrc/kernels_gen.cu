@@ -13,8 +13,7 @@ int gen_default_gt(PassKind k, int P) {
 
 size_t gen_smem_bytes(PassKind k, int P, int GT) {
     const int ns = pass_ns(k), nwv = pass_nw(k) + pass_nv(k) + pass_nf(k);
-    const bool f64 = (k == PASS_MOM || k == PASS_SANDWICH);
-    const size_t wt = f64 ? 8 : 4;
+    const size_t wt = 8;  // FP64 staging for every pass
     const int TC = kGenNT / GT;
     const int XS = (P + 1) | 1;
     size_t b = gen_wt_offset(ns, GT);
@@ -40,17 +39,14 @@ static cudaError_t run(const PassLaunch& L) {
     cudaError_t e;
     if (L.val_u16) {
         auto k = gen_pass_kernel<Pass, uint16_t>;
-        if (smem > 48 * 1024) {
-            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-        }
+        // static shared memory (psi tables) counts against the 48 KB default
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
         k<<<grid, kGenNT, smem, L.stream>>>(L.geo, prm, L.P, L.GT);
     } else {
         auto k = gen_pass_kernel<Pass, float>;
-        if (smem > 48 * 1024) {
-            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-        }
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
         k<<<grid, kGenNT, smem, L.stream>>>(L.geo, prm, L.P, L.GT);
     }
     return cudaGetLastError();

@@ -1,0 +1,748 @@
+// Design-group engine.
+//
+// Designs built from an intercept, a condition and one-hot cell-type /
+// batch columns have few distinct rows: a cell enters every pass only
+// through its design row x_u and its offset o_i (log size factor).  With
+// the cells grouped by design row (and by cluster for the sandwich), one
+// pass computes per (gene, group)
+//   * the terms of zero counts summed over all cells of the group,
+//       sum_i f(exp(a_u + o_i)),  a_u = x_u . beta,
+//     as a Gauss rule for the group's offsets: bins of width 2 in the
+//     offset, each with its cells as nodes (at most 10 cells) or a 10-point
+//     Gauss rule; checked against exact sums before use;
+//   * the corrections of the nonzero counts from the group's range of a
+//     CSR copy whose entries are ordered by group within each gene;
+// and assembles the p x p terms once per group.  A pass then reads every
+// nonzero once and costs O(groups x (nodes + p^2)) per gene instead of
+// O(cells x p^2).  Partial sums land in the layout of the other engines
+// (FP64, one segment, or one per cluster for the sandwich), so the
+// finalize kernels are shared.
+#include <cub/cub.cuh>
+
+#include "internal.h"
+
+namespace devil {
+
+static inline unsigned nblk(int64_t m, int t) { return (unsigned)((m + t - 1) / t); }
+
+// ---------------------------------------------------------------------
+// grouping of the design rows
+// ---------------------------------------------------------------------
+// 64-bit hash of the bit patterns of a row (column-major X): equal rows
+// hash equally; equal hashes are confirmed bit for bit afterwards
+__global__ void row_hash_kernel(const double* X, int64_t n, int P, uint64_t* h, int32_t* idx) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t v = 0x9E3779B97F4A7C15ull;
+    for (int j = 0; j < P; ++j) {
+        uint64_t b = (uint64_t)__double_as_longlong(X[i + (int64_t)j * n]);
+        v ^= b + 0x9E3779B97F4A7C15ull + (v << 6) + (v >> 2);
+        v *= 0xBF58476D1CE4E5B9ull;
+        v ^= v >> 31;
+    }
+    h[i] = v;
+    idx[i] = (int32_t)i;
+}
+
+// run heads of the sorted hashes; rows with equal hashes must be equal
+__global__ void group_heads_kernel(const double* X, int64_t n, int P, const uint64_t* hs,
+                                   const int32_t* is, int32_t* flag, int32_t* bad) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int head = (i == 0) || hs[i] != hs[i - 1];
+    flag[i] = head;
+    if (!head) {
+        const int64_t a = is[i], b = is[i - 1];
+        for (int j = 0; j < P; ++j)
+            if (__double_as_longlong(X[a + (int64_t)j * n]) != __double_as_longlong(X[b + (int64_t)j * n]))
+                *bad = 1;  // hash collision: the caller falls back to the per-cell engines
+    }
+}
+
+// group of every cell (0-based run number) and the first cell of each group
+__global__ void group_assign_kernel(const int32_t* is, const int32_t* incl, const int32_t* flag,
+                                    int64_t n, int32_t* ucell, int32_t* head) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int u = incl[i] - 1;
+    ucell[is[i]] = u;
+    if (flag[i]) head[u] = is[i];
+}
+
+__global__ void group_rows_kernel(const double* X, int64_t n, int P, const int32_t* head, int U,
+                                  double* xg) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= U * P) return;
+    const int u = i / P, j = i - u * P;
+    xg[i] = X[head[u] + (int64_t)j * n];
+}
+
+// fine key u * C + cluster; clusters are contiguous blocks with 1-based
+// exclusive ends (the cluster_ends of the fit)
+__global__ void fine_keys_kernel(const int32_t* ucell, const int32_t* ends, int C, int64_t n,
+                                 int32_t* fkey, int32_t* cell) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int lo = 0, hi = C - 1;  // first cluster whose end exceeds i
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (ends[mid] > i) hi = mid; else lo = mid + 1;
+    }
+    fkey[i] = ucell[i] * C + (C > 1 ? lo : 0);
+    cell[i] = (int32_t)i;
+}
+
+// gstart[k] = first position of key k in the sorted keys (k = 0..K)
+__global__ void group_starts_kernel(const int32_t* ks, int64_t n, int K, int64_t* gstart) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > K) return;
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (ks[mid] < k) lo = mid + 1; else hi = mid;
+    }
+    gstart[k] = lo;
+}
+
+__global__ void gather_keys_kernel(const int32_t* keys, const int32_t* cells, int64_t n,
+                                   int32_t* out) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = keys[cells[i]];
+}
+
+__global__ void exp_kernel(const double* x, int64_t n, double* y) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) y[i] = exp(x[i]);
+}
+
+// ---------------------------------------------------------------------
+// Gauss rules of the groups' offset distributions
+// ---------------------------------------------------------------------
+constexpr int kRuleNT = 256;
+
+// block-wide sum; every thread gets the same value (same association)
+DEV double block_sum(double v, double* red) {
+    v = warp_sum(v);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double r = l < nw ? red[l] : 0.0;
+    return warp_sum(r);
+}
+DEV double block_min(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    double r = l < nw ? red[l] : INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r = fmin(r, __shfl_xor_sync(0xffffffffu, r, o));
+    return r;
+}
+
+// number of eigenvalues below x of the Jacobi matrix with diagonal al[0..m)
+// and squared off-diagonal be[1..m) (Sturm sequence of the LDL^T pivots)
+DEV int jacobi_count_below(const double* al, const double* be, int m, double x) {
+    int c = 0;
+    double d = 1.0;
+    for (int i = 0; i < m; ++i) {
+        d = (al[i] - x) - (i ? be[i] / d : 0.0);
+        if (d == 0.0) d = -1e-300;
+        c += d < 0.0;
+    }
+    return c;
+}
+
+// Gauss rule of one bin of sorted offsets s[perm[c0..c1)] (more than
+// kBinNodes cells, a spread above 1e-13) with m <= kBinNodes nodes, written
+// to os/ow.  In t = (s - c)/h the monic orthogonal polynomials of the bin's
+// measure are run over its cells (discretised Stieltjes procedure, stable
+// at this degree), the nodes are the eigenvalues of the Jacobi matrix
+// (bisection on Sturm counts), the weights the Christoffel numbers scaled
+// to the bin's cell count.  The recurrence stops early when pi_{k+1}
+// vanishes on the support (at most k+1 distinct offsets: the rule is then
+// exact).  Returns m (same value in every thread).
+DEV int bin_rule(const int32_t* perm, const double* off, int64_t c0, int64_t c1, double* tt,
+                 double* p0, double* p1, double* red, double* al, double* be, double* nk,
+                 double* wsum, double* os, double* ow) {
+    const int t = threadIdx.x, nt = blockDim.x;
+    const double cnt = (double)(c1 - c0);
+    const double bmin = off[perm[c0]], bmax = off[perm[c1 - 1]];
+    const double c = 0.5 * (bmax + bmin), h = 0.5 * (bmax - bmin);
+    double st = 0.0;
+    for (int64_t i = c0 + t; i < c1; i += nt) {
+        const double x = (off[perm[i]] - c) / h;
+        tt[i] = x;
+        p0[i] = 1.0;
+        p1[i] = 0.0;
+        st += x;
+    }
+    st = block_sum(st, red);
+    if (t == 0) {
+        al[0] = st / cnt;
+        be[0] = 0.0;
+        nk[0] = cnt;
+    }
+    __syncthreads();
+    int m = kBinNodes;
+    for (int k = 0; k + 1 < kBinNodes; ++k) {
+        const double a = al[k], bb = be[k];
+        double sN = 0.0, sT = 0.0, sS = 0.0;
+        for (int64_t i = c0 + t; i < c1; i += nt) {
+            const double x = tt[i], pk = p0[i], pm = p1[i];
+            const double pn = (x - a) * pk - bb * pm;
+            const double sc = fabs(x - a) * fabs(pk) + bb * fabs(pm);
+            p1[i] = pk;
+            p0[i] = pn;
+            sN += pn * pn;
+            sT += x * pn * pn;
+            sS += sc * sc;
+        }
+        sN = block_sum(sN, red);
+        sT = block_sum(sT, red);
+        sS = block_sum(sS, red);
+        if (!(sN > 1e-26 * sS)) {  // pi_{k+1} is rounding noise on the support
+            m = k + 1;
+            break;
+        }
+        if (t == 0) {
+            al[k + 1] = sT / sN;
+            be[k + 1] = sN / nk[k];
+            nk[k + 1] = sN;
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    double xj = 0.0, wj = 0.0;
+    if (t < m) {
+        // eigenvalue t (ascending); all lie in [-1, 1]
+        double lo = -1.0 - 1e-9, hi = 1.0 + 1e-9;
+        for (int it = 0; it < 200; ++it) {
+            const double mid = 0.5 * (lo + hi);
+            if (mid <= lo || mid >= hi) break;
+            if (jacobi_count_below(al, be, m, mid) > t) hi = mid; else lo = mid;
+        }
+        xj = 0.5 * (lo + hi);
+        // Christoffel number: 1 / sum_k pi_k(x)^2 / (N_k / N_0)
+        double pm = 0.0, pk = 1.0, q = 1.0;
+        for (int k = 0; k + 1 < m; ++k) {
+            const double pn = (xj - al[k]) * pk - be[k] * pm;
+            pm = pk;
+            pk = pn;
+            q += pn * pn * (nk[0] / nk[k + 1]);
+        }
+        wj = cnt / q;
+        wsum[t] = wj;
+    }
+    __syncthreads();
+    if (t < 32) {
+        double v = t < m ? wsum[t] : 0.0;
+        v = warp_sum(v);
+        if (t < m) {
+            os[t] = c + h * xj;
+            ow[t] = wj * (cnt / v);  // weights sum to the bin's cell count
+        }
+    }
+    __syncthreads();
+    return m;
+}
+
+// first position in [lo, hi) of the sorted offsets s[perm[.]] with s >= v
+DEV int64_t lower_bound_off(const int32_t* perm, const double* off, int64_t lo, int64_t hi, double v) {
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (off[perm[mid]] < v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Block per rule.  Rule b < U: coarse group b, cells permC[gsC[b]..gsC[b+1])
+// sorted by offset; rule U + k: fine group k (row, cluster), cells
+// permF[gsF[k]..gsF[k+1]).  The group's offsets are cut into bins of width
+// kBinWidth; a bin of at most kBinNodes cells contributes its cells as
+// nodes (weight 1), a bin of one offset (to 1e-13) one node at its mean,
+// any other bin a kBinNodes-point Gauss rule (bin_rule).  With bins of
+// width 2 the dense terms of the passes, analytic within pi of the real
+// s axis, are integrated to ~1e-15.  The rule is checked on
+// sum_i 1/(1 + exp(s_i - z)) for z at both ends and the middle of the
+// group's range; rerr[b] is the worst relative error and a value above
+// 1e-11 (or more than kMaxBins bins) sets *bad.
+__global__ void __launch_bounds__(kRuleNT) group_rules_kernel(
+    const int32_t* permC, const int64_t* gsC, const int32_t* permF, const int64_t* gsF, int U,
+    const double* off, int64_t n, double* scr, double* rs, double* rw, int32_t* rm, double* rerr,
+    int32_t* bad) {
+    __shared__ double red[32];
+    __shared__ double al[kBinNodes + 1], be[kBinNodes + 1], nk[kBinNodes + 1];
+    __shared__ double wsum[32];
+    __shared__ int64_t rng[2];
+    const int b = blockIdx.x, t = threadIdx.x, nt = blockDim.x;
+    const bool coarse = b < U;
+    const int32_t* perm = coarse ? permC : permF;
+    const int64_t b0 = coarse ? gsC[b] : gsF[b - U];
+    const int64_t b1 = coarse ? gsC[b + 1] : gsF[b - U + 1];
+    const int64_t base = coarse ? 0 : n;  // scratch of coarse and fine rules
+    double* tt = scr + base;
+    double* p0 = scr + 2 * n + base;
+    double* p1 = scr + 4 * n + base;
+    double* os = rs + (int64_t)b * kRuleCap;
+    double* ow = rw + (int64_t)b * kRuleCap;
+    if (b1 <= b0) {
+        if (t == 0) {
+            rm[b] = 0;
+            rerr[b] = 0.0;
+        }
+        return;
+    }
+    const double smin = off[perm[b0]], smax = off[perm[b1 - 1]];
+    const double span = (smax - smin) / kBinWidth;
+    if (!(span < (double)kMaxBins)) {  // offsets too spread (or not finite)
+        if (t == 0) {
+            rm[b] = 0;
+            rerr[b] = INFINITY;
+            atomicExch(bad, 1);
+        }
+        return;
+    }
+    const int nb = (int)span + 1;
+    int nodes = 0;
+    for (int j = 0; j < nb; ++j) {
+        if (t == 0) {
+            rng[0] = j == 0 ? b0 : lower_bound_off(perm, off, b0, b1, smin + j * kBinWidth);
+            rng[1] = j == nb - 1 ? b1 : lower_bound_off(perm, off, b0, b1, smin + (j + 1) * kBinWidth);
+        }
+        __syncthreads();
+        const int64_t c0 = rng[0], c1 = rng[1];
+        __syncthreads();
+        const int64_t cnt = c1 - c0;
+        if (cnt <= 0) continue;
+        if (cnt <= kBinNodes) {
+            if (t < cnt) {
+                os[nodes + t] = off[perm[c0 + t]];
+                ow[nodes + t] = 1.0;
+            }
+            nodes += (int)cnt;
+            continue;
+        }
+        const double bmin = off[perm[c0]], bmax = off[perm[c1 - 1]];
+        if (!(bmax - bmin > 1e-13 * fmax(1.0, fabs(bmax)))) {
+            double sm = 0.0;
+            for (int64_t i = c0 + t; i < c1; i += nt) sm += off[perm[i]];
+            sm = block_sum(sm, red);
+            if (t == 0) {
+                os[nodes] = sm / (double)cnt;
+                ow[nodes] = (double)cnt;
+            }
+            nodes += 1;
+            continue;
+        }
+        nodes += bin_rule(perm, off, c0, c1, tt, p0, p1, red, al, be, nk, wsum, os + nodes,
+                          ow + nodes);
+    }
+    if (t == 0) rm[b] = nodes;
+    __syncthreads();
+    // check the rule against exact sums of three logistic test functions
+    const double mid = 0.5 * (smin + smax);
+    double worst = 0.0;
+    for (int z = 0; z < 3; ++z) {
+        const double zc = z == 0 ? smin : (z == 1 ? mid : smax);
+        double ex = 0.0, ap = 0.0;
+        for (int64_t i = b0 + t; i < b1; i += nt) ex += 1.0 / (1.0 + exp(off[perm[i]] - zc));
+        for (int i = t; i < nodes; i += nt) ap += ow[i] / (1.0 + exp(os[i] - zc));
+        ex = block_sum(ex, red);
+        ap = block_sum(ap, red);
+        const double e = fabs(ap - ex) / ex;
+        worst = e > worst ? e : (e == e ? worst : e);  // NaN sticks
+    }
+    if (t == 0) {
+        rerr[b] = worst;
+        if (!(worst <= 1e-11)) atomicExch(bad, 1);
+    }
+}
+
+// ---------------------------------------------------------------------
+// CSR copy ordered by group within each gene (stable), with per-gene
+// group offsets gptr[g][k] (absolute; gptr[g][K] = row end).  Warp per gene;
+// per-warp cursors in shared memory.
+// ---------------------------------------------------------------------
+template <class VT>
+__global__ void group_csr_kernel(const int64_t* rowptr, const int32_t* col, const VT* val, int64_t G,
+                                 const int32_t* fkey, int K, int64_t* gptr, int32_t* gcol,
+                                 VT* gval) {
+    extern __shared__ int32_t cur_all[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
+    if (g >= G) return;
+    int32_t* cur = cur_all + (int64_t)w * K;
+    for (int k = lane; k < K; k += 32) cur[k] = 0;
+    __syncwarp();
+    const int64_t r0 = rowptr[g], r1 = rowptr[g + 1];
+    for (int64_t e = r0 + lane; e < r1; e += 32) atomicAdd(&cur[fkey[col[e]]], 1);
+    __syncwarp();
+    int64_t* gp = gptr + g * (K + 1);
+    int64_t run = r0;
+    for (int base = 0; base < K; base += 32) {
+        const int k = base + lane;
+        const int v = k < K ? cur[k] : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        const int64_t excl = run + incl - v;
+        if (k < K) {
+            gp[k] = excl;
+            cur[k] = (int32_t)(excl - r0);
+        }
+        run += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) gp[K] = r1;
+    __syncwarp();
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t base = r0; base < r1; base += 32) {
+        const int64_t e = base + lane;
+        const bool valid = e < r1;
+        int c = 0;
+        VT v = VT(0);
+        int k = -1;
+        if (valid) {
+            c = col[e];
+            v = val[e];
+            k = fkey[c];
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        const int rank = __popc(peers & lt);
+        const int pos = valid ? cur[k] + rank : 0;
+        __syncwarp();
+        if (valid) {
+            gcol[r0 + pos] = c;
+            gval[r0 + pos] = v;
+            if (lane == __ffs(peers) - 1) cur[k] += __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------
+// the pass
+// ---------------------------------------------------------------------
+// accumulator for one lane: every term is scaled by q (the node weight for
+// zero-count terms, 1 for the nonzeros)
+template <int NWV, int NS>
+struct GrpAcc {
+    double w[NWV > 0 ? NWV : 1];
+    double s[NS > 0 ? NS : 1];
+    double q;
+    DEV void zero() {
+#pragma unroll
+        for (int i = 0; i < NWV; ++i) w[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < NS; ++i) s[i] = 0.0;
+        q = 1.0;
+    }
+    template <int W>
+    DEV void outer(double v) { w[W] += q * v; }
+    template <int V, int NW>
+    DEV void vec(double v) { w[NW + V] += q * v; }
+    template <int K>
+    DEV void scal(double v) { s[K] += q * v; }
+    template <int K, int NW, int NV>
+    DEV void fscal(double v) { w[NW + NV + K] += q * v; }
+};
+
+template <class Pass, class VT>
+__global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pass::Params prm) {
+    constexpr int NW = Pass::NW, NV = Pass::NV, NF = Pass::NF;
+    constexpr int NWV = NW + NV + NF, NS = Pass::NS, NQ = NWV + NS;
+    if (geo.reset_next && blockIdx.x == 0 && threadIdx.x == 0) *geo.reset_next = 0;
+    const int slot = blockIdx.x;
+    if (slot >= *geo.n_act) return;
+    const int g = __ldg(geo.act + slot);
+    const int P = geo.P, U = geo.U, C = geo.C, K = U * C;
+    const int NGq = geo.fine ? K : U;
+    extern __shared__ double gsm[];
+    double* xg = gsm;          // [U][P]
+    double* bet = xg + U * P;  // [P]
+    double* gs = bet + P;      // [NGq][NQ]
+    const int t = threadIdx.x, nt = blockDim.x;
+    for (int i = t; i < U * P; i += nt) xg[i] = __ldg(geo.xg + i);
+    for (int i = t; i < P; i += nt) bet[i] = __ldg(prm.beta_d + (int64_t)g * P + i);
+    typename Pass::Gene gpar = Pass::load(prm, g);
+    if constexpr (Pass::TABLES) {
+        __shared__ double psitab[2 * kPsiTab];
+        __shared__ double psiscr[kPsiTab];
+        __shared__ double psia[1];
+        if (t == 0) psia[0] = gpar.a;
+        __syncthreads();
+        build_psi_tables(1, psia, psitab, psiscr);
+        gpar.tab.d1 = psitab;
+        gpar.tab.d2 = psitab + kPsiTab;
+        gpar.tab.pa = digamma_d(gpar.a);
+        gpar.tab.ta = trigamma_d(gpar.a);
+    }
+    __syncthreads();
+    const int warp = t >> 5, lane = t & 31, nw = nt >> 5;
+    const VT* __restrict__ gval = static_cast<const VT*>(geo.gval);
+    const int64_t* gp = geo.gptr + (int64_t)g * (K + 1);
+    for (int q = warp; q < NGq; q += nw) {
+        const int u = geo.fine ? q / C : q;
+        double a = lane < P ? xg[u * P + lane] * bet[lane] : 0.0;
+        a = warp_sum(a);
+        const double A = exp(a);
+        GrpAcc<NWV, NS> acc;
+        acc.zero();
+        // zero-count terms over all cells of the group: the group's rule
+        const int ri = (geo.fine && C > 1) ? U + q : u;  // C == 1: fine == coarse
+        const int m = __ldg(geo.rm + ri);
+        for (int j = lane; j < m; j += 32) {
+            acc.q = __ldg(geo.rw + (int64_t)ri * kRuleCap + j);
+            const double mu = exp(a + __ldg(geo.rs + (int64_t)ri * kRuleCap + j));
+            Pass::template dense<double>(gpar, mu, acc);
+        }
+        acc.q = 1.0;
+        // nonzero corrections over the group's CSR range
+        const int64_t e0 = __ldg(gp + (geo.fine ? q : u * C));
+        const int64_t e1 = __ldg(gp + (geo.fine ? q + 1 : u * C + C));
+        int64_t e = e0 + lane;
+        for (; e + 96 < e1; e += 128) {
+            int c[4];
+            float y[4];
+            double ev[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                c[j] = __ldg(geo.gcol + e + 32 * j);
+                y[j] = load_val(gval, e + 32 * j);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) ev[j] = __ldg(geo.E + c[j]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) Pass::template sparse<double>(gpar, A * ev[j], y[j], acc);
+        }
+        for (; e < e1; e += 32) {
+            const int c = __ldg(geo.gcol + e);
+            const float y = load_val(gval, e);
+            Pass::template sparse<double>(gpar, A * __ldg(geo.E + c), y, acc);
+        }
+#pragma unroll
+        for (int i = 0; i < NWV; ++i) {
+            const double v = warp_sum(acc.w[i]);
+            if (lane == 0) gs[q * NQ + i] = v;
+        }
+#pragma unroll
+        for (int i = 0; i < NS; ++i) {
+            const double v = warp_sum(acc.s[i]);
+            if (lane == 0) gs[q * NQ + NWV + i] = v;
+        }
+    }
+    __syncthreads();
+    // assemble the partial sums of the pass: one segment, or one per cluster
+    const int NE = P * (P + 1) / 2;
+    const int NA = NW * NE + NV * P + NF;
+    const int nout = geo.fine ? C : 1;
+    const int per = NA + NS;
+    for (int o = t; o < nout * per; o += nt) {
+        const int seg = o / per, a = o - seg * per;
+        double s = 0.0;
+        if (a < NW * NE) {
+            const int w = a / NE, qq = a - w * NE;
+            int j = 0;
+            while ((j + 1) * (j + 2) / 2 <= qq) ++j;
+            const int i = qq - j * (j + 1) / 2;
+            for (int u = 0; u < U; ++u) {
+                const int q = geo.fine ? u * C + seg : u;
+                s += gs[q * NQ + w] * (xg[u * P + i] * xg[u * P + j]);
+            }
+        } else if (a < NW * NE + NV * P) {
+            const int r = a - NW * NE;
+            const int v = r / P, i = r - v * P;
+            for (int u = 0; u < U; ++u) {
+                const int q = geo.fine ? u * C + seg : u;
+                s += gs[q * NQ + NW + v] * xg[u * P + i];
+            }
+        } else {
+            const int f = a - NW * NE - NV * P;  // fscal (a < NA) or an FP64 scalar
+            const int col = a < NA ? NW + NV + f : NWV + (a - NA);
+            for (int u = 0; u < U; ++u) {
+                const int q = geo.fine ? u * C + seg : u;
+                s += gs[q * NQ + col];
+            }
+        }
+        if (a < NA)
+            geo.partW[((int64_t)seg * geo.slot_stride + slot) * NA + a] = s;
+        else
+            geo.partS[((int64_t)seg * geo.slot_stride + slot) * NS + (a - NA)] = s;
+    }
+}
+
+// init_beta (R/beta.R:12-24) on a grouped design: X' z with
+// z = log1p(y / exp(offset)) (zero where y = 0) is sum_u x_u sum_{i in u,
+// y_i > 0} z_i, so the nonzeros are read once and summed per group;
+// beta_0 = (X'X)^-1 X' z.  Block per gene, warps over groups.
+template <class VT>
+__global__ void grp_init_beta_kernel(const int64_t* gptr, const int32_t* gcol, const VT* gval,
+                                     const double* E, const double* xg, int U, int C, int P,
+                                     const double* ginv, int64_t G, double* beta, float* beta_f) {
+    __shared__ double su[kMaxGroups];
+    __shared__ double r[32];
+    const int64_t g = blockIdx.x;
+    if (g >= G) return;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
+    const int K = U * C;
+    const int64_t* gp = gptr + g * (K + 1);
+    for (int u = warp; u < U; u += nw) {
+        const int64_t e0 = gp[u * C], e1 = gp[u * C + C];
+        double z = 0.0;
+        for (int64_t e = e0 + lane; e < e1; e += 32)
+            z += log1p((double)load_val(gval, e) / E[gcol[e]]);
+        z = warp_sum(z);
+        if (lane == 0) su[u] = z;
+    }
+    __syncthreads();
+    if (t < P) {
+        double v = 0.0;
+        for (int u = 0; u < U; ++u) v += xg[u * P + t] * su[u];
+        r[t] = v;
+    }
+    __syncthreads();
+    if (t < P) {
+        double b = 0.0;
+        for (int j = 0; j < P; ++j) b += ginv[j * P + t] * r[j];
+        beta[g * P + t] = b;
+        beta_f[g * P + t] = (float)b;
+    }
+}
+
+cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* ginv, int64_t G,
+                                 double* beta, float* beta_f, cudaStream_t st) {
+    if (G <= 0) return cudaSuccess;
+    const int nt = 32 * (geo.U < 8 ? (geo.U < 1 ? 1 : geo.U) : 8);
+    if (val_u16)
+        grp_init_beta_kernel<uint16_t><<<(unsigned)G, nt, 0, st>>>(
+            geo.gptr, geo.gcol, static_cast<const uint16_t*>(geo.gval), geo.E, geo.xg, geo.U, geo.C,
+            geo.P, ginv, G, beta, beta_f);
+    else
+        grp_init_beta_kernel<float><<<(unsigned)G, nt, 0, st>>>(
+            geo.gptr, geo.gcol, static_cast<const float*>(geo.gval), geo.E, geo.xg, geo.U, geo.C,
+            geo.P, ginv, G, beta, beta_f);
+    return cudaGetLastError();
+}
+
+template <class Pass>
+static typename Pass::Params grp_params(const PassParamsAny& a);
+template <> PassIRLS::Params grp_params<PassIRLS>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.k}; }
+template <> PassMOM::Params grp_params<PassMOM>(const PassParamsAny& a) { return {a.beta, a.beta_d}; }
+template <> PassMLE::Params grp_params<PassMLE>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.log_theta}; }
+template <> PassSandwich::Params grp_params<PassSandwich>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.theta}; }
+
+size_t grp_smem_bytes(PassKind k, int P, int U, int NGq) {
+    const int nq = pass_nw(k) + pass_nv(k) + pass_nf(k) + pass_ns(k);
+    return ((size_t)U * P + P + (size_t)NGq * nq) * sizeof(double);
+}
+
+int grp_threads(int NGq) {
+    int w = NGq < 8 ? (NGq < 2 ? 2 : NGq) : 8;
+    return 32 * w;
+}
+
+template <class Pass>
+static cudaError_t grp_run(const GrpGeom& geo, const PassParamsAny& pa, PassKind kind, int val_u16,
+                           int max_slots, cudaStream_t st) {
+    const int NGq = geo.fine ? geo.U * geo.C : geo.U;
+    const size_t smem = grp_smem_bytes(kind, geo.P, geo.U, NGq);
+    const int nt = grp_threads(NGq);
+    auto prm = grp_params<Pass>(pa);
+    auto go = [&](auto kern) -> cudaError_t {
+        // static shared memory (psi tables) counts against the 48 KB default
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        kern<<<(unsigned)max_slots, nt, smem, st>>>(geo, prm);
+        return cudaGetLastError();
+    };
+    return val_u16 ? go(grp_pass_kernel<Pass, uint16_t>) : go(grp_pass_kernel<Pass, float>);
+}
+
+cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm, int val_u16,
+                            int max_slots, cudaStream_t st) {
+    if (max_slots <= 0) return cudaSuccess;
+    switch (kind) {
+        case PASS_IRLS: return grp_run<PassIRLS>(geo, prm, kind, val_u16, max_slots, st);
+        case PASS_MOM: return grp_run<PassMOM>(geo, prm, kind, val_u16, max_slots, st);
+        case PASS_MLE: return grp_run<PassMLE>(geo, prm, kind, val_u16, max_slots, st);
+        case PASS_SANDWICH: return grp_run<PassSandwich>(geo, prm, kind, val_u16, max_slots, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------
+// launchers of the grouping steps
+// ---------------------------------------------------------------------
+cudaError_t launch_row_hash(const double* X, int64_t n, int P, uint64_t* h, int32_t* idx,
+                            cudaStream_t st) {
+    row_hash_kernel<<<nblk(n, 256), 256, 0, st>>>(X, n, P, h, idx);
+    return cudaGetLastError();
+}
+cudaError_t launch_group_heads(const double* X, int64_t n, int P, const uint64_t* hs,
+                               const int32_t* is, int32_t* flag, int32_t* bad, cudaStream_t st) {
+    group_heads_kernel<<<nblk(n, 256), 256, 0, st>>>(X, n, P, hs, is, flag, bad);
+    return cudaGetLastError();
+}
+cudaError_t launch_group_assign(const int32_t* is, const int32_t* incl, const int32_t* flag,
+                                int64_t n, int32_t* ucell, int32_t* head, cudaStream_t st) {
+    group_assign_kernel<<<nblk(n, 256), 256, 0, st>>>(is, incl, flag, n, ucell, head);
+    return cudaGetLastError();
+}
+cudaError_t launch_group_rows(const double* X, int64_t n, int P, const int32_t* head, int U,
+                              double* xg, cudaStream_t st) {
+    group_rows_kernel<<<nblk((int64_t)U * P, 256), 256, 0, st>>>(X, n, P, head, U, xg);
+    return cudaGetLastError();
+}
+cudaError_t launch_fine_keys(const int32_t* ucell, const int32_t* ends, int C, int64_t n,
+                             int32_t* fkey, int32_t* cell, cudaStream_t st) {
+    fine_keys_kernel<<<nblk(n, 256), 256, 0, st>>>(ucell, ends, C, n, fkey, cell);
+    return cudaGetLastError();
+}
+cudaError_t launch_group_starts(const int32_t* ks, int64_t n, int K, int64_t* gstart,
+                                cudaStream_t st) {
+    group_starts_kernel<<<nblk(K + 1, 256), 256, 0, st>>>(ks, n, K, gstart);
+    return cudaGetLastError();
+}
+cudaError_t launch_gather_keys(const int32_t* keys, const int32_t* cells, int64_t n, int32_t* out,
+                               cudaStream_t st) {
+    gather_keys_kernel<<<nblk(n, 256), 256, 0, st>>>(keys, cells, n, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_exp(const double* x, int64_t n, double* y, cudaStream_t st) {
+    exp_kernel<<<nblk(n, 256), 256, 0, st>>>(x, n, y);
+    return cudaGetLastError();
+}
+cudaError_t launch_group_rules(const int32_t* permC, const int64_t* gsC, const int32_t* permF,
+                               const int64_t* gsF, int U, int nrules, const double* off, int64_t n,
+                               double* scr, double* rs, double* rw, int32_t* rm, double* rerr,
+                               int32_t* bad, cudaStream_t st) {
+    group_rules_kernel<<<(unsigned)nrules, kRuleNT, 0, st>>>(permC, gsC, permF, gsF, U, off, n, scr,
+                                                             rs, rw, rm, rerr, bad);
+    return cudaGetLastError();
+}
+cudaError_t launch_group_csr(const int64_t* rowptr, const int32_t* col, const void* val, int val_u16,
+                             int64_t G, const int32_t* fkey, int K, int64_t* gptr, int32_t* gcol,
+                             void* gval, cudaStream_t st) {
+    if (G <= 0) return cudaSuccess;
+    int wpb = 12288 / K;  // 48 KB of cursors per block
+    wpb = wpb < 1 ? 1 : (wpb > 8 ? 8 : wpb);
+    const size_t smem = (size_t)wpb * K * sizeof(int32_t);
+    const unsigned grid = (unsigned)((G + wpb - 1) / wpb);
+    if (val_u16)
+        group_csr_kernel<uint16_t><<<grid, 32 * wpb, smem, st>>>(
+            rowptr, col, static_cast<const uint16_t*>(val), G, fkey, K, gptr, gcol,
+            static_cast<uint16_t*>(gval));
+    else
+        group_csr_kernel<float><<<grid, 32 * wpb, smem, st>>>(
+            rowptr, col, static_cast<const float*>(val), G, fkey, K, gptr, gcol,
+            static_cast<float*>(gval));
+    return cudaGetLastError();
+}
+
+}  // namespace devil

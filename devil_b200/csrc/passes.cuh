@@ -690,8 +690,11 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
     int64_t* cend = cursor + GT;                                    // [GT]
     int* cnt = reinterpret_cast<int*>(cend + GT);                   // [GT]
     int* gids = cnt + GT;                                           // [GT]
-    // FP64 passes stage design rows and weights in double
-    using WT = typename std::conditional<Pass::F64, double, float>::type;
+    // design rows and per-cell weights are staged in double for every pass:
+    // the FP32 form of this engine left errors of ~1.5e-5 in beta for slowly
+    // converging genes at p = 12, and FP64 FMAs run at half the FP32 rate on
+    // this part while the engine is bound by shared-memory traffic anyway
+    using WT = double;
     WT* xsm = reinterpret_cast<WT*>(smem_raw + gen_wt_offset(NS, GT));  // [TC][XS]
     WT* wts = xsm + TC * XS;                                        // [NWV][GT][TC]
     float* ys = reinterpret_cast<float*>(wts + NWV * kGenNT);       // [GT][TC]
@@ -730,8 +733,8 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
         gpar.tab.ta = trigamma_d(gpar.a);
     }
 
-    // owned outputs (W-type): o = t + k*NT over [0, GT*NA); per-chunk FP32
-    // sums are folded into FP64 accumulators
+    // owned outputs (W-type): o = t + k*NT over [0, GT*NA); per-chunk sums
+    // are folded into FP64 accumulators
     double acc[kGenKMAX];
     short oi[kGenKMAX], oj[kGenKMAX], og[kGenKMAX], ow[kGenKMAX];
     int nown = 0;
@@ -841,9 +844,8 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
         int o = t + k * kGenNT;
         int g = o / NA, a = o - g * NA;
         int slot = tile * GT + g;
-        if (slot < nact)
-            static_cast<typename Pass::AW*>(geo.partW)[((int64_t)seg * geo.slot_stride + slot) * NA + a] =
-                (typename Pass::AW)acc[k];
+        if (slot < nact)  // FP64 partial sums for every pass of this engine
+            static_cast<double*>(geo.partW)[((int64_t)seg * geo.slot_stride + slot) * NA + a] = acc[k];
     }
     if (NS > 0 && t < GT * NS) {
         constexpr int NSd = NS > 0 ? NS : 1;

@@ -136,6 +136,10 @@ DEVIL_API int64_t devil_ctx_launch_count(const devil_ctx *ctx);
 DEVIL_API int devil_ctx_set_profiling(devil_ctx *ctx, int enable);
 DEVIL_API int devil_ctx_profile(devil_ctx *ctx, int pass_kind, int64_t *launches, double *ms,
                                 double *alg_bytes);
+/* Engine of the last launch of a pass kind on this context (no counterpart
+ * in the reference): 0 register tiles (p <= 8), 1 shared-memory tiles,
+ * 2 design groups (few distinct design rows), -1 none yet. */
+DEVIL_API int devil_ctx_engine(const devil_ctx *ctx, int pass_kind);
 
 /* ---- full pipeline --------------------------------------------------- */
 /* fit_devil(x, design_matrix, clusters, overdispersion, init_overdispersion,

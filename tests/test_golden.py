@@ -66,7 +66,12 @@ def test_gpu_matches_golden(dv, path):
     rel = np.abs(fit["overdispersion"] - g["theta"])[mask] / g["theta"][mask]
     assert rel.size == 0 or rel.max() <= 1e-4
     res = dv.test_de(fit, g["contrast"])
-    ok = same & (g["pval"] > 1e-300)
+    # a bread whose condition number exceeds 1/eps of FP64 (an intercept
+    # drifting to -75 for a gene without counts in a cell group) gives a
+    # sandwich made of rounding in both implementations, the sign of the
+    # contrast variance included: such genes carry no p-value to compare
+    well = np.array([bool(np.all(np.isfinite(b))) and np.linalg.cond(b) < 1e15 for b in g["bread"]])
+    ok = same & well & (g["pval"] > 1e-300)
     lr = np.abs(np.log10(res["pval"][ok]) - np.log10(g["pval"][ok])) / np.maximum(
         1, np.abs(np.log10(g["pval"][ok])))
     assert lr.max() <= 1e-3

@@ -175,6 +175,45 @@ def test_fit_wide_p32(dv, orc):
     check_mats(fit["beta_sandwiches_null"], ref["bread"], same, 1e-4, "bread")
 
 
+def test_groups_match_per_cell_form(dv):
+    """The design-group engine (22 distinct design rows x 40 patients; the
+    zero-count terms of each group from a Gauss rule of its offsets, the
+    nonzeros from the group-ordered CSR) against the per-cell FP64 form on
+    the same data: the two differ only in summation order and the rule's
+    ~1e-15 quadrature error."""
+    P = synthetic.make("clustered", seed=21, G=48, n=40000)
+    ctx = dv.context()
+    # 48 genes leave empty cells: size factors are given (the truth)
+    a = gpu_fit(dv, P, "MLE", clusters=P.clusters, sf=P.sf_true)
+    assert [ctx.engine(k) for k in range(4)] == ["groups"] * 4
+    b = gpu_fit(dv, P, "MLE", clusters=P.clusters, sf=P.sf_true, form="plain")
+    assert ctx.engine(0) == "shared"
+    ia, ib = a["iterations"]["beta_iters"], b["iterations"]["beta_iters"]
+    same = ia == ib
+    assert same.mean() >= 0.97
+    conv = same & (ib < 200)
+    d = np.abs(a["beta"] - b["beta"]) / np.maximum(1.0, np.abs(b["beta"]))
+    assert d[conv].max() <= 1e-7, d[conv].max()
+    check_rel(a["overdispersion"], b["overdispersion"], _theta_mask(b["overdispersion"], conv),
+              1e-6, "theta")
+    check_mats(a["beta_sandwiches_null"], b["beta_sandwiches_null"], conv, 1e-7, "bread")
+    check_mats(a["beta_sandwiches"], b["beta_sandwiches"], conv, 1e-5, "sandwich")
+
+
+def test_groups_single_cell_groups(dv, orc):
+    """Groups of at most ten cells per offset bin use the cells themselves
+    as nodes: a two-group design at n = 300 must match the oracle."""
+    P = synthetic.make("plain_small", seed=13, G=40, n=300)
+    Y = (P.rowptr, P.col, P.val.astype(np.float64), P.n)
+    ref = oracle_fit(orc, P, orc.OD_MLE)
+    fit = dv.fit_devil(Y, P.X, overdispersion="MLE", size_factors="normed_sum",
+                       compute_theta_mom=True)
+    assert dv.context().engine(0) == "groups"
+    same = check_beta(fit, ref)
+    check_rel(fit["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta")
+    check_mats(fit["beta_sandwiches_null"], ref["bread"], same, 1e-4, "bread")
+
+
 def test_plain_form_matches_oracle(dv, orc, sparse_problem):
     P = sparse_problem.subset_genes(np.arange(80))
     ref = oracle_fit(orc, P, orc.OD_MOM, sf=P.sf_true)
