@@ -459,6 +459,7 @@ def main():
                        parallelism=f"genes sharded over {world} rank(s), no exchange during "
                                    f"the fit; p-values all-gathered for BH",
                        passes=passes, engines=engines,
+                       saturated_counts=int(data.get("saturated", 0)),
                        converged_frac=float((out["status"] == 0).float().mean().item()),
                        mean_irls_iters=float(out["iters"].float().mean().item())),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,

@@ -567,7 +567,19 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     void* gval = dp.val_u16 ? (void*)ws<uint16_t>(ctx, "grp_val16", dp.nnz)
                             : (void*)ws<float>(ctx, "grp_val32", dp.nnz);
     int64_t* gptr = ws<int64_t>(ctx, "grp_ptr", (size_t)dp.G * (K + 1));
-    LAUNCH(launch_group_csr(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.G, fkey, K, gptr, gcol, gval, st));
+    const int S = group_csr_segment(dp.nnz, dp.G, K);
+    int64_t* segcnt = ws<int64_t>(ctx, "grp_segcnt", dp.G + 1);
+    int64_t* segbase = ws<int64_t>(ctx, "grp_segbase", dp.G + 1);
+    size_t sb = 0;
+    CK(launch_group_segments(dp.rowptr, dp.G, S, segcnt, segbase, nullptr, &sb, st));
+    LAUNCH(launch_group_segments(dp.rowptr, dp.G, S, segcnt, segbase, ws<char>(ctx, "grp_seg_tmp", sb),
+                                 &sb, st));
+    int64_t nsegs = 0;
+    CK(cudaMemcpyAsync(&nsegs, segbase + dp.G, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int32_t* hist = ws<int32_t>(ctx, "grp_hist", (size_t)std::max<int64_t>(nsegs, 1) * K);
+    LAUNCH(launch_group_csr(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.G, segbase, S, fkey, K, hist,
+                            nsegs, gptr, gcol, gval, st));
     dbg_mark(ctx, "g.csr");
     CK(cudaMemcpyAsync(h + 1, bad + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -1051,7 +1063,8 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     double* ginv = ws<double>(ctx, "ginv", (size_t)P * P);
     int32_t* err = ws<int32_t>(ctx, "qr_err", 1);
     if (!o->init_beta_rough) {
-        LAUNCH(launch_xtx_inverse(dp.Xcm, dp.n, P, ginv, err, st));
+        double* part = ws<double>(ctx, "xtx_part", (size_t)xtx_blocks(dp.n) * P * (P + 1) / 2);
+        LAUNCH(launch_xtx_inverse(dp.Xcm, dp.n, P, part, ginv, err, st));
         int32_t herr = 0;
         CK(cudaMemcpyAsync(&herr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -1437,7 +1450,8 @@ int devil_init_beta(devil_ctx* ctx, const devil_counts* counts, const double* X,
         double* ginv = ws<double>(ctx, "ginv", (size_t)p * p);
         int32_t* err = ws<int32_t>(ctx, "qr_err", 1);
         if (!rough) {
-            LAUNCH(launch_xtx_inverse(dp.Xcm, dp.n, p, ginv, err, ctx->stream));
+            double* part = ws<double>(ctx, "xtx_part", (size_t)xtx_blocks(dp.n) * p * (p + 1) / 2);
+            LAUNCH(launch_xtx_inverse(dp.Xcm, dp.n, p, part, ginv, err, ctx->stream));
             int32_t herr = 0;
             CK(cudaMemcpyAsync(&herr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));

@@ -104,8 +104,16 @@ cudaError_t launch_group_rules(const int32_t* permC, const int64_t* gsC, const i
                                int32_t* bad, cudaStream_t st);
 cudaError_t launch_gather_keys(const int32_t* keys, const int32_t* cells, int64_t n, int32_t* out,
                                cudaStream_t st);
+int group_csr_segment(int64_t nnz, int64_t G, int K);  // entries per segment
+// segbase (G+1) = exclusive scan of ceil(row length / S); segcnt: G+1
+// scratch; a null scan_tmp queries the scan's temporary bytes
+cudaError_t launch_group_segments(const int64_t* rowptr, int64_t G, int S, int64_t* segcnt,
+                                  int64_t* segbase, void* scan_tmp, size_t* scan_bytes,
+                                  cudaStream_t st);
+// hist: nsegs x K (nsegs = segbase[G])
 cudaError_t launch_group_csr(const int64_t* rowptr, const int32_t* col, const void* val, int val_u16,
-                             int64_t G, const int32_t* fkey, int K, int64_t* gptr, int32_t* gcol,
+                             int64_t G, const int64_t* segbase, int S, const int32_t* fkey, int K,
+                             int32_t* hist, int64_t nsegs, int64_t* gptr, int32_t* gcol,
                              void* gval, cudaStream_t st);
 
 // ---- preparation kernels (kernels_prep.cu) ----
@@ -138,7 +146,8 @@ cudaError_t launch_sf_given(const double* sf_in, int64_t n, double offset, int u
 cudaError_t launch_theta0(const double* stats, const double* off, int64_t G, int64_t n,
                           int has_init, double init_value, double* theta0, float* k,
                           cudaStream_t st);
-cudaError_t launch_xtx_inverse(const double* Xcm, int64_t n, int P, double* ginv,
+int xtx_blocks(int64_t n);  // partial-sum blocks launch_xtx_inverse needs
+cudaError_t launch_xtx_inverse(const double* Xcm, int64_t n, int P, double* part, double* ginv,
                                int32_t* err, cudaStream_t st);
 cudaError_t launch_init_beta(const int64_t* rowptr, const int32_t* col, const void* val,
                              int val_u16, const double* Xrm, int xs, const double* off,

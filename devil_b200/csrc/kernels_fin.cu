@@ -3,6 +3,7 @@
 #include <type_traits>
 
 #include "internal.h"
+#include "warp_la.cuh"
 
 namespace devil {
 
@@ -45,38 +46,38 @@ __global__ void irls_finalize_kernel(const TW* partW, int nseg, int slot_stride,
                                      int32_t* n_next, double* beta, float* beta_f, int32_t* iters,
                                      int32_t* status, int max_iter, double eps, const float* kf) {
     extern __shared__ double fsh[];
-    const int NE = P * (P + 1) / 2, NA = NE + P;
+    const int NE = P * (P + 1) / 2, NA = NE + P, LD = wla_ld(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = NA + P * P + P + P;  // sums, H, S, piv (as doubles)
+    const int per = NA + P * LD + 2 * P + P;  // sums, H, S, x, perm
     double* sums = fsh + warp * per;
     double* H = sums + NA;
-    double* S = H + P * P;
-    int* piv = reinterpret_cast<int*>(S + P);
+    double* S = H + P * LD;
+    double* xs = S + P;
+    int* perm = reinterpret_cast<int*>(xs + P);
     const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
     const int nact = *n_act;
     if (slot >= nact) return;
     const int g = act[slot];
     reduce_partials(partW, nseg, slot_stride, slot, NA, NA, sums, lane);
     __syncwarp();
-    if (lane != 0) return;
     // the pass accumulates H / k^2 and -score / k (see PassIRLS)
     const double k = (double)kf[g];
-    unpack_sym(P, sums, H);
-    for (int i = 0; i < P * P; ++i) H[i] *= k * k;
-    for (int i = 0; i < P; ++i) S[i] = -k * sums[NE + i];
-    lu_factor(P, H, piv);
-    lu_solve(P, H, piv, S);
+    warp_unpack_sym(P, sums, k * k, 0.0, H, LD);
+    if (lane < P) S[lane] = -k * sums[NE + lane];
+    warp_lu(H, LD, P, perm);
+    if (lane != 0) return;
+    lu_solve_perm(H, LD, P, perm, S, xs);
     double mx = 0.0;
     for (int i = 0; i < P; ++i) {
-        double b = beta[(int64_t)g * P + i] + S[i];
+        double b = beta[(int64_t)g * P + i] + xs[i];
         beta[(int64_t)g * P + i] = b;
         beta_f[(int64_t)g * P + i] = (float)b;
-        double a = fabs(S[i]);
+        double a = fabs(xs[i]);
         if (a > mx) mx = a;  // NaN entries never compare greater
     }
     const int it = iters[g] + 1;
     iters[g] = it;
-    const bool isnan0 = !(S[0] == S[0]);
+    const bool isnan0 = !(xs[0] == xs[0]);
     const bool conv = mx < eps;
     if (isnan0) {
         status[g] = 2;  // DEVIL_GENE_NAN
@@ -97,7 +98,7 @@ cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slo
                                  const float* k, cudaStream_t st) {
     if (max_slots <= 0) return cudaSuccess;
     const int NA = P * (P + 1) / 2 + P;
-    const size_t per = (size_t)(NA + P * P + 2 * P) * sizeof(double);
+    const size_t per = (size_t)(NA + P * wla_ld(P) + 3 * P) * sizeof(double);
     const int w = fin_warps(per);
     const size_t smem = per * w;
     auto go = [&](auto* pw) -> cudaError_t {
@@ -188,21 +189,39 @@ __global__ void mle_finalize_kernel(const TW* partW, const double* partS, int ns
                                     int32_t* n_next, MleState st, int max_iter, int cox_reid) {
     extern __shared__ double fsh[];
     const int NE = P * (P + 1) / 2, NA = 3 * NE + 2;  // b, db, d2b, two FP32 scalars
+    const int LD = wla_ld(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = NA + 6 + 4 * P * P + P;
+    const int per = NA + 6 + 4 * P * LD + P;
     double* sums = fsh + warp * per;
     double* ss = sums + NA;
     double* B = ss + 6;
-    double* Bi = B + P * P;
-    double* D = Bi + P * P;
-    double* M = D + P * P;
-    int* piv = reinterpret_cast<int*>(M + P * P);
+    double* Bi = B + P * LD;
+    double* D = Bi + P * LD;
+    double* M = D + P * LD;
+    int* perm = reinterpret_cast<int*>(M + P * LD);
     const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
     if (slot >= *n_act) return;
     const int g = act[slot];
     reduce_partials(partW, nseg, slot_stride, slot, NA, NA, sums, lane);
     reduce_partials(partS, nseg, slot_stride, slot, 4, 4, ss + 2, lane);
     __syncwarp();
+    // Cox-Reid terms (warp-parallel): B = b + 1e-6 I (inv_sympd), M = B^-1 db
+    double cr_s = 0.0, cr_d = 0.0, cr_d2 = 0.0;
+    if (cox_reid) {
+        warp_unpack_sym(P, sums, 1.0, 1e-6, B, LD);
+        warp_lu(B, LD, P, perm);
+        warp_lu_inverse(B, LD, P, perm, Bi, LD);
+        warp_unpack_sym(P, sums + NE, 1.0, 0.0, D, LD);  // db
+        warp_matmul(P, Bi, D, M, LD);
+        const double ddetb = warp_sum(lane < P ? M[lane * LD + lane] : 0.0);
+        const double trmm = warp_trace_prod(P, M, M, LD);
+        warp_unpack_sym(P, sums + 2 * NE, 1.0, 0.0, D, LD);  // d2b
+        const double trbd2 = warp_trace_prod(P, Bi, D, LD);
+        const double d2detb = ddetb * ddetb - trmm + trbd2;
+        cr_s = -0.5 * ddetb * kCrFactor;
+        cr_d = (0.5 * ddetb * ddetb - 0.5 * d2detb) * kCrFactor;
+        cr_d2 = -0.5 * ddetb * kCrFactor;
+    }
     if (lane != 0) return;
     // ss[0..5]: sum ll_term, sum mu x/(1+x)^2, sum y theta/(1+x), sum y/(1+x)^2,
     // digamma sum, trigamma sum
@@ -211,33 +230,6 @@ __global__ void mle_finalize_kernel(const TW* partW, const double* partS, int ns
 
     const double x = st.x[g];
     const double theta = exp(x), a = 1.0 / theta;
-    // Cox-Reid terms
-    double cr_s = 0.0, cr_d = 0.0, cr_d2 = 0.0;
-    if (cox_reid) {
-        unpack_sym(P, sums, B);
-        for (int i = 0; i < P; ++i) B[i * P + i] += 1e-6;  // inv_sympd(b + 1e-6 I)
-        lu_factor(P, B, piv);
-        lu_inverse(P, B, piv, Bi);
-        unpack_sym(P, sums + NE, D);  // db
-        // M = Bi * db
-        for (int j = 0; j < P; ++j)
-            for (int i = 0; i < P; ++i) {
-                double s = 0.0;
-                for (int k = 0; k < P; ++k) s += Bi[k * P + i] * D[j * P + k];
-                M[j * P + i] = s;
-            }
-        double ddetb = 0.0, trmm = 0.0, trbd2 = 0.0;
-        for (int i = 0; i < P; ++i) ddetb += M[i * P + i];
-        for (int i = 0; i < P; ++i)
-            for (int k = 0; k < P; ++k) trmm += M[k * P + i] * M[i * P + k];
-        unpack_sym(P, sums + 2 * NE, D);  // d2b
-        for (int i = 0; i < P; ++i)
-            for (int k = 0; k < P; ++k) trbd2 += Bi[k * P + i] * D[i * P + k];
-        double d2detb = ddetb * ddetb - trmm + trbd2;
-        cr_s = -0.5 * ddetb * kCrFactor;
-        cr_d = (0.5 * ddetb * ddetb - 0.5 * d2detb) * kCrFactor;
-        cr_d2 = -0.5 * ddetb * kCrFactor;
-    }
     const double* gs = stats + (int64_t)g * 6;
     const double sum_y = gs[2], sum_prod_y = gs[3], max_y = gs[4];
     // score (src/overdispersion.cpp:139-177)
@@ -331,7 +323,7 @@ cudaError_t launch_mle_finalize(const void* partW, bool wide, const double* part
     (void)mirror;
     if (max_slots <= 0) return cudaSuccess;
     const int NA = 3 * (P * (P + 1) / 2) + 2;
-    const size_t per = (size_t)(NA + 6 + 4 * P * P + P) * sizeof(double);
+    const size_t per = (size_t)(NA + 6 + 4 * P * wla_ld(P) + P) * sizeof(double);
     const int w = fin_warps(per);
     const size_t smem = per * w;
     auto go = [&](auto* pw) -> cudaError_t {
@@ -361,21 +353,21 @@ __global__ void sandwich_finalize_kernel(const double* partW, int nseg, int slot
                                          const int32_t* act, const int32_t* n_act, double* bread,
                                          double* sandwich, double* meat_out) {
     extern __shared__ double fsh[];
-    const int NE = P * (P + 1) / 2, NA = NE + P;
+    const int NE = P * (P + 1) / 2, NA = NE + P, LD = wla_ld(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = NA + 4 * P * P + 2 * P;
+    const int per = NA + 4 * P * LD + 2 * P;
     double* sums = fsh + warp * per;
     double* H = sums + NA;
-    double* Bi = H + P * P;
-    double* Mt = Bi + P * P;
-    double* T = Mt + P * P;
-    double* cur = T + P * P;
-    int* piv = reinterpret_cast<int*>(cur + P);
+    double* Bi = H + P * LD;
+    double* Mt = Bi + P * LD;
+    double* T = Mt + P * LD;
+    double* cur = T + P * LD;
+    int* perm = reinterpret_cast<int*>(cur + P);
     const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
     if (slot >= *n_act) return;
     const int g = act[slot];
     reduce_partials(partW, nseg, slot_stride, slot, NA, NE, sums, lane);  // H part only
-    for (int i = lane; i < P * P; i += 32) Mt[i] = 0.0;
+    for (int i = lane; i < P * LD; i += 32) Mt[i] = 0.0;
     __syncwarp();
     if (n_clusters > 0) {
         // lane i holds component i of the running cluster sum
@@ -387,41 +379,39 @@ __global__ void sandwich_finalize_kernel(const double* partW, int nseg, int slot
                 if (lane < P) cur[lane] = acc;
                 __syncwarp();
                 for (int i = lane; i < P * P; i += 32) {
-                    int r = i % P, c = i / P;
-                    Mt[i] += cur[r] * cur[c];
+                    const int r = i / P, c = i - r * P;
+                    Mt[r * LD + c] += cur[r] * cur[c];
                 }
                 __syncwarp();
                 acc = 0.0;
             }
         }
     }
-    __syncwarp();
-    if (lane != 0) return;
-    unpack_sym(P, sums, H);
-    lu_factor(P, H, piv);
-    lu_inverse(P, H, piv, Bi);
-    double* bo = bread + (int64_t)g * P * P;
-    for (int i = 0; i < P * P; ++i) bo[i] = Bi[i];
+    warp_unpack_sym(P, sums, 1.0, 0.0, H, LD);
+    warp_lu(H, LD, P, perm);
+    warp_lu_inverse(H, LD, P, perm, Bi, LD);
+    double* bo = bread + (int64_t)g * P * P;  // column-major
+    for (int q = lane; q < P * P; q += 32) {
+        const int c = q / P, r = q - c * P;
+        bo[q] = Bi[r * LD + c];
+    }
     if (n_clusters > 0) {
-        double adj = n_clusters > 1 ? (double)n_clusters / (n_clusters - 1.0) : 1.0;
-        for (int i = 0; i < P * P; ++i) Mt[i] *= adj / (double)n;
+        const double adj = n_clusters > 1 ? (double)n_clusters / (n_clusters - 1.0) : 1.0;
+        for (int i = lane; i < P * LD; i += 32) Mt[i] *= adj / (double)n;
+        __syncwarp();
         if (meat_out)
-            for (int i = 0; i < P * P; ++i) meat_out[(int64_t)g * P * P + i] = Mt[i];
+            for (int q = lane; q < P * P; q += 32) {
+                const int c = q / P, r = q - c * P;
+                meat_out[(int64_t)g * P * P + q] = Mt[r * LD + c];
+            }
         if (sandwich) {
-            // T = Bi * Mt ; S = T * Bi * n
-            for (int j = 0; j < P; ++j)
-                for (int i = 0; i < P; ++i) {
-                    double s = 0.0;
-                    for (int k = 0; k < P; ++k) s += Bi[k * P + i] * Mt[j * P + k];
-                    T[j * P + i] = s;
-                }
+            warp_matmul(P, Bi, Mt, T, LD);  // T = Bi Mt
+            warp_matmul(P, T, Bi, H, LD);   // H = T Bi (H is free after the inverse)
             double* so = sandwich + (int64_t)g * P * P;
-            for (int j = 0; j < P; ++j)
-                for (int i = 0; i < P; ++i) {
-                    double s = 0.0;
-                    for (int k = 0; k < P; ++k) s += T[k * P + i] * Bi[j * P + k];
-                    so[j * P + i] = s * (double)n;
-                }
+            for (int q = lane; q < P * P; q += 32) {
+                const int c = q / P, r = q - c * P;
+                so[q] = H[r * LD + c] * (double)n;
+            }
         }
     }
 }
@@ -432,7 +422,7 @@ cudaError_t launch_sandwich_finalize(const double* partW, int nseg, int slot_str
                                      cudaStream_t st) {
     if (max_slots <= 0) return cudaSuccess;
     const int NA = P * (P + 1) / 2 + P;
-    const size_t per = (size_t)(NA + 4 * P * P + 2 * P) * sizeof(double);
+    const size_t per = (size_t)(NA + 4 * P * wla_ld(P) + 2 * P) * sizeof(double);
     const int w = fin_warps(per);
     const size_t smem = per * w;
     if (smem > 48 * 1024) {

@@ -363,44 +363,96 @@ __global__ void __launch_bounds__(kRuleNT) group_rules_kernel(
 }
 
 // ---------------------------------------------------------------------
-// CSR copy ordered by group within each gene (stable), with per-gene
-// group offsets gptr[g][k] (absolute; gptr[g][K] = row end).  Warp per gene;
-// per-warp cursors in shared memory.
+// CSR copy ordered by key within each gene (stable), with per-gene key
+// offsets gptr[g][k] (absolute; gptr[g][K] = row end).  Each row is cut
+// into segments of S entries so that long rows spread over many warps:
+//   1. count the keys of every segment (warp per segment),
+//   2. per gene, turn the counts into the first output position of every
+//      (segment, key) in key-major, segment-minor order (block per gene),
+//   3. scatter every segment's entries from those cursors, in order
+//      (warp per segment; ranks among equal keys from __match_any_sync).
 // ---------------------------------------------------------------------
+__global__ void seg_count_kernel(const int64_t* rowptr, int64_t G, int S, int64_t* nseg) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    const int64_t len = rowptr[g + 1] - rowptr[g];
+    nseg[g] = (len + S - 1) / S;
+}
+
+// gene of global segment s: last g with segbase[g] <= s (segbase has G+1 entries)
+DEV int64_t seg_gene(const int64_t* segbase, int64_t G, int64_t s) {
+    int64_t lo = 0, hi = G;  // invariant: segbase[lo] <= s < segbase[hi]
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (segbase[mid] <= s) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void seg_hist_kernel(const int64_t* rowptr, const int32_t* col, int64_t G,
+                                const int64_t* segbase, int S, const int32_t* fkey, int K,
+                                int32_t* hist) {
+    extern __shared__ int32_t cnt_all[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
+    if (s >= segbase[G]) return;
+    int32_t* cnt = cnt_all + (int64_t)w * K;
+    for (int k = lane; k < K; k += 32) cnt[k] = 0;
+    __syncwarp();
+    const int64_t g = seg_gene(segbase, G, s);
+    const int64_t r0 = rowptr[g] + (s - segbase[g]) * S;
+    const int64_t r1 = min(r0 + S, rowptr[g + 1]);
+    for (int64_t e = r0 + lane; e < r1; e += 32) atomicAdd(&cnt[fkey[col[e]]], 1);
+    __syncwarp();
+    int32_t* h = hist + s * K;
+    for (int k = lane; k < K; k += 32) h[k] = cnt[k];
+}
+
+constexpr int kOffNT = 256;
+__global__ void __launch_bounds__(kOffNT) seg_offsets_kernel(const int64_t* rowptr, int64_t G,
+                                                             const int64_t* segbase, int K,
+                                                             int32_t* hist, int64_t* gptr) {
+    using Scan = cub::BlockScan<int64_t, kOffNT>;
+    __shared__ typename Scan::TempStorage tmp;
+    const int64_t g = blockIdx.x;
+    const int t = threadIdx.x;
+    const int64_t s0 = segbase[g], s1 = segbase[g + 1];
+    const int64_t r0 = rowptr[g];
+    // thread t owns keys [t*per, (t+1)*per)
+    const int per = (K + kOffNT - 1) / kOffNT;
+    const int k0 = min(K, t * per), k1 = min(K, k0 + per);
+    int64_t local = 0;
+    for (int k = k0; k < k1; ++k)
+        for (int64_t s = s0; s < s1; ++s) local += hist[s * K + k];
+    int64_t excl;
+    Scan(tmp).ExclusiveSum(local, excl);
+    int64_t run = excl;  // offset of key k0 relative to the row start
+    for (int k = k0; k < k1; ++k) {
+        gptr[g * (K + 1) + k] = r0 + run;
+        for (int64_t s = s0; s < s1; ++s) {
+            const int32_t c = hist[s * K + k];
+            hist[s * K + k] = (int32_t)run;
+            run += c;
+        }
+    }
+    if (t == 0) gptr[g * (K + 1) + K] = rowptr[g + 1];
+}
+
 template <class VT>
-__global__ void group_csr_kernel(const int64_t* rowptr, const int32_t* col, const VT* val, int64_t G,
-                                 const int32_t* fkey, int K, int64_t* gptr, int32_t* gcol,
-                                 VT* gval) {
+__global__ void seg_scatter_kernel(const int64_t* rowptr, const int32_t* col, const VT* val,
+                                   int64_t G, const int64_t* segbase, int S, const int32_t* fkey,
+                                   int K, const int32_t* hist, int32_t* gcol, VT* gval) {
     extern __shared__ int32_t cur_all[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
-    if (g >= G) return;
+    const int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
+    if (s >= segbase[G]) return;
     int32_t* cur = cur_all + (int64_t)w * K;
-    for (int k = lane; k < K; k += 32) cur[k] = 0;
+    for (int k = lane; k < K; k += 32) cur[k] = hist[s * K + k];
     __syncwarp();
-    const int64_t r0 = rowptr[g], r1 = rowptr[g + 1];
-    for (int64_t e = r0 + lane; e < r1; e += 32) atomicAdd(&cur[fkey[col[e]]], 1);
-    __syncwarp();
-    int64_t* gp = gptr + g * (K + 1);
-    int64_t run = r0;
-    for (int base = 0; base < K; base += 32) {
-        const int k = base + lane;
-        const int v = k < K ? cur[k] : 0;
-        int incl = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int u = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += u;
-        }
-        const int64_t excl = run + incl - v;
-        if (k < K) {
-            gp[k] = excl;
-            cur[k] = (int32_t)(excl - r0);
-        }
-        run += __shfl_sync(0xffffffffu, incl, 31);
-    }
-    if (lane == 0) gp[K] = r1;
-    __syncwarp();
+    const int64_t g = seg_gene(segbase, G, s);
+    const int64_t rs = rowptr[g];
+    const int64_t r0 = rs + (s - segbase[g]) * S;
+    const int64_t r1 = min(r0 + S, rowptr[g + 1]);
     const unsigned lt = (1u << lane) - 1u;
     for (int64_t base = r0; base < r1; base += 32) {
         const int64_t e = base + lane;
@@ -418,8 +470,8 @@ __global__ void group_csr_kernel(const int64_t* rowptr, const int32_t* col, cons
         const int pos = valid ? cur[k] + rank : 0;
         __syncwarp();
         if (valid) {
-            gcol[r0 + pos] = c;
-            gval[r0 + pos] = v;
+            gcol[rs + pos] = c;
+            gval[rs + pos] = v;
             if (lane == __ffs(peers) - 1) cur[k] += __popc(peers);
         }
         __syncwarp();
@@ -452,6 +504,8 @@ struct GrpAcc {
     template <int K, int NW, int NV>
     DEV void fscal(double v) { w[NW + NV + K] += q * v; }
 };
+
+constexpr int kGrpUnr = 8;  // entries per lane per batch of the nonzero loop
 
 template <class Pass, class VT>
 __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pass::Params prm) {
@@ -506,20 +560,44 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
         // nonzero corrections over the group's CSR range
         const int64_t e0 = __ldg(gp + (geo.fine ? q : u * C));
         const int64_t e1 = __ldg(gp + (geo.fine ? q + 1 : u * C + C));
+        // batches of kGrpUnr entries per lane, software-pipelined: the next
+        // batch's cell indices and counts are in flight while this batch
+        // gathers exp(offset) and accumulates
         int64_t e = e0 + lane;
-        for (; e + 96 < e1; e += 128) {
-            int c[4];
-            float y[4];
-            double ev[4];
+        constexpr int U8 = kGrpUnr;
+        if (e + 32 * (U8 - 1) < e1) {
+            int c[U8];
+            float y[U8];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
+            for (int j = 0; j < U8; ++j) {
                 c[j] = __ldg(geo.gcol + e + 32 * j);
                 y[j] = load_val(gval, e + 32 * j);
             }
+            for (;;) {
+                double ev[U8];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) ev[j] = __ldg(geo.E + c[j]);
+                for (int j = 0; j < U8; ++j) ev[j] = __ldg(geo.E + c[j]);
+                const int64_t en = e + 32 * U8;
+                const bool more = en + 32 * (U8 - 1) < e1;
+                int cn[U8];
+                float yn[U8];
+                if (more) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) Pass::template sparse<double>(gpar, A * ev[j], y[j], acc);
+                    for (int j = 0; j < U8; ++j) {
+                        cn[j] = __ldg(geo.gcol + en + 32 * j);
+                        yn[j] = load_val(gval, en + 32 * j);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < U8; ++j) Pass::template sparse<double>(gpar, A * ev[j], y[j], acc);
+                e = en;
+                if (!more) break;
+#pragma unroll
+                for (int j = 0; j < U8; ++j) {
+                    c[j] = cn[j];
+                    y[j] = yn[j];
+                }
+            }
         }
         for (; e < e1; e += 32) {
             const int c = __ldg(geo.gcol + e);
@@ -726,22 +804,44 @@ cudaError_t launch_group_rules(const int32_t* permC, const int64_t* gsC, const i
                                                              rs, rw, rm, rerr, bad);
     return cudaGetLastError();
 }
+int group_csr_segment(int64_t nnz, int64_t G, int K) {
+    int S = 2048;  // entries per segment; the count table stays below 2^27 entries
+    while (((nnz / S) + G) * (int64_t)K > ((int64_t)1 << 27) && S < (1 << 24)) S *= 2;
+    return S;
+}
+
+cudaError_t launch_group_segments(const int64_t* rowptr, int64_t G, int S, int64_t* segcnt,
+                                  int64_t* segbase, void* scan_tmp, size_t* scan_bytes,
+                                  cudaStream_t st) {
+    if (!scan_tmp)  // size query
+        return cub::DeviceScan::ExclusiveSum(nullptr, *scan_bytes, segcnt, segbase, (int)(G + 1));
+    cudaError_t e = cudaMemsetAsync(segcnt + G, 0, sizeof(int64_t), st);
+    if (e != cudaSuccess) return e;
+    if (G > 0) seg_count_kernel<<<nblk(G, 256), 256, 0, st>>>(rowptr, G, S, segcnt);
+    return cub::DeviceScan::ExclusiveSum(scan_tmp, *scan_bytes, segcnt, segbase, (int)(G + 1), st);
+}
+
 cudaError_t launch_group_csr(const int64_t* rowptr, const int32_t* col, const void* val, int val_u16,
-                             int64_t G, const int32_t* fkey, int K, int64_t* gptr, int32_t* gcol,
+                             int64_t G, const int64_t* segbase, int S, const int32_t* fkey, int K,
+                             int32_t* hist, int64_t nsegs, int64_t* gptr, int32_t* gcol,
                              void* gval, cudaStream_t st) {
     if (G <= 0) return cudaSuccess;
-    int wpb = 12288 / K;  // 48 KB of cursors per block
+    int wpb = 12288 / K;  // 48 KB of per-warp key tables per block
     wpb = wpb < 1 ? 1 : (wpb > 8 ? 8 : wpb);
     const size_t smem = (size_t)wpb * K * sizeof(int32_t);
-    const unsigned grid = (unsigned)((G + wpb - 1) / wpb);
-    if (val_u16)
-        group_csr_kernel<uint16_t><<<grid, 32 * wpb, smem, st>>>(
-            rowptr, col, static_cast<const uint16_t*>(val), G, fkey, K, gptr, gcol,
-            static_cast<uint16_t*>(gval));
-    else
-        group_csr_kernel<float><<<grid, 32 * wpb, smem, st>>>(
-            rowptr, col, static_cast<const float*>(val), G, fkey, K, gptr, gcol,
-            static_cast<float*>(gval));
+    const unsigned grid = (unsigned)((nsegs + wpb - 1) / wpb);
+    if (grid > 0) seg_hist_kernel<<<grid, 32 * wpb, smem, st>>>(rowptr, col, G, segbase, S, fkey, K, hist);
+    seg_offsets_kernel<<<(unsigned)G, kOffNT, 0, st>>>(rowptr, G, segbase, K, hist, gptr);
+    if (grid > 0) {
+        if (val_u16)
+            seg_scatter_kernel<uint16_t><<<grid, 32 * wpb, smem, st>>>(
+                rowptr, col, static_cast<const uint16_t*>(val), G, segbase, S, fkey, K, hist, gcol,
+                static_cast<uint16_t*>(gval));
+        else
+            seg_scatter_kernel<float><<<grid, 32 * wpb, smem, st>>>(
+                rowptr, col, static_cast<const float*>(val), G, segbase, S, fkey, K, hist, gcol,
+                static_cast<float*>(gval));
+    }
     return cudaGetLastError();
 }
 

@@ -373,28 +373,73 @@ cudaError_t launch_theta0(const double* stats, const double* off, int64_t G, int
 // ------------------------------------------------------------------
 // (X'X)^-1 in FP64 (one block): the least-squares solve of init_beta
 // ------------------------------------------------------------------
-__global__ void xtx_inverse_kernel(const double* Xcm, int64_t n, int P, double* ginv,
-                                   int32_t* err) {
-    extern __shared__ double sh[];
-    double* Gm = sh;               // P*P
-    double* W = sh + P * P;        // P*P
-    int* piv = reinterpret_cast<int*>(W + P * P);
+// partial X'X over the cells of one block (kXtxCells cells, staged in
+// shared memory 256 at a time, row stride P+1); thread t owns packed
+// pairs t, t + 256, ...
+constexpr int kXtxCells = 8192;
+constexpr int kXtxStage = 256;
+__global__ void __launch_bounds__(256) xtx_partial_kernel(const double* Xcm, int64_t n, int P,
+                                                          double* part) {
+    extern __shared__ double xs[];  // [kXtxStage][P + 1]
     const int NP = P * (P + 1) / 2;
-    for (int q = threadIdx.x >> 5; q < NP; q += blockDim.x >> 5) {
+    const int RS = P + 1;
+    const int64_t c0 = (int64_t)blockIdx.x * kXtxCells;
+    const int64_t c1 = c0 + kXtxCells < n ? c0 + kXtxCells : n;
+    double acc[3] = {0.0, 0.0, 0.0};  // NP <= 528 = 256 * 3 (rounded up)
+    int pi[3], pj[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int q = threadIdx.x + k * 256;
         int j = 0;
         while ((j + 1) * (j + 2) / 2 <= q) ++j;
-        int i = q - j * (j + 1) / 2;
+        pi[k] = q < NP ? q - j * (j + 1) / 2 : 0;
+        pj[k] = q < NP ? j : 0;
+    }
+    for (int64_t cb = c0; cb < c1; cb += kXtxStage) {
+        const int nc = (int)(c1 - cb < kXtxStage ? c1 - cb : kXtxStage);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nc * P; i += blockDim.x) {
+            const int col = i / nc, c = i - col * nc;  // coalesced along cells
+            xs[c * RS + col] = Xcm[(int64_t)col * n + cb + c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (threadIdx.x + k * 256 >= NP) break;
+            double s = 0.0;
+            for (int c = 0; c < nc; ++c) s = fma(xs[c * RS + pi[k]], xs[c * RS + pj[k]], s);
+            acc[k] += s;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int q = threadIdx.x + k * 256;
+        if (q < NP) part[(int64_t)blockIdx.x * NP + q] = acc[k];
+    }
+}
+
+// sum the partials in block order (deterministic), then invert with LU;
+// rank check on the pivots relative to the largest diagonal
+__global__ void xtx_finish_kernel(const double* part, int nb, int P, double* ginv, int32_t* err) {
+    extern __shared__ double sh[];
+    double* Gm = sh;         // P*P
+    double* W = sh + P * P;  // P*P
+    int* piv = reinterpret_cast<int*>(W + P * P);
+    const int NP = P * (P + 1) / 2;
+    for (int q = threadIdx.x; q < NP; q += blockDim.x) {
+        int j = 0;
+        while ((j + 1) * (j + 2) / 2 <= q) ++j;
+        const int i = q - j * (j + 1) / 2;
         double s = 0.0;
-        for (int64_t c = threadIdx.x & 31; c < n; c += 32) s += Xcm[(int64_t)i * n + c] * Xcm[(int64_t)j * n + c];
-        s = warp_sum(s);
-        if ((threadIdx.x & 31) == 0) { Gm[j * P + i] = s; Gm[i * P + j] = s; }
+        for (int b = 0; b < nb; ++b) s += part[(int64_t)b * NP + q];
+        Gm[j * P + i] = s;
+        Gm[i * P + j] = s;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         double dmax = 0.0;
         for (int i = 0; i < P; ++i) dmax = fmax(dmax, fabs(Gm[i * P + i]));
         bool ok = lu_factor(P, Gm, piv);
-        // rank check on the pivots, relative to the largest diagonal
         for (int i = 0; i < P; ++i)
             if (!(fabs(Gm[i * P + i]) > 1e-12 * dmax)) ok = false;
         if (ok) lu_inverse(P, Gm, piv, W);
@@ -402,10 +447,21 @@ __global__ void xtx_inverse_kernel(const double* Xcm, int64_t n, int P, double* 
         *err = ok ? 0 : 1;
     }
 }
-cudaError_t launch_xtx_inverse(const double* Xcm, int64_t n, int P, double* ginv, int32_t* err,
-                               cudaStream_t st) {
-    size_t smem = (size_t)2 * P * P * 8 + (size_t)P * 4 + 16;
-    xtx_inverse_kernel<<<1, 1024, smem, st>>>(Xcm, n, P, ginv, err);
+
+int xtx_blocks(int64_t n) { return (int)((n + kXtxCells - 1) / kXtxCells); }
+
+// (X'X)^-1 in FP64 for the least-squares solve of init_beta: partial
+// sums over cell blocks on every SM, then one block sums and inverts
+cudaError_t launch_xtx_inverse(const double* Xcm, int64_t n, int P, double* part, double* ginv,
+                               int32_t* err, cudaStream_t st) {
+    const int nb = xtx_blocks(n);
+    const size_t sm1 = (size_t)kXtxStage * (P + 1) * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(xtx_partial_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+    if (e != cudaSuccess) return e;
+    xtx_partial_kernel<<<nb, 256, sm1, st>>>(Xcm, n, P, part);
+    const size_t sm2 = (size_t)2 * P * P * 8 + (size_t)P * 4 + 16;
+    xtx_finish_kernel<<<1, 256, sm2, st>>>(part, nb, P, ginv, err);
     return cudaGetLastError();
 }
 
