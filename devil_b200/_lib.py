@@ -34,6 +34,7 @@ EXPORTS = (
     "devil_estimate_mom_dispersion", "devil_fit_dispersion", "devil_compute_hessian",
     "devil_compute_clustered_meat", "devil_nb_adjoint", "devil_cluster_blocks",
     "devil_group_order", "devil_ctx_set_profiling", "devil_ctx_profile", "devil_ctx_engine",
+    "devil_p_adjust_device_static",
     "devil_p_adjust_device",
 )
 
@@ -117,6 +118,7 @@ def load():
         L.devil_ctx_profile.argtypes = [vp, i, C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]
         L.devil_ctx_engine.argtypes = [vp, i]
         L.devil_ctx_engine.restype = i
+        L.devil_p_adjust_device_static.argtypes = [i64, vp, i, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
 

@@ -186,6 +186,20 @@ DEVIL_API int devil_p_adjust(devil_ctx *ctx, int64_t m, const double *p, int met
 DEVIL_API int devil_p_adjust_device(devil_ctx *ctx, int64_t m, const double *p_dev, int method,
                                     double *out_dev);
 
+/* The same adjustment for callers that cannot allocate device memory (no
+ * counterpart in the reference): no context, no cudaMalloc / cudaFree; the
+ * scratch is a 4 MiB file-scope device array held by every GPU that loads
+ * the library, so m <= 65536 (larger m: DEVIL_ERR_ARG with a message in
+ * errbuf).  Runs on `stream` (cudaStream_t, NULL = legacy default) of the
+ * current device.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and should come before any stream capture.  The
+ * array is shared by every call on a device: calls must not overlap in
+ * time (serialise them, e.g. on one stream).  errbuf (may be NULL)
+ * receives a message on failure. */
+DEVIL_API int devil_p_adjust_device_static(int64_t m, const double *p_dev, int method,
+                                           double *out_dev, void *stream, char *errbuf,
+                                           size_t errlen);
+
 /* ---- single steps (each mirrors one reference function) -------------- */
 /* calculate_sf / normed_sum_sf / psinorm_sf (R/size_factors.R:37-117) */
 DEVIL_API int devil_calculate_sf(devil_ctx *ctx, const devil_counts *counts, int method, double *sf);
