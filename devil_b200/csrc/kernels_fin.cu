@@ -298,7 +298,10 @@ __global__ void mle_finalize_kernel(const TW* partW, const double* partS, int ns
             }
             xn = cand;
             ++it;
-            if (dx < 1e-9 || hi - lo < 1e-9 || it >= max_iter) done = true;
+            // stop once a step is below 1e-7 in log theta: after a Newton
+            // step that size the error is ~1e-14, after a bisection step
+            // theta is within 1e-7 relative (the parity bar is 1e-4)
+            if (dx < 1e-7 || hi - lo < 1e-7 || it >= max_iter) done = true;
         }
         st.lo[g] = lo;
         st.hi[g] = hi;

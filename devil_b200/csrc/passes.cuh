@@ -54,24 +54,48 @@ struct PassGeom {
 // ---------------------------------------------------------------------
 // zz holds the cell's products x_i x_j (packed upper triangle), computed
 // once per cell and shared by the gene tile.
+// (a0, a1) += (b, b) * (c0, c1) as one packed FP32x2 FMA (sm_100): two
+// correctly rounded FMAs, the same results as two fmaf, in one instruction
+DEV void fma_x2(float& a0, float& a1, float b, float c0, float c1) {
+    uint64_t acc, bb, cc;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(acc) : "f"(a0), "f"(a1));
+    asm("mov.b64 %0, {%1, %1};" : "=l"(bb) : "f"(b));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(cc) : "f"(c0), "f"(c1));
+    asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(bb), "l"(cc));
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a0), "=f"(a1) : "l"(acc));
+}
+
 template <int P, int NA, int NS, class AW, class AS, class R>
 struct RegAcc {
     AW* a;
     AS* s;
     const R* x;
     const R* zz;
+    static constexpr bool X2 = std::is_same<AW, float>::value && std::is_same<R, float>::value;
     template <int W>
     DEV void outer(R w) {
         constexpr int NE = P * (P + 1) / 2;
         constexpr int base = W * NE;
+        if constexpr (X2) {
 #pragma unroll
-        for (int q = 0; q < NE; ++q) a[base + q] += (AW)(w * zz[q]);
+            for (int q = 0; q + 1 < NE; q += 2) fma_x2(a[base + q], a[base + q + 1], w, zz[q], zz[q + 1]);
+            if constexpr (NE & 1) a[base + NE - 1] = fmaf(w, zz[NE - 1], a[base + NE - 1]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < NE; ++q) a[base + q] += (AW)(w * zz[q]);
+        }
     }
     template <int V, int NW>
     DEV void vec(R w) {
         constexpr int base = NW * (P * (P + 1) / 2) + V * P;
+        if constexpr (X2) {
 #pragma unroll
-        for (int i = 0; i < P; ++i) a[base + i] += (AW)(w * x[i]);
+            for (int i = 0; i + 1 < P; i += 2) fma_x2(a[base + i], a[base + i + 1], w, x[i], x[i + 1]);
+            if constexpr (P & 1) a[base + P - 1] = fmaf(w, x[P - 1], a[base + P - 1]);
+        } else {
+#pragma unroll
+            for (int i = 0; i < P; ++i) a[base + i] += (AW)(w * x[i]);
+        }
     }
     template <int K>
     DEV void scal(AS v) { s[K] += v; }
@@ -520,12 +544,21 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
             for (int jj = 0; jj < P; ++jj)
 #pragma unroll
                 for (int ii = 0; ii <= jj; ++ii) zz[tri_index(ii, jj)] = x[ii] * x[jj];
+            // eta of the gene tile, two genes per packed FMA
+            float e[GT];
+#pragma unroll
+            for (int j = 0; j < GT; ++j) e[j] = o;
+#pragma unroll
+            for (int j = 0; j + 1 < GT; j += 2)
+#pragma unroll
+                for (int i = 0; i < P; ++i) fma_x2(e[j], e[j + 1], x[i], beta[j][i], beta[j + 1][i]);
+            if constexpr (GT & 1) {
+#pragma unroll
+                for (int i = 0; i < P; ++i) e[GT - 1] = fmaf(x[i], beta[GT - 1][i], e[GT - 1]);
+            }
 #pragma unroll
             for (int j = 0; j < GT; ++j) {
-                float e = o;
-#pragma unroll
-                for (int i = 0; i < P; ++i) e = fmaf(x[i], beta[j][i], e);
-                float mu = ex2_approx(e);
+                float mu = ex2_approx(e[j]);
                 RegAcc<P, NAc, NSc, AW, AS, float> acc{aw[j], as[j], x, zz};
                 Pass::template dense<float>(gp[j], mu, acc);
             }
