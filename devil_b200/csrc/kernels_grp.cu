@@ -505,7 +505,9 @@ struct GrpAcc {
     DEV void fscal(double v) { w[NW + NV + K] += q * v; }
 };
 
-constexpr int kGrpUnr = 8;  // entries per lane per batch of the nonzero loop
+constexpr int kGrpUnr = 8;          // entries per lane per batch of the nonzero loop
+constexpr int kGrpChunk = 2048;     // nonzeros per work unit (at least)
+constexpr int kGrpUnitsMax = 128;   // chunks beyond one per group, per gene
 
 template <class Pass, class VT>
 __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pass::Params prm) {
@@ -519,8 +521,10 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
     const int NGq = geo.fine ? K : U;
     extern __shared__ double gsm[];
     double* xg = gsm;          // [U][P]
-    double* bet = xg + U * P;  // [P]
-    double* gs = bet + P;      // [NGq][NQ]
+    double* bet = xg + U * P;              // [P]
+    double* gs = bet + P;                  // [NGq][NQ] group sums
+    double* up = gs + NGq * NQ;            // [NGq + kGrpUnitsMax][NQ] unit sums
+    int* ustart = reinterpret_cast<int*>(up + (NGq + kGrpUnitsMax) * NQ);  // [NGq + 1]
     const int t = threadIdx.x, nt = blockDim.x;
     for (int i = t; i < U * P; i += nt) xg[i] = __ldg(geo.xg + i);
     for (int i = t; i < P; i += nt) bet[i] = __ldg(prm.beta_d + (int64_t)g * P + i);
@@ -541,7 +545,47 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
     const int warp = t >> 5, lane = t & 31, nw = nt >> 5;
     const VT* __restrict__ gval = static_cast<const VT*>(geo.gval);
     const int64_t* gp = geo.gptr + (int64_t)g * (K + 1);
-    for (int q = warp; q < NGq; q += nw) {
+    // Work units: group q's nonzeros in chunks of CH entries (at least one
+    // unit per group; its first unit also takes the rule nodes).  CH grows
+    // with the gene's nonzeros so there are at most NGq + kGrpUnitsMax
+    // units; warps take units round robin, so a large group no longer
+    // holds one warp while the others wait at the assembly barrier.
+    const int64_t CH = max((int64_t)kGrpChunk, (gp[K] - gp[0] + kGrpUnitsMax - 1) / kGrpUnitsMax);
+    if (warp == 0) {
+        int run = 0;
+        for (int base = 0; base < NGq; base += 32) {
+            const int q = base + lane;
+            int c = 0;
+            if (q < NGq) {
+                const int uq = geo.fine ? q / C : q;
+                const int64_t len = __ldg(gp + (geo.fine ? q + 1 : uq * C + C)) -
+                                    __ldg(gp + (geo.fine ? q : uq * C));
+                c = len > CH ? (int)((len + CH - 1) / CH) : 1;
+            }
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (q < NGq) ustart[q] = run + incl - c;
+            run += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) ustart[NGq] = run;
+    }
+    __syncthreads();
+    const int nunits = ustart[NGq];
+    for (int un = warp; un < nunits; un += nw) {
+        int q = 0;  // last group with ustart[q] <= un
+        {
+            int lo = 0, hi = NGq;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (ustart[mid] <= un) lo = mid; else hi = mid;
+            }
+            q = lo;
+        }
+        const int jc = un - ustart[q];
         const int u = geo.fine ? q / C : q;
         double a = lane < P ? xg[u * P + lane] * bet[lane] : 0.0;
         a = warp_sum(a);
@@ -550,7 +594,7 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
         acc.zero();
         // zero-count terms over all cells of the group: the group's rule
         const int ri = (geo.fine && C > 1) ? U + q : u;  // C == 1: fine == coarse
-        const int m = __ldg(geo.rm + ri);
+        const int m = jc == 0 ? __ldg(geo.rm + ri) : 0;
         for (int j = lane; j < m; j += 32) {
             acc.q = __ldg(geo.rw + (int64_t)ri * kRuleCap + j);
             const double mu = exp(a + __ldg(geo.rs + (int64_t)ri * kRuleCap + j));
@@ -558,8 +602,10 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
         }
         acc.q = 1.0;
         // nonzero corrections over the group's CSR range
-        const int64_t e0 = __ldg(gp + (geo.fine ? q : u * C));
-        const int64_t e1 = __ldg(gp + (geo.fine ? q + 1 : u * C + C));
+        const int64_t g0 = __ldg(gp + (geo.fine ? q : u * C));
+        const int64_t g1 = __ldg(gp + (geo.fine ? q + 1 : u * C + C));
+        const int64_t e0 = g0 + jc * CH;
+        const int64_t e1 = min(e0 + CH, g1);
         // batches of kGrpUnr entries per lane, software-pipelined: the next
         // batch's cell indices and counts are in flight while this batch
         // gathers exp(offset) and accumulates
@@ -607,13 +653,21 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
 #pragma unroll
         for (int i = 0; i < NWV; ++i) {
             const double v = warp_sum(acc.w[i]);
-            if (lane == 0) gs[q * NQ + i] = v;
+            if (lane == 0) up[un * NQ + i] = v;
         }
 #pragma unroll
         for (int i = 0; i < NS; ++i) {
             const double v = warp_sum(acc.s[i]);
-            if (lane == 0) gs[q * NQ + NWV + i] = v;
+            if (lane == 0) up[un * NQ + NWV + i] = v;
         }
+    }
+    __syncthreads();
+    // group sums over their units, in unit order (deterministic)
+    for (int i = t; i < NGq * NQ; i += nt) {
+        const int q = i / NQ, c = i - q * NQ;
+        double v = 0.0;
+        for (int un = ustart[q]; un < ustart[q + 1]; ++un) v += up[un * NQ + c];
+        gs[i] = v;
     }
     __syncthreads();
     // assemble the partial sums of the pass: one segment, or one per cluster
@@ -717,12 +771,14 @@ template <> PassSandwich::Params grp_params<PassSandwich>(const PassParamsAny& a
 
 size_t grp_smem_bytes(PassKind k, int P, int U, int NGq) {
     const int nq = pass_nw(k) + pass_nv(k) + pass_nf(k) + pass_ns(k);
-    return ((size_t)U * P + P + (size_t)NGq * nq) * sizeof(double);
+    return ((size_t)U * P + P + (size_t)NGq * nq + (size_t)(NGq + kGrpUnitsMax) * nq) *
+               sizeof(double) +
+           (size_t)(NGq + 1) * sizeof(int);
 }
 
 int grp_threads(int NGq) {
-    int w = NGq < 8 ? (NGq < 2 ? 2 : NGq) : 8;
-    return 32 * w;
+    (void)NGq;  // work units split large groups: 8 warps always have work
+    return 256;
 }
 
 template <class Pass>

@@ -67,10 +67,17 @@ static cudaError_t run(const PassLaunch& L) {
             return cudaGetLastError();
         }
     }
-    if (L.val_u16)
-        reg_pass_kernel<P, PP, GT, kRegNT, Pass, uint16_t><<<grid, kRegNT, 0, L.stream>>>(L.geo, prm);
-    else
-        reg_pass_kernel<P, PP, GT, kRegNT, Pass, float><<<grid, kRegNT, 0, L.stream>>>(L.geo, prm);
+    if constexpr (K == PASS_IRLS) {
+        if (L.val_u16)
+            reg_pass_kernel<P, PP, GT, kRegNT, Pass, uint16_t><<<grid, kRegNT, 0, L.stream>>>(L.geo, prm);
+        else
+            reg_pass_kernel<P, PP, GT, kRegNT, Pass, float><<<grid, kRegNT, 0, L.stream>>>(L.geo, prm);
+    } else {
+        if (L.val_u16)
+            reg_pass_kernel_b1<P, PP, GT, kRegNT, Pass, uint16_t><<<grid, kRegNT, 0, L.stream>>>(L.geo, prm);
+        else
+            reg_pass_kernel_b1<P, PP, GT, kRegNT, Pass, float><<<grid, kRegNT, 0, L.stream>>>(L.geo, prm);
+    }
     return cudaGetLastError();
 }
 

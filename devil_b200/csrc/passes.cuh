@@ -427,7 +427,7 @@ DEV void load_row(const float* __restrict__ X, int64_t c, float* x) {
 }
 
 template <int P, int PP, int GT, int NT, class Pass, class VT>
-__global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pass::Params prm) {
+DEV void reg_pass_body(PassGeom geo, typename Pass::Params prm) {
     constexpr int NE = P * (P + 1) / 2;
     constexpr int NA = Pass::NW * NE + Pass::NV * P + Pass::NF;
     constexpr int NS = Pass::NS;
@@ -678,6 +678,19 @@ __global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pas
             geo.partS[((int64_t)seg * geo.slot_stride + slot) * NS + s] = v;
         }
     }
+}
+
+// Two entry points with the same body.  The IRLS pass runs best with the
+// compiler's default register budget for 256 threads (120 registers at
+// p = 4, four genes per thread); the MOM, MLE and bread passes measured
+// faster when told one block per SM is enough (more registers, no spills).
+template <int P, int PP, int GT, int NT, class Pass, class VT>
+__global__ void __launch_bounds__(NT) reg_pass_kernel(PassGeom geo, typename Pass::Params prm) {
+    reg_pass_body<P, PP, GT, NT, Pass, VT>(geo, prm);
+}
+template <int P, int PP, int GT, int NT, class Pass, class VT>
+__global__ void __launch_bounds__(NT, 1) reg_pass_kernel_b1(PassGeom geo, typename Pass::Params prm) {
+    reg_pass_body<P, PP, GT, NT, Pass, VT>(geo, prm);
 }
 
 // ---------------------------------------------------------------------
