@@ -15,11 +15,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdevil_b200.so")
 
 # status codes (include/devil_b200.h)
-OK, ERR_ARG, ERR_CUDA, ERR_ZERO_COLUMN, ERR_SINGULAR, ERR_UNSORTED, ERR_NOMEM, ERR_UNSUPPORTED = range(8)
+(OK, ERR_ARG, ERR_CUDA, ERR_ZERO_COLUMN, ERR_SINGULAR, ERR_UNSORTED, ERR_NOMEM, ERR_UNSUPPORTED,
+ ERR_NUMERIC) = range(9)
 COUNTS_DENSE_F64, COUNTS_DENSE_F32, COUNTS_CSR_U16, COUNTS_CSR_F32, COUNTS_CSC_F64 = range(5)
 DENSE_GENE_MAJOR, DENSE_CELL_MAJOR = 0, 1
 SF_NONE, SF_NORMED_SUM, SF_PSINORM, SF_GIVEN = range(4)
-OD_NONE, OD_MOM, OD_MLE = range(3)
+OD_NONE, OD_MOM, OD_MLE, OD_NEW = range(4)
 FORM_CHOSEN, FORM_PLAIN = 0, 1
 ADJ_NONE, ADJ_BH, ADJ_BONFERRONI, ADJ_HOLM, ADJ_HOCHBERG, ADJ_BY = range(6)
 GENE_CONVERGED, GENE_MAX_ITER, GENE_NAN = range(3)
@@ -34,7 +35,7 @@ EXPORTS = (
     "devil_estimate_mom_dispersion", "devil_fit_dispersion", "devil_compute_hessian",
     "devil_compute_clustered_meat", "devil_nb_adjoint", "devil_cluster_blocks",
     "devil_group_order", "devil_ctx_set_profiling", "devil_ctx_profile", "devil_ctx_engine",
-    "devil_p_adjust_device_static",
+    "devil_p_adjust_device_static", "devil_fit_overdispersion_new",
     "devil_p_adjust_device",
 )
 
@@ -108,6 +109,8 @@ def load():
         L.devil_beta_fit.argtypes = [vp, C.POINTER(Counts), vp, i, vp, vp, vp, i, dbl, i, vp, vp]
         L.devil_estimate_mom_dispersion.argtypes = [vp, C.POINTER(Counts), vp, i, vp, vp, vp]
         L.devil_fit_dispersion.argtypes = [vp, C.POINTER(Counts), vp, i, vp, vp, i, i, vp, vp]
+        L.devil_fit_overdispersion_new.argtypes = [vp, C.POINTER(Counts), vp, i, vp, vp, i, dbl, vp,
+                                                   vp]
         L.devil_compute_hessian.argtypes = [vp, C.POINTER(Counts), vp, i, vp, vp, vp, vp]
         L.devil_compute_clustered_meat.argtypes = [vp, C.POINTER(Counts), vp, i, vp, vp, vp, vp,
                                                    i, vp]

@@ -186,8 +186,7 @@ def _od_mode(overdispersion):
         if overdispersion == "MOM":
             return L.OD_MOM
         if overdispersion in ("new", "I"):
-            raise NotImplementedError("overdispersion = 'new'/'I' (fit_overdispersion_cppp) is not "
-                                      "part of the B200 path")
+            return L.OD_NEW
     raise ValueError(f"Unknown overdispersion mode: {overdispersion}")
 
 
@@ -442,6 +441,25 @@ def estimate_mom_dispersion(count_matrix, design_matrix, beta_matrix, sf, device
     ctx.check(L.load().devil_estimate_mom_dispersion(ctx.h, counts.ref, _ptr(Xf), p, _ptr(b),
                                                      _ptr(s), _ptr(out)))
     return out
+
+
+def fit_overdispersion_new(y, X, mu_beta, off, max_iter=200, eps_theta=1e-3, device=0):
+    """fit_overdispersion_cppp (src/new_overdispersion.cpp:195-481), the
+    overdispersion = "new" / "I" method, for every gene (rows of y).
+    Returns (kappa, kappa_iters).  Raises DevilError (status ERR_NUMERIC,
+    with the reference's message) where the reference would stop()."""
+    counts = _CountsHold(y)
+    G, n = counts.shape
+    Xf, p = _design(X, n)
+    b = np.ascontiguousarray(mu_beta, np.float64).reshape(G, p)
+    o = np.ascontiguousarray(off, np.float64)
+    out = np.empty(G)
+    it = np.empty(G, np.int32)
+    ctx = L.context(device)
+    ctx.check(L.load().devil_fit_overdispersion_new(ctx.h, counts.ref, _ptr(Xf), p, _ptr(b), _ptr(o),
+                                                    int(max_iter), float(eps_theta), _ptr(out),
+                                                    _ptr(it)))
+    return out, it
 
 
 def fit_dispersion(beta, model_matrix, y, offset_vector, tolerance=1e-3, max_iter=200,

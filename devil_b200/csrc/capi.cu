@@ -1036,6 +1036,92 @@ void check_kernel_err(devil_ctx* ctx) {
     }
 }
 
+// Gauss-Hermite rule (weight exp(-x^2)) of order m: eigenvalues of the
+// Jacobi matrix (zero diagonal, off-diagonal sqrt(k/2)) by bisection on
+// Sturm counts, weights sqrt(pi) / sum_k q_k(x)^2 over the orthonormal
+// Hermite polynomials q_k (Golub-Welsch, as src/new_overdispersion.cpp:22-47)
+void gauss_hermite_rule(int m, double* x, double* w) {
+    const double hi0 = std::sqrt(2.0 * m) + 1.0;
+    for (int j = 0; j < m; ++j) {
+        double lo = -hi0, hi = hi0;
+        for (int it = 0; it < 200; ++it) {
+            const double mid = 0.5 * (lo + hi);
+            if (mid <= lo || mid >= hi) break;
+            int below = 0;
+            double d = 1.0;
+            for (int i = 0; i < m; ++i) {
+                d = -mid - (i ? 0.5 * i / d : 0.0);
+                if (d == 0.0) d = -1e-300;
+                below += d < 0.0;
+            }
+            if (below > j) hi = mid; else lo = mid;
+        }
+        const double xj = 0.5 * (lo + hi);
+        double qm = 0.0, q = 1.0, sum = 1.0;
+        for (int k = 0; k + 1 < m; ++k) {
+            const double qn = (xj * q - (k ? std::sqrt(0.5 * k) : 0.0) * qm) / std::sqrt(0.5 * (k + 1));
+            qm = q;
+            q = qn;
+            sum += q * q;
+        }
+        x[j] = xj;
+        w[j] = std::sqrt(M_PI) / sum;
+    }
+}
+
+// overdispersion = "new" (fit_overdispersion_cppp) for every gene at the
+// fitted beta; the reference's stop() conditions fail the whole call, as
+// they fail fit_devil in R (R/main.R:443-454 under bplapply)
+void run_new_od(devil_ctx* ctx, const DevProblem& dp, const double* beta_d, double* theta,
+                int32_t* iters, int max_iter, double eps) {
+    if (dp.G == 0) return;
+    cudaStream_t st = ctx->stream;
+    const int m = 16;  // newton_max, also the Gauss-Hermite order (src/new_overdispersion.cpp:310)
+    double hx[16], hw[16];
+    gauss_hermite_rule(m, hx, hw);
+    double* gx = ws<double>(ctx, "nod_gx", m);
+    double* gw = ws<double>(ctx, "nod_gw", m);
+    h2d(ctx, gx, hx, m);
+    h2d(ctx, gw, hw, m);
+    double* xcs = ws<double>(ctx, "nod_xcolsum", dp.P);
+    int32_t* err = ws<int32_t>(ctx, "nod_err", dp.G);
+    NodArgs a{};
+    a.G = dp.G;
+    a.n = dp.n;
+    a.P = dp.P;
+    a.xs = dp.xs;
+    a.Xd = dp.Xdrm;
+    a.off = dp.off;
+    a.xcolsum = xcs;
+    a.rowptr = dp.rowptr;
+    a.col = dp.col;
+    a.val = dp.val;
+    a.val_u16 = dp.val_u16;
+    a.beta = beta_d;
+    a.stats = dp.stats;
+    a.max_iter = max_iter;
+    a.eps = eps;
+    a.gh_m = m;
+    a.max_newton = m;
+    a.gx = gx;
+    a.gw = gw;
+    a.theta = theta;
+    a.iters = iters;
+    a.err = err;
+    LAUNCH(launch_new_od(a, dp.Xcm, xcs, st));
+    std::vector<int32_t> he(dp.G);
+    CK(cudaMemcpyAsync(he.data(), err, dp.G * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));  // also keeps hx/hw alive until the copies ran
+    for (int64_t g = 0; g < dp.G; ++g) {
+        if (!he[g]) continue;
+        static const char* msg[] = {"", "kappa update requires C1 > n",
+                                    "Mode-finding failed: h''(mu0) >= 0 or non-finite.",
+                                    "GH quadrature underflow.", "kappa residual not finite at start."};
+        fail(ctx, DEVIL_ERR_NUMERIC, "%s (gene %lld)", msg[he[g] >= 1 && he[g] <= 4 ? he[g] : 0],
+             (long long)g);
+    }
+}
+
 struct FitBuffers {
     double* beta;
     float* beta_f;
@@ -1090,10 +1176,15 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
             CK(cudaMemcpyAsync(fb.theta, tm, G * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
     dbg_mark(ctx, "mom");
+    // theta_iters: NA for "old"/"MLE", 0 for MOM and FALSE (R/main.R:424-461)
     if (o->overdispersion == DEVIL_OD_MLE) {
         run_mle(ctx, dp, fb.beta_f, fb.beta, tm, fb.theta, nullptr, o->max_iter, 1, o->form);
-    } else if (o->overdispersion == DEVIL_OD_NONE) {
-        CK(cudaMemsetAsync(fb.theta, 0, G * sizeof(double), st));
+        LAUNCH(launch_fill_i32(fb.titers, INT32_MIN, G, st));
+    } else if (o->overdispersion == DEVIL_OD_NEW) {
+        run_new_od(ctx, dp, fb.beta, fb.theta, fb.titers, o->max_iter, o->tolerance);
+    } else {
+        if (o->overdispersion == DEVIL_OD_NONE) CK(cudaMemsetAsync(fb.theta, 0, G * sizeof(double), st));
+        LAUNCH(launch_fill_i32(fb.titers, 0, G, st));
     }
     dbg_mark(ctx, "mle");
     run_sandwich(ctx, dp, fb.beta_f, fb.beta, fb.theta, ends_host, n_clusters, fb.bread,
@@ -1122,7 +1213,7 @@ void alloc_fit_buffers(devil_ctx* ctx, int64_t G, int P, bool theta_mom, bool cl
 
 void validate_opts(devil_ctx* ctx, const devil_fit_opts* o) {
     if (!o) fail(ctx, DEVIL_ERR_ARG, "opts is NULL");
-    if (o->overdispersion < 0 || o->overdispersion > 2)
+    if (o->overdispersion < 0 || o->overdispersion > 3)
         fail(ctx, DEVIL_ERR_UNSUPPORTED, "overdispersion mode %d not supported", o->overdispersion);
     if (o->form != DEVIL_FORM_CHOSEN && o->form != DEVIL_FORM_PLAIN)
         fail(ctx, DEVIL_ERR_ARG, "unknown form %d", o->form);
@@ -1285,8 +1376,7 @@ int devil_fit(devil_ctx* ctx, const devil_counts* counts, const double* X, int p
         d2h(ctx, res->offset_vector, dp.off, dp.n);
         CK(cudaStreamSynchronize(ctx->stream));
         if (res->theta_iters) {
-            int32_t v = opts->overdispersion == DEVIL_OD_MLE ? INT32_MIN : 0;
-            for (int64_t g = 0; g < G; ++g) res->theta_iters[g] = v;
+            CK(cudaMemcpy(res->theta_iters, fb.titers, G * sizeof(int32_t), cudaMemcpyDeviceToHost));
         }
     });
 }
@@ -1318,6 +1408,7 @@ int devil_fit_device(devil_ctx* ctx, const devil_counts* counts_dev, const doubl
         if (r->sandwich && n_clusters > 0) fb.sandwich = r->sandwich;
         if (r->meat && n_clusters > 0) fb.meat = r->meat;
         if (r->theta_mom && opts->compute_theta_mom) fb.theta_mom = r->theta_mom;
+        if (r->theta_iters) fb.titers = r->theta_iters;
         fit_pipeline(ctx, dp, cluster_ends_host, n_clusters, opts, fb);
         if (r->size_factors)
             CK(cudaMemcpyAsync(r->size_factors, dp.sf, dp.n * 8, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1551,6 +1642,29 @@ int devil_fit_dispersion(devil_ctx* ctx, const devil_counts* counts, const doubl
         check_kernel_err(ctx);
         d2h(ctx, theta, th, dp.G);
         d2h(ctx, newton_iters, it, dp.G);
+        CK(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int devil_fit_overdispersion_new(devil_ctx* ctx, const devil_counts* counts, const double* X,
+                                 int p, const double* beta, const double* offset_vector,
+                                 int max_iter, double eps_theta, double* theta,
+                                 int32_t* kappa_iters) {
+    return guarded(ctx, [&] {
+        check_counts(ctx, counts);
+        if (!X || !beta || !offset_vector || !theta) fail(ctx, DEVIL_ERR_ARG, "missing argument");
+        DevProblem dp;
+        upload_counts(ctx, counts, dp);
+        prepare_design(ctx, dp, X, p, false);
+        upload_offsets(ctx, dp, offset_vector);
+        float* bf;
+        double* bd;
+        upload_beta(ctx, dp, beta, &bf, &bd);
+        double* th = ws<double>(ctx, "theta", dp.G);
+        int32_t* it = ws<int32_t>(ctx, "nod_iters_out", dp.G);
+        run_new_od(ctx, dp, bd, th, it, max_iter, eps_theta);
+        d2h(ctx, theta, th, dp.G);
+        d2h(ctx, kappa_iters, it, dp.G);
         CK(cudaStreamSynchronize(ctx->stream));
     });
 }

@@ -81,6 +81,30 @@ struct GrpGeom {
     double* partS;
     int slot_stride;
 };
+// ---- overdispersion "new" (kernels_newod.cu) ----
+struct NodArgs {
+    int64_t G, n;
+    int P, xs;
+    const double* Xd;       // [n][xs] row-major FP64 design
+    const double* off;      // [n]
+    const double* xcolsum;  // [P] column sums of the design
+    const int64_t* rowptr;
+    const int32_t* col;
+    const void* val;
+    int val_u16;
+    const double* beta;     // [G][P]
+    const double* stats;    // [G][6] gene statistics (mean, var, ...)
+    int max_iter;
+    double eps;             // eps_theta (the fit tolerance)
+    int gh_m, max_newton;   // Gauss-Hermite order and mode-search steps (newton_max)
+    const double* gx;       // [gh_m] Gauss-Hermite nodes
+    const double* gw;       // [gh_m] weights
+    double* theta;          // [G] kappa
+    int32_t* iters;         // [G] kappa_iters
+    int32_t* err;           // [G] 0, or the reference's stop() condition (1..4)
+};
+cudaError_t launch_new_od(const NodArgs& a, const double* Xcm, double* xcolsum, cudaStream_t st);
+
 cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm, int val_u16,
                             int max_slots, cudaStream_t st);
 cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* ginv, int64_t G,

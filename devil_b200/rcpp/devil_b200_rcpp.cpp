@@ -83,13 +83,14 @@ List devil_b200_fit(SEXP input_matrix, NumericMatrix design_matrix, SEXP size_fa
     o.tolerance = tolerance;
     o.init_beta_rough = init_beta_rough;
     o.offset = offset;
-    // overdispersion: "MOM", "old"/"MLE" or FALSE (R/main.R:415-459)
+    // overdispersion: "MOM", "old"/"MLE", "new"/"I" or FALSE (R/main.R:415-459)
     if (TYPEOF(overdispersion) == LGLSXP && !as<bool>(overdispersion)) {
         o.overdispersion = DEVIL_OD_NONE;
     } else {
         std::string od = as<std::string>(overdispersion);
         if (od == "MOM") o.overdispersion = DEVIL_OD_MOM;
         else if (od == "old" || od == "MLE") o.overdispersion = DEVIL_OD_MLE;
+        else if (od == "new" || od == "I") o.overdispersion = DEVIL_OD_NEW;
         else stop("Unknown overdispersion mode: " + od);
     }
     NumericVector sf_given;

@@ -45,6 +45,7 @@ extern "C" {
 #define DEVIL_ERR_UNSORTED     5   /* clusters not in contiguous blocks   */
 #define DEVIL_ERR_NOMEM        6   /* device allocation failed            */
 #define DEVIL_ERR_UNSUPPORTED  7   /* option outside this implementation  */
+#define DEVIL_ERR_NUMERIC      8   /* a numerical stop() of the reference  */
 
 /* ---- per-gene fit status (devil_fit_result.status) ------------------- */
 #define DEVIL_GENE_CONVERGED   0   /* max|delta| < tolerance               */
@@ -81,6 +82,7 @@ typedef struct devil_counts {
 #define DEVIL_OD_NONE        0   /* overdispersion = FALSE (Poisson)       */
 #define DEVIL_OD_MOM         1
 #define DEVIL_OD_MLE         2   /* "old" / "MLE"                          */
+#define DEVIL_OD_NEW         3   /* "new" / "I": fit_overdispersion_cppp   */
 
 #define DEVIL_FORM_CHOSEN    0   /* tiled, compacted, grouped kernels       */
 #define DEVIL_FORM_PLAIN     1   /* straightforward FP32 SIMT comparison    */
@@ -227,6 +229,17 @@ DEVIL_API int devil_estimate_mom_dispersion(devil_ctx *ctx, const devil_counts *
 DEVIL_API int devil_fit_dispersion(devil_ctx *ctx, const devil_counts *counts, const double *X, int p,
                          const double *beta, const double *offset_vector, int max_iter,
                          int cox_reid, double *theta, int32_t *newton_iters);
+
+/* fit_overdispersion_cppp (src/new_overdispersion.cpp:195-481), the
+ * overdispersion = "new" / "I" method: fixed-point search for k = 1/kappa
+ * with Laplace-centred Gauss-Hermite integrals (order newton_max = 16) and
+ * Aitken / secant / Brent safeguards, tolerance eps_theta.  kappa_iters is
+ * the reference's kappa_iters.  DEVIL_ERR_NUMERIC (with the reference's
+ * message) when a gene reaches one of the reference's stop() conditions. */
+DEVIL_API int devil_fit_overdispersion_new(devil_ctx *ctx, const devil_counts *counts,
+                                           const double *X, int p, const double *beta,
+                                           const double *offset_vector, int max_iter,
+                                           double eps_theta, double *theta, int32_t *kappa_iters);
 
 /* compute_hessian (src/variance.cpp:22-47): bread = (X' W X)^-1 per gene */
 DEVIL_API int devil_compute_hessian(devil_ctx *ctx, const devil_counts *counts, const double *X, int p,

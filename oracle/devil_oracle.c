@@ -971,6 +971,11 @@ int orc_test_de(int64_t G, int p, const double *beta, const double *bread, const
 /* ------------------------------------------------------------------ */
 /* cpu_fit pipeline  (R/main.R:375-523)                                */
 /* ------------------------------------------------------------------ */
+double orc_fit_overdispersion_new(int64_t n, int p, const double *y, const double *X,
+                                  const double *beta, const double *off, int max_iter,
+                                  double eps_theta, int newton_max, int *iters, int *converged,
+                                  int *err);
+
 /* overdispersion: 0 = FALSE (Poisson), 1 = MOM, 2 = MLE ("old"/"MLE").
  * theta0: per-gene initial dispersion (estimate_dispersion or user value).
  * beta0 : G x p initial coefficients (row-major per gene).
@@ -1009,6 +1014,11 @@ int orc_cpu_fit(int64_t G, int64_t n, int p, const int64_t *rowptr, const int32_
             } else if (overdispersion == 1) {
                 th = theta_mom ? theta_mom[g] : orc_mom_dispersion(n, p, y, X, b, sf);
                 ti = 0;
+            } else if (overdispersion == 3) {
+                int it, cv, er;
+                th = orc_fit_overdispersion_new(n, p, y, X, b, offv, max_iter, tolerance, 16, &it,
+                                                &cv, &er);
+                ti = it;
             } else {
                 th = 0.0; ti = 0;
             }
@@ -1034,6 +1044,316 @@ int orc_cpu_fit(int64_t G, int64_t n, int p, const int64_t *rowptr, const int32_
     }
     free(sf);
     return ORC_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* overdispersion = "new" / "I": fit_overdispersion_cppp                 */
+/* (src/new_overdispersion.cpp:195-481)                                 */
+/* ------------------------------------------------------------------ */
+
+/* Gauss-Hermite rule (weight exp(-x^2)) of order m: nodes are the
+ * eigenvalues of the Jacobi matrix (zero diagonal, off-diagonal sqrt(k/2)),
+ * found by bisection on Sturm counts; weights sqrt(pi) / sum_k q_k(x)^2
+ * with q_k the orthonormal Hermite polynomials (Christoffel numbers).  The
+ * reference builds the same rule with an Eigen eigensolver
+ * (src/new_overdispersion.cpp:22-47). */
+void orc_gauss_hermite(int m, double *x, double *w)
+{
+    const double hi0 = sqrt(2.0 * m) + 1.0;
+    for (int j = 0; j < m; j++) {
+        double lo = -hi0, hi = hi0;
+        for (int it = 0; it < 200; it++) {
+            double mid = 0.5 * (lo + hi);
+            if (mid <= lo || mid >= hi) break;
+            int c = 0;
+            double d = 1.0;
+            for (int i = 0; i < m; i++) {
+                double b2 = i ? 0.5 * i : 0.0;
+                d = -mid - (i ? b2 / d : 0.0);
+                if (d == 0.0) d = -1e-300;
+                c += d < 0.0;
+            }
+            if (c > j) hi = mid; else lo = mid;
+        }
+        double xj = 0.5 * (lo + hi);
+        double qm = 0.0, q = 1.0, sum = 1.0;
+        for (int k = 0; k + 1 < m; k++) {
+            double qn = (xj * q - (k ? sqrt(0.5 * k) : 0.0) * qm) / sqrt(0.5 * (k + 1));
+            qm = q; q = qn;
+            sum += q * q;
+        }
+        x[j] = xj;
+        w[j] = sqrt(M_PI) / sum;
+    }
+}
+
+typedef struct { double mu0, sigma0, h_mu0; } orc_laplace;
+
+/* h(x) = p log x + s (x log x - lgamma x) - t x and its derivatives
+ * (src/new_overdispersion.cpp:55-68) */
+static double nod_g(double s, double t, double x) { return s * (x * log(x) - lgamma(x)) - t * x; }
+static double nod_g1(double s, double t, double x) { return s * (log(x) + 1.0 - orc_digamma(x)) - t; }
+static double nod_g2(double s, double x) { return s * (1.0 / x - orc_trigamma(x)); }
+
+/* find_mode (src/new_overdispersion.cpp:71-97); returns -1 on failure */
+static int nod_mode(double p, double s, double t, int max_newton, double tol, double x0,
+                    orc_laplace *lp)
+{
+    double x = x0 > 1e-9 ? x0 : 1e-9;
+    for (int i = 0; i < max_newton; i++) {
+        double g1v = p / x + nod_g1(s, t, x);
+        if (fabs(g1v) < tol) break;
+        double g2v = -p / (x * x) + nod_g2(s, x);
+        double xn = x - g1v / g2v;
+        if (!(xn > 0.0) || !isfinite(xn)) xn = 0.5 * x;
+        if (fabs(xn - x) < tol * (1.0 + fabs(x))) { x = xn; break; }
+        x = xn;
+    }
+    double curv = -(-p / (x * x) + nod_g2(s, x));
+    if (!(curv > 0.0) || !isfinite(curv)) return -1;
+    lp->mu0 = x > 1e-12 ? x : 1e-12;
+    lp->sigma0 = sqrt(1.0 / curv);
+    lp->h_mu0 = p * log(lp->mu0) + nod_g(s, t, lp->mu0);
+    return 0;
+}
+
+/* log_integral_at (src/new_overdispersion.cpp:99-126); -1 on underflow */
+static int nod_log_integral(double p, double s, double t, int m, const double *gx,
+                            const double *gw, const orc_laplace *lp, double *out)
+{
+    const double scale = lp->sigma0 * sqrt(2.0);
+    double max_lt = -INFINITY;
+    for (int i = 0; i < m; i++) {
+        double xx = lp->mu0 + scale * gx[i];
+        if (xx <= 0.0 || !isfinite(xx)) continue;
+        double r = (p * log(xx) + nod_g(s, t, xx)) - lp->h_mu0 + gx[i] * gx[i];
+        double lt = log(gw[i]) + r;
+        if (lt > max_lt) max_lt = lt;
+    }
+    long double acc = 0.0L;
+    for (int i = 0; i < m; i++) {
+        double xx = lp->mu0 + scale * gx[i];
+        if (xx <= 0.0 || !isfinite(xx)) continue;
+        double r = (p * log(xx) + nod_g(s, t, xx)) - lp->h_mu0 + gx[i] * gx[i];
+        acc += expl((long double)(log(gw[i]) + r - max_lt));
+    }
+    if (!(acc > 0.0L)) return -1;
+    *out = lp->h_mu0 + log(scale) + max_lt + log((double)acc);
+    return 0;
+}
+
+/* H_log_gh_cpp (src/new_overdispersion.cpp:129-141): log of the integral
+ * of x^p exp(s (x log x - lgamma x) - t x) over x > 0 by Laplace-centred
+ * Gauss-Hermite quadrature; NAN when t <= s or the mode search fails */
+double orc_h_log_gh(double p, double s, double t, int m, int max_newton, double tol)
+{
+    if (!(t > s)) return NAN;
+    if (m < 4) m = 4;
+    if (m > 64) m = 64;
+    double gx[64], gw[64], out;
+    orc_gauss_hermite(m, gx, gw);
+    double x0 = (p + s) / (t - s);
+    if (x0 < 1e-3) x0 = 1e-3;
+    orc_laplace lp;
+    if (nod_mode(p, s, t, max_newton, tol, x0, &lp)) return NAN;
+    if (nod_log_integral(p, s, t, m, gx, gw, &lp, &out)) return NAN;
+    return out;
+}
+
+/* per-gene state of fit_overdispersion_cppp */
+typedef struct {
+    int64_t n;
+    int p;
+    const double *y, *wq;
+    double xbeta_sum;
+    int gh_m, max_newton;
+    double tol;
+    const double *gx, *gw;
+    int err;   /* 1: C1 <= n, 2: mode search failed, 3: quadrature underflow */
+} nod_ctx;
+
+/* F_k (src/new_overdispersion.cpp:288-311): the fixed-point map */
+static double nod_F(nod_ctx *c, double kk)
+{
+    if (c->err) return NAN;
+    double sd = 0.0, sl = 0.0, sm = 0.0;
+    for (int64_t i = 0; i < c->n; i++) {
+        double wi = c->wq[i], yi = c->y[i];
+        double kw = kk * wi;
+        sd += orc_digamma(kk + yi);
+        sl += log1p(kw);
+        sm += (kk + yi) * wi / (1.0 + kw);
+    }
+    double C1 = c->xbeta_sum - (sd - sl) + sm;
+    if (!(C1 > (double)c->n)) { c->err = 1; return NAN; }
+    double sN = (double)c->n;
+    orc_laplace l1, l2;
+    double x01 = (0.5 + sN) / (C1 - sN);
+    if (x01 < 1e-3) x01 = 1e-3;
+    if (nod_mode(0.5, sN, C1, c->max_newton, c->tol, x01, &l1)) { c->err = 2; return NAN; }
+    if (nod_mode(-0.5, sN, C1, c->max_newton, c->tol, l1.mu0, &l2)) { c->err = 2; return NAN; }
+    double lp, lm;
+    if (nod_log_integral(0.5, sN, C1, c->gh_m, c->gx, c->gw, &l1, &lp)) { c->err = 3; return NAN; }
+    if (nod_log_integral(-0.5, sN, C1, c->gh_m, c->gx, c->gw, &l2, &lm)) { c->err = 3; return NAN; }
+    return exp(lp - lm);
+}
+static double nod_f(nod_ctx *c, double kk) { return log(nod_F(c, kk)) - log(kk); }
+
+static double nod_clamp(double k) { return k < 1e-4 ? 1e-4 : (k > 1e4 ? 1e4 : k); }
+
+/* the reference's Brent root finder (src/new_overdispersion.cpp:343-373) */
+static double nod_brent(nod_ctx *c, double a, double b, double fa, double fb)
+{
+    double cc = a, fc = fa, d = b - a, e = d;
+    const double tol = c->tol, epsm = DBL_EPSILON;
+    for (int it = 0; it < 60; it++) {
+        if (fabs(fc) < fabs(fb)) { a = b; b = cc; cc = a; fa = fb; fb = fc; fc = fa; }
+        double tol1 = 2.0 * epsm * fabs(b) + 0.5 * tol;
+        double xm = 0.5 * (cc - b);
+        if (fabs(xm) <= tol1 || fb == 0.0) return b;
+        double sv, pv, qv;
+        if (fabs(e) >= tol1 && fabs(fa) > fabs(fb)) {
+            sv = fb / fa;
+            if (a == cc) { pv = 2.0 * xm * sv; qv = 1.0 - sv; }
+            else {
+                double r = fb / fc, t = fa / fc;
+                pv = sv * (2.0 * xm * t * (t - r) - (b - a) * (r - 1.0));
+                qv = (t - 1.0) * (r - 1.0) * (sv - 1.0);
+            }
+            if (pv > 0) qv = -qv;
+            pv = fabs(pv);
+            double m1 = 3.0 * xm * qv - fabs(tol1 * qv), m2 = fabs(e * qv);
+            if (2.0 * pv < (m1 < m2 ? m1 : m2)) { e = d; d = pv / qv; }
+            else { d = xm; e = d; }
+        } else { d = xm; e = d; }
+        a = b; fa = fb;
+        b += (fabs(d) > tol1 ? d : (xm > 0 ? tol1 : -tol1));
+        fb = nod_f(c, b);
+        if ((fb > 0 && fc > 0) || (fb < 0 && fc < 0)) { cc = a; fc = fa; e = d = b - a; }
+    }
+    return b;
+}
+
+/* fit_overdispersion_cppp for one gene (dense y): returns kappa (= theta);
+ * *iters = kappa_iters, *converged, *err as in nod_ctx (4: residual not
+ * finite at the start).  The kappa argument of the reference is unused
+ * there (it restarts from the moment estimate of y) and is not taken. */
+double orc_fit_overdispersion_new(int64_t n, int p, const double *y, const double *X,
+                                  const double *beta, const double *off, int max_iter,
+                                  double eps_theta, int newton_max, int *iters, int *converged,
+                                  int *err)
+{
+    double *wq = (double *)malloc(sizeof(double) * n);
+    double xbs = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+        double xb = 0.0;
+        for (int j = 0; j < p; j++) xb += X[(int64_t)j * n + i] * beta[j];
+        xbs += xb;
+        wq[i] = exp(-(xb + off[i]));
+    }
+    double gx[64], gw[64];
+    int m = newton_max < 4 ? 4 : (newton_max > 64 ? 64 : newton_max);
+    orc_gauss_hermite(m, gx, gw);
+    nod_ctx c = {n, p, y, wq, xbs, m, newton_max, eps_theta, gx, gw, 0};
+    /* moment start (src/new_overdispersion.cpp:225-254) */
+    double ym = 0.0;
+    for (int64_t i = 0; i < n; i++) ym += y[i];
+    ym /= (double)n;
+    double yv = 0.0;
+    if (n > 1) {
+        for (int64_t i = 0; i < n; i++) yv += (y[i] - ym) * (y[i] - ym);
+        yv /= (double)(n - 1);
+    }
+    double kap = (yv - ym) / (ym * ym);
+    if (!isfinite(kap) || kap <= 0.0) kap = 0.01;
+    double k = 1.0 / kap;
+    if (!isfinite(k)) k = 1e-4;
+    k = nod_clamp(k);
+    const double kmin = 1e-4, jump = 10.0;
+    int conv = 0, it_k = 0, bad = 0;
+    *err = 0;
+
+    double k0 = nod_clamp(k), f0 = nod_f(&c, k0);
+    if (!isfinite(f0)) { *err = c.err ? c.err : 4; free(wq); *iters = 0; *converged = 0; return NAN; }
+    double h = 1e-6 * k0 > 1e-8 ? 1e-6 * k0 : 1e-8;
+    double fp0 = (nod_f(&c, k0 + h) - f0) / h;
+    if (isfinite(fp0) && fabs(fp0) > 1e-10) {
+        double kn = nod_clamp(k0 - f0 / fp0), fn = nod_f(&c, kn);
+        if (isfinite(fn) && fabs(fn) < fabs(f0)) { k0 = kn; f0 = fn; }
+    }
+    double k1 = nod_F(&c, k0);
+    double cap = jump * (k0 > 1.0 ? k0 : 1.0);
+    if (k1 > cap) k1 = cap;
+    k1 = nod_clamp(k1);
+    double f1 = nod_f(&c, k1);
+    if (f0 * f1 < 0) {
+        k = nod_brent(&c, k0 < k1 ? k0 : k1, k0 < k1 ? k1 : k0, f0, f1);
+        conv = 1;
+    } else {
+        for (it_k = 0; it_k < max_iter; it_k++) {
+            double aj = jump / (1.0 + 0.1 * it_k);
+            double k2 = nod_F(&c, k1);
+            double c2 = aj * (k1 > 1.0 ? k1 : 1.0);
+            if (k2 > c2) k2 = c2;
+            k2 = nod_clamp(k2);
+            double f2 = nod_f(&c, k2);
+            double d1 = k1 - k0, d2 = k2 - k1, den = d2 - d1;
+            double ka = fabs(den) > 1e-14 ? k0 - d1 * d1 / den : k2;
+            if (!(ka > 0) || !isfinite(ka)) ka = k2;
+            double c3 = aj * (k2 > 1.0 ? k2 : 1.0);
+            if (ka > c3) ka = c3;
+            ka = nod_clamp(ka);
+            double kp = ka, fp = nod_f(&c, kp);
+            int bt = 0;
+            while ((fabs(fp) >= fabs(f1) || !isfinite(fp)) && bt < 8) {
+                kp = 0.5 * (kp + k1);
+                fp = nod_f(&c, kp);
+                bt++;
+            }
+            if (!(fabs(fp) < fabs(f1))) {
+                bad++;
+                if (bad == 1 && fabs(f1 - f0) > 1e-14) {
+                    double ks = nod_clamp(k1 - f1 * (k1 - k0) / (f1 - f0)), fs = nod_f(&c, ks);
+                    if (isfinite(fs) && fabs(fs) < fabs(f1)) { kp = ks; fp = fs; bad = 0; }
+                }
+                if (bad >= 1) {
+                    double a = k1 < k2 ? k1 : k2, b = k1 < k2 ? k2 : k1;
+                    if (f1 * f2 < 0) { k = nod_brent(&c, a, b, f1, f2); conv = 1; break; }
+                }
+                if (bad >= 1) {
+                    /* find_bracket (src/new_overdispersion.cpp:324-339) */
+                    double lo = -1.0, hi = -1.0, fc = nod_f(&c, k1);
+                    for (int ex = 1; ex <= 10; ex++) {
+                        double fac = pow(2.0, ex);
+                        double l = k1 / fac > kmin ? k1 / fac : kmin;
+                        double u = k1 * fac < 1e4 ? k1 * fac : 1e4;
+                        double fl = nod_f(&c, l);
+                        if (fl * fc < 0) { lo = l; hi = k1; break; }
+                        double fu = nod_f(&c, u);
+                        if (fc * fu < 0) { lo = k1; hi = u; break; }
+                        if (fl * fu < 0) { lo = l; hi = u; break; }
+                    }
+                    if (lo > 0) {
+                        double flo = nod_f(&c, lo), fhi = nod_f(&c, hi);
+                        k = nod_brent(&c, lo, hi, flo, fhi);
+                        conv = 1;
+                        break;
+                    }
+                }
+                kp = k2; fp = f2;
+            } else {
+                bad = 0;
+            }
+            if (fabs(kp - k1) < eps_theta * (1.0 + k1)) { k = kp; conv = 1; break; }
+            k0 = k1; f0 = f1; k1 = kp; f1 = fp;
+        }
+        if (!conv) k = k1 > kmin ? k1 : kmin;
+    }
+    free(wq);
+    *iters = it_k + 1;
+    *converged = conv;
+    if (c.err) { *err = c.err; return NAN; }
+    return 1.0 / k;
 }
 
 /* single-gene wrappers used by the tests (dense y) */

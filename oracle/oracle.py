@@ -20,7 +20,7 @@ _LIB = None
 
 SF_NORMED_SUM = 0
 SF_PSINORM = 1
-OD_NONE, OD_MOM, OD_MLE = 0, 1, 2
+OD_NONE, OD_MOM, OD_MLE, OD_NEW = 0, 1, 2, 3
 ADJ = {"none": 0, "BH": 1, "fdr": 1, "bonferroni": 2, "holm": 3, "hochberg": 4, "BY": 5}
 
 _d = C.POINTER(C.c_double)
@@ -67,6 +67,14 @@ def lib():
             f.restype = C.c_double
             f.argtypes = [C.c_int64, C.c_int, _d, _d, _d, C.c_double, C.c_int]
         L.orc_compute_hessian.argtypes = [C.c_int64, C.c_int, _d, C.c_double, _d, _d, _d, _d]
+        L.orc_gauss_hermite.argtypes = [C.c_int, _d, _d]
+        L.orc_gauss_hermite.restype = None
+        L.orc_h_log_gh.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double]
+        L.orc_h_log_gh.restype = C.c_double
+        _ip = C.POINTER(C.c_int)
+        L.orc_fit_overdispersion_new.argtypes = [C.c_int64, C.c_int, _d, _d, _d, _d, C.c_int,
+                                                 C.c_double, C.c_int, _ip, _ip, _ip]
+        L.orc_fit_overdispersion_new.restype = C.c_double
         L.orc_compute_scores.argtypes = [C.c_int64, C.c_int, _d, _d, _d, C.c_double, _d, _d]
         L.orc_compute_scores.restype = None
         L.orc_clustered_meat_fast.argtypes = [C.c_int64, C.c_int, _d, _d, _d, C.c_double, _d, _i32,
@@ -197,6 +205,30 @@ def fit_dispersion(beta, X, y, offv, max_iter=200, cr=True):
     th = lib().orc_fit_dispersion(n, p, _p(_f64(y)), _p(Xc), _p(_f64(beta)), _p(_f64(offv)),
                                   int(max_iter), int(bool(cr)), C.byref(it))
     return th, it.value
+
+
+def gauss_hermite(m):
+    """Gauss-Hermite nodes and weights (weight exp(-x^2)) of order m."""
+    x = np.zeros(m)
+    w = np.zeros(m)
+    lib().orc_gauss_hermite(int(m), _p(x), _p(w))
+    return x, w
+
+
+def h_log_gh(p, s, t, m=32, max_newton=8, tol=1e-12):
+    """H_log_gh_cpp (src/new_overdispersion.cpp:129-141)."""
+    return lib().orc_h_log_gh(float(p), float(s), float(t), int(m), int(max_newton), float(tol))
+
+
+def fit_overdispersion_new(y, X, beta, offv, max_iter=200, eps=1e-3, newton_max=16):
+    """fit_overdispersion_cppp (src/new_overdispersion.cpp:195-481) for one
+    gene; returns (kappa, kappa_iters, converged, err)."""
+    Xc, n, p = _colmajor(X)
+    it, cv, er = C.c_int(0), C.c_int(0), C.c_int(0)
+    k = lib().orc_fit_overdispersion_new(n, p, _p(_f64(y)), _p(Xc), _p(_f64(beta)), _p(_f64(offv)),
+                                         int(max_iter), float(eps), int(newton_max), C.byref(it),
+                                         C.byref(cv), C.byref(er))
+    return k, it.value, cv.value, er.value
 
 
 def nb_score(y, mu, X, log_theta, cr=True):

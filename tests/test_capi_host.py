@@ -90,8 +90,7 @@ def test_group_data_dimension_errors(dv):
 def test_argument_errors_before_gpu(dv):
     with pytest.raises(ValueError, match="Unknown overdispersion"):
         dv.api._od_mode("bogus")
-    with pytest.raises(NotImplementedError):
-        dv.api._od_mode("new")
+    assert dv.api._od_mode("new") == dv.api._od_mode("I") == 3
     with pytest.raises(ValueError, match="should be one of"):
         dv.api._sf_mode("bogus", 3)
     with pytest.raises(RuntimeError, match="edgeR"):

@@ -296,3 +296,98 @@ def test_clustered_meat_entry(dv, orc):
     ref = np.stack([orc.clustered_meat_fast(P.X, y, bb, t, sf, ends)
                     for y, bb, t in zip(P.dense(), b, th)])
     check_mats(meat, ref, np.ones(P.G, bool), 1e-4, "meat")
+
+
+NEW_OD_EPS = 1e-3  # eps_theta of the fit (its tolerance)
+
+
+def _k_close(theta_a, theta_b, width):
+    """|k_a - k_b| <= width * eps * (1 + k_b) with k = 1 / theta: the "new"
+    method only determines k to its tolerance eps (1 + k)."""
+    ka, kb = 1.0 / np.asarray(theta_a), 1.0 / np.asarray(theta_b)
+    return np.abs(ka - kb) <= width * NEW_OD_EPS * (1.0 + kb)
+
+
+def _new_od_stable(orc, P, beta, off, theta, pert):
+    """Genes whose oracle k = 1/kappa stays within the method's tolerance
+    when beta is scaled by 1 +- pert and when the offsets move by 1e-13.  fit_overdispersion_cppp stops its
+    search at |dk| < eps (1 + k) and takes discrete branches (Aitken,
+    backtracking, secant, bracketing, Brent) on the sign and size of
+    f(k) = log F(k) - log k, which is nearly flat for near-Poisson genes:
+    there the reference's own result moves by orders of magnitude under
+    rounding-level changes of its inputs, so no second implementation can
+    match it.  Parity is asserted on the genes where it is well defined."""
+    D = P.dense()
+    rng = np.random.default_rng(0)
+    off2 = off + 1e-13 * rng.choice([-1.0, 1.0], size=len(off))
+    ok = np.ones(P.G, bool)
+    for g in range(P.G):
+        for b, o in ((beta[g] * (1.0 + pert), off), (beta[g] * (1.0 - pert), off), (beta[g], off2)):
+            k = orc.fit_overdispersion_new(D[g], P.X, b, o)[0]
+            if not _k_close(k, theta[g], 1.0):
+                ok[g] = False
+                break
+    return ok
+
+
+def test_new_overdispersion_fit_matches_oracle(dv, orc):
+    """fit_devil(overdispersion = "new") against the oracle's
+    fit_overdispersion_cppp at the fitted beta (normed_sum size factors:
+    no gene reaches the reference's stop conditions)."""
+    P = synthetic.make("plain_sparse", seed=11, G=200, n=2000)
+    ref = oracle_fit(orc, P, orc.OD_NEW)
+    fit = gpu_fit(dv, P, "new")
+    check_beta(fit, ref)
+    # kappa given beta: the oracle's search at the GPU's beta (the FP32
+    # per-cell beta differs from the FP64 one at ~1e-7, which moves the
+    # search's discrete branches on some genes)
+    D = P.dense()
+    offg = fit["offset_vector"]
+    kg = np.array([orc.fit_overdispersion_new(D[g], P.X, fit["beta"][g], offg)[0]
+                   for g in range(P.G)])
+    stable = _new_od_stable(orc, P, fit["beta"], offg, kg, 1e-12)
+    assert stable.mean() >= 0.4
+    close = _k_close(fit["overdispersion"], kg, 2.0)
+    # a gene left on the flat part of f(k) can still branch differently on
+    # the GPU's own rounding (summation order over cells, digamma ulps)
+    assert close[stable].mean() >= 0.95, np.flatnonzero(stable & ~close)
+    # and against the FP64 fit where both searches are stable
+    both = stable & _new_od_stable(orc, P, ref["beta"], ref["off"], ref["theta"], 1e-6)
+    assert _k_close(fit["overdispersion"], ref["theta"], 2.0)[both].mean() >= 0.95
+
+
+def test_new_overdispersion_single_step(dv, orc):
+    """devil_fit_overdispersion_new at the oracle's beta (FP64 on both
+    sides), checked on the genes where the reference's search is stable."""
+    P = synthetic.make("clustered", seed=4, G=60, n=2000)
+    Y = P.csr_f64()
+    off = np.zeros(P.n)  # logs summing to zero, as normed_sum size factors give
+    th0 = orc.estimate_dispersion(Y, off)
+    b0 = orc.init_beta(Y, P.X, off)
+    r = orc.cpu_fit(Y, P.X, off, th0, b0, orc.OD_MOM, 200, 1e-3)
+    k, it = dv.fit_overdispersion_new((P.rowptr, P.col, P.val, P.n), P.X, r["beta"], off)
+    D = P.dense()
+    ref = [orc.fit_overdispersion_new(D[g], P.X, r["beta"][g], off) for g in range(P.G)]
+    ko = np.array([x[0] for x in ref])
+    io = np.array([x[1] for x in ref])
+    stable = _new_od_stable(orc, P, r["beta"], off, ko, 1e-12)
+    assert stable.mean() >= 0.4
+    close = _k_close(k, ko, 2.0)
+    assert close[stable].mean() >= 0.95, np.flatnonzero(stable & ~close)
+    assert (it[stable] == io[stable]).mean() >= 0.9
+
+
+def test_new_overdispersion_stop_is_an_error(dv, orc):
+    """Where the reference stops (C1 <= n for some gene) the call fails
+    with DEVIL_ERR_NUMERIC and the reference's message."""
+    from devil_b200 import DevilError
+    from devil_b200 import _lib as L
+    P = synthetic.make("plain_sparse", seed=5, G=20, n=3000)
+    off = np.log(P.sf_true)
+    Y = P.csr_f64()
+    r = orc.cpu_fit(Y, P.X, off, orc.estimate_dispersion(Y, off), orc.init_beta(Y, P.X, off),
+                    orc.OD_MOM, 200, 1e-3)
+    with pytest.raises(DevilError) as e:
+        dv.fit_overdispersion_new((P.rowptr, P.col, P.val, P.n), P.X, r["beta"], off)
+    assert e.value.code == L.ERR_NUMERIC
+    assert "C1 > n" in str(e.value)

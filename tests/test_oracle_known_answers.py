@@ -245,3 +245,69 @@ def test_t_pvalue_vs_scipy(orc, df):
         got = orc.two_sided_t_pvalue(t, df)
         if ref > 1e-300:
             assert rel_err(got, ref) < 1e-10, (t, df, got, ref)
+
+
+# ----------------------------------------------------------------------
+# overdispersion = "new" (src/new_overdispersion.cpp)
+# ----------------------------------------------------------------------
+@pytest.mark.parametrize("m", [4, 16, 32])
+def test_gauss_hermite_matches_numpy(orc, m):
+    """The Golub-Welsch Hermite rule of get_gh (src/new_overdispersion.cpp:22-47)."""
+    x, w = orc.gauss_hermite(m)
+    xr, wr = np.polynomial.hermite.hermgauss(m)
+    assert np.abs(x - xr).max() < 1e-12
+    assert np.abs(w / wr - 1.0).max() < 1e-10
+
+
+@pytest.mark.parametrize("p,s,t", [(0.5, 100.0, 130.0), (-0.5, 100.0, 130.0),
+                                   (0.5, 20.0, 60.0), (0.5, 5000.0, 5100.5)])
+def test_h_log_gh_matches_quadrature(orc, p, s, t):
+    """H_log_gh_cpp (src/new_overdispersion.cpp:129-141): the log of
+    int x^p exp(s (x log x - lgamma x) - t x) dx by Laplace-centred
+    Gauss-Hermite, against adaptive quadrature around the mode."""
+    from scipy import integrate, special
+
+    def h(x):
+        return p * np.log(x) + s * (x * np.log(x) - special.gammaln(x)) - t * x
+
+    xs = np.linspace(1e-3, 200, 400001)
+    hv = h(xs)
+    i = int(np.argmax(hv))
+    hm, xm = hv[i], xs[i]
+    width = 40 * xm / np.sqrt(s) + 1.0
+    val = integrate.quad(lambda x: np.exp(h(x) - hm), max(1e-9, xm - width), xm + width,
+                         points=[xm], limit=500, epsabs=0, epsrel=1e-12)[0]
+    assert abs(orc.h_log_gh(p, s, t, 32, 8, 1e-12) - (hm + np.log(val))) < 1e-3
+
+
+def test_new_overdispersion_near_truth_and_mle(orc):
+    """fit_overdispersion_cppp on large simulated NB genes lands near the
+    generating theta and the Cox-Reid MLE."""
+    rng = np.random.default_rng(3)
+    n = 20000
+    X = np.ones((n, 1))
+    off = np.zeros(n)
+    for th, mu in [(0.5, 2.0), (2.0, 5.0)]:
+        y = rng.poisson(rng.gamma(1 / th, th * mu, n)).astype(float)
+        beta = np.array([np.log(y.mean())])
+        k, it, conv, err = orc.fit_overdispersion_new(y, X, beta, off)
+        mle, _ = orc.fit_dispersion(beta, X, y, off)
+        assert err == 0 and conv == 1 and it >= 1
+        assert abs(k - th) / th < 0.1
+        assert abs(k - mle) / mle < 0.01
+
+
+def test_new_overdispersion_stop_condition(orc):
+    """The reference stops when C1 <= n (src/new_overdispersion.cpp:303-304):
+    with size factors whose logs do not sum to zero a near-Poisson gene
+    reaches it at the large-k end of the search."""
+    from devil_b200 import synthetic
+    P = synthetic.make("plain_sparse", seed=5, G=20, n=3000)
+    off = np.log(P.sf_true)
+    Y = P.csr_f64()
+    b0 = orc.init_beta(Y, P.X, off)
+    th0 = orc.estimate_dispersion(Y, off)
+    r = orc.cpu_fit(Y, P.X, off, th0, b0, orc.OD_MOM, 200, 1e-3)
+    D = P.dense()
+    errs = [orc.fit_overdispersion_new(D[g], P.X, r["beta"][g], off)[3] for g in range(P.G)]
+    assert 1 in errs and 0 in errs
