@@ -35,7 +35,7 @@ EXPORTS = (
     "devil_estimate_mom_dispersion", "devil_fit_dispersion", "devil_compute_hessian",
     "devil_compute_clustered_meat", "devil_nb_adjoint", "devil_cluster_blocks",
     "devil_group_order", "devil_ctx_set_profiling", "devil_ctx_profile", "devil_ctx_engine",
-    "devil_p_adjust_device_static", "devil_fit_overdispersion_new",
+    "devil_p_adjust_device_static", "devil_fit_overdispersion_new", "devil_fit_batch",
     "devil_p_adjust_device",
 )
 
@@ -58,6 +58,11 @@ class FitOpts(C.Structure):
                 ("size_factor_values", C.c_void_p), ("offset", C.c_double),
                 ("has_init_overdispersion", C.c_int), ("init_overdispersion", C.c_double),
                 ("compute_theta_mom", C.c_int), ("form", C.c_int)]
+
+
+class Problem(C.Structure):
+    _fields_ = [("counts", Counts), ("X", C.c_void_p), ("p", C.c_int),
+                ("cluster_ends", C.c_void_p), ("n_clusters", C.c_int)]
 
 
 class FitResult(C.Structure):
@@ -119,6 +124,8 @@ def load():
         L.devil_group_order.argtypes = [i64, vp, vp]
         L.devil_ctx_set_profiling.argtypes = [vp, i]
         L.devil_ctx_profile.argtypes = [vp, i, C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]
+        L.devil_fit_batch.argtypes = [vp, i, C.POINTER(Problem), C.POINTER(FitOpts),
+                                      C.POINTER(FitResult), i]
         L.devil_ctx_engine.argtypes = [vp, i]
         L.devil_ctx_engine.restype = i
         L.devil_p_adjust_device_static.argtypes = [i64, vp, i, vp, vp, C.c_char_p, C.c_size_t]

@@ -208,32 +208,13 @@ def _sf_mode(size_factors, n):
     return L.SF_GIVEN, sf
 
 
-def fit_devil(x, design_matrix, clusters=None, overdispersion="MOM", init_overdispersion=None,
-              init_beta_rough=False, offset=0.0, size_factors=None, verbose=False, max_iter=200,
-              tolerance=1e-3, CUDA=True, batch_size=1024, form="chosen", compute_theta_mom=False,
-              device=0):
-    """Fit the per-gene NB GLM (fit_devil, R/main.R:164-273) on the GPU.
-
-    ``CUDA`` and ``batch_size`` are accepted for signature compatibility;
-    the B200 path always runs on the GPU and schedules genes itself.
-    ``form`` = "chosen" (default) or "plain" (the straightforward FP32 SIMT
-    comparison form)."""
-    del verbose, CUDA, batch_size
-    counts = _CountsHold(x)
-    G, n = counts.shape
-    Xf, p = _design(design_matrix, n)
-    od = _od_mode(overdispersion)
-    sfm, sfv = _sf_mode(size_factors, n)
-    ends = None
-    if clusters is not None:
-        if len(clusters) != n:
-            raise ValueError("clusters must have one entry per cell")
-        _, ends = cluster_blocks(clusters)
+def _fit_opts(overdispersion, init_overdispersion, init_beta_rough, offset, sfm, sfv, max_iter,
+              tolerance, compute_theta_mom, form):
     opts = L.FitOpts()
     L.load().devil_fit_opts_default(C.byref(opts))
     opts.max_iter = int(max_iter)
     opts.tolerance = float(tolerance)
-    opts.overdispersion = od
+    opts.overdispersion = _od_mode(overdispersion)
     opts.init_beta_rough = int(bool(init_beta_rough))
     opts.size_factors = sfm
     opts.size_factor_values = _ptr(sfv)
@@ -243,47 +224,123 @@ def fit_devil(x, design_matrix, clusters=None, overdispersion="MOM", init_overdi
         opts.init_overdispersion = float(init_overdispersion)
     opts.compute_theta_mom = int(bool(compute_theta_mom))
     opts.form = L.FORM_PLAIN if form == "plain" else L.FORM_CHOSEN
-    beta = np.empty((G, p))
-    theta = np.empty(G)
-    iters = np.empty(G, np.int32)
-    titers = np.empty(G, np.int32)
-    bread = np.empty((G, p, p))
-    sw = np.empty((G, p, p)) if ends is not None else None
-    tm = np.empty(G) if compute_theta_mom else None
-    status = np.empty(G, np.int32)
-    sfo = np.empty(n)
-    offo = np.empty(n)
-    meat = np.empty((G, p, p)) if ends is not None else None
-    res = L.FitResult(_ptr(beta), _ptr(theta), _ptr(iters), _ptr(titers), _ptr(bread), _ptr(sw),
-                      _ptr(tm), _ptr(status), _ptr(sfo), _ptr(offo), _ptr(meat))
+    return opts
+
+
+class _FitSlots:
+    """Host inputs and output arrays of one fit (kept alive for the call)."""
+
+    def __init__(self, x, design_matrix, clusters, compute_theta_mom):
+        self.x = x
+        self.design_matrix = design_matrix
+        self.counts = _CountsHold(x)
+        G, n = self.counts.shape
+        self.G, self.n = G, n
+        self.Xf, self.p = _design(design_matrix, n)
+        p = self.p
+        self.ends = None
+        if clusters is not None:
+            if len(clusters) != n:
+                raise ValueError("clusters must have one entry per cell")
+            _, self.ends = cluster_blocks(clusters)
+        self.beta = np.empty((G, p))
+        self.theta = np.empty(G)
+        self.iters = np.empty(G, np.int32)
+        self.titers = np.empty(G, np.int32)
+        self.bread = np.empty((G, p, p))
+        self.sw = np.empty((G, p, p)) if self.ends is not None else None
+        self.tm = np.empty(G) if compute_theta_mom else None
+        self.status = np.empty(G, np.int32)
+        self.sfo = np.empty(n)
+        self.offo = np.empty(n)
+        self.meat = np.empty((G, p, p)) if self.ends is not None else None
+        self.res = L.FitResult(_ptr(self.beta), _ptr(self.theta), _ptr(self.iters),
+                               _ptr(self.titers), _ptr(self.bread), _ptr(self.sw), _ptr(self.tm),
+                               _ptr(self.status), _ptr(self.sfo), _ptr(self.offo),
+                               _ptr(self.meat))
+
+    def result(self, size_factors, max_iter, tolerance):
+        # per-gene matrices are column-major p x p; present them as [g, i, j]
+        bread = np.ascontiguousarray(np.transpose(self.bread, (0, 2, 1)))
+        sw = meat = None
+        if self.sw is not None:
+            sw = np.ascontiguousarray(np.transpose(self.sw, (0, 2, 1)))
+            meat = np.ascontiguousarray(np.transpose(self.meat, (0, 2, 1)))
+        th_it = self.titers.astype(np.float64)
+        th_it[self.titers == L.NA_INT] = np.nan
+        return dict(
+            beta=self.beta,
+            beta_sandwiches_null=bread,
+            beta_sandwiches=sw,
+            overdispersion=self.theta,
+            iterations=dict(beta_iters=self.iters, theta_iters=th_it),
+            size_factors=self.sfo if size_factors is not None else np.ones(self.n),
+            offset_vector=self.offo,
+            design_matrix=np.asarray(self.design_matrix),
+            input_matrix=self.x,
+            input_parameters=dict(max_iter=max_iter, tolerance=tolerance),
+            status=self.status,
+            theta_mom=self.tm,
+            meat=meat,
+        )
+
+
+def fit_devil(x, design_matrix, clusters=None, overdispersion="MOM", init_overdispersion=None,
+              init_beta_rough=False, offset=0.0, size_factors=None, verbose=False, max_iter=200,
+              tolerance=1e-3, CUDA=True, batch_size=1024, form="chosen", compute_theta_mom=False,
+              device=0):
+    """Fit the per-gene NB GLM (fit_devil, R/main.R:164-273) on the GPU.
+
+    ``CUDA`` and ``batch_size`` are accepted for signature compatibility;
+    the B200 path always runs on the GPU and schedules genes itself.
+    ``form`` = "chosen" (default) or "plain" (the per-cell, one gene per
+    block comparison form)."""
+    del verbose, CUDA, batch_size
+    f = _FitSlots(x, design_matrix, clusters, compute_theta_mom)
+    sfm, sfv = _sf_mode(size_factors, f.n)
+    opts = _fit_opts(overdispersion, init_overdispersion, init_beta_rough, offset, sfm, sfv,
+                     max_iter, tolerance, compute_theta_mom, form)
     ctx = L.context(device)
-    rc = L.load().devil_fit(ctx.h, counts.ref, _ptr(Xf), p, _ptr(ends),
-                            0 if ends is None else len(ends), C.byref(opts), C.byref(res))
+    rc = L.load().devil_fit(ctx.h, f.counts.ref, _ptr(f.Xf), f.p, _ptr(f.ends),
+                            0 if f.ends is None else len(f.ends), C.byref(opts), C.byref(f.res))
     if rc == L.ERR_ZERO_COLUMN:
         raise ValueError(L.load().devil_last_error(ctx.h).decode())
     ctx.check(rc)
-    # per-gene matrices are column-major p x p; present them as [g, i, j]
-    bread = np.ascontiguousarray(np.transpose(bread, (0, 2, 1)))
-    if sw is not None:
-        sw = np.ascontiguousarray(np.transpose(sw, (0, 2, 1)))
-        meat = np.ascontiguousarray(np.transpose(meat, (0, 2, 1)))
-    th_it = titers.astype(np.float64)
-    th_it[titers == L.NA_INT] = np.nan
-    return dict(
-        beta=beta,
-        beta_sandwiches_null=bread,
-        beta_sandwiches=sw,
-        overdispersion=theta,
-        iterations=dict(beta_iters=iters, theta_iters=th_it),
-        size_factors=sfo if size_factors is not None else np.ones(n),
-        offset_vector=offo,
-        design_matrix=np.asarray(design_matrix),
-        input_matrix=x,
-        input_parameters=dict(max_iter=max_iter, tolerance=tolerance),
-        status=status,
-        theta_mom=tm,
-        meat=meat,
-    )
+    return f.result(size_factors, max_iter, tolerance)
+
+
+def fit_devil_batch(problems, overdispersion="MOM", init_overdispersion=None,
+                    init_beta_rough=False, offset=0.0, size_factors=None, max_iter=200,
+                    tolerance=1e-3, form="chosen", compute_theta_mom=False, workers=4, device=0):
+    """fit_devil for many independent problems in one call (devil_fit_batch).
+
+    ``problems`` is a sequence of (x, design_matrix) or (x, design_matrix,
+    clusters); the options apply to every problem (size_factors: None or a
+    method name).  The problems run on ``workers`` concurrent GPU streams.
+    Returns one fit dict per problem, as fit_devil."""
+    if size_factors is not None and not isinstance(size_factors, str):
+        raise ValueError("fit_devil_batch takes size_factors as None or a method name")
+    slots = []
+    for pr in problems:
+        x, X = pr[0], pr[1]
+        cl = pr[2] if len(pr) > 2 else None
+        slots.append(_FitSlots(x, X, cl, compute_theta_mom))
+    sfm, _ = _sf_mode(size_factors, 1)
+    opts = _fit_opts(overdispersion, init_overdispersion, init_beta_rough, offset, sfm, None,
+                     max_iter, tolerance, compute_theta_mom, form)
+    n = len(slots)
+    arr = (L.Problem * max(n, 1))()
+    res = (L.FitResult * max(n, 1))()
+    for i, f in enumerate(slots):
+        arr[i].counts = f.counts.s
+        arr[i].X = _ptr(f.Xf)
+        arr[i].p = f.p
+        arr[i].cluster_ends = _ptr(f.ends)
+        arr[i].n_clusters = 0 if f.ends is None else len(f.ends)
+        res[i] = f.res
+    ctx = L.context(device)
+    ctx.check(L.load().devil_fit_batch(ctx.h, n, arr, C.byref(opts), res, int(workers)))
+    return [f.result(size_factors, max_iter, tolerance) for f in slots]
 
 
 # ----------------------------------------------------------------------

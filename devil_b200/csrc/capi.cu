@@ -10,7 +10,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <map>
+#include <thread>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -1379,6 +1381,49 @@ int devil_fit(devil_ctx* ctx, const devil_counts* counts, const double* X, int p
             CK(cudaMemcpy(res->theta_iters, fb.titers, G * sizeof(int32_t), cudaMemcpyDeviceToHost));
         }
     });
+}
+
+int devil_fit_batch(devil_ctx* ctx, int n_problems, const devil_problem* problems,
+                    const devil_fit_opts* opts, devil_fit_result* results, int workers) {
+    if (!ctx) return DEVIL_ERR_ARG;
+    if (n_problems < 0 || (n_problems > 0 && (!problems || !results)) || !opts) {
+        ctx->err = "devil_fit_batch: need problems, results and opts";
+        return DEVIL_ERR_ARG;
+    }
+    if (n_problems == 0) return DEVIL_OK;
+    workers = std::max(1, std::min(std::min(workers, 8), n_problems));
+    std::vector<devil_ctx*> wc(workers, nullptr);
+    for (int w = 0; w < workers; ++w) {
+        const int rc = devil_ctx_create(ctx->device, &wc[w]);
+        if (rc != DEVIL_OK) {
+            for (auto* c : wc)
+                if (c) devil_ctx_destroy(c);
+            ctx->err = "devil_fit_batch: could not create a worker context";
+            return rc;
+        }
+    }
+    std::vector<int> rcs(n_problems, DEVIL_OK);
+    std::vector<std::string> msgs(n_problems);
+    std::atomic<int> next(0);
+    auto work = [&](int w) {
+        for (int i = next.fetch_add(1); i < n_problems; i = next.fetch_add(1)) {
+            const devil_problem& pr = problems[i];
+            rcs[i] = devil_fit(wc[w], &pr.counts, pr.X, pr.p, pr.cluster_ends, pr.n_clusters, opts,
+                               &results[i]);
+            if (rcs[i] != DEVIL_OK) msgs[i] = devil_last_error(wc[w]);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int w = 1; w < workers; ++w) th.emplace_back(work, w);
+    work(0);
+    for (auto& t : th) t.join();
+    for (auto* c : wc) devil_ctx_destroy(c);
+    for (int i = 0; i < n_problems; ++i)
+        if (rcs[i] != DEVIL_OK) {
+            ctx->err = "problem " + std::to_string(i) + ": " + msgs[i];
+            return rcs[i];
+        }
+    return DEVIL_OK;
 }
 
 int devil_fit_device(devil_ctx* ctx, const devil_counts* counts_dev, const double* X_dev, int p,

@@ -154,6 +154,24 @@ DEVIL_API int devil_fit(devil_ctx *ctx, const devil_counts *counts, const double
               const int32_t *cluster_ends, int n_clusters, const devil_fit_opts *opts,
               devil_fit_result *res);
 
+/* Many independent problems (each its own genes, cells, design and
+ * clusters; the configuration of many uneven DE problems): the fit of
+ * every problem as devil_fit, spread over `workers` concurrent streams of
+ * the context's device (1..8; each worker holds its own context) so that
+ * the kernels of small problems overlap.  results[i] receives problem i.
+ * On failure the status of the first failing problem is returned and the
+ * context's message names the problem.  The reference fits one problem
+ * per fit_devil call (R/main.R:164-273). */
+typedef struct devil_problem {
+    devil_counts counts;           /* host counts                           */
+    const double *X;               /* n x p column-major                    */
+    int p;
+    const int32_t *cluster_ends;   /* NULL or n_clusters ends               */
+    int n_clusters;
+} devil_problem;
+DEVIL_API int devil_fit_batch(devil_ctx *ctx, int n_problems, const devil_problem *problems,
+                              const devil_fit_opts *opts, devil_fit_result *results, int workers);
+
 /* same, with the count matrix (CSR formats only) and every input/output
  * already in device memory.  X_dev is n x p column-major doubles.
  * Asynchronous on the context stream. */

@@ -391,3 +391,37 @@ def test_new_overdispersion_stop_is_an_error(dv, orc):
         dv.fit_overdispersion_new((P.rowptr, P.col, P.val, P.n), P.X, r["beta"], off)
     assert e.value.code == L.ERR_NUMERIC
     assert "C1 > n" in str(e.value)
+
+
+def test_fit_batch_uneven_problems(dv):
+    """devil_fit_batch over uneven problems (different genes, cells, design
+    width and clusters) on concurrent streams gives, problem by problem,
+    exactly what devil_fit gives."""
+    cases = [("plain_small", 1, 40, 400, False), ("plain_sparse", 2, 120, 3000, False),
+             ("clustered", 3, 80, 2500, True), ("wide", 4, 24, 4000, False),
+             ("plain_sparse", 5, 60, 800, False)]
+    probs = []
+    for cfg, seed, G, n, cl in cases:
+        P = synthetic.make(cfg, seed=seed, G=G, n=n)
+        x = (P.rowptr, P.col, P.val.astype(np.float64) if P.val.dtype != np.uint16 else P.val, P.n)
+        probs.append((x, P.X, P.clusters) if cl else (x, P.X))
+    kw = dict(overdispersion="MOM", size_factors=None)
+    fits = dv.fit_devil_batch(probs, workers=3, **kw)
+    assert len(fits) == len(probs)
+    for pr, f in zip(probs, fits):
+        one = dv.fit_devil(pr[0], pr[1], clusters=pr[2] if len(pr) > 2 else None, **kw)
+        np.testing.assert_array_equal(f["beta"], one["beta"])
+        np.testing.assert_array_equal(f["overdispersion"], one["overdispersion"])
+        np.testing.assert_array_equal(f["iterations"]["beta_iters"], one["iterations"]["beta_iters"])
+        np.testing.assert_array_equal(f["beta_sandwiches_null"], one["beta_sandwiches_null"])
+        if len(pr) > 2:
+            np.testing.assert_array_equal(f["beta_sandwiches"], one["beta_sandwiches"])
+
+
+def test_fit_batch_names_the_failing_problem(dv):
+    from devil_b200 import DevilError
+    P = synthetic.make("plain_sparse", seed=2, G=30, n=500)
+    x = (P.rowptr, P.col, P.val, P.n)
+    bad_X = np.zeros_like(P.X)  # rank deficient design
+    with pytest.raises(DevilError, match="problem 1"):
+        dv.fit_devil_batch([(x, P.X), (x, bad_X)], workers=2)
