@@ -417,6 +417,19 @@ def main():
                 "alg_bytes_per_launch": round(alg_per_launch, 1),
                 "share_of_step": round(t_ms / args.steps / ms, 4)}
 
+    # The register-engine IRLS pass is bound on the SM side, not by HBM: per
+    # active gene and cell it evaluates exp2 and a reciprocal on the special
+    # function units (16 results per clock per SM, nominal) besides the
+    # FMAs.  Report its gene-cell rate against that SFU ceiling as well.
+    if roof is not None and engines["irls"] == "register" and t_ms > 0:
+        gene_cells = float(out["iters"].double().sum().item()) * n * args.steps
+        sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
+        ceiling = 148 * 16 * sm_mhz * 1e6 / 2.0  # two SFU results per gene-cell
+        achieved_gc = gene_cells / (t_ms / 1e3)
+        roof["compute"] = {"unit": "gene-cells/s", "achieved": round(achieved_gc, -6),
+                           "sfu_ceiling": round(ceiling, -6), "frac": round(achieved_gc / ceiling, 4),
+                           "note": "nominal SFU rate at the sampled SM clock; 2 SFU ops per gene-cell"}
+
     passes = {name: {"launches": prof[k][0], "ms_per_step": round(prof[k][1] / args.steps, 3)}
               for k, name in enumerate(["irls", "mom", "mle", "bread_meat"])}
 
