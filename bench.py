@@ -371,6 +371,15 @@ def main():
             ctx.check(lib.devil_test_de(ctx.h, G, p, ptr(hb["beta"]), ptr(hb["bread"]), None, n,
                                         contrast.ctypes.data_as(C.c_void_p), L.ADJ_BH, 10.0,
                                         ptr(hb["pval"]), ptr(hb["padj"]), ptr(hb["lfc"])))
+            if world > 1:
+                # global BH over every rank's p-values, as in the device step
+                with torch.cuda.stream(ext):
+                    dist.all_gather_into_tensor(gathered, hb["pval"].to(dev, non_blocking=True))
+                ctx.check(lib.devil_p_adjust_device(ctx.h, G * world, ptr(gathered), L.ADJ_BH,
+                                                    ptr(gadj)))
+                with torch.cuda.stream(ext):
+                    hb["padj"].copy_(gadj[rank * G:(rank + 1) * G], non_blocking=True)
+                ctx.synchronize()
 
         step_host()  # workspace growth happens here, outside the timed region
         ctx.synchronize()
@@ -390,6 +399,9 @@ def main():
             ems = float(t.item())
         h2d = (G + 1) * 8 + nnz * 4 + nnz * 2 + n * p * 8 + G * p * 8 + G * p * p * 8
         d2h = G * p * 8 + G * 8 * 2 + G * 4 * 2 + G * p * p * 8 + n * 16 + G * 8 * 3
+        if world > 1:  # p-values up for the gather, globally adjusted slice back
+            h2d += G * 8
+            d2h += G * 8
         e2e = {"value": world * G / (ems / 1e3), "unit": "genes/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": ems}
 
