@@ -408,6 +408,7 @@ def main():
     # ---- roofline of the dominant kernel (IRLS cell pass) ----
     engines = {name: ctx.engine(k) for k, name in enumerate(["irls", "mom", "mle", "bread_meat"])}
     kernel = {"register": f"reg_pass_kernel<P={p},PassIRLS,uint16> (register tiles)",
+              "tensor": f"tc_irls_kernel<P={p},uint16> (tcgen05 kind::tf32 Hessian, 128-gene tiles)",
               "shared": f"gen_pass_kernel<PassIRLS,uint16> (shared-memory tiles, p={p})",
               "groups": f"grp_pass_kernel<PassIRLS,uint16> (design groups, p={p})"}.get(
                   engines["irls"], engines["irls"])
@@ -429,11 +430,12 @@ def main():
                 "alg_bytes_per_launch": round(alg_per_launch, 1),
                 "share_of_step": round(t_ms / args.steps / ms, 4)}
 
-    # The register-engine IRLS pass is bound on the SM side, not by HBM: per
-    # active gene and cell it evaluates exp2 and a reciprocal on the special
+    # The IRLS cell pass is bound on the SM side, not by HBM: per active
+    # gene and cell it evaluates exp2 and a reciprocal on the special
     # function units (16 results per clock per SM, nominal) besides the
-    # FMAs.  Report its gene-cell rate against that SFU ceiling as well.
-    if roof is not None and engines["irls"] == "register" and t_ms > 0:
+    # FMAs (register engine) or the TF32 MMAs (tensor engine).  Report its
+    # gene-cell rate against that SFU ceiling as well.
+    if roof is not None and engines["irls"] in ("register", "tensor") and t_ms > 0:
         gene_cells = float(out["iters"].double().sum().item()) * n * args.steps
         sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
         ceiling = 148 * 16 * sm_mhz * 1e6 / 2.0  # two SFU results per gene-cell
@@ -478,7 +480,7 @@ def main():
         "scaling": "weak", "vs_baseline": None,
         # per-cell arithmetic of the IRLS pass: FP32 in the register engine,
         # FP64 in the shared-memory and design-group engines
-        "dtype": "f32" if engines["irls"] == "register" else "f64", "data": "synthetic",
+        "dtype": "f32" if engines["irls"] in ("register", "tensor") else "f64", "data": "synthetic",
         "config": dict(workload_desc(args.config, G, n, p, nnz), form=args.form,
                        l2="inputs exceed L2 (CSR of all genes, re-read every IRLS pass)",
                        parallelism=f"genes sharded over {world} rank(s), no exchange during "

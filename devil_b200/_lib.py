@@ -171,9 +171,9 @@ class Context:
 
     def engine(self, kind: int) -> str:
         """Engine of the last launch of pass kind 0 IRLS, 1 MOM, 2 MLE,
-        3 bread/meat: "register", "shared", "groups" or "none"."""
+        3 bread/meat: "register", "shared", "groups", "tensor" or "none"."""
         e = load().devil_ctx_engine(self.h, int(kind))
-        return {0: "register", 1: "shared", 2: "groups"}.get(e, "none")
+        return {0: "register", 1: "shared", 2: "groups", 3: "tensor"}.get(e, "none")
 
     def synchronize(self):
         self.check(load().devil_ctx_synchronize(self.h))

@@ -185,6 +185,9 @@ struct DevProblem {
     int64_t nnz = 0;
     const double* Xcm = nullptr;
     float* Xrm = nullptr;
+    // products image of the tensor-core IRLS engine (p <= 4), built by its
+    // first launch
+    mutable float4* zimg = nullptr;
     double* Xdrm = nullptr;  // row-major FP64 copy for the FP64 passes
     double* sf = nullptr;
     double* off = nullptr;
@@ -644,6 +647,7 @@ PassPlan plan_for(PassKind k, const DevProblem& dp, int form) {
     const int P = dp.P;
     if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, 1};
     if (dp.grp.active) return {ENGINE_GRP, 1};
+    if (k == PASS_IRLS && P <= tc_max_p() && tc_enabled()) return {ENGINE_TC, tc_tile_genes()};
     if (P <= reg_max_p()) {
         int gt = reg_default_gt(k, P);
         if (k == PASS_MLE) {
@@ -668,7 +672,9 @@ PassPlan plan_for(PassKind k, const DevProblem& dp, int form) {
 // number of cell-segment work items for `tiles` gene tiles
 int choose_nseg(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, int tiles, int form) {
     if (form == DEVIL_FORM_PLAIN || plan.engine == ENGINE_GRP) return 1;
-    const int target = ctx->sm_count * 2;
+    // tensor-core blocks carry 128 genes each: ask for several waves of
+    // them so that the last wave's tail stays short
+    const int target = ctx->sm_count * (plan.engine == ENGINE_TC ? 8 : 2);
     int want = (target + tiles - 1) / tiles;
     return std::max(1, std::min(want, dp.nfine));
 }
@@ -747,6 +753,12 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
         LAUNCH(launch_grp_pass(kind, gg, prm, dp.val_u16, tiles, ctx->stream));
     } else if (plan.engine == ENGINE_REG) {
         LAUNCH(launch_reg_pass(L));
+    } else if (plan.engine == ENGINE_TC) {
+        if (!dp.zimg) {
+            dp.zimg = ws<float4>(ctx, "tc_zimg", (size_t)tc_zimg_float4s(dp.n));
+            LAUNCH(launch_tc_zimg(dp.Xrm, dp.xs, dp.n, dp.P, dp.zimg, ctx->stream));
+        }
+        LAUNCH(launch_tc_pass(L, dp.zimg));
     } else {
         LAUNCH(launch_gen_pass(L));
     }
@@ -831,7 +843,8 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
         launch_pass(ctx, dp, PASS_IRLS, plan, nseg, tiles, dp.fine_bound, dp.fine_ptr,
                     dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
         ++launched;
-        LAUNCH(launch_irls_finalize(pb.partW, plan.engine != ENGINE_REG, nseg, tiles * plan.GT, dp.P, act[cur], cnt + cur,
+        const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC;
+        LAUNCH(launch_irls_finalize(pb.partW, part_f64, nseg, tiles * plan.GT, dp.P, act[cur], cnt + cur,
                                     (int)hint, act[nxt], cnt + nxt, beta, beta_f, iters, status,
                                     max_iter, eps, k, st));
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));

@@ -11,7 +11,7 @@
 namespace devil {
 
 enum PassKind { PASS_IRLS = 0, PASS_MOM = 1, PASS_MLE = 2, PASS_SANDWICH = 3 };
-enum Engine { ENGINE_REG = 0, ENGINE_GEN = 1, ENGINE_GRP = 2 };
+enum Engine { ENGINE_REG = 0, ENGINE_GEN = 1, ENGINE_GRP = 2, ENGINE_TC = 3 };
 
 inline int pass_nw(PassKind k) { return k == PASS_MLE ? 3 : (k == PASS_MOM ? 0 : 1); }
 inline int pass_nv(PassKind k) { return (k == PASS_IRLS || k == PASS_SANDWICH) ? 1 : 0; }
@@ -53,6 +53,16 @@ int gen_default_gt(PassKind k, int P);
 size_t gen_smem_bytes(PassKind k, int P, int GT);
 
 cudaError_t launch_reg_pass(const PassLaunch& L);
+
+// ---- tensor-core IRLS engine (kernels_tc.cu) ----
+int tc_max_p();
+int tc_tile_genes();     // genes per block tile (the MMA's M)
+int tc_chunk_cells();
+bool tc_enabled();       // DEVIL_TC=1 selects the engine for the IRLS pass
+int64_t tc_zimg_quads(int64_t n);    // cell quads covered by the product image
+int64_t tc_zimg_float4s(int64_t n);  // its size in float4
+cudaError_t launch_tc_zimg(const float* Xrm, int xs, int64_t n, int P, float4* zimg, cudaStream_t st);
+cudaError_t launch_tc_pass(const PassLaunch& L, const float4* zimg);
 cudaError_t launch_gen_pass(const PassLaunch& L);
 
 // ---- design-group engine (kernels_grp.cu) ----

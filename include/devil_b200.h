@@ -140,7 +140,8 @@ DEVIL_API int devil_ctx_profile(devil_ctx *ctx, int pass_kind, int64_t *launches
                                 double *alg_bytes);
 /* Engine of the last launch of a pass kind on this context (no counterpart
  * in the reference): 0 register tiles (p <= 8), 1 shared-memory tiles,
- * 2 design groups (few distinct design rows), -1 none yet. */
+ * 2 design groups (few distinct design rows), 3 tensor cores (IRLS pass,
+ * p <= 4), -1 none yet. */
 DEVIL_API int devil_ctx_engine(const devil_ctx *ctx, int pass_kind);
 
 /* ---- full pipeline --------------------------------------------------- */

@@ -425,3 +425,30 @@ def test_fit_batch_names_the_failing_problem(dv):
     bad_X = np.zeros_like(P.X)  # rank deficient design
     with pytest.raises(DevilError, match="problem 1"):
         dv.fit_devil_batch([(x, P.X), (x, bad_X)], workers=2)
+
+
+@pytest.mark.parametrize("p", [4, 3, 2, 1])
+def test_tensor_core_irls_matches_oracle(dv, orc, sparse_problem, monkeypatch, p):
+    """The opt-in tcgen05 IRLS engine (DEVIL_TC=1, p <= 4): the Hessian's
+    dense part as split-TF32 MMAs, the score and the nonzero corrections in
+    FP32.  Same bars as the register engine against the oracle, and the two
+    engines agree to FP32 rounding on genes with the same iteration count."""
+    import dataclasses
+
+    # continuous covariates in every design (a design of few distinct rows
+    # goes to the design-group engine instead)
+    cols = {4: [0, 1, 2, 3], 3: [0, 1, 2], 2: [0, 2], 1: [2]}[p]
+    P = dataclasses.replace(sparse_problem, X=np.ascontiguousarray(sparse_problem.X[:, cols]), p=p)
+    ref = oracle_fit(orc, P, orc.OD_MLE)
+    reg = gpu_fit(dv, P, "MLE")
+    assert dv.context().engine(0) == "register"
+    monkeypatch.setenv("DEVIL_TC", "1")
+    tc = gpu_fit(dv, P, "MLE")
+    assert dv.context().engine(0) == "tensor"
+    same = check_beta(tc, ref)
+    check_rel(tc["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta MLE")
+    it_tc, it_reg = tc["iterations"]["beta_iters"], reg["iterations"]["beta_iters"]
+    assert (it_tc == it_reg).mean() >= 0.97
+    both = (it_tc == it_reg) & (it_reg < 200)
+    d = np.abs(tc["beta"] - reg["beta"]) / np.maximum(1.0, np.abs(reg["beta"]))
+    assert d[both].max() <= 2e-6, d[both].max()
