@@ -12,6 +12,7 @@
 #include <cstring>
 #include <atomic>
 #include <map>
+#include <mutex>
 #include <thread>
 #include <string>
 #include <unordered_map>
@@ -21,6 +22,43 @@
 #include "internal.h"
 
 using namespace devil;
+
+namespace devil {
+// resident blocks per SM of the kernel a pass would launch, from the CUDA
+// occupancy calculator; cached per configuration (all contexts, all threads)
+int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16) {
+    static std::mutex mu;
+    static std::map<int64_t, int> cache;
+    const int64_t key = ((((int64_t)kind * 8 + engine) * 64 + P) * 512 + GT) * 2 + (val_u16 ? 1 : 0);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    PassLaunch L{};
+    L.kind = kind;
+    L.engine = engine;
+    L.P = P;
+    L.xs_pad = P <= 8 ? (P <= 1 ? 1 : (P <= 2 ? 2 : (P <= 4 ? 4 : 8))) : (P + 3) & ~3;
+    L.GT = GT;
+    L.val_u16 = val_u16;
+    L.nseg = 1;
+    L.ntiles = 1;
+    int occ = 0;
+    L.occ_out = &occ;
+    cudaError_t e = cudaErrorInvalidValue;
+    if (engine == ENGINE_REG) e = launch_reg_pass(L);
+    else if (engine == ENGINE_GEN) e = launch_gen_pass(L);
+    else if (engine == ENGINE_TC) e = launch_tc_pass(L, nullptr);
+    if (e != cudaSuccess || occ < 1) {
+        cudaGetLastError();  // a failed query leaves no sticky error; use one block per SM
+        occ = 1;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = occ;
+    return occ;
+}
+}  // namespace devil
 
 struct DevBuf {
     void* p = nullptr;
@@ -641,9 +679,10 @@ GrpGeom grp_geom(const DevProblem& dp) {
 struct PassPlan {
     Engine engine;
     int GT;
+    PassKind kind = PASS_IRLS;
 };
 
-PassPlan plan_for(PassKind k, const DevProblem& dp, int form) {
+PassPlan plan_engine(PassKind k, const DevProblem& dp, int form) {
     const int P = dp.P;
     if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, 1};
     if (dp.grp.active) return {ENGINE_GRP, 1};
@@ -669,14 +708,38 @@ PassPlan plan_for(PassKind k, const DevProblem& dp, int form) {
     return {ENGINE_GEN, gen_default_gt(k, P)};
 }
 
-// number of cell-segment work items for `tiles` gene tiles
+PassPlan plan_for(PassKind k, const DevProblem& dp, int form) {
+    PassPlan p = plan_engine(k, dp, form);
+    p.kind = k;
+    return p;
+}
+
+// number of cell-segment work items for `tiles` gene tiles.  The grid has
+// tiles x nseg blocks; `cap` of them are resident at once (SMs x the
+// kernel's occupancy).  At least one full wave (four for the heavy
+// tensor-core blocks), then the smallest nseg whose last wave is nearly
+// full: with 1.1 waves the second wave would keep 90 % of the SMs idle
+// (active-gene counts in the IRLS tail produce exactly such grids).
 int choose_nseg(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, int tiles, int form) {
     if (form == DEVIL_FORM_PLAIN || plan.engine == ENGINE_GRP) return 1;
-    // tensor-core blocks carry 128 genes each: ask for several waves of
-    // them so that the last wave's tail stays short
-    const int target = ctx->sm_count * (plan.engine == ENGINE_TC ? 8 : 2);
-    int want = (target + tiles - 1) / tiles;
-    return std::max(1, std::min(want, dp.nfine));
+    const int occ = pass_blocks_per_sm(plan.kind, plan.engine, dp.P, plan.GT, dp.val_u16);
+    const int64_t cap = (int64_t)ctx->sm_count * std::max(1, occ);
+    const int64_t min_waves = plan.engine == ENGINE_TC ? 4 : 1;
+    int want = (int)((min_waves * cap + tiles - 1) / tiles);
+    want = std::max(1, std::min(want, dp.nfine));
+    const int hi = std::min(dp.nfine, 4 * want);
+    int best = want;
+    double best_eff = 0.0;
+    for (int ns = want; ns <= hi; ++ns) {
+        const double waves = (double)tiles * ns / (double)cap;
+        const double eff = waves / std::ceil(waves);
+        if (eff > best_eff + 1e-9) {
+            best = ns;
+            best_eff = eff;
+        }
+        if (eff >= 0.92) break;
+    }
+    return best;
 }
 
 // largest nseg * tiles * GT over every active-gene count the loops can see

@@ -42,6 +42,7 @@ struct PassLaunch {
     PassGeom geo;
     PassParamsAny prm;
     cudaStream_t stream;
+    int* occ_out = nullptr;  // non-null: report the kernel's resident blocks per SM, launch nothing
 };
 
 // engine choice helpers
@@ -53,6 +54,9 @@ int gen_default_gt(PassKind k, int P);
 size_t gen_smem_bytes(PassKind k, int P, int GT);
 
 cudaError_t launch_reg_pass(const PassLaunch& L);
+
+// resident blocks per SM of the kernel a pass launch would use (cached)
+int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16);
 
 // ---- tensor-core IRLS engine (kernels_tc.cu) ----
 int tc_max_p();

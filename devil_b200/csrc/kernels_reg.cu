@@ -50,6 +50,16 @@ static cudaError_t run(const PassLaunch& L) {
     if (L.xs_pad != PP) return cudaErrorInvalidValue;
     dim3 grid(L.nseg, L.ntiles);
     auto prm = make_params<K>(L.prm);
+    if (L.occ_out) {
+        const void* f;
+        if constexpr (K == PASS_IRLS)
+            f = L.val_u16 ? (const void*)reg_pass_kernel<P, PP, GT, kRegNT, Pass, uint16_t>
+                          : (const void*)reg_pass_kernel<P, PP, GT, kRegNT, Pass, float>;
+        else
+            f = L.val_u16 ? (const void*)reg_pass_kernel_b1<P, PP, GT, kRegNT, Pass, uint16_t>
+                          : (const void*)reg_pass_kernel_b1<P, PP, GT, kRegNT, Pass, float>;
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, f, kRegNT, 0);
+    }
     if constexpr (!Pass::F64) {
         if (L.use_tma) {
             constexpr size_t smem = 2 * TmaChunk<PP>::STAGE_FLOATS * sizeof(float);

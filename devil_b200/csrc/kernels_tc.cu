@@ -510,11 +510,13 @@ cudaError_t run_tc(const PassLaunch& L, const float4* zimg) {
         auto k = tc_irls_kernel<P, uint16_t>;
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
         if (e != cudaSuccess) return e;
+        if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kTcNT, kTcSmem);
         k<<<grid, kTcNT, kTcSmem, L.stream>>>(L.geo, prm, zimg);
     } else {
         auto k = tc_irls_kernel<P, float>;
         e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
         if (e != cudaSuccess) return e;
+        if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kTcNT, kTcSmem);
         k<<<grid, kTcNT, kTcSmem, L.stream>>>(L.geo, prm, zimg);
     }
     return cudaGetLastError();
