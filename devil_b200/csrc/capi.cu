@@ -686,7 +686,7 @@ PassPlan plan_engine(PassKind k, const DevProblem& dp, int form) {
     const int P = dp.P;
     if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, 1};
     if (dp.grp.active) return {ENGINE_GRP, 1};
-    if (k == PASS_IRLS && P <= tc_max_p() && tc_enabled()) return {ENGINE_TC, tc_tile_genes()};
+    if (P <= tc_max_p() && tc_enabled(k)) return {ENGINE_TC, tc_tile_genes(k)};
     if (P <= reg_max_p()) {
         int gt = reg_default_gt(k, P);
         if (k == PASS_MLE) {
@@ -986,7 +986,8 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
         launch_pass(ctx, dp, PASS_MLE, plan, nseg, tiles, dp.fine_bound,
                     dp.fine_ptr, dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
         ++launched;
-        LAUNCH(launch_mle_finalize(pb.partW, plan.engine != ENGINE_REG, pb.partS, nseg, tiles * plan.GT, dp.P, dp.stats, dp.n,
+        const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC;
+        LAUNCH(launch_mle_finalize(pb.partW, part_f64, pb.partS, nseg, tiles * plan.GT, dp.P, dp.stats, dp.n,
                                    act[cur], cnt + cur, (int)hint, act[nxt], cnt + nxt, s, max_iter,
                                    cox_reid, nullptr, st));
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));

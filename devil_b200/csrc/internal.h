@@ -60,9 +60,9 @@ int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16)
 
 // ---- tensor-core IRLS engine (kernels_tc.cu) ----
 int tc_max_p();
-int tc_tile_genes();     // genes per block tile (the MMA's M)
+int tc_tile_genes(PassKind k);  // genes per block tile: 128 (IRLS), 32 (MLE)
 int tc_chunk_cells();
-bool tc_enabled();       // DEVIL_TC=1 selects the engine for the IRLS pass
+bool tc_enabled(PassKind k);  // DEVIL_TC=1 (IRLS), DEVIL_TC_MLE=1 (MLE) select the engine
 int64_t tc_zimg_quads(int64_t n);    // cell quads covered by the product image
 int64_t tc_zimg_float4s(int64_t n);  // its size in float4
 cudaError_t launch_tc_zimg(const float* Xrm, int xs, int64_t n, int P, float4* zimg, cudaStream_t st);

@@ -116,6 +116,13 @@ DEV void tc_mma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t accumulate) {
         "l"(ad), "l"(bd), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
+DEV void tc_mma_n(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t accumulate, uint32_t idesc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
+        "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
 DEV void tc_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                      smem_u32(bar))
@@ -466,6 +473,355 @@ __global__ void __launch_bounds__(kTcNT) tc_irls_kernel(PassGeom geo, PassIRLS::
     if (abort_flag && tid == 0) atomicExch(geo.err, 1);
 }
 
+// ---------------------------------------------------------------------
+// MLE pass (PassMLE in passes.cuh; src/overdispersion.cpp:95-242): the
+// Cox-Reid matrices b = X' diag(w) X, db = X' diag(-w^2) X and
+// d2b = X' diag(2 w^3) X (w = mu / (1 + mu theta)) on the tensor cores.
+// A tile is 32 genes; the MMA's 128 rows are the three weights of the 32
+// genes (rows 32 b + gene, b = 0, 1, 2) and 32 zero rows.  One thread per
+// (gene, quad of cells) computes the weights and the two FP32 scalar sums
+// of the dense terms; the nonzero terms (FP64, per-gene digamma tables)
+// run after the cell loop, a warp per gene.  Per K-step two MMAs:
+//     D[0..31]  += R_hi [Z_hi; Z_lo]      (N = 32)
+//     D[0..15]  += R_lo  Z_hi              (N = 16; R_lo Z_lo ~ 2^-22 dropped)
+// so a run region is 32 columns and the Hessian-like sums are columns
+// 0..15 plus 16..31.
+// ---------------------------------------------------------------------
+constexpr int kMleG = 32;                    // genes per tile
+constexpr uint32_t kMleRegion = kTcN;        // 32 columns per run region
+constexpr uint32_t kMleCols = 2 * kMleRegion;
+constexpr uint32_t kIdesc16 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcZ >> 3) << 17) |
+                              ((uint32_t)(kTcM >> 4) << 24);
+
+struct ScalAcc {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    template <int K>
+    DEV void scal(double v) { s[K] += v; }
+};
+
+// per-warp table of psi(v + a) - psi(a) and psi1(v + a) - psi1(a),
+// v = 0..kPsiTab-1 (prefix sums of 1/(a+j) and -1/(a+j)^2)
+DEV void warp_psi_table(double a, double* d1, double* d2) {
+    const int lane = threadIdx.x & 31;
+    double c1 = 0.0, c2 = 0.0;
+    for (int base = 0; base < kPsiTab; base += 32) {
+        const int v = base + lane;
+        const double t = v == 0 ? 0.0 : 1.0 / (a + (v - 1));
+        double s1 = t, s2 = -t * t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double u1 = __shfl_up_sync(0xffffffffu, s1, o);
+            const double u2 = __shfl_up_sync(0xffffffffu, s2, o);
+            if (lane >= o) {
+                s1 += u1;
+                s2 += u2;
+            }
+        }
+        d1[v] = c1 + s1;
+        d2[v] = c2 + s2;
+        c1 += __shfl_sync(0xffffffffu, s1, 31);
+        c2 += __shfl_sync(0xffffffffu, s2, 31);
+    }
+    __syncwarp();
+}
+
+template <int P, class VT>
+__global__ void __launch_bounds__(kTcNT) tc_mle_kernel(PassGeom geo, PassMLE::Params prm,
+                                                      const float4* __restrict__ zimg) {
+    constexpr int NE = P * (P + 1) / 2;
+    constexpr int NA = 3 * NE + 2;
+    constexpr int PP = P <= 1 ? 1 : (P <= 2 ? 2 : 4);
+    static_assert(NE <= kTcZ, "products fit the MMA's N");
+    // epilogue scratch in the first R stage: dense scalar sums, the R_lo
+    // halves of the drained rows, nonzero sums, digamma tables
+    constexpr int kFs = 0;                               // float [8][32][2]
+    constexpr int kHlo = kFs + 8 * kMleG * 2 * 4;        // float [3][32][16]
+    constexpr int kSpar = kHlo + 3 * kMleG * 16 * 4;     // double [32][4]
+    constexpr int kPsi = kSpar + kMleG * 4 * 8;          // double [8 warps][2][kPsiTab]
+    static_assert(kPsi + 8 * 2 * kPsiTab * 8 <= kTcStage, "epilogue scratch fits the first R stage");
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t tslot;
+    __shared__ int abort_flag;
+
+    if (geo.reset_next && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *geo.reset_next = 0;
+    const int nact = *geo.n_act;
+    const int tile = blockIdx.y;
+    if (tile * kMleG >= nact) return;
+    const int seg = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const VT* __restrict__ val = static_cast<const VT*>(geo.val);
+
+    // dense phase: gene = tile slot lane, cells = quad `warp` of each chunk
+    int slot0 = tile * kMleG + lane;
+    if (slot0 >= nact) slot0 = tile * kMleG;  // duplicate a valid gene; not written
+    const int gene = __ldg(geo.act + slot0);
+    float beta[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) beta[i] = __ldg(prm.beta + (int64_t)gene * P + i) * kLog2e;
+    const float thf = (float)exp(__ldg(prm.log_theta + gene));
+    const int nfs = geo.nbound - 1;
+    const int b0 = (int)(((int64_t)seg * nfs) / geo.nseg);
+    const int b1 = (int)(((int64_t)(seg + 1) * nfs) / geo.nseg);
+    const int c0 = __ldg(geo.bound + b0), c1 = __ldg(geo.bound + b1);
+
+    auto in_stage = [&](int s) { return tc_smem + 2 * kTcStage + s * kTcInBytes; };
+    auto fetch_inputs = [&](int kc) {
+        unsigned char* ib = in_stage(kc & 3);
+        const int cs = c0 + kc * kTcKC;
+        cp_async<16>(ib + tid * 16, zimg + (int64_t)(cs >> 2) * kTcN + tid);
+        constexpr int NX = kTcKC * PP / 4;
+        constexpr int CPX = 4 / PP;
+        if (tid < NX) {
+            const int cell = cs + tid * CPX;
+            const int valid = min(max(c1 - cell, 0), CPX);
+            cp_async_zfill(ib + kTcInX + tid * 16, valid ? (const void*)(geo.X + (int64_t)cell * PP) : geo.X,
+                           (uint32_t)(valid * PP * 4));
+        } else if (tid >= 64 && tid < 64 + kTcKC / 4) {
+            const int pc = tid - 64;
+            const int cell = cs + 4 * pc;
+            const int valid = min(max(c1 - cell, 0), 4);
+            cp_async_zfill(ib + kTcInOff + pc * 16, valid ? (const void*)(geo.off + cell) : geo.off,
+                           (uint32_t)(valid * 4));
+        }
+    };
+    const int nchunk = (c1 - c0 + kTcKC - 1) / kTcKC;
+    if (nchunk > 0) fetch_inputs(0);
+    cp_async_commit();
+    if (nchunk > 1) fetch_inputs(1);
+    cp_async_commit();
+    // rows 96..127 (no weight) stay zero in both stages
+    for (int i = tid; i < 2 * 2 * kMleG * (kTcKC / 4); i += kTcNT) {
+        const int buf = i / (kMleG * (kTcKC / 4)), r = i % (kMleG * (kTcKC / 4));
+        const int q = r / kMleG, row = 3 * kMleG + r % kMleG;
+        *reinterpret_cast<float4*>(tc_smem + buf * kTcABytes + stage_off(row, q, kTcM)) =
+            make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    cp_async_wait<1>();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+
+    if (tid == 0) {
+        abort_flag = 0;
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tslot)),
+                     "r"(kMleCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tslot;
+
+    float fs0 = 0.f, fs1 = 0.f;
+    // drained rows: warp w (w & 3 = weight b < 3) owns row 32 b + lane,
+    // columns 0..15 (warps 0..3) or 16..31 (warps 4..7)
+    float hacc[16];
+#pragma unroll
+    for (int a = 0; a < 16; ++a) hacc[a] = 0.f;
+    const bool drains = (warp & 3) < 3;
+    const uint32_t lanes = ((uint32_t)(32 * (warp & 3)) << 16) + (warp < 4 ? 0u : (uint32_t)kTcZ);
+    int drained = 0;
+    int issued = 0;
+    for (int k = 0; k < nchunk; ++k) {
+        const int st = k & 1;
+        bool ok = true;
+        if (k >= 2) {
+            ok = mbar_wait_bounded(&bars[st], (uint32_t)(((k >> 1) - 1) & 1));
+            if (!ok) atomicExch(&abort_flag, 1);
+        }
+        ok = __all_sync(0xffffffffu, ok);
+        if (k >= 2 && (k - 2) % kTcRun == kTcRun - 1) {
+            if (drains && ok) {
+                float t[16];
+                tc_ld16(tmem + lanes + kMleRegion * (uint32_t)(drained & 1), t);
+#pragma unroll
+                for (int a = 0; a < 16; ++a) hacc[a] += t[a];
+            }
+            ++drained;
+        }
+        if (k + 2 < nchunk) fetch_inputs(k + 2);
+        cp_async_commit();
+        unsigned char* sAh = tc_smem + st * kTcStage;
+        unsigned char* sAl = sAh + kTcABytes;
+        const unsigned char* ib = in_stage(k & 3);
+        const float* xs = reinterpret_cast<const float*>(ib + kTcInX);
+        const float* os = reinterpret_cast<const float*>(ib + kTcInOff);
+        const int cs = c0 + k * kTcKC;
+        {
+            const int q = warp;
+            float wv[3][4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                float x[P];
+#pragma unroll
+                for (int i = 0; i < P; ++i) x[i] = xs[(4 * q + t) * PP + i];
+                float e = os[4 * q + t] * kLog2e;
+#pragma unroll
+                for (int i = 0; i < P; ++i) e = fmaf(x[i], beta[i], e);
+                const float mu = ex2_approx(e);
+                // PassMLE::dense
+                const float xx = mu * thf;
+                const float r = rcp_approx(1.f + xx);
+                const float w = mu * r;
+                wv[0][t] = w;
+                wv[1][t] = -w * w;
+                wv[2][t] = 2.f * w * w * w;
+                // zero-filled cells past the last one meet Z = 0 in the
+                // MMAs but would add to these sums
+                if (cs + 4 * q + t < c1) {
+                    fs0 += nb_ll_term<float>(xx, r);
+                    fs1 += w * xx * r;
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                float hi[4], lo[4];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    hi[t] = __uint_as_float(__float_as_uint(wv[b][t]) & 0xFFFFE000u);
+                    lo[t] = wv[b][t] - hi[t];
+                }
+                const int off = stage_off(kMleG * b + lane, q, kTcM);
+                *reinterpret_cast<float4*>(sAh + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+                *reinterpret_cast<float4*>(sAl + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+            }
+        }
+        cp_async_wait<1>();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        if (abort_flag) break;
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t dreg = tmem + kMleRegion * (uint32_t)((k / kTcRun) & 1);
+            const uint32_t sB = smem_u32(ib);
+#pragma unroll
+            for (int s = 0; s < kTcKC / 8; ++s) {
+                const uint32_t acc = (k % kTcRun != 0 || s > 0) ? 1u : 0u;
+                const uint64_t bd = umma_desc(sB + s * 2 * kTcN * 16, kTcN * 16, 128);
+                const uint64_t ah = umma_desc(smem_u32(sAh) + s * 2 * kTcM * 16, kTcM * 16, 128);
+                const uint64_t al = umma_desc(smem_u32(sAl) + s * 2 * kTcM * 16, kTcM * 16, 128);
+                tc_mma(dreg, ah, bd, acc);                // R_hi [Z_hi; Z_lo]
+                tc_mma_n(dreg, al, bd, 1u, kIdesc16);     // R_lo Z_hi (the first 16 rows of B)
+            }
+            tc_commit(&bars[st]);
+        }
+        issued = k + 1;
+    }
+    cp_async_wait<0>();
+    if (issued > 0 &&
+        !mbar_wait_bounded(&bars[(issued - 1) & 1], (uint32_t)(((issued - 1) >> 1) & 1)))
+        atomicExch(&abort_flag, 1);
+    tc_fence_after();
+    __syncthreads();
+    if (!abort_flag) {
+        const int runs = (issued + kTcRun - 1) / kTcRun;
+        for (; drained < runs; ++drained)
+            if (drains) {
+                float t[16];
+                tc_ld16(tmem + lanes + kMleRegion * (uint32_t)(drained & 1), t);
+#pragma unroll
+                for (int a = 0; a < 16; ++a) hacc[a] += t[a];
+            }
+    }
+    __syncthreads();
+
+    float* fsr = reinterpret_cast<float*>(tc_smem + kFs);
+    float* hlo = reinterpret_cast<float*>(tc_smem + kHlo);
+    double* spar = reinterpret_cast<double*>(tc_smem + kSpar);
+    double* psi = reinterpret_cast<double*>(tc_smem + kPsi) + warp * 2 * kPsiTab;
+    fsr[(warp * kMleG + lane) * 2 + 0] = fs0;
+    fsr[(warp * kMleG + lane) * 2 + 1] = fs1;
+    if (warp >= 4 && drains) {
+#pragma unroll
+        for (int a = 0; a < 16; ++a) hlo[((warp - 4) * kMleG + lane) * 16 + a] = hacc[a];
+    }
+
+    // nonzero terms (PassMLE::sparse, FP64): warp w takes genes w, w + 8, ...
+    for (int gi = warp; gi < kMleG; gi += 8) {
+        int slot = tile * kMleG + gi;
+        if (slot >= nact) slot = tile * kMleG;
+        const int g = __ldg(geo.act + slot);
+        const double th = exp(__ldg(prm.log_theta + g));
+        const double a = 1.0 / th;
+        warp_psi_table(a, psi, psi + kPsiTab);
+        PassMLE::Gene G{th, a, (float)th, PsiTable{psi, psi + kPsiTab, digamma_d(a), trigamma_d(a)}};
+        float bg[P];
+#pragma unroll
+        for (int i = 0; i < P; ++i) bg[i] = __ldg(prm.beta + (int64_t)g * P + i) * kLog2e;
+        ScalAcc acc;
+        const int64_t* sp = geo.segptr + (int64_t)g * geo.nbound;
+        const int64_t e0 = __ldg(sp + b0), e1 = __ldg(sp + b1);
+        for (int64_t eb = e0 + lane; eb < e1; eb += 64) {
+            int cc[2];
+            float yy[2];
+            bool okk[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int64_t e = eb + 32 * u;
+                okk[u] = e < e1;
+                cc[u] = okk[u] ? __ldg(geo.col + e) : c0;
+                yy[u] = okk[u] ? load_val(val, e) : 0.f;
+            }
+            float xr[2][P], ol[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                load_row<P, PP>(geo.X, cc[u], xr[u]);
+                ol[u] = __ldg(geo.off + cc[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                if (!okk[u]) continue;
+                float el = ol[u] * kLog2e;
+#pragma unroll
+                for (int i = 0; i < P; ++i) el = fmaf(xr[u][i], bg[i], el);
+                PassMLE::sparse<float>(G, ex2_approx(el), yy[u], acc);
+            }
+        }
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) acc.s[k2] = warp_sum(acc.s[k2]);
+        if (lane == 0) {
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2) spar[gi * 4 + k2] = acc.s[k2];
+        }
+        __syncwarp();  // the table is rebuilt for the next gene
+    }
+    __syncthreads();
+
+    const int slot = tile * kMleG + lane;
+    if (slot < nact && !abort_flag) {
+        float* out = static_cast<float*>(geo.partW) + ((int64_t)seg * geo.slot_stride + slot) * NA;
+        if (warp < 3) {  // weight b = warp: b, db, d2b
+#pragma unroll
+            for (int a = 0; a < NE; ++a) out[warp * NE + a] = hacc[a] + hlo[(warp * kMleG + lane) * 16 + a];
+        } else if (warp == 3) {
+            float f0 = 0.f, f1 = 0.f;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) {
+                f0 += fsr[(w * kMleG + lane) * 2 + 0];
+                f1 += fsr[(w * kMleG + lane) * 2 + 1];
+            }
+            out[3 * NE + 0] = f0;
+            out[3 * NE + 1] = f1;
+            double* outs = geo.partS + ((int64_t)seg * geo.slot_stride + slot) * 4;
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2) outs[k2] = spar[lane * 4 + k2];
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kMleCols)
+                     : "memory");
+    if (abort_flag && tid == 0) atomicExch(geo.err, 1);
+}
+
 // Z image: for every quad of 4 cells, 32 rows of 4 TF32 values: rows
 // 0..15 the high parts of the products x_i x_j (packed upper-triangle
 // order, then zeros), rows 16..31 the low parts; cells at or beyond n are
@@ -522,10 +878,32 @@ cudaError_t run_tc(const PassLaunch& L, const float4* zimg) {
     return cudaGetLastError();
 }
 
+template <int P>
+cudaError_t run_tc_mle(const PassLaunch& L, const float4* zimg) {
+    if (L.GT != kMleG) return cudaErrorInvalidValue;
+    dim3 grid(L.nseg, L.ntiles);
+    PassMLE::Params prm{L.prm.beta, L.prm.beta_d, L.prm.log_theta};
+    cudaError_t e;
+    if (L.val_u16) {
+        auto k = tc_mle_kernel<P, uint16_t>;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        if (e != cudaSuccess) return e;
+        if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kTcNT, kTcSmem);
+        k<<<grid, kTcNT, kTcSmem, L.stream>>>(L.geo, prm, zimg);
+    } else {
+        auto k = tc_mle_kernel<P, float>;
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        if (e != cudaSuccess) return e;
+        if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kTcNT, kTcSmem);
+        k<<<grid, kTcNT, kTcSmem, L.stream>>>(L.geo, prm, zimg);
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 int tc_max_p() { return 4; }
-int tc_tile_genes() { return kTcM; }
+int tc_tile_genes(PassKind k) { return k == PASS_MLE ? kMleG : kTcM; }
 int tc_chunk_cells() { return kTcKC; }
 
 // Opt-in (DEVIL_TC=1): at p <= 4 the register engine is faster on B200.
@@ -534,7 +912,12 @@ int tc_chunk_cells() { return kTcKC; }
 // on the hi/lo split, the shared-memory stores and the per-chunk
 // synchronisation (measured: IRLS 171 ms vs 133 ms per step on the
 // 20,000 x 100,000 benchmark fit).
-bool tc_enabled() {
+bool tc_enabled(PassKind k) {
+    if (k == PASS_MLE) {
+        const char* e = getenv("DEVIL_TC_MLE");
+        return e && atoi(e) == 1;
+    }
+    if (k != PASS_IRLS) return false;
     const char* e = getenv("DEVIL_TC");
     return e && atoi(e) == 1;
 }
@@ -553,7 +936,17 @@ cudaError_t launch_tc_zimg(const float* Xrm, int xs, int64_t n, int P, float4* z
 
 // L.GT = 128 genes per tile; the grid has L.ntiles rows of blocks
 cudaError_t launch_tc_pass(const PassLaunch& L, const float4* zimg) {
-    if (L.kind != PASS_IRLS || L.xs_pad != (L.P <= 1 ? 1 : (L.P <= 2 ? 2 : 4))) return cudaErrorInvalidValue;
+    if (L.xs_pad != (L.P <= 1 ? 1 : (L.P <= 2 ? 2 : 4))) return cudaErrorInvalidValue;
+    if (L.kind == PASS_MLE) {
+        switch (L.P) {
+            case 1: return run_tc_mle<1>(L, zimg);
+            case 2: return run_tc_mle<2>(L, zimg);
+            case 3: return run_tc_mle<3>(L, zimg);
+            case 4: return run_tc_mle<4>(L, zimg);
+        }
+        return cudaErrorInvalidValue;
+    }
+    if (L.kind != PASS_IRLS) return cudaErrorInvalidValue;
     switch (L.P) {
         case 1: return run_tc<1>(L, zimg);
         case 2: return run_tc<2>(L, zimg);

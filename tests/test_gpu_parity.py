@@ -452,3 +452,21 @@ def test_tensor_core_irls_matches_oracle(dv, orc, sparse_problem, monkeypatch, p
     both = (it_tc == it_reg) & (it_reg < 200)
     d = np.abs(tc["beta"] - reg["beta"]) / np.maximum(1.0, np.abs(reg["beta"]))
     assert d[both].max() <= 2e-6, d[both].max()
+
+
+@pytest.mark.parametrize("p", [4, 3])
+def test_tensor_core_mle_matches_oracle(dv, orc, sparse_problem, monkeypatch, p):
+    """The opt-in tcgen05 MLE pass (DEVIL_TC_MLE=1, p <= 4): the Cox-Reid
+    matrices b, db, d2b as split-TF32 MMAs over 32-gene tiles, the scalar
+    and nonzero terms on the CUDA cores.  theta against the oracle with the
+    register engine's bar."""
+    import dataclasses
+
+    cols = {4: [0, 1, 2, 3], 3: [0, 1, 2]}[p]
+    P = dataclasses.replace(sparse_problem, X=np.ascontiguousarray(sparse_problem.X[:, cols]), p=p)
+    ref = oracle_fit(orc, P, orc.OD_MLE)
+    monkeypatch.setenv("DEVIL_TC_MLE", "1")
+    tc = gpu_fit(dv, P, "MLE")
+    assert dv.context().engine(2) == "tensor"
+    same = check_beta(tc, ref)
+    check_rel(tc["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta MLE")
