@@ -22,6 +22,7 @@ DENSE_GENE_MAJOR, DENSE_CELL_MAJOR = 0, 1
 SF_NONE, SF_NORMED_SUM, SF_PSINORM, SF_GIVEN = range(4)
 OD_NONE, OD_MOM, OD_MLE, OD_NEW = range(4)
 FORM_CHOSEN, FORM_PLAIN = 0, 1
+PREC_FP32, PREC_TC_TF32, PREC_TC_BF16X3 = 0, 1, 2
 ADJ_NONE, ADJ_BH, ADJ_BONFERRONI, ADJ_HOLM, ADJ_HOCHBERG, ADJ_BY = range(6)
 GENE_CONVERGED, GENE_MAX_ITER, GENE_NAN = range(3)
 NA_INT = -(2 ** 31)
@@ -57,7 +58,7 @@ class FitOpts(C.Structure):
                 ("init_beta_rough", C.c_int), ("size_factors", C.c_int),
                 ("size_factor_values", C.c_void_p), ("offset", C.c_double),
                 ("has_init_overdispersion", C.c_int), ("init_overdispersion", C.c_double),
-                ("compute_theta_mom", C.c_int), ("form", C.c_int)]
+                ("compute_theta_mom", C.c_int), ("form", C.c_int), ("precision", C.c_int)]
 
 
 class Problem(C.Structure):

@@ -208,8 +208,11 @@ def _sf_mode(size_factors, n):
     return L.SF_GIVEN, sf
 
 
+_PRECISION = {"fp32": 0, "tc_tf32": 1, "tc_bf16x3": 2}
+
+
 def _fit_opts(overdispersion, init_overdispersion, init_beta_rough, offset, sfm, sfv, max_iter,
-              tolerance, compute_theta_mom, form):
+              tolerance, compute_theta_mom, form, precision="fp32"):
     opts = L.FitOpts()
     L.load().devil_fit_opts_default(C.byref(opts))
     opts.max_iter = int(max_iter)
@@ -224,6 +227,9 @@ def _fit_opts(overdispersion, init_overdispersion, init_beta_rough, offset, sfm,
         opts.init_overdispersion = float(init_overdispersion)
     opts.compute_theta_mom = int(bool(compute_theta_mom))
     opts.form = L.FORM_PLAIN if form == "plain" else L.FORM_CHOSEN
+    if precision not in _PRECISION:
+        raise ValueError(f"precision must be one of {sorted(_PRECISION)}")
+    opts.precision = _PRECISION[precision]
     return opts
 
 
@@ -288,18 +294,20 @@ class _FitSlots:
 def fit_devil(x, design_matrix, clusters=None, overdispersion="MOM", init_overdispersion=None,
               init_beta_rough=False, offset=0.0, size_factors=None, verbose=False, max_iter=200,
               tolerance=1e-3, CUDA=True, batch_size=1024, form="chosen", compute_theta_mom=False,
-              device=0):
+              device=0, precision="fp32"):
     """Fit the per-gene NB GLM (fit_devil, R/main.R:164-273) on the GPU.
 
     ``CUDA`` and ``batch_size`` are accepted for signature compatibility;
     the B200 path always runs on the GPU and schedules genes itself.
     ``form`` = "chosen" (default) or "plain" (the per-cell, one gene per
-    block comparison form)."""
+    block comparison form).  ``precision`` = "fp32" (default: FP32 FMAs on
+    the CUDA cores) or "tc_tf32" (the IRLS and MLE Hessian contractions as
+    tcgen05 MMAs on split-TF32 operands, p <= 4); "tc_bf16x3" is rejected."""
     del verbose, CUDA, batch_size
     f = _FitSlots(x, design_matrix, clusters, compute_theta_mom)
     sfm, sfv = _sf_mode(size_factors, f.n)
     opts = _fit_opts(overdispersion, init_overdispersion, init_beta_rough, offset, sfm, sfv,
-                     max_iter, tolerance, compute_theta_mom, form)
+                     max_iter, tolerance, compute_theta_mom, form, precision)
     ctx = L.context(device)
     rc = L.load().devil_fit(ctx.h, f.counts.ref, _ptr(f.Xf), f.p, _ptr(f.ends),
                             0 if f.ends is None else len(f.ends), C.byref(opts), C.byref(f.res))
@@ -311,7 +319,8 @@ def fit_devil(x, design_matrix, clusters=None, overdispersion="MOM", init_overdi
 
 def fit_devil_batch(problems, overdispersion="MOM", init_overdispersion=None,
                     init_beta_rough=False, offset=0.0, size_factors=None, max_iter=200,
-                    tolerance=1e-3, form="chosen", compute_theta_mom=False, workers=4, device=0):
+                    tolerance=1e-3, form="chosen", compute_theta_mom=False, workers=4, device=0,
+                    precision="fp32"):
     """fit_devil for many independent problems in one call (devil_fit_batch).
 
     ``problems`` is a sequence of (x, design_matrix) or (x, design_matrix,
@@ -327,7 +336,7 @@ def fit_devil_batch(problems, overdispersion="MOM", init_overdispersion=None,
         slots.append(_FitSlots(x, X, cl, compute_theta_mom))
     sfm, _ = _sf_mode(size_factors, 1)
     opts = _fit_opts(overdispersion, init_overdispersion, init_beta_rough, offset, sfm, None,
-                     max_iter, tolerance, compute_theta_mom, form)
+                     max_iter, tolerance, compute_theta_mom, form, precision)
     n = len(slots)
     arr = (L.Problem * max(n, 1))()
     res = (L.FitResult * max(n, 1))()

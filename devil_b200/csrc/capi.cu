@@ -226,6 +226,7 @@ struct DevProblem {
     // products image of the tensor-core IRLS engine (p <= 4), built by its
     // first launch
     mutable float4* zimg = nullptr;
+    int precision = DEVIL_PREC_FP32;  // DEVIL_PREC_*: tensor-core passes at p <= 4
     double* Xdrm = nullptr;  // row-major FP64 copy for the FP64 passes
     double* sf = nullptr;
     double* off = nullptr;
@@ -686,7 +687,9 @@ PassPlan plan_engine(PassKind k, const DevProblem& dp, int form) {
     const int P = dp.P;
     if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, 1};
     if (dp.grp.active) return {ENGINE_GRP, 1};
-    if (P <= tc_max_p() && tc_enabled(k)) return {ENGINE_TC, tc_tile_genes(k)};
+    const bool tc = tc_enabled(k) ||
+                    (dp.precision == DEVIL_PREC_TC_TF32 && (k == PASS_IRLS || k == PASS_MLE));
+    if (P <= tc_max_p() && tc) return {ENGINE_TC, tc_tile_genes(k)};
     if (P <= reg_max_p()) {
         int gt = reg_default_gt(k, P);
         if (k == PASS_MLE) {
@@ -1222,6 +1225,7 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     cudaStream_t st = ctx->stream;
     const int64_t G = dp.G;
     const int P = dp.P;
+    dp.precision = o->precision;
     dbg_mark(ctx, "groups");
     LAUNCH(launch_theta0(dp.stats, dp.off, G, dp.n, o->has_init_overdispersion,
                          o->init_overdispersion, fb.theta0, fb.k, st));
@@ -1296,6 +1300,11 @@ void validate_opts(devil_ctx* ctx, const devil_fit_opts* o) {
         fail(ctx, DEVIL_ERR_UNSUPPORTED, "overdispersion mode %d not supported", o->overdispersion);
     if (o->form != DEVIL_FORM_CHOSEN && o->form != DEVIL_FORM_PLAIN)
         fail(ctx, DEVIL_ERR_ARG, "unknown form %d", o->form);
+    if (o->precision == DEVIL_PREC_TC_BF16X3)
+        fail(ctx, DEVIL_ERR_UNSUPPORTED,
+             "precision tc_bf16x3 is not provided; DEVIL_PREC_TC_TF32 (split TF32) reaches FP32 accuracy");
+    if (o->precision != DEVIL_PREC_FP32 && o->precision != DEVIL_PREC_TC_TF32)
+        fail(ctx, DEVIL_ERR_ARG, "unknown precision %d", o->precision);
 }
 
 template <class F>

@@ -87,6 +87,15 @@ typedef struct devil_counts {
 #define DEVIL_FORM_CHOSEN    0   /* tiled, compacted, grouped kernels       */
 #define DEVIL_FORM_PLAIN     1   /* straightforward FP32 SIMT comparison    */
 
+/* arithmetic of the per-cell Hessian contractions (IRLS and MLE passes) */
+#define DEVIL_PREC_FP32      0   /* FP32 FMAs on the CUDA cores (default)   */
+#define DEVIL_PREC_TC_TF32   1   /* tcgen05 MMAs on split TF32 (hi + lo)    */
+                                 /* operands, FP32 accumulation; p <= 4,    */
+                                 /* other p fall back to DEVIL_PREC_FP32    */
+#define DEVIL_PREC_TC_BF16X3 2   /* not provided (DEVIL_ERR_UNSUPPORTED):   */
+                                 /* the split-TF32 path already reaches     */
+                                 /* FP32 accuracy                           */
+
 typedef struct devil_fit_opts {
     int max_iter;                 /* default 200                           */
     double tolerance;             /* default 1e-3 (rounded to float, as    */
@@ -100,6 +109,7 @@ typedef struct devil_fit_opts {
     double init_overdispersion;
     int compute_theta_mom;        /* also return the MOM theta at beta     */
     int form;                     /* DEVIL_FORM_*                          */
+    int precision;                /* DEVIL_PREC_* (default FP32)           */
 } devil_fit_opts;
 
 DEVIL_API void devil_fit_opts_default(devil_fit_opts *opts);

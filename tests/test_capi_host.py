@@ -97,6 +97,20 @@ def test_argument_errors_before_gpu(dv):
         dv.api._sf_mode("edgeR", 3)
     with pytest.raises(ValueError, match="older version"):
         dv.test_de({"beta": np.zeros((2, 2))}, [0, 1])
+    with pytest.raises(ValueError, match="precision must be one of"):
+        dv.api._fit_opts("MOM", None, False, 0.0, 0, None, 200, 1e-3, False, "chosen", "fp16")
+    opts = dv.api._fit_opts("MOM", None, False, 0.0, 0, None, 200, 1e-3, False, "chosen", "tc_tf32")
+    assert opts.precision == 1 and opts.form == 0
+
+
+def test_fit_opts_layout_matches_header():
+    """The ctypes mirror of devil_fit_opts lists the header's fields in order."""
+    import re
+    from devil_b200 import _lib as L
+    hdr = open(os.path.join(ROOT, "include", "devil_b200.h")).read()
+    body = hdr[hdr.index("typedef struct devil_fit_opts {"):hdr.index("} devil_fit_opts;")]
+    fields = re.findall(r"^\s+(?:const\s+)?\w+\s*\*?\s*(\w+);", body, re.M)
+    assert fields == [f for f, _ in L.FitOpts._fields_]
 
 
 def test_null_context_is_an_error_not_a_crash(dv):

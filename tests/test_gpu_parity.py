@@ -43,10 +43,10 @@ def oracle_fit(orc, P, od, clusters_ends=None, sf="normed_sum", max_iter=200, to
 
 
 def gpu_fit(dv, P, od, clusters=None, sf="normed_sum", max_iter=200, tol=1e-3, form="chosen",
-            init_rough=False):
+            init_rough=False, precision="fp32"):
     return dv.fit_devil((P.rowptr, P.col, P.val, P.n), P.X, clusters=clusters, overdispersion=od,
                         size_factors=sf, max_iter=max_iter, tolerance=tol, form=form,
-                        compute_theta_mom=True, init_beta_rough=init_rough)
+                        compute_theta_mom=True, init_beta_rough=init_rough, precision=precision)
 
 
 def check_beta(fit, ref, tol=BETA_TOL, agree=ITER_AGREE, max_iter=200):
@@ -470,3 +470,19 @@ def test_tensor_core_mle_matches_oracle(dv, orc, sparse_problem, monkeypatch, p)
     assert dv.context().engine(2) == "tensor"
     same = check_beta(tc, ref)
     check_rel(tc["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta MLE")
+
+
+def test_precision_tc_tf32_option(dv, orc, sparse_problem):
+    """precision="tc_tf32" (DEVIL_PREC_TC_TF32 in the C ABI) puts the IRLS and
+    MLE passes on the tensor-core engines; results keep the oracle bars.
+    "tc_bf16x3" is refused with DEVIL_ERR_UNSUPPORTED."""
+    P = sparse_problem
+    ref = oracle_fit(orc, P, orc.OD_MLE)
+    fit = gpu_fit(dv, P, "MLE", precision="tc_tf32")
+    ctx = dv.context()
+    assert [ctx.engine(k) for k in range(4)] == ["tensor", "register", "tensor", "register"]
+    same = check_beta(fit, ref)
+    check_rel(fit["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta MLE")
+    check_mats(fit["beta_sandwiches_null"], ref["bread"], same & (ref["theta"] < 1e3), 1e-4, "bread")
+    with pytest.raises(RuntimeError, match="tc_bf16x3"):
+        gpu_fit(dv, P, "MLE", precision="tc_bf16x3")
