@@ -31,7 +31,7 @@ NA_INT = -(2 ** 31)
 EXPORTS = (
     "devil_version", "devil_fit_opts_default", "devil_ctx_create", "devil_ctx_destroy",
     "devil_last_error", "devil_ctx_stream", "devil_ctx_synchronize", "devil_ctx_launch_count",
-    "devil_fit", "devil_fit_device", "devil_test_de", "devil_test_de_device", "devil_p_adjust",
+    "devil_fit", "devil_fit_device", "devil_fit_async", "devil_test_de", "devil_test_de_device", "devil_p_adjust",
     "devil_calculate_sf", "devil_estimate_dispersion", "devil_init_beta", "devil_beta_fit",
     "devil_estimate_mom_dispersion", "devil_fit_dispersion", "devil_compute_hessian",
     "devil_compute_clustered_meat", "devil_nb_adjoint", "devil_cluster_blocks",
@@ -105,6 +105,8 @@ def load():
         L.devil_fit.argtypes = [vp, C.POINTER(Counts), vp, i, vp, i, C.POINTER(FitOpts),
                                 C.POINTER(FitResult)]
         L.devil_fit_device.argtypes = L.devil_fit.argtypes
+        L.devil_fit_async.argtypes = [vp, vp] + list(L.devil_fit.argtypes[1:])
+        L.devil_fit_async.restype = i
         L.devil_test_de.argtypes = [vp, i64, i, vp, vp, vp, i64, vp, i, dbl, vp, vp, vp]
         L.devil_test_de_device.argtypes = L.devil_test_de.argtypes
         L.devil_p_adjust.argtypes = [vp, i64, vp, i, vp]

@@ -1548,6 +1548,17 @@ int devil_fit_device(devil_ctx* ctx, const devil_counts* counts_dev, const doubl
     });
 }
 
+int devil_fit_async(devil_ctx* ctx, void* stream, const devil_counts* counts_dev, const double* X_dev,
+                    int p, const int32_t* cluster_ends_host, int n_clusters,
+                    const devil_fit_opts* opts, devil_fit_result* r) {
+    if (!ctx) return DEVIL_ERR_ARG;
+    cudaStream_t own = ctx->stream;
+    if (stream) ctx->stream = static_cast<cudaStream_t>(stream);
+    const int rc = devil_fit_device(ctx, counts_dev, X_dev, p, cluster_ends_host, n_clusters, opts, r);
+    ctx->stream = own;
+    return rc;
+}
+
 // ------------------------------------------------------------------
 int devil_test_de_device(devil_ctx* ctx, int64_t G, int p, const double* beta_dev,
                          const double* bread_dev, const double* sandwich_dev, int64_t n_samples,

@@ -190,6 +190,18 @@ DEVIL_API int devil_fit_device(devil_ctx *ctx, const devil_counts *counts_dev, c
                      const int32_t *cluster_ends_host, int n_clusters,
                      const devil_fit_opts *opts, devil_fit_result *res_dev);
 
+/* devil_fit_device ordered on the caller's CUDA stream (cudaStream_t;
+ * NULL = the context's own stream) instead of the context's: the work
+ * starts after everything the caller queued on `stream` before the call,
+ * and the results are complete once the work queued on `stream` by the
+ * call has finished.  The host thread still waits inside the call for the
+ * active-gene counts of the IRLS and theta loops (read through mapped
+ * memory).  The context's own stream is restored before returning. */
+DEVIL_API int devil_fit_async(devil_ctx *ctx, void *stream, const devil_counts *counts_dev,
+                              const double *X_dev, int p, const int32_t *cluster_ends_host,
+                              int n_clusters, const devil_fit_opts *opts,
+                              devil_fit_result *res_dev);
+
 /* ---- DE test --------------------------------------------------------- */
 #define DEVIL_ADJ_NONE        0
 #define DEVIL_ADJ_BH          1   /* "BH" / "fdr"                          */
