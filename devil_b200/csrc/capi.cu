@@ -24,6 +24,20 @@
 using namespace devil;
 
 namespace devil {
+cudaError_t raise_dyn_smem_raw(const void* func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> cap;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = cap[{func, dev}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 // resident blocks per SM of the kernel a pass would launch, from the CUDA
 // occupancy calculator; cached per configuration (all contexts, all threads)
 int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16) {

@@ -55,6 +55,17 @@ size_t gen_smem_bytes(PassKind k, int P, int GT);
 
 cudaError_t launch_reg_pass(const PassLaunch& L);
 
+// Raise the kernel's dynamic shared-memory cap to at least `bytes` on the
+// current device; never lowers it.  The cap is process-wide per kernel, so
+// concurrent callers (devil_fit_batch workers with different problem
+// shapes) must not set it to their own size just before another caller's
+// larger launch.
+cudaError_t raise_dyn_smem_raw(const void* func, size_t bytes);
+template <class K>
+cudaError_t raise_dyn_smem(K* kern, size_t bytes) {
+    return raise_dyn_smem_raw(reinterpret_cast<const void*>(kern), bytes);
+}
+
 // resident blocks per SM of the kernel a pass launch would use (cached)
 int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16);
 

@@ -104,9 +104,7 @@ cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slo
     auto go = [&](auto* pw) -> cudaError_t {
         using TW = std::remove_const_t<std::remove_pointer_t<decltype(pw)>>;
         if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(irls_finalize_kernel<TW>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
+            cudaError_t e = raise_dyn_smem(irls_finalize_kernel<TW>, smem);
             if (e != cudaSuccess) return e;
         }
         irls_finalize_kernel<TW><<<nblk(max_slots, w), 32 * w, smem, st>>>(
@@ -332,9 +330,7 @@ cudaError_t launch_mle_finalize(const void* partW, bool wide, const double* part
     auto go = [&](auto* pw) -> cudaError_t {
         using TW = std::remove_const_t<std::remove_pointer_t<decltype(pw)>>;
         if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(mle_finalize_kernel<TW>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
+            cudaError_t e = raise_dyn_smem(mle_finalize_kernel<TW>, smem);
             if (e != cudaSuccess) return e;
         }
         mle_finalize_kernel<TW><<<nblk(max_slots, w), 32 * w, smem, st>>>(
@@ -429,8 +425,7 @@ cudaError_t launch_sandwich_finalize(const double* partW, int nseg, int slot_str
     const int w = fin_warps(per);
     const size_t smem = per * w;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(sandwich_finalize_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = raise_dyn_smem(sandwich_finalize_kernel, smem);
         if (e != cudaSuccess) return e;
     }
     sandwich_finalize_kernel<<<nblk(max_slots, w), 32 * w, smem, st>>>(

@@ -40,13 +40,13 @@ static cudaError_t run(const PassLaunch& L) {
     if (L.val_u16) {
         auto k = gen_pass_kernel<Pass, uint16_t>;
         // static shared memory (psi tables) counts against the 48 KB default
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = raise_dyn_smem(k, smem);
         if (e != cudaSuccess) return e;
         if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kGenNT, smem);
         k<<<grid, kGenNT, smem, L.stream>>>(L.geo, prm, L.P, L.GT);
     } else {
         auto k = gen_pass_kernel<Pass, float>;
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = raise_dyn_smem(k, smem);
         if (e != cudaSuccess) return e;
         if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kGenNT, smem);
         k<<<grid, kGenNT, smem, L.stream>>>(L.geo, prm, L.P, L.GT);

@@ -790,7 +790,7 @@ static cudaError_t grp_run(const GrpGeom& geo, const PassParamsAny& pa, PassKind
     auto prm = grp_params<Pass>(pa);
     auto go = [&](auto kern) -> cudaError_t {
         // static shared memory (psi tables) counts against the 48 KB default
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = raise_dyn_smem(kern, smem);
         if (e != cudaSuccess) return e;
         kern<<<(unsigned)max_slots, nt, smem, st>>>(geo, prm);
         return cudaGetLastError();

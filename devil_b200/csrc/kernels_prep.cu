@@ -456,8 +456,7 @@ cudaError_t launch_xtx_inverse(const double* Xcm, int64_t n, int P, double* part
                                int32_t* err, cudaStream_t st) {
     const int nb = xtx_blocks(n);
     const size_t sm1 = (size_t)kXtxStage * (P + 1) * sizeof(double);
-    cudaError_t e = cudaFuncSetAttribute(xtx_partial_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1);
+    cudaError_t e = raise_dyn_smem(xtx_partial_kernel, sm1);
     if (e != cudaSuccess) return e;
     xtx_partial_kernel<<<nb, 256, sm1, st>>>(Xcm, n, P, part);
     const size_t sm2 = (size_t)2 * P * P * 8 + (size_t)P * 4 + 16;

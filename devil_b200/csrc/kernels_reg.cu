@@ -65,12 +65,12 @@ static cudaError_t run(const PassLaunch& L) {
             constexpr size_t smem = 2 * TmaChunk<PP>::STAGE_FLOATS * sizeof(float);
             if (L.val_u16) {
                 auto k = tma_pass_kernel<P, PP, GT, kRegNT, Pass, uint16_t>;
-                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaError_t e = raise_dyn_smem(k, smem);
                 if (e != cudaSuccess) return e;
                 k<<<grid, kRegNT, smem, L.stream>>>(L.geo, prm);
             } else {
                 auto k = tma_pass_kernel<P, PP, GT, kRegNT, Pass, float>;
-                cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaError_t e = raise_dyn_smem(k, smem);
                 if (e != cudaSuccess) return e;
                 k<<<grid, kRegNT, smem, L.stream>>>(L.geo, prm);
             }

@@ -864,13 +864,13 @@ cudaError_t run_tc(const PassLaunch& L, const float4* zimg) {
     cudaError_t e;
     if (L.val_u16) {
         auto k = tc_irls_kernel<P, uint16_t>;
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        e = raise_dyn_smem(k, kTcSmem);
         if (e != cudaSuccess) return e;
         if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kTcNT, kTcSmem);
         k<<<grid, kTcNT, kTcSmem, L.stream>>>(L.geo, prm, zimg);
     } else {
         auto k = tc_irls_kernel<P, float>;
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        e = raise_dyn_smem(k, kTcSmem);
         if (e != cudaSuccess) return e;
         if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kTcNT, kTcSmem);
         k<<<grid, kTcNT, kTcSmem, L.stream>>>(L.geo, prm, zimg);
@@ -886,13 +886,13 @@ cudaError_t run_tc_mle(const PassLaunch& L, const float4* zimg) {
     cudaError_t e;
     if (L.val_u16) {
         auto k = tc_mle_kernel<P, uint16_t>;
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        e = raise_dyn_smem(k, kTcSmem);
         if (e != cudaSuccess) return e;
         if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kTcNT, kTcSmem);
         k<<<grid, kTcNT, kTcSmem, L.stream>>>(L.geo, prm, zimg);
     } else {
         auto k = tc_mle_kernel<P, float>;
-        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+        e = raise_dyn_smem(k, kTcSmem);
         if (e != cudaSuccess) return e;
         if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kTcNT, kTcSmem);
         k<<<grid, kTcNT, kTcSmem, L.stream>>>(L.geo, prm, zimg);

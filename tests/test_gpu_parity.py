@@ -486,3 +486,26 @@ def test_precision_tc_tf32_option(dv, orc, sparse_problem):
     check_mats(fit["beta_sandwiches_null"], ref["bread"], same & (ref["theta"] < 1e3), 1e-4, "bread")
     with pytest.raises(RuntimeError, match="tc_bf16x3"):
         gpu_fit(dv, P, "MLE", precision="tc_bf16x3")
+
+
+def test_fit_batch_concurrent_shapes(dv):
+    """Workers that fit problems of different shapes at the same time need
+    different dynamic shared memory for the same kernels (design-group pass,
+    finalizes); the per-kernel cap is process-wide, so a worker must never
+    lower it under another worker's launch.  Grouped designs of different
+    widths and group counts, many workers, several rounds."""
+    cases = [("clustered", 31, 64, 3000, True), ("wide", 32, 16, 4000, False),
+             ("clustered", 33, 48, 1500, False), ("wide", 34, 24, 2500, False),
+             ("plain_small", 35, 40, 600, False), ("plain_sparse", 36, 64, 2000, False)]
+    probs = []
+    for cfg, seed, G, n, cl in cases:
+        P = synthetic.make(cfg, seed=seed, G=G, n=n)
+        x = (P.rowptr, P.col, P.val.astype(np.float64) if P.val.dtype != np.uint16 else P.val, P.n)
+        probs.append((x, P.X, P.clusters) if cl else (x, P.X))
+    kw = dict(overdispersion="MLE", size_factors=None)
+    ref = [dv.fit_devil(pr[0], pr[1], clusters=pr[2] if len(pr) > 2 else None, **kw) for pr in probs]
+    for _ in range(3):
+        fits = dv.fit_devil_batch(probs * 2, workers=8, **kw)
+        for f, one in zip(fits, ref * 2):
+            np.testing.assert_array_equal(f["beta"], one["beta"])
+            np.testing.assert_array_equal(f["overdispersion"], one["overdispersion"])
