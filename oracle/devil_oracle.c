@@ -1,7 +1,7 @@
 /*
  * devil_oracle.c -- FP64 CPU restatement of devil's per-gene negative-binomial
  * GLM path.  TEST INFRASTRUCTURE ONLY: the parity tests, the smoke check and
- * the CPU-baseline leg of bench.py call it as the checker.  The product
+ * the CPU-baseline leg of bench.py compare against it or time it.  The product
  * (libdevil_b200.so) never links or calls anything in this directory.
  *
  * Every function names the reference file:line it restates (paths are

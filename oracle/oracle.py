@@ -1,8 +1,8 @@
 """ctypes front end of the FP64 oracle (libdevil_oracle.so).
 
 TEST INFRASTRUCTURE ONLY.  The parity tests, ``__graft_entry__.smoke()`` and
-the CPU-baseline leg of ``bench.py`` use this module as the checker; the
-product package ``devil_b200`` never imports it.
+the CPU-baseline leg of ``bench.py`` compare against this module or time it;
+the product package ``devil_b200`` never imports it.
 
 Each wrapper restates one function of devil's R/C++ path; the C source
 (devil_oracle.c) cites the reference file:line of each.

@@ -1,7 +1,7 @@
 """Golden fixtures (tests/golden/*.npz, made by tests/golden/make_golden.py).
 
 CPU: the oracle reproduces every stored vector (regression pin of the
-checker).  GPU: fit_devil / test_de through libdevil_b200.so match the
+oracle).  GPU: fit_devil / test_de through libdevil_b200.so match the
 stored vectors to the path's tolerances."""
 import glob
 import os

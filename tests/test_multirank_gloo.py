@@ -1,6 +1,6 @@
 """World-size-2 gloo test of the multi-rank host logic: genes sharded across
 ranks, p-values all-gathered, BH applied globally.  The per-gene numbers
-come from the oracle (the checker), so no GPU is needed; the result must
+come from the oracle, so no GPU is needed; the result must
 equal the single-process BH of the whole gene set exactly."""
 import os
 import socket
