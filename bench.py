@@ -77,8 +77,29 @@ def oracle_step(orc, rowptr, col, val, n, X, off, c):
     th0 = orc.estimate_dispersion(Y, off)
     b0 = orc.init_beta(Y, X, off)
     r = orc.cpu_fit(Y, X, off, th0, b0, orc.OD_MLE, 200, 1e-3, theta_mom=True)
-    orc.test_de(r["beta"], r["bread"], None, n, c)
+    r["pval"] = orc.test_de(r["beta"], r["bread"], None, n, c)[0]
     return r
+
+
+def parity_summary(beta, iters, theta, ref, beta_tol=1e-5):
+    """Agreement of the GPU fit with the FP64 oracle on the same genes, with
+    the bars of the parity tests: iteration counts, |d beta| (absolute for
+    |beta| <= 1, relative above) and relative d theta on genes that converge
+    in both with the same count (theta resolvable: 1e-3 < theta < 1e3)."""
+    beta, ref_beta = np.asarray(beta, float), np.asarray(ref["beta"], float)
+    iters, ref_it = np.asarray(iters), np.asarray(ref["iters"])
+    same = iters == ref_it
+    conv = same & (ref_it < 200)
+    db = np.abs(beta - ref_beta) / np.maximum(1.0, np.abs(ref_beta))
+    th, ref_th = np.asarray(theta, float), np.asarray(ref["theta"], float)
+    tm = conv & (ref_th > 1e-3) & (ref_th < 1e3)
+    dth = np.abs(th - ref_th) / np.maximum(np.abs(ref_th), 1e-300)
+    max_db = float(np.nanmax(db[conv])) if conv.any() else None
+    return {"genes": int(len(iters)), "iters_agree": round(float(same.mean()), 4),
+            "converged_compared": int(conv.sum()), "max_dbeta": max_db,
+            "max_rel_dtheta": float(np.nanmax(dth[tm])) if tm.any() else None,
+            "bar_dbeta": beta_tol,
+            "within_bar": bool(max_db is not None and max_db <= beta_tol)}
 
 
 def timed_oracle(orc, prob_rows, n, X, off, c, target_s):
@@ -93,9 +114,9 @@ def timed_oracle(orc, prob_rows, n, X, off, c, target_s):
     k2 = int(max(8, min(2048, target_s / max(per_gene, 1e-6))))
     rp, cl, vl = prob_rows(k2)
     t0 = time.perf_counter()
-    oracle_step(orc, rp, cl, vl, n, X, off, c)
+    r = oracle_step(orc, rp, cl, vl, n, X, off, c)
     dt = time.perf_counter() - t0
-    return k2, dt
+    return k2, dt, r
 
 
 def run_reference(args):
@@ -449,6 +470,7 @@ def main():
 
     # ---- CPU baseline: the oracle on a sample of this workload ----
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as orc
@@ -469,10 +491,19 @@ def main():
             sel = np.concatenate([np.arange(s, e) for s, e in zip(starts, ends_)])
             return rp, h_col_np[sel], h_val_np[sel]
 
-        k, dt = timed_oracle(orc, rows, n, data["X"], off_np, contrast, args.cpu_seconds)
+        k, dt, ref = timed_oracle(orc, rows, n, data["X"], off_np, contrast, args.cpu_seconds)
         cpu = {"value": k / dt, "unit": "genes/s", "cores": orc.num_threads(), "kind": "port",
                "sample": f"{k} randomly chosen genes of this workload (full n={n}), the FP64 "
                          f"restatement of cpu_fit + test_de with OpenMP over genes; genes/s"}
+        # the same genes of the timed GPU fit against the oracle's results
+        try:
+            idx = order[:k]
+            parity = parity_summary(out["beta"].view(G, p).cpu().numpy()[idx],
+                                    out["iters"].cpu().numpy()[idx],
+                                    out["theta"].cpu().numpy()[idx], ref)
+            parity["reference"] = "FP64 oracle on the CPU-baseline sample (same genes, offsets)"
+        except Exception as ex:  # the measurement stands without it
+            parity = {"error": f"{type(ex).__name__}: {ex}"}
 
     line = {
         "metric": METRIC, "value": value, "unit": "genes/s", "n_gpus": world,
@@ -489,7 +520,7 @@ def main():
                        saturated_counts=int(data.get("saturated", 0)),
                        converged_frac=float((out["status"] == 0).float().mean().item()),
                        mean_irls_iters=float(out["iters"].float().mean().item())),
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+        "roofline": roof, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "clocks": clk,
         "gpu_launches": int(launches),
     }
     if rank == 0:
