@@ -40,10 +40,11 @@ cudaError_t raise_dyn_smem_raw(const void* func, size_t bytes) {
 
 // resident blocks per SM of the kernel a pass would launch, from the CUDA
 // occupancy calculator; cached per configuration (all contexts, all threads)
-int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16) {
+int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16, int plain) {
     static std::mutex mu;
     static std::map<int64_t, int> cache;
-    const int64_t key = ((((int64_t)kind * 8 + engine) * 64 + P) * 512 + GT) * 2 + (val_u16 ? 1 : 0);
+    const int64_t key =
+        (((((int64_t)kind * 8 + engine) * 64 + P) * 512 + GT) * 2 + (val_u16 ? 1 : 0)) * 2 + (plain ? 1 : 0);
     {
         std::lock_guard<std::mutex> lk(mu);
         auto it = cache.find(key);
@@ -58,6 +59,7 @@ int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16)
     L.val_u16 = val_u16;
     L.nseg = 1;
     L.ntiles = 1;
+    L.plain = plain;
     int occ = 0;
     L.occ_out = &occ;
     cudaError_t e = cudaErrorInvalidValue;
@@ -695,11 +697,14 @@ struct PassPlan {
     Engine engine;
     int GT;
     PassKind kind = PASS_IRLS;
+    int plain = 0;  // the plain comparison form
 };
 
 PassPlan plan_engine(PassKind k, const DevProblem& dp, int form) {
     const int P = dp.P;
-    if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, 1};
+    // the plain comparison form: every pass on the per-cell shared-memory
+    // engine, FP32 per-cell arithmetic for the FP32 passes (IRLS, MLE)
+    if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, gen_default_gt(k, P), k, 1};
     if (dp.grp.active) return {ENGINE_GRP, 1};
     const bool tc = tc_enabled(k) ||
                     (dp.precision == DEVIL_PREC_TC_TF32 && (k == PASS_IRLS || k == PASS_MLE));
@@ -738,8 +743,9 @@ PassPlan plan_for(PassKind k, const DevProblem& dp, int form) {
 // full: with 1.1 waves the second wave would keep 90 % of the SMs idle
 // (active-gene counts in the IRLS tail produce exactly such grids).
 int choose_nseg(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, int tiles, int form) {
-    if (form == DEVIL_FORM_PLAIN || plan.engine == ENGINE_GRP) return 1;
-    const int occ = pass_blocks_per_sm(plan.kind, plan.engine, dp.P, plan.GT, dp.val_u16);
+    (void)form;
+    if (plan.engine == ENGINE_GRP) return 1;
+    const int occ = pass_blocks_per_sm(plan.kind, plan.engine, dp.P, plan.GT, dp.val_u16, plan.plain);
     const int64_t cap = (int64_t)ctx->sm_count * std::max(1, occ);
     const int64_t min_waves = plan.engine == ENGINE_TC ? 4 : 1;
     int want = (int)((min_waves * cap + tiles - 1) / tiles);
@@ -819,6 +825,7 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
     L.geo.slot_stride = tiles * plan.GT;
     L.prm = prm;
     L.stream = ctx->stream;
+    L.plain = plan.plain;
     size_t e0 = ctx->profiling ? prof_event(ctx) : 0;
     ctx->last_engine[kind] = (int)plan.engine;
     if (plan.engine == ENGINE_GRP) {
@@ -910,13 +917,9 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
     int64_t launched = 0;
     for (int t = 0; t < max_iter; ++t) {
         const int cur = t & 1, nxt = cur ^ 1;
-        int64_t hint;
-        if (form == DEVIL_FORM_PLAIN) {
-            CK(cudaStreamSynchronize(st));
-            hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
-        } else {
-            hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
-        }
+        // active-gene count of LAG iterations ago (an upper bound: blocks
+        // beyond the current count exit at once)
+        const int64_t hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
@@ -994,9 +997,7 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     // one far-left evaluation plus at most max_iter Newton evaluations
     for (int t = 0; t <= max_iter; ++t) {
         const int cur = t & 1, nxt = cur ^ 1;
-        int64_t hint;
-        if (form == DEVIL_FORM_PLAIN) CK(cudaStreamSynchronize(st));
-        hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
+        const int64_t hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
@@ -1082,7 +1083,7 @@ void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, con
     // cluster-aligned segments: every cluster block split into pieces of
     // at most L cells (1-based exclusive ends, R/main.R:193)
     const int64_t n = dp.n;
-    int want = (form == DEVIL_FORM_PLAIN) ? 1 : (ctx->sm_count * 2 + tiles - 1) / tiles;
+    int want = (ctx->sm_count * 2 + tiles - 1) / tiles;
     int64_t L = std::max<int64_t>(1024, (n + want - 1) / std::max(1, want));
     std::vector<int32_t> hb{0};
     std::vector<int32_t> hc;

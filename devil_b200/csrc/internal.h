@@ -43,6 +43,7 @@ struct PassLaunch {
     PassParamsAny prm;
     cudaStream_t stream;
     int* occ_out = nullptr;  // non-null: report the kernel's resident blocks per SM, launch nothing
+    int plain = 0;           // the plain comparison form (FP32 staging in the shared-memory engine)
 };
 
 // engine choice helpers
@@ -51,7 +52,8 @@ int tma_chunk_cells(int xs);  // fine-segment size the TMA engine expects
 int reg_default_gt(PassKind k, int P);
 bool reg_gt_supported(PassKind k, int P, int GT);
 int gen_default_gt(PassKind k, int P);
-size_t gen_smem_bytes(PassKind k, int P, int GT);
+size_t gen_smem_bytes(PassKind k, int P, int GT, int plain);
+bool gen_f32_staging(PassKind k, int plain);
 
 cudaError_t launch_reg_pass(const PassLaunch& L);
 
@@ -67,7 +69,7 @@ cudaError_t raise_dyn_smem(K* kern, size_t bytes) {
 }
 
 // resident blocks per SM of the kernel a pass launch would use (cached)
-int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16);
+int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16, int plain = 0);
 
 // ---- tensor-core IRLS engine (kernels_tc.cu) ----
 int tc_max_p();

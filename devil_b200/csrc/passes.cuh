@@ -712,9 +712,15 @@ __host__ __device__ __forceinline__ size_t gen_wt_offset(int NS, int GT) {
     return (b + 15) & ~(size_t)15;
 }
 
-template <class Pass, class VT>
+// F32W: the plain comparison form -- per-(gene, cell) weights computed in
+// FP32 from the FP32 design, offsets and beta (exp2 / reciprocal on the
+// special function units), staged and contracted in FP32 with FP32 sums per
+// chunk of cells.  Only for passes whose per-cell arithmetic is FP32
+// (Pass::F64 false); the FP64 passes (MOM, bread/meat) are FP64 in every form.
+template <class Pass, class VT, bool F32W = false>
 __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename Pass::Params prm,
                                                           int P, int GT) {
+    static_assert(!(F32W && Pass::F64), "FP32 staging only for FP32 passes");
     constexpr int NWV = Pass::NW + Pass::NV + Pass::NF;
     constexpr int NS = Pass::NS;
     using AS = typename Pass::AS;
@@ -736,11 +742,11 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
     int64_t* cend = cursor + GT;                                    // [GT]
     int* cnt = reinterpret_cast<int*>(cend + GT);                   // [GT]
     int* gids = cnt + GT;                                           // [GT]
-    // design rows and per-cell weights are staged in double for every pass:
-    // the FP32 form of this engine left errors of ~1.5e-5 in beta for slowly
-    // converging genes at p = 12, and FP64 FMAs run at half the FP32 rate on
-    // this part while the engine is bound by shared-memory traffic anyway
-    using WT = double;
+    // design rows and per-cell weights are staged in double in the chosen
+    // form: FP32 staging left errors of ~1.5e-5 in beta for slowly converging
+    // genes at p = 12, and FP64 FMAs run at half the FP32 rate on this part
+    // while the engine is bound by shared-memory traffic anyway
+    using WT = typename std::conditional<F32W, float, double>::type;
     WT* xsm = reinterpret_cast<WT*>(smem_raw + gen_wt_offset(NS, GT));  // [TC][XS]
     WT* wts = xsm + TC * XS;                                        // [NWV][GT][TC]
     float* ys = reinterpret_cast<float*>(wts + NWV * kGenNT);       // [GT][TC]
@@ -762,7 +768,7 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
     __syncthreads();
     for (int i = t; i < GT * P; i += kGenNT) {
         int j = i / P, k = i - j * P;
-        betas[i] = __ldg(prm.beta + (int64_t)gids[j] * P + k);
+        betas[i] = __ldg(prm.beta + (int64_t)gids[j] * P + k) * (F32W ? kLog2e : 1.f);
     }
     const int gA = t / TC, cA = t - gA * TC;
     typename Pass::Gene gpar = Pass::load(prm, gids[gA]);
@@ -820,8 +826,8 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
         // stage X rows (+ the constant 1 column) and offsets; clear the tile
         for (int i = t; i < nc * P; i += kGenNT) {
             int c = i / P, k = i - c * P;
-            if constexpr (Pass::F64)
-                xsm[c * XS + k] = __ldg(geo.Xd + (int64_t)(cb + c) * geo.xs + k);
+            if constexpr (Pass::F64 || !F32W)
+                xsm[c * XS + k] = (WT)__ldg(geo.Xd + (int64_t)(cb + c) * geo.xs + k);
             else
                 xsm[c * XS + k] = __ldg(geo.X + (int64_t)(cb + c) * geo.xs + k);
         }
@@ -844,19 +850,30 @@ __global__ void __launch_bounds__(kGenNT) gen_pass_kernel(PassGeom geo, typename
         if (cA == 0) cursor[gA] += cnt[gA];
         // per-(gene, cell) weights
         {
-            // per-(gene, cell) weights in FP64 for every pass: this engine's
+            // per-(gene, cell) weights: FP64 in the chosen form (this engine's
             // cost is the outer-product phase, and FP64 here keeps the
-            // per-step error of slowly converging genes small
-            RecAcc<NWV, NS, AS, double> rec;
+            // per-step error of slowly converging genes small), FP32 in the
+            // plain form
+            RecAcc<NWV, NS, AS, WT> rec;
             rec.zero();
             if (cA < nc) {
                 const int64_t c = cb + cA;
-                double e = __ldg(geo.offd + c);
-                for (int i = 0; i < P; ++i) e = fma(__ldg(geo.Xd + c * geo.xs + i), __ldg(bd + i), e);
-                double mu = exp(e);
-                float y = ys[gA * TC + cA];
-                Pass::template dense<double>(gpar, mu, rec);
-                if (y != 0.f) Pass::template sparse<double>(gpar, mu, y, rec);
+                const float y = ys[gA * TC + cA];
+                if constexpr (F32W) {
+                    // eta in log2 units: x . (log2(e) beta) + log2(e) off
+                    const float* bf = betas + gA * P;
+                    float e = __ldg(geo.off + c) * kLog2e;
+                    for (int i = 0; i < P; ++i) e = fmaf(xsm[cA * XS + i], bf[i], e);
+                    const float mu = ex2_approx(e);
+                    Pass::template dense<float>(gpar, mu, rec);
+                    if (y != 0.f) Pass::template sparse<float>(gpar, mu, y, rec);
+                } else {
+                    double e = __ldg(geo.offd + c);
+                    for (int i = 0; i < P; ++i) e = fma(__ldg(geo.Xd + c * geo.xs + i), __ldg(bd + i), e);
+                    double mu = exp(e);
+                    Pass::template dense<double>(gpar, mu, rec);
+                    if (y != 0.f) Pass::template sparse<double>(gpar, mu, y, rec);
+                }
             }
 #pragma unroll
             for (int w = 0; w < NWV; ++w) wts[(w * GT + gA) * TC + cA] = (WT)rec.w[w];

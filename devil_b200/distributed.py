@@ -63,3 +63,34 @@ def global_adjust(local_p, method="BH", group=None, adjust=None):
     adj = adjust(full, method)
     assert len(full) == int(sizes.sum()) and world == len(sizes)
     return adj[start:start + len(local_p)]
+
+
+def global_adjust_tensor(local, method, adjust, group=None, sizes=None):
+    """p.adjust over every rank's p-values, kept in torch tensors on the
+    device of ``local`` (with NCCL: the GPU, so the gathered vector never
+    crosses to the host).
+
+    ``local`` is this rank's 1-D float64 tensor of p-values (ranks may hold
+    different numbers of genes); ``adjust(full, method)`` returns the
+    adjustment of the gathered vector in rank order (NaN = NA, not counted);
+    ``sizes`` (the per-rank lengths, when already known) saves the exchange
+    of the lengths.  Returns this rank's slice of the adjusted vector."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    if sizes is None:
+        n = torch.tensor([local.numel()], dtype=torch.int64, device=local.device)
+        parts = [torch.zeros_like(n) for _ in range(world)]
+        dist.all_gather(parts, n, group=group)
+        sizes = [int(s.item()) for s in parts]
+    mx = max(sizes)
+    pad = torch.full((mx,), float("nan"), dtype=torch.float64, device=local.device)
+    pad[: local.numel()] = local
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    full = torch.cat([parts[r][: sizes[r]] for r in range(world)])
+    adj = adjust(full, method)
+    start = int(sum(sizes[:rank]))
+    return adj[start:start + local.numel()]

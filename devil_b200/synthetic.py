@@ -15,7 +15,13 @@ shapes, sparsity and value distributions of the benchmark workloads:
   round(Dirichlet(1) * n), patient offsets N(0, 0.3) added to eta, p=12
   (intercept, condition, 10 cell-type indicators for 11 types).
 * ``wide``         -- G=20,000 x n=1,000,000, p=32 (intercept, condition,
-  30 indicators for 31 cell types), gene means LogNormal(-1, 2).
+  30 indicators for 31 cell types), gene means LogNormal(-3.8, 2): about 8%
+  nonzeros (1.6e9 entries at full size).  The location of the gene means is
+  set by that density; with LogNormal(-1, 2) the same model gives about 34%
+  nonzeros (``mean_loc=-1.0`` reproduces it).
+* ``binary``       -- G=20,000 x n=1,000,000, p=2 (intercept + binary
+  condition, 50/50), the model of ``plain_small`` with beta0 ~ N(-3, 1.5):
+  about 10% nonzeros, CSR uint16.
 
 Counts are NB with Var = mu + theta * mu^2 (theta is the dispersion devil
 returns), drawn as a Gamma-Poisson mixture: lambda ~ Gamma(shape=1/theta,
@@ -41,8 +47,10 @@ CONFIGS = {
                          patients=1, dense=False),
     "clustered": dict(G=20000, n=500000, p=12, b0_loc=-3.0, b0_sd=1.5, covariates=0, types=11,
                       patients=40, dense=False),
-    "wide": dict(G=20000, n=1000000, p=32, b0_loc=None, b0_sd=None, covariates=0, types=31,
-                 patients=1, dense=False),
+    "wide": dict(G=20000, n=1000000, p=32, b0_loc=None, b0_sd=None, mean_loc=-3.8, covariates=0,
+                 types=31, patients=1, dense=False),
+    "binary": dict(G=20000, n=1000000, p=2, b0_loc=-3.0, b0_sd=1.5, covariates=0, types=0,
+                   patients=1, dense=False),
 }
 
 
@@ -112,9 +120,12 @@ def patient_sizes(n: int, k: int, rng: np.random.Generator):
 
 
 def make(config: str = "plain_small", seed: int = 0, G: int | None = None, n: int | None = None,
-         chunk_cells: int = 1 << 24) -> Problem:
-    """Draw one problem with numpy (PCG64).  G / n override the config sizes."""
+         chunk_cells: int = 1 << 24, mean_loc: float | None = None) -> Problem:
+    """Draw one problem with numpy (PCG64).  G / n override the config sizes;
+    mean_loc the location of the gene means (configs that draw them)."""
     cfg = dict(CONFIGS[config])
+    if mean_loc is not None:
+        cfg["mean_loc"] = float(mean_loc)
     G = cfg["G"] if G is None else int(G)
     n = cfg["n"] if n is None else int(n)
     p = cfg["p"]
@@ -124,7 +135,7 @@ def make(config: str = "plain_small", seed: int = 0, G: int | None = None, n: in
     theta = rng.lognormal(0.0, 1.0, G)
     beta = np.zeros((G, p))
     if cfg["b0_loc"] is None:
-        beta[:, 0] = np.log(rng.lognormal(-1.0, 2.0, G))
+        beta[:, 0] = np.log(rng.lognormal(cfg["mean_loc"], 2.0, G))
     else:
         beta[:, 0] = rng.normal(cfg["b0_loc"], cfg["b0_sd"], G)
     de = rng.random(G) < 0.1
@@ -168,7 +179,8 @@ def make(config: str = "plain_small", seed: int = 0, G: int | None = None, n: in
 
 
 def make_torch(config: str = "plain_sparse", seed: int = 0, G: int | None = None,
-               n: int | None = None, device="cuda", chunk_cells: int = 1 << 27):
+               n: int | None = None, device="cuda", chunk_cells: int = 1 << 27,
+               mean_loc: float | None = None):
     """Draw the same model on a torch device (full-size benchmark inputs).
 
     Returns a dict of device tensors: rowptr (int64), col (int32), val
@@ -177,6 +189,8 @@ def make_torch(config: str = "plain_sparse", seed: int = 0, G: int | None = None
     import torch
 
     cfg = dict(CONFIGS[config])
+    if mean_loc is not None:
+        cfg["mean_loc"] = float(mean_loc)
     G = cfg["G"] if G is None else int(G)
     n = cfg["n"] if n is None else int(n)
     p = cfg["p"]
@@ -186,7 +200,7 @@ def make_torch(config: str = "plain_sparse", seed: int = 0, G: int | None = None
     theta = rng.lognormal(0.0, 1.0, G)
     beta = np.zeros((G, p))
     if cfg["b0_loc"] is None:
-        beta[:, 0] = np.log(rng.lognormal(-1.0, 2.0, G))
+        beta[:, 0] = np.log(rng.lognormal(cfg["mean_loc"], 2.0, G))
     else:
         beta[:, 0] = rng.normal(cfg["b0_loc"], cfg["b0_sd"], G)
     de = rng.random(G) < 0.1

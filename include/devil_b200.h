@@ -85,7 +85,11 @@ typedef struct devil_counts {
 #define DEVIL_OD_NEW         3   /* "new" / "I": fit_overdispersion_cppp   */
 
 #define DEVIL_FORM_CHOSEN    0   /* tiled, compacted, grouped kernels       */
-#define DEVIL_FORM_PLAIN     1   /* straightforward FP32 SIMT comparison    */
+#define DEVIL_FORM_PLAIN     1   /* comparison form: every pass per cell on */
+                                 /* the shared-memory SIMT engine, FP32     */
+                                 /* per-cell arithmetic and chunk sums for  */
+                                 /* IRLS and MLE (MOM, bread/meat FP64 as   */
+                                 /* in every form), no design grouping      */
 
 /* arithmetic of the per-cell Hessian contractions (IRLS and MLE passes) */
 #define DEVIL_PREC_FP32      0   /* FP32 FMAs on the CUDA cores (default)   */

@@ -253,6 +253,93 @@ static void linear_predictor(int64_t n, int p, const double *X, const double *be
     }
 }
 
+/* Sums over the cells of one gene.  The cells are taken in blocks of
+ * ORC_BLK whose design rows are copied into a row-major buffer; a callback
+ * fills, per cell of the block, nw "outer" weights, nv "vector" weights and
+ * ns scalars, and the helper adds
+ *     out[k]          += sum_c w_k(c) x_c x_c^T     (k < nw, p x p)
+ *     out[nw p^2 + k] += sum_c v_k(c) x_c           (k < nv, p)
+ *     out[... + k]    += sum_c s_k(c)                (k < ns)
+ * with the p x p sums over the upper triangle of contiguous rows (a loop
+ * the compiler vectorises) and mirrored at the end.  When the caller is not
+ * already inside a parallel region and n is large, the blocks are split
+ * into one contiguous range per thread and the per-thread partial sums are
+ * added in thread order, so the result does not depend on scheduling.  The
+ * arithmetic of every term is the reference's; only the order of the
+ * floating-point additions differs from a plain loop over the cells. */
+#define ORC_BLK 128
+typedef void (*orc_cellfn)(void *ctx, int64_t c0, int nc, int p, const double *xr, double *w);
+
+static void orc_cell_sums(int64_t n, int p, const double *X, int nw, int nv, int ns,
+                          orc_cellfn fn, void *ctx, double *out)
+{
+    const int nq = nw + nv + ns;
+    const size_t per = (size_t)nw * p * p + (size_t)nv * p + (size_t)ns;
+    int nt = 1;
+#ifdef _OPENMP
+    const int par = !omp_in_parallel() && n >= 32768;
+    if (par) nt = omp_get_max_threads();
+#else
+    const int par = 0;
+#endif
+    double *part = (double *)calloc((size_t)nt * (per > 0 ? per : 1), sizeof(double));
+    #pragma omp parallel num_threads(nt) if (par)
+    {
+        int t = 0, T = 1;
+#ifdef _OPENMP
+        t = omp_get_thread_num();
+        T = omp_get_num_threads();
+#endif
+        double *xr = (double *)malloc(sizeof(double) * ORC_BLK * p);
+        double *w = (double *)malloc(sizeof(double) * ORC_BLK * (nq > 0 ? nq : 1));
+        double *acc = part + (size_t)t * per;
+        const int64_t nb = (n + ORC_BLK - 1) / ORC_BLK;
+        const int64_t b0 = nb * t / T, b1 = nb * (t + 1) / T;
+        for (int64_t blk = b0; blk < b1; blk++) {
+            const int64_t c0 = blk * ORC_BLK;
+            const int nc = (int)(n - c0 < ORC_BLK ? n - c0 : ORC_BLK);
+            for (int j = 0; j < p; j++) {
+                const double *xc = X + (int64_t)j * n + c0;
+                for (int c = 0; c < nc; c++) xr[c * p + j] = xc[c];
+            }
+            fn(ctx, c0, nc, p, xr, w);
+            for (int k = 0; k < nw; k++) {
+                double *H = acc + (size_t)k * p * p;
+                const double *wk = w + k * ORC_BLK;
+                for (int c = 0; c < nc; c++) {
+                    const double *x = xr + c * p;
+                    for (int a = 0; a < p; a++) {
+                        const double sa = wk[c] * x[a];
+                        double *Ha = H + a * p;
+                        for (int b = a; b < p; b++) Ha[b] += sa * x[b];
+                    }
+                }
+            }
+            for (int k = 0; k < nv; k++) {
+                double *v = acc + (size_t)nw * p * p + (size_t)k * p;
+                const double *wk = w + (nw + k) * ORC_BLK;
+                for (int c = 0; c < nc; c++)
+                    for (int a = 0; a < p; a++) v[a] += wk[c] * xr[c * p + a];
+            }
+            for (int k = 0; k < ns; k++) {
+                double *sv = acc + (size_t)nw * p * p + (size_t)nv * p + k;
+                const double *wk = w + (nw + nv + k) * ORC_BLK;
+                for (int c = 0; c < nc; c++) *sv += wk[c];
+            }
+        }
+        free(xr); free(w);
+    }
+    if (per) memset(out, 0, sizeof(double) * per);
+    for (int t = 0; t < nt; t++)
+        for (size_t i = 0; i < per; i++) out[i] += part[(size_t)t * per + i];
+    for (int k = 0; k < nw; k++) {  /* upper triangle (row a, col b >= a) -> symmetric */
+        double *H = out + (size_t)k * p * p;
+        for (int a = 0; a < p; a++)
+            for (int b = a + 1; b < p; b++) H[b * p + a] = H[a * p + b];
+    }
+    free(part);
+}
+
 /* ------------------------------------------------------------------ */
 /* size factors and offset  (R/size_factors.R)                         */
 /* ------------------------------------------------------------------ */
@@ -428,32 +515,38 @@ void orc_init_beta_rough(int64_t G, int64_t n, int p, const int64_t *rowptr, con
 /* k_in is the float the reference receives (theta_0 rounded to float);
  * eps is the float tolerance.  beta holds beta_0 on entry, the fit on exit.
  * Returns the iteration count. */
+/* per cell of one IRLS iteration: outer weight mu_g w_q, score weight
+ * mu_g w_q - 1 */
+typedef struct { const double *beta, *off, *y; double k; } irls_cells;
+static void irls_cellfn(void *vc, int64_t c0, int nc, int p, const double *xr, double *w)
+{
+    const irls_cells *q = (const irls_cells *)vc;
+    for (int c = 0; c < nc; c++) {
+        double eta = 0.0;
+        for (int j = 0; j < p; j++) eta += xr[c * p + j] * q->beta[j];
+        const double w_q = exp(-eta - q->off[c0 + c]);
+        const double mu_g = (q->k + q->y[c0 + c]) / (1.0 + q->k * w_q);
+        const double mw = mu_g * w_q;
+        w[c] = mw;
+        w[ORC_BLK + c] = mw - 1.0;
+    }
+}
+
 int orc_beta_fit(int64_t n, int p, const double *y, const double *X, double *beta,
                  const double *offv, float k_in, int max_iter, float eps)
 {
     float k = (float)(1.0 / (double)k_in);       /* k = 1.0 / k; stored in a float */
     double kd = (double)k;
     double epsd = (double)eps;
-    double *H = (double *)calloc((size_t)p * p, sizeof(double));
+    double *sums = (double *)calloc((size_t)p * p + p, sizeof(double));
+    double *H = sums, *sc = sums + (size_t)p * p;
     double *Z = (double *)calloc((size_t)p * p, sizeof(double));
-    double *sc = (double *)calloc(p, sizeof(double));
     double *delta = (double *)calloc(p, sizeof(double));
+    irls_cells q = { beta, offv, y, kd };
     int converged = 0, iter = 0;
     while (!converged && iter < max_iter) {
-        memset(H, 0, sizeof(double) * p * p);
-        memset(sc, 0, sizeof(double) * p);
-        for (int64_t c = 0; c < n; c++) {
-            double eta = 0.0;
-            for (int j = 0; j < p; j++) eta += X[(int64_t)j * n + c] * beta[j];
-            double w_q = exp(-eta - offv[c]);
-            double mu_g = (kd + y[c]) / (1.0 + kd * w_q);
-            double mw = mu_g * w_q;
-            for (int a = 0; a < p; a++) {
-                double xa = X[(int64_t)a * n + c];
-                sc[a] += xa * (mw - 1.0);
-                for (int b = 0; b < p; b++) H[b * p + a] += xa * mw * X[(int64_t)b * n + c];
-            }
-        }
+        /* H = X' diag(mu_g w_q) X, sc = X' (mu_g w_q - 1) */
+        orc_cell_sums(n, p, X, 1, 1, 0, irls_cellfn, &q, sums);
         for (int i = 0; i < p * p; i++) H[i] *= kd;
         lu_inverse(p, H, Z);
         for (int a = 0; a < p; a++) {
@@ -467,26 +560,35 @@ int orc_beta_fit(int64_t n, int p, const double *y, const double *X, double *bet
         iter++;
         if (delta[0] != delta[0]) converged = 1;
     }
-    free(H); free(Z); free(sc); free(delta);
+    free(sums); free(Z); free(delta);
     return iter;
 }
 
 /* ------------------------------------------------------------------ */
 /* MOM theta  (src/mom_overdispersion.cpp:24-53)                       */
 /* ------------------------------------------------------------------ */
+typedef struct { const double *beta, *sf, *y; } mom_cells;
+static void mom_cellfn(void *vc, int64_t c0, int nc, int p, const double *xr, double *w)
+{
+    const mom_cells *q = (const mom_cells *)vc;
+    for (int c = 0; c < nc; c++) {
+        double eta = 0.0;
+        for (int j = 0; j < p; j++) eta += xr[c * p + j] * q->beta[j];
+        const double mu = q->sf[c0 + c] * exp(eta);
+        const double diff = q->y[c0 + c] - mu;
+        w[c] = diff * diff - mu;
+        w[ORC_BLK + c] = mu * mu;
+    }
+}
+
 double orc_mom_dispersion(int64_t n, int p, const double *y, const double *X, const double *beta,
                           const double *sf)
 {
     double corr = (double)n / (double)(n - p);
-    double num = 0.0, den = 0.0;
-    for (int64_t c = 0; c < n; c++) {
-        double eta = 0.0;
-        for (int j = 0; j < p; j++) eta += X[(int64_t)j * n + c] * beta[j];
-        double mu = sf[c] * exp(eta);
-        double diff = y[c] - mu;
-        num += diff * diff - mu;
-        den += mu * mu;
-    }
+    mom_cells q = { beta, sf, y };
+    double nd[2];
+    orc_cell_sums(n, p, X, 0, 0, 2, mom_cellfn, &q, nd);
+    const double num = nd[0], den = nd[1];
     double th = 0.0;
     if (den > 0.0) { th = corr * num / den; if (th < 0.0) th = 0.0; }
     return th;
@@ -504,26 +606,32 @@ typedef struct {
 } nbdata;
 
 /* b = X^T diag(w) X and friends for the Cox-Reid terms */
+typedef struct { const double *mu; double theta; int nw; } cr_cells;
+static void cr_cellfn(void *vc, int64_t c0, int nc, int p, const double *xr, double *w)
+{
+    const cr_cells *q = (const cr_cells *)vc;
+    (void)p; (void)xr;
+    for (int c = 0; c < nc; c++) {
+        const double ww = 1.0 / (1.0 / q->mu[c0 + c] + q->theta);
+        const double dw = -ww * ww;
+        w[c] = ww;
+        if (q->nw > 1) w[ORC_BLK + c] = dw;
+        if (q->nw > 2) w[2 * ORC_BLK + c] = -2.0 * dw * ww;
+    }
+}
+
 static void cr_mats(const nbdata *d, double theta, double *b, double *db, double *d2b)
 {
-    int p = d->p; int64_t n = d->n;
-    memset(b, 0, sizeof(double) * p * p);
-    if (db) memset(db, 0, sizeof(double) * p * p);
-    if (d2b) memset(d2b, 0, sizeof(double) * p * p);
-    for (int64_t c = 0; c < n; c++) {
-        double w = 1.0 / (1.0 / d->mu[c] + theta);
-        double dw = -w * w;
-        double d2w = -2.0 * dw * w;
-        for (int a = 0; a < p; a++) {
-            double xa = d->X[(int64_t)a * n + c];
-            for (int bb = 0; bb < p; bb++) {
-                double xx = xa * d->X[(int64_t)bb * n + c];
-                b[bb * p + a] += xx * w;
-                if (db) db[bb * p + a] += xx * dw;
-                if (d2b) d2b[bb * p + a] += xx * d2w;
-            }
-        }
-    }
+    const int p = d->p;
+    const int nw = d2b ? 3 : (db ? 2 : 1);
+    const size_t pp = (size_t)p * p;
+    double *m = (double *)malloc(sizeof(double) * nw * pp);
+    cr_cells q = { d->mu, theta, nw };
+    orc_cell_sums(d->n, p, d->X, nw, 0, 0, cr_cellfn, &q, m);
+    memcpy(b, m, sizeof(double) * pp);
+    if (db) memcpy(db, m + pp, sizeof(double) * pp);
+    if (d2b) memcpy(d2b, m + 2 * pp, sizeof(double) * pp);
+    free(m);
 }
 
 /* inv_sympd(b + 1e-6 I) -- symmetric positive definite inverse */
@@ -580,6 +688,31 @@ static void digamma_sums(const nbdata *d, double a, double *dig, double *trig)
     *dig = sd; if (trig) *trig = st;
 }
 
+/* per-cell terms of the score's ll_part (src/overdispersion.cpp:159-175),
+ * including the reference's branches on mu*theta */
+typedef struct { const double *mu, *y; double theta, a; } score_cells;
+static void score_cellfn(void *vc, int64_t c0, int nc, int p, const double *xr, double *w)
+{
+    const score_cells *q = (const score_cells *)vc;
+    (void)p; (void)xr;
+    for (int c = 0; c < nc; c++) {
+        const double mu = q->mu[c0 + c], y = q->y[c0 + c];
+        const double mt = mu * q->theta;
+        double ll;
+        if (mt < 1e-10) {
+            ll = mt * mt * (1.0 / (1.0 + mt) - 0.5);
+        } else if (mt < 1e-4) {
+            double inv = 1.0 / (1.0 + mt);
+            double ub = mt * mt * inv, lb = mt * mt * (inv - 0.5);
+            double sug = log1p(mt) - mu / (mu + q->a);
+            ll = fmax(fmin(sug, ub), lb);
+        } else {
+            ll = log1p(mt) - mu / (mu + q->a);
+        }
+        w[c] = ll + y / (mu + q->a);
+    }
+}
+
 /* conventional_score_function_fast (src/overdispersion.cpp:95-178) */
 double orc_nb_score(const nbdata *d, double log_theta, int cr)
 {
@@ -613,24 +746,24 @@ double orc_nb_score(const nbdata *d, double log_theta, int cr)
         dig = sd * a;
         if (dig > sum_y - corr) dig = sum_y - corr;
     }
-    double ll = 0.0;
-    for (int64_t c = 0; c < n; c++) {
-        double mu = d->mu[c], y = d->y[c];
-        double mt = mu * theta;
-        if (mt < 1e-10) {
-            ll += mt * mt * (1.0 / (1.0 + mt) - 0.5);
-        } else if (mt < 1e-4) {
-            double inv = 1.0 / (1.0 + mt);
-            double ub = mt * mt * inv, lb = mt * mt * (inv - 0.5);
-            double sug = log1p(mt) - mu / (mu + a);
-            ll += fmax(fmin(sug, ub), lb);
-        } else {
-            ll += log1p(mt) - mu / (mu + a);
-        }
-        ll += y / (mu + a);
-    }
+    score_cells q = { d->mu, d->y, theta, a };
+    double ll;
+    orc_cell_sums(n, 0, NULL, 0, 0, 1, score_cellfn, &q, &ll);
     ll *= a;
     return ll - dig + cr_term * theta;
+}
+
+/* per-cell terms of the derivative (src/overdispersion.cpp:223-233) */
+static void deriv_cellfn(void *vc, int64_t c0, int nc, int p, const double *xr, double *w)
+{
+    const score_cells *q = (const score_cells *)vc;
+    (void)p; (void)xr;
+    for (int c = 0; c < nc; c++) {
+        const double mu = q->mu[c0 + c], y = q->y[c0 + c];
+        const double den = 1.0 + mu * q->theta;
+        w[c] = log1p(mu * q->theta) + (y - mu) / (mu + q->a);
+        w[ORC_BLK + c] = (mu * mu * q->theta + y) / den / den;
+    }
 }
 
 /* conventional_deriv_score_function_fast (src/overdispersion.cpp:186-242) */
@@ -663,15 +796,27 @@ double orc_nb_deriv_score(const nbdata *d, double log_theta, int cr)
     digamma_sums(d, a, &sd, &st);
     double dig = sd;
     double trig = a2 * st;
-    double l1 = 0.0, l2 = 0.0;
-    for (int64_t c = 0; c < n; c++) {
-        double mu = d->mu[c], y = d->y[c];
-        double den = 1.0 + mu * theta;
-        l1 += log1p(mu * theta) + (y - mu) / (mu + a);
-        l2 += (mu * mu * theta + y) / den / den;
-    }
+    score_cells q = { d->mu, d->y, theta, a };
+    double l12[2];
+    orc_cell_sums(n, 0, NULL, 0, 0, 2, deriv_cellfn, &q, l12);
+    const double l1 = l12[0], l2 = l12[1];
     double ll = -2.0 * a * (l1 - dig) + (l2 + trig);
     return ll + cr_term * theta * theta + (l1 - dig) * a + cr_term2 * theta;
+}
+
+/* mu = exp(X beta + off), 0 -> 1e-6 (R/overdispersion.R:41-42); written per
+ * cell, no sums */
+typedef struct { const double *beta, *off; double *mu; } mu_cells;
+static void mu_cellfn(void *vc, int64_t c0, int nc, int p, const double *xr, double *w)
+{
+    const mu_cells *q = (const mu_cells *)vc;
+    (void)w;
+    for (int c = 0; c < nc; c++) {
+        double eta = 0.0;
+        for (int j = 0; j < p; j++) eta += xr[c * p + j] * q->beta[j];
+        double m = exp(eta + q->off[c0 + c]);
+        q->mu[c0 + c] = m == 0.0 ? 1e-6 : m;
+    }
 }
 
 /* fit_dispersion (R/overdispersion.R:25-115), re-expressed as a bracketed
@@ -685,12 +830,8 @@ double orc_fit_dispersion(int64_t n, int p, const double *y, const double *X, co
     for (int64_t c = 0; c < n; c++) if (y[c] != 0.0) { allzero = 0; break; }
     if (allzero) return 0.0;
     double *mu = (double *)malloc(sizeof(double) * n);
-    for (int64_t c = 0; c < n; c++) {
-        double eta = 0.0;
-        for (int j = 0; j < p; j++) eta += X[(int64_t)j * n + c] * beta[j];
-        mu[c] = exp(eta + offv[c]);
-        if (mu[c] == 0.0) mu[c] = 1e-6;
-    }
+    mu_cells mq = { beta, offv, mu };
+    orc_cell_sums(n, p, X, 0, 0, 0, mu_cellfn, &mq, NULL);
     nbdata d = { n, p, y, mu, X };
     double m = 0.0;
     for (int64_t c = 0; c < n; c++) m += y[c];
@@ -737,20 +878,25 @@ double orc_fit_dispersion(int64_t n, int p, const double *y, const double *X, co
 /* bread and meat  (src/variance.cpp:22-47, :64-85, :104-137, :157-178, */
 /* :186-228)                                                            */
 /* ------------------------------------------------------------------ */
+typedef struct { const double *beta, *sf, *y; double th; } hess_cells;
+static void hess_cellfn(void *vc, int64_t c0, int nc, int p, const double *xr, double *w)
+{
+    const hess_cells *q = (const hess_cells *)vc;
+    for (int c = 0; c < nc; c++) {
+        double eta = 0.0;
+        for (int j = 0; j < p; j++) eta += xr[c * p + j] * q->beta[j];
+        const double mu = q->sf[c0 + c] * exp(eta);
+        const double den = 1.0 + q->th * mu;
+        w[c] = (q->y[c0 + c] * q->th + 1.0) * mu / (den * den);
+    }
+}
+
 int orc_compute_hessian(int64_t n, int p, const double *beta, double overdispersion,
                         const double *y, const double *X, const double *sf, double *bread)
 {
     double *H = (double *)calloc((size_t)p * p, sizeof(double));
-    for (int64_t c = 0; c < n; c++) {
-        double eta = 0.0;
-        for (int j = 0; j < p; j++) eta += X[(int64_t)j * n + c] * beta[j];
-        double mu = sf[c] * exp(eta);
-        double den = 1.0 + overdispersion * mu;
-        double s = (y[c] * overdispersion + 1.0) * mu / (den * den);
-        for (int a = 0; a < p; a++)
-            for (int b = 0; b < p; b++)
-                H[b * p + a] += X[(int64_t)a * n + c] * s * X[(int64_t)b * n + c];
-    }
+    hess_cells q = { beta, sf, y, overdispersion };
+    orc_cell_sums(n, p, X, 1, 0, 0, hess_cellfn, &q, H);
     int st = lu_inverse(p, H, bread);
     free(H);
     return st;
@@ -993,7 +1139,13 @@ int orc_cpu_fit(int64_t G, int64_t n, int p, const int64_t *rowptr, const int32_
     double *sf = (double *)malloc(sizeof(double) * n);
     for (int64_t c = 0; c < n; c++) sf[c] = exp(offv[c]);
     if (g_end > G) g_end = G;
-    #pragma omp parallel
+    /* many genes: one thread per gene; few genes: one gene at a time with
+     * its cell sums split over the threads (orc_cell_sums) */
+    int nth = 1;
+#ifdef _OPENMP
+    nth = omp_get_max_threads();
+#endif
+    #pragma omp parallel if (g_end - g_begin >= 4 * (int64_t)nth)
     {
         double *y = (double *)malloc(sizeof(double) * n);
         double *meat = (double *)malloc(sizeof(double) * p * p);

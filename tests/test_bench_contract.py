@@ -58,12 +58,13 @@ def test_parity_summary_applies_the_test_bars():
     ref = {"beta": np.array([[0.5, -2.0], [3.0, 0.1], [-1.0, 0.0], [9.0, 9.0]]),
            "iters": np.array([5, 7, 200, 4]), "theta": np.array([0.5, 2e-4, 1.0, 10.0])}
     beta = ref["beta"] + np.array([[2e-6, 0.0], [0.0, 0.0], [0.5, 0.5], [0.0, 0.0]])
-    beta[1, 0] = 3.0 * (1 + 4e-6)  # |beta| > 1: relative
+    beta[1, 0] = 3.0 + 4e-6
     iters = np.array([5, 7, 200, 5])  # gene 3 differs by one step: not compared
     theta = ref["theta"] * np.array([1 + 1e-5, 5.0, 1.0, 1.0])  # gene 1: theta < 1e-3, ignored
     s = bench.parity_summary(beta, iters, theta, ref)
     assert s["genes"] == 4 and s["iters_agree"] == 0.75 and s["converged_compared"] == 2
-    assert abs(s["max_dbeta"] - 4e-6) < 1e-12 and s["within_bar"]
+    assert abs(s["max_abs_dbeta"] - 4e-6) < 1e-12 and s["within_bar"]
     assert abs(s["max_rel_dtheta"] - 1e-5) < 1e-12
-    beta[0, 1] += 5e-5  # |beta| = 2: 2.5e-5 relative
+    # the bar is absolute: 2e-5 on |beta| = 2 fails it
+    beta[0, 1] += 2e-5
     assert not bench.parity_summary(beta, iters, theta, ref)["within_bar"]

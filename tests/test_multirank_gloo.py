@@ -36,6 +36,13 @@ def _worker(rank, world, port, pvals, out_path):
         b, e = D.shard_ranges(rowptr, world, n_cells=100)[rank]
         local = pvals[b:e]
         adj = D.global_adjust(local, "BH", adjust=lambda p, m: oracle.p_adjust(p, m))
+        # the tensor form the multi-GPU benchmark step runs (device tensors
+        # under NCCL; CPU tensors here), with the same adjuster
+        import torch
+        adj_t = D.global_adjust_tensor(
+            torch.as_tensor(local, dtype=torch.float64), "BH",
+            adjust=lambda full, m: torch.as_tensor(oracle.p_adjust(full.numpy(), m)))
+        np.testing.assert_array_equal(adj_t.numpy(), adj)
         np.save(out_path + f".{rank}.npy", np.concatenate([[b, e], adj]))
     finally:
         dist.destroy_process_group()
