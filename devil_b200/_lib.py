@@ -23,7 +23,7 @@ SF_NONE, SF_NORMED_SUM, SF_PSINORM, SF_GIVEN = range(4)
 OD_NONE, OD_MOM, OD_MLE, OD_NEW = range(4)
 FORM_CHOSEN, FORM_PLAIN = 0, 1
 PREC_FP32, PREC_TC_TF32, PREC_TC_BF16X3 = 0, 1, 2
-ADJ_NONE, ADJ_BH, ADJ_BONFERRONI, ADJ_HOLM, ADJ_HOCHBERG, ADJ_BY = range(6)
+ADJ_NONE, ADJ_BH, ADJ_BONFERRONI, ADJ_HOLM, ADJ_HOCHBERG, ADJ_BY, ADJ_HOMMEL = range(7)
 GENE_CONVERGED, GENE_MAX_ITER, GENE_NAN = range(3)
 NA_INT = -(2 ** 31)
 

@@ -20,7 +20,16 @@ import numpy as np
 from . import _lib as L
 
 _ADJ = {"BH": L.ADJ_BH, "fdr": L.ADJ_BH, "bonferroni": L.ADJ_BONFERRONI, "holm": L.ADJ_HOLM,
-        "hochberg": L.ADJ_HOCHBERG, "BY": L.ADJ_BY, "none": L.ADJ_NONE}
+        "hochberg": L.ADJ_HOCHBERG, "BY": L.ADJ_BY, "hommel": L.ADJ_HOMMEL, "none": L.ADJ_NONE}
+
+
+def _adjust_code(method):
+    """stats::p.adjust's method argument (match.arg over p.adjust.methods)."""
+    if method not in _ADJ:
+        raise ValueError("'arg' should be one of \u201cholm\u201d, \u201chochberg\u201d, "
+                         "\u201chommel\u201d, \u201cbonferroni\u201d, \u201cBH\u201d, "
+                         "\u201cBY\u201d, \u201cfdr\u201d, \u201cnone\u201d")
+    return _ADJ[method]
 
 
 def _ptr(a):
@@ -364,8 +373,7 @@ def test_de(devil_fit, contrast, clusters=None, pval_adjust_method="BH", max_lfc
         raise ValueError("The fit object was created with an older version of devil and is no "
                          "longer supported. Please re-fit your model with the current version of "
                          "fit_devil().")
-    if pval_adjust_method not in _ADJ:
-        raise NotImplementedError(f"p-value adjustment '{pval_adjust_method}' is not supported")
+    adj = _adjust_code(pval_adjust_method)
     beta = np.ascontiguousarray(devil_fit["beta"], np.float64)
     G, p = beta.shape
     c = np.ascontiguousarray(np.asarray(contrast, np.float64).reshape(-1))
@@ -378,7 +386,7 @@ def test_de(devil_fit, contrast, clusters=None, pval_adjust_method="BH", max_lfc
     pv, pa, lf = np.empty(G), np.empty(G), np.empty(G)
     ctx = L.context(device)
     ctx.check(L.load().devil_test_de(ctx.h, G, p, _ptr(beta), _ptr(bread), _ptr(sw), nsamples,
-                                     _ptr(c), _ADJ[pval_adjust_method], float(max_lfc), _ptr(pv),
+                                     _ptr(c), adj, float(max_lfc), _ptr(pv),
                                      _ptr(pa), _ptr(lf)))
     names = devil_fit.get("gene_names")
     if names is None:
@@ -402,7 +410,7 @@ def p_adjust(p, method="BH", device=0):
     p = np.ascontiguousarray(p, np.float64)
     out = np.empty_like(p)
     ctx = L.context(device)
-    ctx.check(L.load().devil_p_adjust(ctx.h, len(p), _ptr(p), _ADJ[method], _ptr(out)))
+    ctx.check(L.load().devil_p_adjust(ctx.h, len(p), _ptr(p), _adjust_code(method), _ptr(out)))
     return out
 
 

@@ -1581,7 +1581,7 @@ int devil_test_de_device(devil_ctx* ctx, int64_t G, int p, const double* beta_de
                          double* pval_dev, double* adj_dev, double* lfc_dev) {
     return guarded(ctx, [&] {
         if (p < 1 || p > 64 || !contrast_host) fail(ctx, DEVIL_ERR_ARG, "bad p or contrast");
-        if (adjust_method < 0 || adjust_method > 5) fail(ctx, DEVIL_ERR_UNSUPPORTED, "adjust method");
+        if (adjust_method < 0 || adjust_method > DEVIL_ADJ_HOMMEL) fail(ctx, DEVIL_ERR_UNSUPPORTED, "adjust method");
         double* c = ws<double>(ctx, "contrast", p);
         h2d(ctx, c, contrast_host, p);
         LAUNCH(launch_test_pvalues(G, p, beta_dev, bread_dev, sandwich_dev, (double)(n_samples - 2), c,
@@ -1620,7 +1620,7 @@ int devil_test_de(devil_ctx* ctx, int64_t G, int p, const double* beta, const do
 
 int devil_p_adjust(devil_ctx* ctx, int64_t m, const double* p, int method, double* out) {
     return guarded(ctx, [&] {
-        if (method < 0 || method > 5) fail(ctx, DEVIL_ERR_UNSUPPORTED, "adjust method");
+        if (method < 0 || method > DEVIL_ADJ_HOMMEL) fail(ctx, DEVIL_ERR_UNSUPPORTED, "adjust method");
         double* pd = ws<double>(ctx, "pa_in", m);
         double* od = ws<double>(ctx, "pa_out", m);
         h2d(ctx, pd, p, m);
@@ -1635,7 +1635,7 @@ int devil_p_adjust(devil_ctx* ctx, int64_t m, const double* p, int method, doubl
 int devil_p_adjust_device(devil_ctx* ctx, int64_t m, const double* p_dev, int method,
                           double* out_dev) {
     return guarded(ctx, [&] {
-        if (method < 0 || method > 5) fail(ctx, DEVIL_ERR_UNSUPPORTED, "adjust method");
+        if (method < 0 || method > DEVIL_ADJ_HOMMEL) fail(ctx, DEVIL_ERR_UNSUPPORTED, "adjust method");
         size_t tb = p_adjust_temp_bytes(m);
         void* tmp = ws<char>(ctx, "padj_tmp", tb);
         LAUNCH(launch_p_adjust(m, p_dev, method, out_dev, tmp, tb, ctx->stream));

@@ -129,6 +129,16 @@ __global__ void padj_prepare_kernel(const double* p, int64_t m, double* keys, in
     if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(nvalid, cnt);
 }
 
+DEV double dm_times(int64_t m, double v) { return (double)m * v; }
+
+// s + e += v as a double-double (error-free TwoSum of the high parts)
+DEV void dd_add(double& s, double& e, double v) {
+    const double t = s + v;
+    const double bp = t - s;
+    e += (s - (t - bp)) + (v - bp);
+    s = t;
+}
+
 // one block: scan over the sorted valid p-values (ascending ranks 1..n)
 __global__ void padj_scan_kernel(const double* sk, const int32_t* sidx, const int32_t* nvalid_p,
                                  int64_t m, const double* p, int method, double* out) {
@@ -138,22 +148,34 @@ __global__ void padj_scan_kernel(const double* sk, const int32_t* sidx, const in
     for (int64_t i = t; i < m; i += T) out[i] = p[i];
     __syncthreads();
     if (method == 0 || n <= 1) return;
+    // hommel with two p-values is hochberg (as stats::p.adjust switches);
+    // n >= 3 runs in the hommel kernels
+    if (method == 6) {
+        if (n >= 3) return;
+        method = 4;
+    }
     const double dn = (double)n;
     double q = 1.0;
     if (method == 5) {
-        double s = 0.0;
-        for (int64_t k = 1 + t; k <= n; k += T) s += 1.0 / (double)k;
-        __shared__ double qs[32];
-        s = warp_sum(s);
-        if ((t & 31) == 0) qs[t >> 5] = s;
+        // q = sum(1/(1:n)) of the double-rounded terms, summed in
+        // double-double and rounded once: the correctly rounded sum (R sums
+        // in extended precision)
+        double hs = 0.0, he = 0.0;
+        for (int64_t k = 1 + t; k <= n; k += T) dd_add(hs, he, 1.0 / (double)k);
+        __shared__ double qh[1024], ql[1024];
+        qh[t] = hs;
+        ql[t] = he;
         __syncthreads();
         if (t == 0) {
-            double a = 0.0;
-            for (int w = 0; w < (T >> 5); ++w) a += qs[w];
-            qs[0] = a;
+            double a = 0.0, ae = 0.0;
+            for (int w = 0; w < T; ++w) {
+                dd_add(a, ae, qh[w]);
+                ae += ql[w];
+            }
+            qh[0] = a + ae;
         }
         __syncthreads();
-        q = qs[0];
+        q = qh[0];
     }
     auto val = [&](int64_t k) -> double {  // k = 0-based ascending rank
         double pk = sk[k];
@@ -206,6 +228,69 @@ __global__ void padj_scan_kernel(const double* sk, const int32_t* sidx, const in
     }
 }
 
+// Hommel (stats::p.adjust, "hommel") on the ascending p-values s[0..n):
+//   pa = min_i n s_i / i;  for m = n-1 .. 2:
+//     q1 = min_{j=2..m} m s_{n-m+j} / j                  (1-based ranks)
+//     q_i = min(m s_i, q1) for i <= n-m+1, q_{n-m+1} beyond
+//     pa = max(pa, q)
+//   result = max(pa, s).
+// Every m is independent given the sorted p-values, and pa is a max over
+// m, so the O(n^2) loop of the reference runs as two parallel kernels:
+// q1 for every m (a block per m), then, per rank i, the max over m.
+__global__ void hommel_q1_kernel(const double* s, const int32_t* nvalid_p, double* q1) {
+    const int64_t n = *nvalid_p;
+    const int64_t m = blockIdx.x + 2;  // 2 .. n-1
+    if (n < 3 || m > n - 1) return;
+    const double dm = (double)m;
+    double v = INFINITY;
+    for (int64_t j = 2 + threadIdx.x; j <= m; j += blockDim.x)
+        v = fmin(v, dm * s[n - m + j - 1] / (double)j);
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = fmin(r, red[w]);
+        q1[m] = r;
+    }
+}
+
+__global__ void hommel_pa_kernel(const double* s, const int32_t* sidx, const int32_t* nvalid_p,
+                                 const double* q1, double* out) {
+    const int64_t n = *nvalid_p;
+    if (n < 3) return;
+    const double dn = (double)n;
+    // pa0 = min_i n s_i / i, the same in every thread (one warp-strided pass
+    // per thread over all ranks would cost n^2: read it from the block)
+    __shared__ double red[32];
+    __shared__ double pa0s;
+    double v = INFINITY;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) v = fmin(v, dn * s[i] / (double)(i + 1));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) r = fmin(r, red[w]);
+        pa0s = r;
+    }
+    __syncthreads();
+    const double pa0 = pa0s;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r1 = i + 1;  // 1-based rank
+        double pa = pa0;
+        for (int64_t m = 2; m <= n - 1; ++m) {
+            const int64_t k = r1 <= n - m + 1 ? i : n - m;  // rank n-m+1, 0-based
+            pa = fmax(pa, fmin(dm_times(m, s[k]), q1[m]));
+        }
+        out[sidx[i]] = fmax(pa, s[i]);  // <= 1: every q_m is at most s_n
+    }
+}
+
 static size_t cub_sort_bytes(int64_t m) {
     size_t b = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, b, (const double*)nullptr, (double*)nullptr,
@@ -232,12 +317,19 @@ cudaError_t launch_p_adjust(int64_t m, const double* p, int method, double* out,
     int32_t* i_in = reinterpret_cast<int32_t*>(b); b += align_up(4 * (size_t)m);
     int32_t* i_out = reinterpret_cast<int32_t*>(b); b += align_up(4 * (size_t)m);
     int32_t* nvalid = reinterpret_cast<int32_t*>(b);
+    double* q1 = k_in;  // hommel's per-m minima: the unsorted keys are dead after the sort
     cudaError_t e = cudaMemsetAsync(nvalid, 0, sizeof(int32_t), st);
     if (e != cudaSuccess) return e;
     padj_prepare_kernel<<<(unsigned)std::min<int64_t>(nblk(m, 256), 1024), 256, 0, st>>>(p, m, k_in, i_in, nvalid);
     e = cub::DeviceRadixSort::SortPairs(cub_tmp, sb, k_in, k_out, i_in, i_out, (int)m, 0, 64, st);
     if (e != cudaSuccess) return e;
     padj_scan_kernel<<<1, 1024, 0, st>>>(k_out, i_out, nvalid, m, p, method, out);
+    if (method == 6 && m >= 3) {
+        // blocks for every m the valid count can reach; those beyond n - 1 exit
+        hommel_q1_kernel<<<(unsigned)(m - 2), 256, 0, st>>>(k_out, nvalid, q1);
+        hommel_pa_kernel<<<(unsigned)std::min<int64_t>(nblk(m, 256), 1184), 256, 0, st>>>(
+            k_out, i_out, nvalid, q1, out);
+    }
     return cudaGetLastError();
 }
 

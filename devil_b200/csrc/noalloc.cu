@@ -62,7 +62,7 @@ DEVIL_API int devil_p_adjust_device_static(int64_t m, const double* p_dev, int m
         put_err(errbuf, errlen, "devil_p_adjust_device_static: need m >= 0 and device p / out");
         return DEVIL_ERR_ARG;
     }
-    if (method < DEVIL_ADJ_NONE || method > DEVIL_ADJ_BY) {
+    if (method < DEVIL_ADJ_NONE || method > DEVIL_ADJ_HOMMEL) {
         put_err(errbuf, errlen, "devil_p_adjust_device_static: unknown adjustment method");
         return DEVIL_ERR_ARG;
     }

@@ -213,6 +213,8 @@ DEVIL_API int devil_fit_async(devil_ctx *ctx, void *stream, const devil_counts *
 #define DEVIL_ADJ_HOLM        3
 #define DEVIL_ADJ_HOCHBERG    4
 #define DEVIL_ADJ_BY          5
+#define DEVIL_ADJ_HOMMEL      6   /* O(n^2) as in stats::p.adjust; n = 2 is */
+                                  /* hochberg                              */
 
 /* test_de (R/test.R:85-134): lfc = beta . contrast; p from the t
  * distribution with df = n_samples - 2 using contrast' H contrast; when

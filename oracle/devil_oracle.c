@@ -1048,21 +1048,72 @@ static int cmp_asc(const void *a, const void *b)
     return (x->i < y->i) ? -1 : (x->i > y->i);
 }
 
-/* method: 0 none, 1 BH, 2 bonferroni, 3 holm, 4 hochberg, 5 BY.
- * NaN entries are left NaN and do not count toward n. */
+/* sum(1/(1:n)) of the double-rounded terms, rounded once (double-double
+ * accumulation); R's sum() accumulates in extended precision */
+static double harmonic_rounded(int64_t n)
+{
+    double s = 0.0, e = 0.0;
+    for (int64_t k = 1; k <= n; k++) {
+        double v = 1.0 / (double)k;
+        double t = s + v, bp = t - s;
+        e += (s - (t - bp)) + (v - bp);
+        s = t;
+    }
+    return s + e;
+}
+
+/* Hommel's method as stats::p.adjust states it, on the ascending valid
+ * p-values s[0..n) (n >= 3); writes the adjusted value of rank k to r[k]. */
+static void hommel_sorted(int64_t n, const double *s, double *r)
+{
+    double *q = (double *)malloc(sizeof(double) * n);
+    double *pa = (double *)malloc(sizeof(double) * n);
+    double mn = INFINITY;
+    for (int64_t i = 1; i <= n; i++) { double t = (double)n * s[i - 1] / (double)i; if (t < mn) mn = t; }
+    for (int64_t i = 0; i < n; i++) q[i] = pa[i] = mn;
+    for (int64_t m = n - 1; m >= 2; m--) {
+        /* i1 = 1..n-m+1, i2 = n-m+2..n */
+        double q1 = INFINITY;
+        for (int64_t j = 2; j <= m; j++) {
+            double t = (double)m * s[n - m + j - 1] / (double)j;
+            if (t < q1) q1 = t;
+        }
+        for (int64_t i = 1; i <= n - m + 1; i++) q[i - 1] = fmin((double)m * s[i - 1], q1);
+        for (int64_t i = n - m + 2; i <= n; i++) q[i - 1] = q[n - m];
+        for (int64_t i = 0; i < n; i++) pa[i] = fmax(pa[i], q[i]);
+    }
+    for (int64_t i = 0; i < n; i++) r[i] = fmax(pa[i], s[i]);
+    free(q); free(pa);
+}
+
+/* method: 0 none, 1 BH, 2 bonferroni, 3 holm, 4 hochberg, 5 BY, 6 hommel
+ * (stats::p.adjust, called at R/test.R:127).  NaN entries are left NaN and
+ * do not count toward n (p.adjust's default n = length(p) is evaluated
+ * after the NAs are dropped).  With n = 2, hommel is hochberg, as
+ * p.adjust switches. */
 int orc_p_adjust(int64_t m, const double *p, int method, double *out)
 {
     pi_pair *v = (pi_pair *)malloc(sizeof(pi_pair) * (m > 0 ? m : 1));
     int64_t n = 0;
     for (int64_t i = 0; i < m; i++) { out[i] = p[i]; if (!isnan(p[i])) { v[n].p = p[i]; v[n].i = i; n++; } }
     if (n <= 1 || method == 0) { free(v); return ORC_OK; }
+    if (method == 6 && n == 2) method = 4;
     double dn = (double)n;
+    if (method == 6) {
+        qsort(v, n, sizeof(pi_pair), cmp_asc);
+        double *s = (double *)malloc(sizeof(double) * n), *r = (double *)malloc(sizeof(double) * n);
+        for (int64_t k = 0; k < n; k++) s[k] = v[k].p;
+        hommel_sorted(n, s, r);
+        for (int64_t k = 0; k < n; k++) out[v[k].i] = r[k];
+        free(s); free(r); free(v);
+        return ORC_OK;
+    }
     if (method == 2) {
         for (int64_t k = 0; k < n; k++) out[v[k].i] = fmin(1.0, dn * v[k].p);
     } else if (method == 1 || method == 5 || method == 4) {
         qsort(v, n, sizeof(pi_pair), cmp_desc);
         double q = 1.0;
-        if (method == 5) { q = 0.0; for (int64_t k = 1; k <= n; k++) q += 1.0 / (double)k; }
+        if (method == 5) q = harmonic_rounded(n);
         double cm = INFINITY;
         for (int64_t k = 0; k < n; k++) {
             double i = (double)(n - k);               /* i = lp:1 */

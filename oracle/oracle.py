@@ -21,7 +21,8 @@ _LIB = None
 SF_NORMED_SUM = 0
 SF_PSINORM = 1
 OD_NONE, OD_MOM, OD_MLE, OD_NEW = 0, 1, 2, 3
-ADJ = {"none": 0, "BH": 1, "fdr": 1, "bonferroni": 2, "holm": 3, "hochberg": 4, "BY": 5}
+ADJ = {"none": 0, "BH": 1, "fdr": 1, "bonferroni": 2, "holm": 3, "hochberg": 4, "BY": 5,
+       "hommel": 6}
 
 _d = C.POINTER(C.c_double)
 _i32 = C.POINTER(C.c_int32)

@@ -55,9 +55,9 @@ def test_gpu_matches_golden(dv, path):
     same = fit["iterations"]["beta_iters"] == g["iters"]
     assert same.mean() >= 0.95
     conv = same & (g["iters"] < 200)
-    # 1e-5 absolute for |beta| <= 1, relative above (FP32 per-cell arithmetic)
-    dr = np.abs(fit["beta"] - g["beta"]) / np.maximum(1, np.abs(g["beta"]))
-    assert dr[conv].max() <= 1e-5
+    # the acceptance bar: |d beta| <= 1e-5 absolute on genes converging in both
+    da = np.abs(fit["beta"] - g["beta"])
+    assert da[conv].max() <= 1e-5
     capped = same & (g["iters"] >= 200)
     if capped.any():
         rel = np.abs(fit["beta"] - g["beta"])[capped] / np.maximum(1, np.abs(g["beta"][capped]))

@@ -2,7 +2,8 @@
 oracle (cpu_fit, R/main.R:375-523) on the same seeded inputs.
 
 Bars (from the path's acceptance criteria):
-  * beta: |d beta| <= 1e-5 on genes whose IRLS iteration counts agree;
+  * beta: |d beta| <= 1e-5 (absolute) on genes that converge in both with
+    the same IRLS iteration count;
     iteration counts agree on >= 97% of genes (a gene whose max|delta|
     lands within FP32 rounding of the tolerance may take one step more or
     less; those genes differ by at most one step < tolerance);
@@ -50,19 +51,17 @@ def gpu_fit(dv, P, od, clusters=None, sf="normed_sum", max_iter=200, tol=1e-3, f
 
 
 def check_beta(fit, ref, tol=BETA_TOL, agree=ITER_AGREE, max_iter=200):
-    """|dbeta| <= tol * max(1, |beta|) on genes that converge in both with the
-    same iteration count (absolute 1e-5 for |beta| <= 1).  Coefficients of
-    magnitude > 1 are held to 1e-5 relative: the per-cell arithmetic is FP32,
-    eta carries ~1e-7 * |x beta| of rounding, and a slowly converging IRLS
-    (linear rate rho near 1, e.g. an intercept drifting towards -inf for a
-    cell group without counts) amplifies per-step rounding by 1/(1 - rho).
-    Genes stopped by max_iter have not converged (the bar does not apply);
-    they are checked at 1e-4 relative."""
+    """|d beta| <= tol (absolute, the acceptance bar) on genes that converge
+    in both with the same iteration count.  Genes stopped by max_iter have
+    not converged (the bar does not apply: e.g. an intercept drifting
+    towards -inf for a cell group without counts moves by ~1 per step);
+    they are checked at 1e-4 relative.  Genes one step apart differ by that
+    step, which is below the tolerance (1e-3)."""
     it_g = fit["iterations"]["beta_iters"]
     it_o = ref["iters"]
     same = it_g == it_o
     assert same.mean() >= agree, f"iteration counts agree on only {same.mean():.3f}"
-    d = np.abs(fit["beta"] - ref["beta"]) / np.maximum(1.0, np.abs(ref["beta"]))
+    d = np.abs(fit["beta"] - ref["beta"])
     conv = same & (it_o < max_iter)
     if conv.any():
         g = np.flatnonzero(conv)[np.argmax(np.nanmax(d[conv], axis=1))]
@@ -76,7 +75,7 @@ def check_beta(fit, ref, tol=BETA_TOL, agree=ITER_AGREE, max_iter=200):
     # genes off by one iteration: the extra step is below the tolerance
     if (~same).any():
         assert np.all(np.abs(it_g[~same] - it_o[~same]) <= 1)
-        assert np.nanmax(d[~same]) <= 10 * 1e-3
+        assert np.nanmax(d[~same] / np.maximum(1.0, np.abs(ref["beta"][~same]))) <= 10 * 1e-3
     return conv
 
 
@@ -103,6 +102,12 @@ def check_pvals(p_g, p_o, mask, tol=1e-3):
     lg, lo = np.log10(p_g[ok]), np.log10(p_o[ok])
     r = np.abs(lg - lo) / np.maximum(1.0, np.abs(lo))
     assert r.size == 0 or r.max() <= tol, f"log10 p rel err {r.max():.3e}"
+
+
+def small_problem(cfg, seed, G, n):
+    """A config at test size; the wide design with gene means LogNormal(-1, 2)
+    so that a few dozen genes at a few thousand cells carry counts."""
+    return synthetic.make(cfg, seed=seed, G=G, n=n, mean_loc=-1.0 if cfg == "wide" else None)
 
 
 @pytest.fixture(scope="module")
@@ -168,7 +173,9 @@ def test_fit_clustered_p12(dv, orc):
 
 
 def test_fit_wide_p32(dv, orc):
-    P = synthetic.make("wide", seed=2, G=24, n=4000)
+    # gene means LogNormal(-1, 2): at n = 4000 the headline location (-3.8)
+    # leaves most of 24 genes with a handful of counts
+    P = synthetic.make("wide", seed=2, G=24, n=4000, mean_loc=-1.0)
     ref = oracle_fit(orc, P, orc.OD_MOM, sf=None)
     fit = gpu_fit(dv, P, "MOM", sf=None)
     same = check_beta(fit, ref)
@@ -402,7 +409,7 @@ def test_fit_batch_uneven_problems(dv):
              ("plain_sparse", 5, 60, 800, False)]
     probs = []
     for cfg, seed, G, n, cl in cases:
-        P = synthetic.make(cfg, seed=seed, G=G, n=n)
+        P = small_problem(cfg, seed, G, n)
         x = (P.rowptr, P.col, P.val.astype(np.float64) if P.val.dtype != np.uint16 else P.val, P.n)
         probs.append((x, P.X, P.clusters) if cl else (x, P.X))
     kw = dict(overdispersion="MOM", size_factors=None)
@@ -499,7 +506,7 @@ def test_fit_batch_concurrent_shapes(dv):
              ("plain_small", 35, 40, 600, False), ("plain_sparse", 36, 64, 2000, False)]
     probs = []
     for cfg, seed, G, n, cl in cases:
-        P = synthetic.make(cfg, seed=seed, G=G, n=n)
+        P = small_problem(cfg, seed, G, n)
         x = (P.rowptr, P.col, P.val.astype(np.float64) if P.val.dtype != np.uint16 else P.val, P.n)
         probs.append((x, P.X, P.clusters) if cl else (x, P.X))
     kw = dict(overdispersion="MLE", size_factors=None)

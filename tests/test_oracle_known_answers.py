@@ -311,3 +311,48 @@ def test_new_overdispersion_stop_condition(orc):
     D = P.dense()
     errs = [orc.fit_overdispersion_new(D[g], P.X, r["beta"][g], off)[3] for g in range(P.G)]
     assert 1 in errs and 0 in errs
+
+
+def _hommel_as_in_p_adjust(p):
+    """stats::p.adjust(p, "hommel") line by line in numpy (no NAs)."""
+    p = np.asarray(p, float)
+    n = len(p)
+    i = np.arange(1, n + 1)
+    o = np.argsort(p, kind="stable")
+    ps = p[o]
+    ro = np.argsort(o, kind="stable")
+    q = pa = np.full(n, np.min(n * ps / i))
+    for m in range(n - 1, 1, -1):
+        i1 = np.arange(1, n - m + 2)
+        i2 = np.arange(n - m + 2, n + 1)
+        q1 = np.min(m * ps[i2 - 1] / np.arange(2, m + 1))
+        q = q.copy()
+        q[i1 - 1] = np.minimum(m * ps[i1 - 1], q1)
+        q[i2 - 1] = q[n - m]
+        pa = np.maximum(pa, q)
+    return np.maximum(pa, ps)[ro]
+
+
+def test_p_adjust_hommel(orc):
+    # the restatement of p.adjust's hommel branch; n = 2 switches to hochberg
+    rng = np.random.default_rng(8)
+    for n in (3, 4, 11, 60):
+        p = rng.uniform(size=n) ** 2
+        np.testing.assert_array_equal(orc.p_adjust(p, "hommel"), _hommel_as_in_p_adjust(p))
+    np.testing.assert_allclose(orc.p_adjust([0.01, 0.02, 0.03, 0.04, 0.05], "hommel"),
+                               [0.05] * 5, rtol=1e-15)
+    p2 = np.array([0.04, 0.01])
+    np.testing.assert_array_equal(orc.p_adjust(p2, "hommel"), orc.p_adjust(p2, "hochberg"))
+    # Hommel is never less powerful than Hochberg
+    p = rng.uniform(size=40) ** 3
+    assert np.all(orc.p_adjust(p, "hommel") <= orc.p_adjust(p, "hochberg") + 1e-15)
+
+
+def test_p_adjust_by_constant_is_correctly_rounded(orc):
+    from fractions import Fraction
+    n = 1000
+    exact = float(sum(Fraction(1.0 / k) for k in range(1, n + 1)))  # sum of the double terms
+    p = np.full(n, 1e-6)
+    got = orc.p_adjust(p, "BY")
+    # BY on equal p-values: min over ranks of q n / i p = q p at i = n
+    assert got[0] == min(1.0, exact * n / n * 1e-6)
