@@ -93,6 +93,7 @@ struct devil_ctx {
     int sm_count = 148;
     int use_tma = 0;
     int use_groups = 1;
+    int grp_slices = 1;  // slice-major IRLS pass of the design-group engine (DEVIL_GRP_SLICES=0: block per gene)
     int debug = 0;  // DEVIL_DEBUG=1: engine choices on stderr
     // profiling: CUDA events around every pass launch, per pass kind
     int profiling = 0;
@@ -257,12 +258,18 @@ struct DevProblem {
         int U = 0, C = 1;
         double* xg = nullptr;
         double* E = nullptr;
-        int32_t* gcol = nullptr;
-        void* gval = nullptr;
-        int64_t* gptr = nullptr;
+        int S = 0;                    // slices
+        void* gent = nullptr;         // slice-ordered CSR copy (GrpEnt entries)
+        int64_t* gptr = nullptr;      // [G][S + 1]
+        int32_t *sl_start = nullptr, *sl_key = nullptr, *kslice = nullptr;
         double* rs = nullptr;
         double* rw = nullptr;
         int32_t* rm = nullptr;
+        double* res = nullptr;
+        // sparse design rows and the assembly's (group, weight) lists
+        int32_t *rptr = nullptr, *rcol = nullptr, *qptr = nullptr, *qu = nullptr, *vptr = nullptr,
+                *vu = nullptr;
+        double *rval = nullptr, *qv = nullptr, *vv = nullptr;
     } grp;
 };
 
@@ -572,6 +579,22 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     int32_t* fkey = ws<int32_t>(ctx, "grp_fkey", n);
     int32_t* cells = ix;  // reuse
     LAUNCH(launch_fine_keys(ucell, ends_d, C, n, fkey, cells, st));
+    auto bits_for = [](int K) {
+        int b = 1;
+        while ((1 << b) < K) ++b;
+        return b;
+    };
+    // the cells renumbered in key order (stable: original order within a
+    // key), so that every key is a contiguous range of the new numbering
+    int32_t* pnew = ws<int32_t>(ctx, "grp_pnew", n);
+    int32_t* ksorted = ws<int32_t>(ctx, "grp_ksorted", n);
+    int64_t* kst = ws<int64_t>(ctx, "grp_kst", K + 1);
+    tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, fkey, ksorted, cells, pnew, (int)n, 0, bits_for(K));
+    CK(cub::DeviceRadixSort::SortPairs(ws<char>(ctx, "grp_sort_tmp0", tb), tb, fkey, ksorted, cells,
+                                       pnew, (int)n, 0, bits_for(K), st));
+    ctx->launches++;
+    LAUNCH(launch_group_starts(ksorted, n, K, kst, st));
     // cells by offset, then (stable) by group and by fine group: each
     // group's cells sorted by offset, as the rules need
     double* offs = ws<double>(ctx, "grp_offs", n);
@@ -581,11 +604,6 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     CK(cub::DeviceRadixSort::SortPairs(ws<char>(ctx, "grp_sort_tmp", tb), tb, dp.off, offs, cells,
                                        byoff, (int)n, 0, 64, st));
     ctx->launches++;
-    auto bits_for = [](int K) {
-        int b = 1;
-        while ((1 << b) < K) ++b;
-        return b;
-    };
     int32_t* kin = ws<int32_t>(ctx, "grp_kin", n);
     int32_t* kout = ws<int32_t>(ctx, "grp_kout", n);
     int32_t* permC = ws<int32_t>(ctx, "grp_permC", n);
@@ -611,8 +629,36 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
         LAUNCH(launch_group_starts(kout, n, K, gsF, st));
     }
     dbg_mark(ctx, "g.sort");
-    double* E = ws<double>(ctx, "grp_E", n);
-    LAUNCH(launch_exp(dp.off, n, E, st));
+    // slices: each key's range cut into pieces of at most kSliceCells cells
+    std::vector<int64_t> hks(K + 1);
+    CK(cudaMemcpyAsync(hks.data(), kst, (K + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<int32_t> sl_start{0}, sl_key, kslice(K + 1);
+    for (int k = 0; k < K; ++k) {
+        kslice[k] = (int32_t)sl_key.size();
+        const int64_t a = hks[k], cnt = hks[k + 1] - hks[k];
+        const int64_t pieces = (cnt + kSliceCells - 1) / kSliceCells;
+        for (int64_t q = 1; q <= pieces; ++q) {
+            sl_start.push_back((int32_t)(a + cnt * q / pieces));
+            sl_key.push_back(k);
+        }
+    }
+    kslice[K] = (int32_t)sl_key.size();
+    const int NSL = (int)sl_key.size();
+    if (NSL < 1 || NSL > kMaxSlices) {
+        if (ctx->debug) fprintf(stderr, "devil_b200: design not grouped (%d slices)\n", NSL);
+        return;
+    }
+    int32_t* d_sl_start = ws<int32_t>(ctx, "grp_sl_start", NSL + 1);
+    int32_t* d_sl_key = ws<int32_t>(ctx, "grp_sl_key", NSL);
+    int32_t* d_kslice = ws<int32_t>(ctx, "grp_kslice", K + 1);
+    h2d(ctx, d_sl_start, sl_start.data(), NSL + 1);
+    h2d(ctx, d_sl_key, sl_key.data(), NSL);
+    h2d(ctx, d_kslice, kslice.data(), K + 1);
+    int32_t* cslice = ws<int32_t>(ctx, "grp_cslice", n);
+    int32_t* cloc = ws<int32_t>(ctx, "grp_cloc", n);
+    double* E = ws<double>(ctx, "grp_E", n);  // exp(offset) in slice order
+    LAUNCH(launch_slice_cells(pnew, d_sl_start, NSL, n, dp.off, cslice, cloc, E, st));
     const int nrules = U + (C > 1 ? K : 0);
     double* rs = ws<double>(ctx, "grp_rs", (size_t)nrules * kRuleCap);
     double* rw = ws<double>(ctx, "grp_rw", (size_t)nrules * kRuleCap);
@@ -622,12 +668,11 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     LAUNCH(launch_group_rules(permC, gsC, permF, gsF, U, nrules, dp.off, n, scr, rs, rw, rm, rerr,
                               bad + 1, st));
     dbg_mark(ctx, "g.rules");
-    // CSR copy ordered by key within each gene
-    int32_t* gcol = ws<int32_t>(ctx, "grp_col", dp.nnz);
-    void* gval = dp.val_u16 ? (void*)ws<uint16_t>(ctx, "grp_val16", dp.nnz)
-                            : (void*)ws<float>(ctx, "grp_val32", dp.nnz);
-    int64_t* gptr = ws<int64_t>(ctx, "grp_ptr", (size_t)dp.G * (K + 1));
-    const int S = group_csr_segment(dp.nnz, dp.G, K);
+    // CSR copy ordered by slice within each gene: 4-byte entries (index in
+    // the slice, 16-bit count) or 8-byte ones for float counts
+    void* gent = ws<char>(ctx, "grp_ent", (size_t)std::max<int64_t>(dp.nnz, 4) * (dp.val_u16 ? 4 : 8));
+    int64_t* gptr = ws<int64_t>(ctx, "grp_ptr", (size_t)dp.G * (NSL + 1));
+    const int S = group_csr_segment(dp.nnz, dp.G, NSL);
     int64_t* segcnt = ws<int64_t>(ctx, "grp_segcnt", dp.G + 1);
     int64_t* segbase = ws<int64_t>(ctx, "grp_segbase", dp.G + 1);
     size_t sb = 0;
@@ -637,9 +682,9 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     int64_t nsegs = 0;
     CK(cudaMemcpyAsync(&nsegs, segbase + dp.G, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    int32_t* hist = ws<int32_t>(ctx, "grp_hist", (size_t)std::max<int64_t>(nsegs, 1) * K);
-    LAUNCH(launch_group_csr(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.G, segbase, S, fkey, K, hist,
-                            nsegs, gptr, gcol, gval, st));
+    int32_t* hist = ws<int32_t>(ctx, "grp_hist", (size_t)std::max<int64_t>(nsegs, 1) * NSL);
+    LAUNCH(launch_group_csr(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.G, segbase, S, cslice, cloc,
+                            NSL, hist, nsegs, gptr, gent, st));
     dbg_mark(ctx, "g.csr");
     CK(cudaMemcpyAsync(h + 1, bad + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -659,15 +704,79 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
                 h[1] ? ": check failed, per-cell engines" : "");
     }
     if (h[1]) return;  // a rule missed its accuracy check: per-cell engines
+    // exp of every rule node's offset (mu = exp(x_u . beta) * exp(s) in the passes)
+    double* res = ws<double>(ctx, "grp_res", (size_t)nrules * kRuleCap);
+    LAUNCH(launch_exp(rs, (int64_t)nrules * kRuleCap, res, st));
+    // Sparse design rows and, per output of the p x p assembly, the groups
+    // whose entries are nonzero (ascending group, so the sums keep a fixed
+    // order).  A one-hot row (intercept, condition, one cell type) has three
+    // nonzeros: six (group, pair) terms instead of p(p+1)/2.
+    std::vector<double> hx((size_t)U * P);
+    CK(cudaMemcpyAsync(hx.data(), xg, hx.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const int NE = P * (P + 1) / 2;
+    std::vector<int32_t> rptr(U + 1, 0), rcol, qptr(NE + 1, 0), qu, vptr(P + 1, 0), vu;
+    std::vector<double> rval, qv, vv;
+    for (int u = 0; u < U; ++u) {
+        for (int j = 0; j < P; ++j)
+            if (hx[(size_t)u * P + j] != 0.0) {
+                rcol.push_back(j);
+                rval.push_back(hx[(size_t)u * P + j]);
+            }
+        rptr[u + 1] = (int32_t)rcol.size();
+    }
+    for (int j = 0; j < P; ++j)
+        for (int i = 0; i <= j; ++i) {
+            for (int u = 0; u < U; ++u) {
+                const double xi = hx[(size_t)u * P + i], xj = hx[(size_t)u * P + j];
+                if (xi != 0.0 && xj != 0.0) {
+                    qu.push_back(u);
+                    qv.push_back(xi * xj);
+                }
+            }
+            qptr[j * (j + 1) / 2 + i + 1] = (int32_t)qu.size();
+        }
+    for (int i = 0; i < P; ++i) {
+        for (int u = 0; u < U; ++u)
+            if (hx[(size_t)u * P + i] != 0.0) {
+                vu.push_back(u);
+                vv.push_back(hx[(size_t)u * P + i]);
+            }
+        vptr[i + 1] = (int32_t)vu.size();
+    }
+    auto up_i = [&](const char* nm, const std::vector<int32_t>& v) {
+        int32_t* d = ws<int32_t>(ctx, nm, std::max<size_t>(v.size(), 1));
+        h2d(ctx, d, v.data(), v.size());
+        return d;
+    };
+    auto up_d = [&](const char* nm, const std::vector<double>& v) {
+        double* d = ws<double>(ctx, nm, std::max<size_t>(v.size(), 1));
+        h2d(ctx, d, v.data(), v.size());
+        return d;
+    };
     auto& g = dp.grp;
+    g.rptr = up_i("grp_rptr", rptr);
+    g.rcol = up_i("grp_rcol", rcol);
+    g.rval = up_d("grp_rval", rval);
+    g.qptr = up_i("grp_qptr", qptr);
+    g.qu = up_i("grp_qu", qu);
+    g.qv = up_d("grp_qv", qv);
+    g.vptr = up_i("grp_vptr", vptr);
+    g.vu = up_i("grp_vu", vu);
+    g.vv = up_d("grp_vv", vv);
+    g.res = res;
+    CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
     g.active = true;
     g.U = U;
     g.C = C;
+    g.S = NSL;
     g.xg = xg;
     g.E = E;
-    g.gcol = gcol;
-    g.gval = gval;
+    g.gent = gent;
     g.gptr = gptr;
+    g.sl_start = d_sl_start;
+    g.sl_key = d_sl_key;
+    g.kslice = d_kslice;
     g.rs = rs;
     g.rw = rw;
     g.rm = rm;
@@ -680,13 +789,26 @@ GrpGeom grp_geom(const DevProblem& dp) {
     gg.U = gr.U;
     gg.C = gr.C;
     gg.xg = gr.xg;
+    gg.S = gr.S;
     gg.E = gr.E;
-    gg.gcol = gr.gcol;
-    gg.gval = gr.gval;
+    gg.gent = gr.gent;
     gg.gptr = gr.gptr;
+    gg.sl_start = gr.sl_start;
+    gg.sl_key = gr.sl_key;
+    gg.kslice = gr.kslice;
     gg.rs = gr.rs;
     gg.rw = gr.rw;
     gg.rm = gr.rm;
+    gg.res = gr.res;
+    gg.rptr = gr.rptr;
+    gg.rcol = gr.rcol;
+    gg.rval = gr.rval;
+    gg.qptr = gr.qptr;
+    gg.qu = gr.qu;
+    gg.qv = gr.qv;
+    gg.vptr = gr.vptr;
+    gg.vu = gr.vu;
+    gg.vv = gr.vv;
     return gg;
 }
 
@@ -837,7 +959,14 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
         gg.partW = static_cast<double*>(pb.partW);
         gg.partS = pb.partS;
         gg.slot_stride = tiles;
-        LAUNCH(launch_grp_pass(kind, gg, prm, dp.val_u16, tiles, ctx->stream));
+        if (kind == PASS_IRLS && !fine && ctx->grp_slices) {
+            // slice-major IRLS pass: per-(gene, slice) sums, then the assembly
+            gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * 2);
+            LAUNCH(launch_grp_irls(gg, prm, dp.val_u16, tiles, grp_irls_tile(tiles, gg.S, ctx->sm_count),
+                                   ctx->stream));
+        } else {
+            LAUNCH(launch_grp_pass(kind, gg, prm, dp.val_u16, tiles, ctx->stream));
+        }
     } else if (plan.engine == ENGINE_REG) {
         LAUNCH(launch_reg_pass(L));
     } else if (plan.engine == ENGINE_TC) {
@@ -868,7 +997,9 @@ void prof_add_bytes(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const i
     int64_t h[2] = {0, 0};
     CK(cudaMemcpyAsync(h, acc, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    const double ebytes = dp.val_u16 ? 6.0 : 8.0;
+    // CSR entries: value + 4-byte cell index; the design-group copy packs a
+    // 16-bit index within the slice with the value (4 B for 16-bit counts)
+    const double ebytes = plan.engine == ENGINE_GRP ? (dp.val_u16 ? 4.0 : 8.0) : (dp.val_u16 ? 6.0 : 8.0);
     const int na = pass_na(kind, dp.P), ns = pass_ns(kind);
     const double per_gene = 4.0 * dp.P + 8.0 + 4.0 * na + 8.0 * ns + 16.0;
     // per launch: the design and offsets, or the group rows, rules and exp(offset)
@@ -1379,6 +1510,8 @@ int devil_ctx_create(int device, devil_ctx** out) {
         // the design-group engine is on unless DEVIL_GROUPS=0 (A/B timing)
         const char* ug = getenv("DEVIL_GROUPS");
         ctx->use_groups = (ug && !atoi(ug)) ? 0 : 1;
+        const char* gsl = getenv("DEVIL_GRP_SLICES");
+        ctx->grp_slices = (gsl && !atoi(gsl)) ? 0 : 1;
         const char* dbg = getenv("DEVIL_DEBUG");
         ctx->debug = (dbg && atoi(dbg)) ? 1 : 0;
         int32_t* err = ws<int32_t>(ctx, "kernel_err", 1);

@@ -90,17 +90,59 @@ constexpr int kRuleCap = kMaxBins * kBinNodes;  // node capacity of one rule
 constexpr int kMaxGroups = 256;       // distinct design rows
 constexpr int kMaxFine = 4096;        // (design row, cluster) pairs
 constexpr int kMinCellsPerGroup = 32; // grouping pays when groups are larger
+constexpr int kSliceCells = 8192;     // cells per slice (its exp(offset) fits shared memory)
+constexpr int kMaxSlices = 12288;     // the CSR copy's per-warp key table stays <= 48 KB
+
+// One entry of the slice-ordered CSR copy of the design-group engine: the
+// cell's index within its slice and the count.
+template <class VT> struct GrpEnt;
+template <> struct GrpEnt<uint16_t> {
+    using T = uint32_t;  // low 16 bits: index within the slice; high 16 bits: the count
+    static __device__ __forceinline__ T pack(int32_t loc, uint16_t v) {
+        return (uint32_t)loc | ((uint32_t)v << 16);
+    }
+    static __device__ __forceinline__ int loc(T e) { return (int)(e & 0xffffu); }
+    static __device__ __forceinline__ float y(T e) { return (float)(e >> 16); }
+};
+template <> struct GrpEnt<float> {
+    using T = uint2;     // x: index within the slice; y: the count's float bits
+    static __device__ __forceinline__ T pack(int32_t loc, float v) {
+        return make_uint2((unsigned)loc, __float_as_uint(v));
+    }
+    static __device__ __forceinline__ int loc(T e) { return (int)e.x; }
+    static __device__ __forceinline__ float y(T e) { return __uint_as_float(e.y); }
+};
+
 struct GrpGeom {
     int P, U, C;           // design columns, groups, clusters folded into the keys (1: none)
+    int S;                 // slices
     int fine;              // 1: groups are (row, cluster) pairs, one output segment per cluster
     const double* xg;      // [U][P] distinct design rows
-    const double* E;       // [n] exp(offset)
-    const int32_t* gcol;   // CSR copy, entries ordered by key u * C + c within each gene
-    const void* gval;
-    const int64_t* gptr;   // [G][U*C + 1] absolute start of every key's entries
+    const double* E;       // [n] exp(offset), cells in slice order
+    const void* gent;      // CSR copy: GrpEnt entries ordered by slice within each gene
+    const int64_t* gptr;   // [G][S + 1] absolute start of every slice's entries
+    const int32_t* sl_start;  // [S + 1] first cell (slice order) of every slice
+    const int32_t* sl_key;    // [S] its key u * C + c
+    const int32_t* kslice;    // [U*C + 1] first slice of every key (slices ordered by key)
+    double* gsum;          // slice-major IRLS: [slots][S][NQ] per-(gene, slice) sums
     const double* rs;      // [rules][kRuleCap] node offsets; rules 0..U-1 coarse, U.. fine
     const double* rw;      // [rules][kRuleCap] node weights
     const int32_t* rm;     // [rules] node counts
+    const double* res;     // [rules][kRuleCap] exp(node offset)
+    // the design rows as sparse rows (nonzero entries of xg, ascending
+    // column), and for every output of the p x p assembly the list of the
+    // groups that contribute to it (ascending group) with their weight:
+    //   outer output q = (i <= j, packed upper triangle): x_ui x_uj
+    //   vector output i: x_ui
+    const int32_t* rptr;   // [U + 1]
+    const int32_t* rcol;
+    const double* rval;
+    const int32_t* qptr;   // [P(P+1)/2 + 1]
+    const int32_t* qu;
+    const double* qv;
+    const int32_t* vptr;   // [P + 1]
+    const int32_t* vu;
+    const double* vv;
     const int32_t* act;
     const int32_t* n_act;
     int32_t* reset_next;
@@ -134,6 +176,16 @@ cudaError_t launch_new_od(const NodArgs& a, const double* Xcm, double* xcolsum, 
 
 cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm, int val_u16,
                             int max_slots, cudaStream_t st);
+// the IRLS pass of the design-group engine, slice-major: a block stages one
+// slice's exp(offset) in shared memory and runs `tile` genes over it, then
+// a block per gene assembles the p x p sums (geo.gsum: slots x S x 2)
+int grp_irls_tile(int64_t hint, int S, int sm_count);
+cudaError_t launch_grp_irls(const GrpGeom& geo, const PassParamsAny& prm, int val_u16, int max_slots,
+                            int tile, cudaStream_t st);
+// cells in key order: sl_cell / sl_loc per original cell, E in slice order
+cudaError_t launch_slice_cells(const int32_t* pnew, const int32_t* sl_start, int S, int64_t n,
+                               const double* off, int32_t* cslice, int32_t* cloc, double* E,
+                               cudaStream_t st);
 cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* ginv, int64_t G,
                                  double* beta, float* beta_f, cudaStream_t st);
 cudaError_t launch_row_hash(const double* X, int64_t n, int P, uint64_t* h, int32_t* idx,
@@ -161,11 +213,12 @@ int group_csr_segment(int64_t nnz, int64_t G, int K);  // entries per segment
 cudaError_t launch_group_segments(const int64_t* rowptr, int64_t G, int S, int64_t* segcnt,
                                   int64_t* segbase, void* scan_tmp, size_t* scan_bytes,
                                   cudaStream_t st);
-// hist: nsegs x K (nsegs = segbase[G])
+// hist: nsegs x K (nsegs = segbase[G]); ckey / cloc: slice and index within
+// the slice of every cell; gent: GrpEnt entries
 cudaError_t launch_group_csr(const int64_t* rowptr, const int32_t* col, const void* val, int val_u16,
-                             int64_t G, const int64_t* segbase, int S, const int32_t* fkey, int K,
-                             int32_t* hist, int64_t nsegs, int64_t* gptr, int32_t* gcol,
-                             void* gval, cudaStream_t st);
+                             int64_t G, const int64_t* segbase, int S, const int32_t* ckey,
+                             const int32_t* cloc, int K, int32_t* hist, int64_t nsegs,
+                             int64_t* gptr, void* gent, cudaStream_t st);
 
 // ---- preparation kernels (kernels_prep.cu) ----
 cudaError_t launch_dense_count(const void* Y, int is_f64, int cell_major, int64_t G, int64_t n,

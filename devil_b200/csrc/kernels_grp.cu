@@ -10,11 +10,17 @@
 //     as a Gauss rule for the group's offsets: bins of width 2 in the
 //     offset, each with its cells as nodes (at most 10 cells) or a 10-point
 //     Gauss rule; checked against exact sums before use;
-//   * the corrections of the nonzero counts from the group's range of a
-//     CSR copy whose entries are ordered by group within each gene;
-// and assembles the p x p terms once per group.  A pass then reads every
-// nonzero once and costs O(groups x (nodes + p^2)) per gene instead of
-// O(cells x p^2).  Partial sums land in the layout of the other engines
+//   * the corrections of the nonzero counts from a CSR copy in which every
+//     gene's entries are ordered by "slice": the cells are renumbered so
+//     that each (design row, cluster) group is a contiguous range, cut into
+//     slices of at most kSliceCells cells; an entry is 4 bytes (the cell's
+//     16-bit index within its slice and the 16-bit count), and exp(offset)
+//     is stored in the new cell order, so one slice's values fit in shared
+//     memory;
+// and assembles the p x p terms from the group sums.  A pass then reads
+// every nonzero once and costs O(nnz + groups x nodes) per gene, plus the
+// assembly over the (group, output) pairs whose design entries are nonzero
+// (for one-hot rows: a handful per group), instead of O(cells x p^2).  Partial sums land in the layout of the other engines
 // (FP64, one segment, or one per cluster for the sandwich), so the
 // finalize kernels are shared.
 #include <cub/cub.cuh>
@@ -390,7 +396,7 @@ DEV int64_t seg_gene(const int64_t* segbase, int64_t G, int64_t s) {
 }
 
 __global__ void seg_hist_kernel(const int64_t* rowptr, const int32_t* col, int64_t G,
-                                const int64_t* segbase, int S, const int32_t* fkey, int K,
+                                const int64_t* segbase, int S, const int32_t* ckey, int K,
                                 int32_t* hist) {
     extern __shared__ int32_t cnt_all[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -402,7 +408,7 @@ __global__ void seg_hist_kernel(const int64_t* rowptr, const int32_t* col, int64
     const int64_t g = seg_gene(segbase, G, s);
     const int64_t r0 = rowptr[g] + (s - segbase[g]) * S;
     const int64_t r1 = min(r0 + S, rowptr[g + 1]);
-    for (int64_t e = r0 + lane; e < r1; e += 32) atomicAdd(&cnt[fkey[col[e]]], 1);
+    for (int64_t e = r0 + lane; e < r1; e += 32) atomicAdd(&cnt[ckey[col[e]]], 1);
     __syncwarp();
     int32_t* h = hist + s * K;
     for (int k = lane; k < K; k += 32) h[k] = cnt[k];
@@ -440,8 +446,9 @@ __global__ void __launch_bounds__(kOffNT) seg_offsets_kernel(const int64_t* rowp
 
 template <class VT>
 __global__ void seg_scatter_kernel(const int64_t* rowptr, const int32_t* col, const VT* val,
-                                   int64_t G, const int64_t* segbase, int S, const int32_t* fkey,
-                                   int K, const int32_t* hist, int32_t* gcol, VT* gval) {
+                                   int64_t G, const int64_t* segbase, int S, const int32_t* ckey,
+                                   const int32_t* cloc, int K, const int32_t* hist,
+                                   typename GrpEnt<VT>::T* gent) {
     extern __shared__ int32_t cur_all[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
@@ -463,15 +470,14 @@ __global__ void seg_scatter_kernel(const int64_t* rowptr, const int32_t* col, co
         if (valid) {
             c = col[e];
             v = val[e];
-            k = fkey[c];
+            k = ckey[c];
         }
         const unsigned peers = __match_any_sync(0xffffffffu, k);
         const int rank = __popc(peers & lt);
         const int pos = valid ? cur[k] + rank : 0;
         __syncwarp();
         if (valid) {
-            gcol[rs + pos] = c;
-            gval[rs + pos] = v;
+            gent[rs + pos] = GrpEnt<VT>::pack(cloc[c], v);
             if (lane == __ffs(peers) - 1) cur[k] += __popc(peers);
         }
         __syncwarp();
@@ -507,26 +513,40 @@ struct GrpAcc {
 
 constexpr int kGrpUnr = 8;          // entries per lane per batch of the nonzero loop
 constexpr int kGrpChunk = 2048;     // nonzeros per work unit (at least)
-constexpr int kGrpUnitsMax = 128;   // chunks beyond one per group, per gene
+constexpr int kGrpUnitsMax = 128;   // chunks beyond one per slice, per gene
 
+// x_u . beta over the nonzero entries of design row u (warp-wide sum)
+DEV double row_dot(const GrpGeom& geo, int u, const double* bet, int lane) {
+    double a = 0.0;
+    const int r1 = __ldg(geo.rptr + u + 1);
+    for (int e = __ldg(geo.rptr + u) + lane; e < r1; e += 32) a += __ldg(geo.rval + e) * bet[__ldg(geo.rcol + e)];
+    return warp_sum(a);
+}
+
+// The design-group pass, block per gene (MOM, MLE, bread/meat; the IRLS
+// pass runs slice-major, grp_irls_slices_kernel).  Work units of a gene:
+// one "rule unit" per group q (the zero-count terms of the group's cells
+// from its Gauss rule), then the gene's nonzeros slice by slice in chunks of
+// at least kGrpChunk entries.  Warps take units round robin; the group sums
+// are then formed in unit order (deterministic) and assembled.
 template <class Pass, class VT>
 __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pass::Params prm) {
+    using Ent = GrpEnt<VT>;
+    using ET = typename Ent::T;
     constexpr int NW = Pass::NW, NV = Pass::NV, NF = Pass::NF;
     constexpr int NWV = NW + NV + NF, NS = Pass::NS, NQ = NWV + NS;
     if (geo.reset_next && blockIdx.x == 0 && threadIdx.x == 0) *geo.reset_next = 0;
     const int slot = blockIdx.x;
     if (slot >= *geo.n_act) return;
     const int g = __ldg(geo.act + slot);
-    const int P = geo.P, U = geo.U, C = geo.C, K = U * C;
-    const int NGq = geo.fine ? K : U;
+    const int P = geo.P, U = geo.U, C = geo.C, S = geo.S;
+    const int NGq = geo.fine ? U * C : U;
     extern __shared__ double gsm[];
-    double* xg = gsm;          // [U][P]
-    double* bet = xg + U * P;              // [P]
-    double* gs = bet + P;                  // [NGq][NQ] group sums
-    double* up = gs + NGq * NQ;            // [NGq + kGrpUnitsMax][NQ] unit sums
-    int* ustart = reinterpret_cast<int*>(up + (NGq + kGrpUnitsMax) * NQ);  // [NGq + 1]
+    double* bet = gsm;                                   // [P]
+    double* gs = bet + P;                                // [NGq][NQ] group sums
+    double* up = gs + NGq * NQ;                          // [NGq + S + kGrpUnitsMax][NQ] unit sums
+    int* sstart = reinterpret_cast<int*>(up + (NGq + S + kGrpUnitsMax) * NQ);  // [S + 1]
     const int t = threadIdx.x, nt = blockDim.x;
-    for (int i = t; i < U * P; i += nt) xg[i] = __ldg(geo.xg + i);
     for (int i = t; i < P; i += nt) bet[i] = __ldg(prm.beta_d + (int64_t)g * P + i);
     typename Pass::Gene gpar = Pass::load(prm, g);
     if constexpr (Pass::TABLES) {
@@ -541,26 +561,20 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
         gpar.tab.pa = digamma_d(gpar.a);
         gpar.tab.ta = trigamma_d(gpar.a);
     }
-    __syncthreads();
     const int warp = t >> 5, lane = t & 31, nw = nt >> 5;
-    const VT* __restrict__ gval = static_cast<const VT*>(geo.gval);
-    const int64_t* gp = geo.gptr + (int64_t)g * (K + 1);
-    // Work units: group q's nonzeros in chunks of CH entries (at least one
-    // unit per group; its first unit also takes the rule nodes).  CH grows
-    // with the gene's nonzeros so there are at most NGq + kGrpUnitsMax
-    // units; warps take units round robin, so a large group no longer
-    // holds one warp while the others wait at the assembly barrier.
-    const int64_t CH = max((int64_t)kGrpChunk, (gp[K] - gp[0] + kGrpUnitsMax - 1) / kGrpUnitsMax);
+    const ET* __restrict__ gent = static_cast<const ET*>(geo.gent);
+    const int64_t* gp = geo.gptr + (int64_t)g * (S + 1);
+    // chunk size grows with the gene's nonzeros so that there are at most
+    // S + kGrpUnitsMax nonzero units
+    const int64_t CH = max((int64_t)kGrpChunk, (gp[S] - gp[0] + kGrpUnitsMax - 1) / kGrpUnitsMax);
     if (warp == 0) {
         int run = 0;
-        for (int base = 0; base < NGq; base += 32) {
-            const int q = base + lane;
+        for (int base = 0; base < S; base += 32) {
+            const int sl = base + lane;
             int c = 0;
-            if (q < NGq) {
-                const int uq = geo.fine ? q / C : q;
-                const int64_t len = __ldg(gp + (geo.fine ? q + 1 : uq * C + C)) -
-                                    __ldg(gp + (geo.fine ? q : uq * C));
-                c = len > CH ? (int)((len + CH - 1) / CH) : 1;
+            if (sl < S) {
+                const int64_t len = __ldg(gp + sl + 1) - __ldg(gp + sl);
+                c = (int)((len + CH - 1) / CH);
             }
             int incl = c;
 #pragma unroll
@@ -568,87 +582,78 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
                 const int v = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += v;
             }
-            if (q < NGq) ustart[q] = run + incl - c;
+            if (sl < S) sstart[sl] = run + incl - c;
             run += __shfl_sync(0xffffffffu, incl, 31);
         }
-        if (lane == 0) ustart[NGq] = run;
+        if (lane == 0) sstart[S] = run;
     }
     __syncthreads();
-    const int nunits = ustart[NGq];
+    const int nunits = NGq + sstart[S];
     for (int un = warp; un < nunits; un += nw) {
-        int q = 0;  // last group with ustart[q] <= un
-        {
-            int lo = 0, hi = NGq;
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (ustart[mid] <= un) lo = mid; else hi = mid;
-            }
-            q = lo;
-        }
-        const int jc = un - ustart[q];
-        const int u = geo.fine ? q / C : q;
-        double a = lane < P ? xg[u * P + lane] * bet[lane] : 0.0;
-        a = warp_sum(a);
-        const double A = exp(a);
         GrpAcc<NWV, NS> acc;
         acc.zero();
-        // zero-count terms over all cells of the group: the group's rule
-        const int ri = (geo.fine && C > 1) ? U + q : u;  // C == 1: fine == coarse
-        const int m = jc == 0 ? __ldg(geo.rm + ri) : 0;
-        for (int j = lane; j < m; j += 32) {
-            acc.q = __ldg(geo.rw + (int64_t)ri * kRuleCap + j);
-            const double mu = exp(a + __ldg(geo.rs + (int64_t)ri * kRuleCap + j));
-            Pass::template dense<double>(gpar, mu, acc);
-        }
-        acc.q = 1.0;
-        // nonzero corrections over the group's CSR range
-        const int64_t g0 = __ldg(gp + (geo.fine ? q : u * C));
-        const int64_t g1 = __ldg(gp + (geo.fine ? q + 1 : u * C + C));
-        const int64_t e0 = g0 + jc * CH;
-        const int64_t e1 = min(e0 + CH, g1);
-        // batches of kGrpUnr entries per lane, software-pipelined: the next
-        // batch's cell indices and counts are in flight while this batch
-        // gathers exp(offset) and accumulates
-        int64_t e = e0 + lane;
-        constexpr int U8 = kGrpUnr;
-        if (e + 32 * (U8 - 1) < e1) {
-            int c[U8];
-            float y[U8];
-#pragma unroll
-            for (int j = 0; j < U8; ++j) {
-                c[j] = __ldg(geo.gcol + e + 32 * j);
-                y[j] = load_val(gval, e + 32 * j);
+        if (un < NGq) {
+            // zero-count terms of every cell of group q: its rule
+            const int q = un;
+            const int u = geo.fine ? q / C : q;
+            const int ri = (geo.fine && C > 1) ? U + q : u;  // C == 1: fine == coarse
+            const double A = exp(row_dot(geo, u, bet, lane));
+            const int m = __ldg(geo.rm + ri);
+            for (int j = lane; j < m; j += 32) {
+                acc.q = __ldg(geo.rw + (int64_t)ri * kRuleCap + j);
+                const double mu = A * __ldg(geo.res + (int64_t)ri * kRuleCap + j);
+                Pass::template dense<double>(gpar, mu, acc);
             }
-            for (;;) {
-                double ev[U8];
+        } else {
+            // a chunk of the nonzeros of slice sl
+            const int cu = un - NGq;
+            int sl = 0;  // last slice with sstart[sl] <= cu
+            {
+                int lo = 0, hi = S;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (sstart[mid] <= cu) lo = mid; else hi = mid;
+                }
+                sl = lo;
+            }
+            const int jc = cu - sstart[sl];
+            const int u = __ldg(geo.sl_key + sl) / C;
+            const double A = exp(row_dot(geo, u, bet, lane));
+            const double* __restrict__ Es = geo.E + __ldg(geo.sl_start + sl);
+            const int64_t e0 = __ldg(gp + sl) + jc * CH;
+            const int64_t e1 = min(e0 + CH, __ldg(gp + sl + 1));
+            // batches of kGrpUnr entries per lane, software-pipelined: the
+            // next batch's entries are in flight while this batch gathers
+            // exp(offset) and accumulates
+            int64_t e = e0 + lane;
+            constexpr int U8 = kGrpUnr;
+            if (e + 32 * (U8 - 1) < e1) {
+                ET c[U8];
 #pragma unroll
-                for (int j = 0; j < U8; ++j) ev[j] = __ldg(geo.E + c[j]);
-                const int64_t en = e + 32 * U8;
-                const bool more = en + 32 * (U8 - 1) < e1;
-                int cn[U8];
-                float yn[U8];
-                if (more) {
+                for (int j = 0; j < U8; ++j) c[j] = gent[e + 32 * j];
+                for (;;) {
+                    double ev[U8];
 #pragma unroll
-                    for (int j = 0; j < U8; ++j) {
-                        cn[j] = __ldg(geo.gcol + en + 32 * j);
-                        yn[j] = load_val(gval, en + 32 * j);
+                    for (int j = 0; j < U8; ++j) ev[j] = __ldg(Es + Ent::loc(c[j]));
+                    const int64_t en = e + 32 * U8;
+                    const bool more = en + 32 * (U8 - 1) < e1;
+                    ET cn[U8];
+                    if (more) {
+#pragma unroll
+                        for (int j = 0; j < U8; ++j) cn[j] = gent[en + 32 * j];
                     }
-                }
 #pragma unroll
-                for (int j = 0; j < U8; ++j) Pass::template sparse<double>(gpar, A * ev[j], y[j], acc);
-                e = en;
-                if (!more) break;
+                    for (int j = 0; j < U8; ++j) Pass::template sparse<double>(gpar, A * ev[j], Ent::y(c[j]), acc);
+                    e = en;
+                    if (!more) break;
 #pragma unroll
-                for (int j = 0; j < U8; ++j) {
-                    c[j] = cn[j];
-                    y[j] = yn[j];
+                    for (int j = 0; j < U8; ++j) c[j] = cn[j];
                 }
             }
-        }
-        for (; e < e1; e += 32) {
-            const int c = __ldg(geo.gcol + e);
-            const float y = load_val(gval, e);
-            Pass::template sparse<double>(gpar, A * __ldg(geo.E + c), y, acc);
+            for (; e < e1; e += 32) {
+                const ET c = gent[e];
+                Pass::template sparse<double>(gpar, A * __ldg(Es + Ent::loc(c)), Ent::y(c), acc);
+            }
         }
 #pragma unroll
         for (int i = 0; i < NWV; ++i) {
@@ -662,11 +667,14 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
         }
     }
     __syncthreads();
-    // group sums over their units, in unit order (deterministic)
+    // group sums in unit order: the rule unit, then the chunks of the
+    // group's slices (slices are ordered by key u * C + c)
     for (int i = t; i < NGq * NQ; i += nt) {
         const int q = i / NQ, c = i - q * NQ;
-        double v = 0.0;
-        for (int un = ustart[q]; un < ustart[q + 1]; ++un) v += up[un * NQ + c];
+        double v = up[q * NQ + c];
+        const int k0 = geo.fine ? q : q * C, k1 = geo.fine ? q + 1 : q * C + C;
+        const int s0 = __ldg(geo.kslice + k0), s1 = __ldg(geo.kslice + k1);
+        for (int un = sstart[s0]; un < sstart[s1]; ++un) v += up[(NGq + un) * NQ + c];
         gs[i] = v;
     }
     __syncthreads();
@@ -679,20 +687,20 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
         const int seg = o / per, a = o - seg * per;
         double s = 0.0;
         if (a < NW * NE) {
+            // the groups whose design entries i and j are both nonzero
             const int w = a / NE, qq = a - w * NE;
-            int j = 0;
-            while ((j + 1) * (j + 2) / 2 <= qq) ++j;
-            const int i = qq - j * (j + 1) / 2;
-            for (int u = 0; u < U; ++u) {
+            for (int e = __ldg(geo.qptr + qq); e < __ldg(geo.qptr + qq + 1); ++e) {
+                const int u = __ldg(geo.qu + e);
                 const int q = geo.fine ? u * C + seg : u;
-                s += gs[q * NQ + w] * (xg[u * P + i] * xg[u * P + j]);
+                s += gs[q * NQ + w] * __ldg(geo.qv + e);
             }
         } else if (a < NW * NE + NV * P) {
             const int r = a - NW * NE;
             const int v = r / P, i = r - v * P;
-            for (int u = 0; u < U; ++u) {
+            for (int e = __ldg(geo.vptr + i); e < __ldg(geo.vptr + i + 1); ++e) {
+                const int u = __ldg(geo.vu + e);
                 const int q = geo.fine ? u * C + seg : u;
-                s += gs[q * NQ + NW + v] * xg[u * P + i];
+                s += gs[q * NQ + NW + v] * __ldg(geo.vv + e);
             }
         } else {
             const int f = a - NW * NE - NV * P;  // fscal (a < NA) or an FP64 scalar
@@ -709,33 +717,190 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
     }
 }
 
+// ---------------------------------------------------------------------
+// IRLS pass, slice-major.  Block (slice s, tile of active genes): the
+// slice's exp(offset) values are staged in shared memory once, then each
+// warp takes the tile's genes in turn: A = exp(x_u . beta), the rule terms
+// of group u when s is the group's first slice, and the gene's entries of
+// the slice streamed as 16-byte loads (4 entries each for 16-bit counts),
+// exp(offset) read from shared memory.  The per-(gene, slice) sums go to
+// geo.gsum; grp_assemble_kernel forms the p x p terms per gene.
+// ---------------------------------------------------------------------
+constexpr int kSlNT = 512;
+
+// streaming 16-byte load that does not allocate in L1 (each entry is read
+// once per pass)
+DEV uint4 ld_stream(const uint4* p) {
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+
+template <class VT>
+__global__ void __launch_bounds__(kSlNT) grp_irls_slices_kernel(GrpGeom geo, PassIRLS::Params prm,
+                                                                int tile) {
+    using Ent = GrpEnt<VT>;
+    using ET = typename Ent::T;
+    constexpr int EPL = sizeof(uint4) / sizeof(ET);  // entries per 16-byte load
+    if (geo.reset_next && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *geo.reset_next = 0;
+    const int nact = *geo.n_act;
+    const int j0 = blockIdx.y * tile;
+    if (j0 >= nact) return;
+    const int j1 = min(nact, j0 + tile);
+    const int s = blockIdx.x, S = geo.S, P = geo.P;
+    extern __shared__ double Es[];  // [kSliceCells] exp(offset) of the slice's cells
+    __shared__ double bet[32][32];  // per warp: beta of its current gene
+    const int c0 = __ldg(geo.sl_start + s), nc = __ldg(geo.sl_start + s + 1) - c0;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
+    for (int i = t; i < nc; i += blockDim.x) Es[i] = __ldg(geo.E + c0 + i);
+    const int u = __ldg(geo.sl_key + s) / geo.C;
+    const bool first = s == __ldg(geo.kslice + u * geo.C);  // the group's rule goes here
+    const int m = first ? __ldg(geo.rm + u) : 0;
+    __syncthreads();
+    const ET* __restrict__ gent = static_cast<const ET*>(geo.gent);
+    for (int jj = j0 + warp; jj < j1; jj += nw) {
+        const int g = __ldg(geo.act + jj);
+        if (lane < P) bet[warp][lane] = __ldg(prm.beta_d + (int64_t)g * P + lane);
+        __syncwarp();
+        const double A = exp(row_dot(geo, u, bet[warp], lane));
+        const PassIRLS::Gene gpar = PassIRLS::load(prm, g);
+        GrpAcc<2, 0> acc;
+        acc.zero();
+        for (int j = lane; j < m; j += 32) {
+            acc.q = __ldg(geo.rw + (int64_t)u * kRuleCap + j);
+            PassIRLS::dense<double>(gpar, A * __ldg(geo.res + (int64_t)u * kRuleCap + j), acc);
+        }
+        acc.q = 1.0;
+        const int64_t* gp = geo.gptr + (int64_t)g * (S + 1) + s;
+        const int64_t e0 = __ldg(gp), e1 = __ldg(gp + 1);
+        // entries up to the first 16-byte boundary, whole 16-byte groups,
+        // the rest
+        const int64_t a0 = min(e1, (e0 + EPL - 1) / EPL * EPL);
+        const int64_t a1 = max(a0, e1 / EPL * EPL);
+        if (e0 + lane < a0) {
+            const ET c = gent[e0 + lane];
+            PassIRLS::sparse<double>(gpar, A * Es[Ent::loc(c)], Ent::y(c), acc);
+        }
+        const uint4* v4 = reinterpret_cast<const uint4*>(gent);
+        for (int64_t b = a0 / EPL + lane; b < a1 / EPL; b += 32) {
+            const uint4 v = ld_stream(v4 + b);
+            const ET* c = reinterpret_cast<const ET*>(&v);
+#pragma unroll
+            for (int q = 0; q < EPL; ++q)
+                PassIRLS::sparse<double>(gpar, A * Es[Ent::loc(c[q])], Ent::y(c[q]), acc);
+        }
+        if (a1 + lane < e1) {
+            const ET c = gent[a1 + lane];
+            PassIRLS::sparse<double>(gpar, A * Es[Ent::loc(c)], Ent::y(c), acc);
+        }
+        const double w0 = warp_sum(acc.w[0]), w1 = warp_sum(acc.w[1]);
+        if (lane == 0) {
+            double* o = geo.gsum + ((int64_t)jj * S + s) * 2;
+            o[0] = w0;
+            o[1] = w1;
+        }
+        __syncwarp();
+    }
+}
+
+// Per active gene: group sums over the gene's slices (in slice order) and
+// the p x p assembly of the IRLS pass (outer0 and vec0, one segment).
+__global__ void __launch_bounds__(256) grp_assemble_irls_kernel(GrpGeom geo) {
+    const int slot = blockIdx.x;
+    if (slot >= *geo.n_act) return;
+    const int P = geo.P, U = geo.U, C = geo.C, S = geo.S;
+    extern __shared__ double gs[];  // [U][2]
+    const int t = threadIdx.x, nt = blockDim.x;
+    const double* gsum = geo.gsum + (int64_t)slot * S * 2;
+    for (int i = t; i < U * 2; i += nt) {
+        const int q = i >> 1, c = i & 1;
+        double v = 0.0;
+        for (int sl = __ldg(geo.kslice + q * C); sl < __ldg(geo.kslice + q * C + C); ++sl)
+            v += gsum[sl * 2 + c];
+        gs[i] = v;
+    }
+    __syncthreads();
+    const int NE = P * (P + 1) / 2;
+    const int NA = NE + P;
+    for (int a = t; a < NA; a += nt) {
+        double s = 0.0;
+        if (a < NE) {
+            for (int e = __ldg(geo.qptr + a); e < __ldg(geo.qptr + a + 1); ++e)
+                s += gs[__ldg(geo.qu + e) * 2] * __ldg(geo.qv + e);
+        } else {
+            const int i = a - NE;
+            for (int e = __ldg(geo.vptr + i); e < __ldg(geo.vptr + i + 1); ++e)
+                s += gs[__ldg(geo.vu + e) * 2 + 1] * __ldg(geo.vv + e);
+        }
+        geo.partW[(int64_t)slot * NA + a] = s;
+    }
+}
+
+int grp_irls_tile(int64_t hint, int S, int sm_count) {
+    // about six blocks per SM over the whole grid, tiles of 32..1024 genes
+    const int64_t want = (hint * S + (int64_t)sm_count * 6 - 1) / ((int64_t)sm_count * 6);
+    return (int)std::max<int64_t>(32, std::min<int64_t>(1024, want));
+}
+
+cudaError_t launch_grp_irls(const GrpGeom& geo, const PassParamsAny& pa, int val_u16, int max_slots,
+                            int tile, cudaStream_t st) {
+    if (max_slots <= 0) return cudaSuccess;
+    PassIRLS::Params prm{pa.beta, pa.beta_d, pa.k};
+    const size_t smem = (size_t)kSliceCells * sizeof(double);
+    dim3 grid((unsigned)geo.S, (unsigned)((max_slots + tile - 1) / tile));
+    cudaError_t e;
+    if (val_u16) {
+        auto k = grp_irls_slices_kernel<uint16_t>;
+        e = raise_dyn_smem(k, smem);
+        if (e != cudaSuccess) return e;
+        k<<<grid, kSlNT, smem, st>>>(geo, prm, tile);
+    } else {
+        auto k = grp_irls_slices_kernel<float>;
+        e = raise_dyn_smem(k, smem);
+        if (e != cudaSuccess) return e;
+        k<<<grid, kSlNT, smem, st>>>(geo, prm, tile);
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    grp_assemble_irls_kernel<<<(unsigned)max_slots, 256, (size_t)geo.U * 2 * sizeof(double), st>>>(geo);
+    return cudaGetLastError();
+}
+
 // init_beta (R/beta.R:12-24) on a grouped design: X' z with
 // z = log1p(y / exp(offset)) (zero where y = 0) is sum_u x_u sum_{i in u,
 // y_i > 0} z_i, so the nonzeros are read once and summed per group;
 // beta_0 = (X'X)^-1 X' z.  Block per gene, warps over groups.
 template <class VT>
-__global__ void grp_init_beta_kernel(const int64_t* gptr, const int32_t* gcol, const VT* gval,
-                                     const double* E, const double* xg, int U, int C, int P,
-                                     const double* ginv, int64_t G, double* beta, float* beta_f) {
+__global__ void grp_init_beta_kernel(GrpGeom geo, const double* ginv, int64_t G, double* beta,
+                                     float* beta_f) {
+    using Ent = GrpEnt<VT>;
+    using ET = typename Ent::T;
     __shared__ double su[kMaxGroups];
     __shared__ double r[32];
     const int64_t g = blockIdx.x;
     if (g >= G) return;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
-    const int K = U * C;
-    const int64_t* gp = gptr + g * (K + 1);
+    const int U = geo.U, C = geo.C, P = geo.P, S = geo.S;
+    const int64_t* gp = geo.gptr + g * (S + 1);
+    const ET* gent = static_cast<const ET*>(geo.gent);
     for (int u = warp; u < U; u += nw) {
-        const int64_t e0 = gp[u * C], e1 = gp[u * C + C];
         double z = 0.0;
-        for (int64_t e = e0 + lane; e < e1; e += 32)
-            z += log1p((double)load_val(gval, e) / E[gcol[e]]);
+        for (int sl = __ldg(geo.kslice + u * C); sl < __ldg(geo.kslice + u * C + C); ++sl) {
+            const double* Es = geo.E + __ldg(geo.sl_start + sl);
+            for (int64_t e = gp[sl] + lane; e < gp[sl + 1]; e += 32) {
+                const ET c = gent[e];
+                z += log1p((double)Ent::y(c) / Es[Ent::loc(c)]);
+            }
+        }
         z = warp_sum(z);
         if (lane == 0) su[u] = z;
     }
     __syncthreads();
     if (t < P) {
         double v = 0.0;
-        for (int u = 0; u < U; ++u) v += xg[u * P + t] * su[u];
+        for (int u = 0; u < U; ++u) v += geo.xg[u * P + t] * su[u];
         r[t] = v;
     }
     __syncthreads();
@@ -752,13 +917,9 @@ cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* 
     if (G <= 0) return cudaSuccess;
     const int nt = 32 * (geo.U < 8 ? (geo.U < 1 ? 1 : geo.U) : 8);
     if (val_u16)
-        grp_init_beta_kernel<uint16_t><<<(unsigned)G, nt, 0, st>>>(
-            geo.gptr, geo.gcol, static_cast<const uint16_t*>(geo.gval), geo.E, geo.xg, geo.U, geo.C,
-            geo.P, ginv, G, beta, beta_f);
+        grp_init_beta_kernel<uint16_t><<<(unsigned)G, nt, 0, st>>>(geo, ginv, G, beta, beta_f);
     else
-        grp_init_beta_kernel<float><<<(unsigned)G, nt, 0, st>>>(
-            geo.gptr, geo.gcol, static_cast<const float*>(geo.gval), geo.E, geo.xg, geo.U, geo.C,
-            geo.P, ginv, G, beta, beta_f);
+        grp_init_beta_kernel<float><<<(unsigned)G, nt, 0, st>>>(geo, ginv, G, beta, beta_f);
     return cudaGetLastError();
 }
 
@@ -769,30 +930,23 @@ template <> PassMOM::Params grp_params<PassMOM>(const PassParamsAny& a) { return
 template <> PassMLE::Params grp_params<PassMLE>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.log_theta}; }
 template <> PassSandwich::Params grp_params<PassSandwich>(const PassParamsAny& a) { return {a.beta, a.beta_d, a.theta}; }
 
-size_t grp_smem_bytes(PassKind k, int P, int U, int NGq) {
+size_t grp_smem_bytes(PassKind k, int P, int NGq, int S) {
     const int nq = pass_nw(k) + pass_nv(k) + pass_nf(k) + pass_ns(k);
-    return ((size_t)U * P + P + (size_t)NGq * nq + (size_t)(NGq + kGrpUnitsMax) * nq) *
-               sizeof(double) +
-           (size_t)(NGq + 1) * sizeof(int);
-}
-
-int grp_threads(int NGq) {
-    (void)NGq;  // work units split large groups: 8 warps always have work
-    return 256;
+    return ((size_t)P + (size_t)NGq * nq + (size_t)(NGq + S + kGrpUnitsMax) * nq) * sizeof(double) +
+           (size_t)(S + 1) * sizeof(int);
 }
 
 template <class Pass>
 static cudaError_t grp_run(const GrpGeom& geo, const PassParamsAny& pa, PassKind kind, int val_u16,
                            int max_slots, cudaStream_t st) {
     const int NGq = geo.fine ? geo.U * geo.C : geo.U;
-    const size_t smem = grp_smem_bytes(kind, geo.P, geo.U, NGq);
-    const int nt = grp_threads(NGq);
+    const size_t smem = grp_smem_bytes(kind, geo.P, NGq, geo.S);
     auto prm = grp_params<Pass>(pa);
     auto go = [&](auto kern) -> cudaError_t {
         // static shared memory (psi tables) counts against the 48 KB default
         cudaError_t e = raise_dyn_smem(kern, smem);
         if (e != cudaSuccess) return e;
-        kern<<<(unsigned)max_slots, nt, smem, st>>>(geo, prm);
+        kern<<<(unsigned)max_slots, 256, smem, st>>>(geo, prm);
         return cudaGetLastError();
     };
     return val_u16 ? go(grp_pass_kernel<Pass, uint16_t>) : go(grp_pass_kernel<Pass, float>);
@@ -808,6 +962,32 @@ cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsA
         case PASS_SANDWICH: return grp_run<PassSandwich>(geo, prm, kind, val_u16, max_slots, st);
     }
     return cudaErrorInvalidValue;
+}
+
+// cells in slice order: for position i of the key-sorted cells (pnew[i] is
+// the original cell), its slice (the last with sl_start <= i), its index in
+// the slice, and exp(offset) in slice order
+__global__ void slice_cells_kernel(const int32_t* pnew, const int32_t* sl_start, int S, int64_t n,
+                                   const double* off, int32_t* cslice, int32_t* cloc, double* E) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int lo = 0, hi = S;  // sl_start[lo] <= i < sl_start[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (sl_start[mid] <= i) lo = mid; else hi = mid;
+    }
+    const int c = pnew[i];
+    cslice[c] = lo;
+    cloc[c] = (int32_t)(i - sl_start[lo]);
+    E[i] = exp(off[c]);
+}
+
+cudaError_t launch_slice_cells(const int32_t* pnew, const int32_t* sl_start, int S, int64_t n,
+                               const double* off, int32_t* cslice, int32_t* cloc, double* E,
+                               cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    slice_cells_kernel<<<nblk(n, 256), 256, 0, st>>>(pnew, sl_start, S, n, off, cslice, cloc, E);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------
@@ -878,25 +1058,25 @@ cudaError_t launch_group_segments(const int64_t* rowptr, int64_t G, int S, int64
 }
 
 cudaError_t launch_group_csr(const int64_t* rowptr, const int32_t* col, const void* val, int val_u16,
-                             int64_t G, const int64_t* segbase, int S, const int32_t* fkey, int K,
-                             int32_t* hist, int64_t nsegs, int64_t* gptr, int32_t* gcol,
-                             void* gval, cudaStream_t st) {
+                             int64_t G, const int64_t* segbase, int S, const int32_t* ckey,
+                             const int32_t* cloc, int K, int32_t* hist, int64_t nsegs,
+                             int64_t* gptr, void* gent, cudaStream_t st) {
     if (G <= 0) return cudaSuccess;
     int wpb = 12288 / K;  // 48 KB of per-warp key tables per block
     wpb = wpb < 1 ? 1 : (wpb > 8 ? 8 : wpb);
     const size_t smem = (size_t)wpb * K * sizeof(int32_t);
     const unsigned grid = (unsigned)((nsegs + wpb - 1) / wpb);
-    if (grid > 0) seg_hist_kernel<<<grid, 32 * wpb, smem, st>>>(rowptr, col, G, segbase, S, fkey, K, hist);
+    if (grid > 0) seg_hist_kernel<<<grid, 32 * wpb, smem, st>>>(rowptr, col, G, segbase, S, ckey, K, hist);
     seg_offsets_kernel<<<(unsigned)G, kOffNT, 0, st>>>(rowptr, G, segbase, K, hist, gptr);
     if (grid > 0) {
         if (val_u16)
             seg_scatter_kernel<uint16_t><<<grid, 32 * wpb, smem, st>>>(
-                rowptr, col, static_cast<const uint16_t*>(val), G, segbase, S, fkey, K, hist, gcol,
-                static_cast<uint16_t*>(gval));
+                rowptr, col, static_cast<const uint16_t*>(val), G, segbase, S, ckey, cloc, K, hist,
+                static_cast<GrpEnt<uint16_t>::T*>(gent));
         else
             seg_scatter_kernel<float><<<grid, 32 * wpb, smem, st>>>(
-                rowptr, col, static_cast<const float*>(val), G, segbase, S, fkey, K, hist, gcol,
-                static_cast<float*>(gval));
+                rowptr, col, static_cast<const float*>(val), G, segbase, S, ckey, cloc, K, hist,
+                static_cast<GrpEnt<float>::T*>(gent));
     }
     return cudaGetLastError();
 }
