@@ -959,11 +959,11 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
         gg.partW = static_cast<double*>(pb.partW);
         gg.partS = pb.partS;
         gg.slot_stride = tiles;
-        if (kind == PASS_IRLS && !fine && ctx->grp_slices) {
-            // slice-major IRLS pass: per-(gene, slice) sums, then the assembly
-            gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * 2);
-            LAUNCH(launch_grp_irls(gg, prm, dp.val_u16, tiles, grp_irls_tile(tiles, gg.S, ctx->sm_count),
-                                   ctx->stream));
+        if ((kind == PASS_IRLS || kind == PASS_MLE) && !fine && ctx->grp_slices) {
+            // slice-major pass: per-(gene, slice) sums, then the assembly
+            gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * grp_slices_nq(kind));
+            LAUNCH(launch_grp_slices(kind, gg, prm, dp.val_u16, tiles,
+                                     grp_slices_tile(tiles, gg.S, ctx->sm_count), ctx->stream));
         } else {
             LAUNCH(launch_grp_pass(kind, gg, prm, dp.val_u16, tiles, ctx->stream));
         }

@@ -176,12 +176,14 @@ cudaError_t launch_new_od(const NodArgs& a, const double* Xcm, double* xcolsum, 
 
 cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm, int val_u16,
                             int max_slots, cudaStream_t st);
-// the IRLS pass of the design-group engine, slice-major: a block stages one
-// slice's exp(offset) in shared memory and runs `tile` genes over it, then
-// a block per gene assembles the p x p sums (geo.gsum: slots x S x 2)
-int grp_irls_tile(int64_t hint, int S, int sm_count);
-cudaError_t launch_grp_irls(const GrpGeom& geo, const PassParamsAny& prm, int val_u16, int max_slots,
-                            int tile, cudaStream_t st);
+// the IRLS and MLE passes of the design-group engine, slice-major: a block
+// stages one slice's exp(offset) in shared memory and runs `tile` genes
+// over it, then a block per gene assembles the p x p sums
+// (geo.gsum: slots x S x grp_slices_nq(kind) doubles)
+int grp_slices_tile(int64_t hint, int S, int sm_count);
+int grp_slices_nq(PassKind k);
+cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm,
+                              int val_u16, int max_slots, int tile, cudaStream_t st);
 // cells in key order: sl_cell / sl_loc per original cell, E in slice order
 cudaError_t launch_slice_cells(const int32_t* pnew, const int32_t* sl_start, int S, int64_t n,
                                const double* off, int32_t* cslice, int32_t* cloc, double* E,

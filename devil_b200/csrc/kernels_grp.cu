@@ -718,15 +718,16 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
 }
 
 // ---------------------------------------------------------------------
-// IRLS pass, slice-major.  Block (slice s, tile of active genes): the
-// slice's exp(offset) values are staged in shared memory once, then each
-// warp takes the tile's genes in turn: A = exp(x_u . beta), the rule terms
-// of group u when s is the group's first slice, and the gene's entries of
-// the slice streamed as 16-byte loads (4 entries each for 16-bit counts),
-// exp(offset) read from shared memory.  The per-(gene, slice) sums go to
-// geo.gsum; grp_assemble_kernel forms the p x p terms per gene.
+// IRLS and MLE passes, slice-major.  Block (slice s, tile of active genes):
+// the slice's exp(offset) values are staged in shared memory once, then
+// each warp takes the tile's genes in turn: A = exp(x_u . beta), the rule
+// terms of group u when s is the group's first slice, and the gene's
+// entries of the slice streamed as 16-byte loads (4 entries each for 16-bit
+// counts), exp(offset) read from shared memory.  The per-(gene, slice) sums
+// go to geo.gsum; grp_assemble_kernel forms the p x p terms per gene.
 // ---------------------------------------------------------------------
 constexpr int kSlNT = 512;
+constexpr int kSlUnr = 4;  // 16-byte loads in flight per lane
 
 // streaming 16-byte load that does not allocate in L1 (each entry is read
 // once per pass)
@@ -738,11 +739,12 @@ DEV uint4 ld_stream(const uint4* p) {
     return v;
 }
 
-template <class VT>
-__global__ void __launch_bounds__(kSlNT) grp_irls_slices_kernel(GrpGeom geo, PassIRLS::Params prm,
-                                                                int tile) {
+template <class Pass, class VT>
+__global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typename Pass::Params prm,
+                                                           int tile) {
     using Ent = GrpEnt<VT>;
     using ET = typename Ent::T;
+    constexpr int NWV = Pass::NW + Pass::NV + Pass::NF, NS = Pass::NS, NQ = NWV + NS;
     constexpr int EPL = sizeof(uint4) / sizeof(ET);  // entries per 16-byte load
     if (geo.reset_next && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *geo.reset_next = 0;
     const int nact = *geo.n_act;
@@ -751,7 +753,7 @@ __global__ void __launch_bounds__(kSlNT) grp_irls_slices_kernel(GrpGeom geo, Pas
     const int j1 = min(nact, j0 + tile);
     const int s = blockIdx.x, S = geo.S, P = geo.P;
     extern __shared__ double Es[];  // [kSliceCells] exp(offset) of the slice's cells
-    __shared__ double bet[32][32];  // per warp: beta of its current gene
+    __shared__ double bet[kSlNT / 32][32];  // per warp: beta of its current gene
     const int c0 = __ldg(geo.sl_start + s), nc = __ldg(geo.sl_start + s + 1) - c0;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
     for (int i = t; i < nc; i += blockDim.x) Es[i] = __ldg(geo.E + c0 + i);
@@ -765,12 +767,16 @@ __global__ void __launch_bounds__(kSlNT) grp_irls_slices_kernel(GrpGeom geo, Pas
         if (lane < P) bet[warp][lane] = __ldg(prm.beta_d + (int64_t)g * P + lane);
         __syncwarp();
         const double A = exp(row_dot(geo, u, bet[warp], lane));
-        const PassIRLS::Gene gpar = PassIRLS::load(prm, g);
-        GrpAcc<2, 0> acc;
+        typename Pass::Gene gpar = Pass::load(prm, g);
+        if constexpr (Pass::TABLES) {  // no per-gene tables here: direct sums for small counts
+            gpar.tab.pa = digamma_d(gpar.a);
+            gpar.tab.ta = trigamma_d(gpar.a);
+        }
+        GrpAcc<NWV, NS> acc;
         acc.zero();
         for (int j = lane; j < m; j += 32) {
             acc.q = __ldg(geo.rw + (int64_t)u * kRuleCap + j);
-            PassIRLS::dense<double>(gpar, A * __ldg(geo.res + (int64_t)u * kRuleCap + j), acc);
+            Pass::template dense<double>(gpar, A * __ldg(geo.res + (int64_t)u * kRuleCap + j), acc);
         }
         acc.q = 1.0;
         const int64_t* gp = geo.gptr + (int64_t)g * (S + 1) + s;
@@ -781,91 +787,144 @@ __global__ void __launch_bounds__(kSlNT) grp_irls_slices_kernel(GrpGeom geo, Pas
         const int64_t a1 = max(a0, e1 / EPL * EPL);
         if (e0 + lane < a0) {
             const ET c = gent[e0 + lane];
-            PassIRLS::sparse<double>(gpar, A * Es[Ent::loc(c)], Ent::y(c), acc);
+            Pass::template sparse<double>(gpar, A * Es[Ent::loc(c)], Ent::y(c), acc);
         }
-        const uint4* v4 = reinterpret_cast<const uint4*>(gent);
-        for (int64_t b = a0 / EPL + lane; b < a1 / EPL; b += 32) {
-            const uint4 v = ld_stream(v4 + b);
-            const ET* c = reinterpret_cast<const ET*>(&v);
+        // whole 16-byte groups, kSlUnr loads in flight per lane before any
+        // is consumed (the segments are short: the latency of each batch
+        // is what the pass waits on)
+        const uint4* vb = reinterpret_cast<const uint4*>(gent) + a0 / EPL;
+        const int nb = (int)(a1 / EPL - a0 / EPL);
+        constexpr int UNR = NS > 0 ? 2 : kSlUnr;  // MLE: fewer, its accumulators need the registers
+        for (int base = lane; base < nb; base += 32 * UNR) {
+            uint4 v[UNR];
 #pragma unroll
-            for (int q = 0; q < EPL; ++q)
-                PassIRLS::sparse<double>(gpar, A * Es[Ent::loc(c[q])], Ent::y(c[q]), acc);
+            for (int q = 0; q < UNR; ++q)
+                if (base + 32 * q < nb) v[q] = ld_stream(vb + base + 32 * q);
+#pragma unroll
+            for (int q = 0; q < UNR; ++q) {
+                if (base + 32 * q < nb) {
+                    const ET* c = reinterpret_cast<const ET*>(&v[q]);
+#pragma unroll
+                    for (int r = 0; r < EPL; ++r)
+                        Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[r])], Ent::y(c[r]), acc);
+                }
+            }
         }
         if (a1 + lane < e1) {
             const ET c = gent[a1 + lane];
-            PassIRLS::sparse<double>(gpar, A * Es[Ent::loc(c)], Ent::y(c), acc);
+            Pass::template sparse<double>(gpar, A * Es[Ent::loc(c)], Ent::y(c), acc);
         }
-        const double w0 = warp_sum(acc.w[0]), w1 = warp_sum(acc.w[1]);
-        if (lane == 0) {
-            double* o = geo.gsum + ((int64_t)jj * S + s) * 2;
-            o[0] = w0;
-            o[1] = w1;
+        double* o = geo.gsum + ((int64_t)jj * S + s) * NQ;
+#pragma unroll
+        for (int i = 0; i < NWV; ++i) {
+            const double v = warp_sum(acc.w[i]);
+            if (lane == 0) o[i] = v;
+        }
+#pragma unroll
+        for (int i = 0; i < NS; ++i) {
+            const double v = warp_sum(acc.s[i]);
+            if (lane == 0) o[NWV + i] = v;
         }
         __syncwarp();
     }
 }
 
 // Per active gene: group sums over the gene's slices (in slice order) and
-// the p x p assembly of the IRLS pass (outer0 and vec0, one segment).
-__global__ void __launch_bounds__(256) grp_assemble_irls_kernel(GrpGeom geo) {
+// the assembly of the pass's partial sums (one segment).
+template <class Pass>
+__global__ void __launch_bounds__(256) grp_assemble_kernel(GrpGeom geo) {
+    constexpr int NW = Pass::NW, NV = Pass::NV, NF = Pass::NF;
+    constexpr int NWV = NW + NV + NF, NS = Pass::NS, NQ = NWV + NS;
     const int slot = blockIdx.x;
     if (slot >= *geo.n_act) return;
     const int P = geo.P, U = geo.U, C = geo.C, S = geo.S;
-    extern __shared__ double gs[];  // [U][2]
+    extern __shared__ double gs[];  // [U][NQ]
     const int t = threadIdx.x, nt = blockDim.x;
-    const double* gsum = geo.gsum + (int64_t)slot * S * 2;
-    for (int i = t; i < U * 2; i += nt) {
-        const int q = i >> 1, c = i & 1;
+    const double* gsum = geo.gsum + (int64_t)slot * S * NQ;
+    for (int i = t; i < U * NQ; i += nt) {
+        const int q = i / NQ, c = i - q * NQ;
         double v = 0.0;
         for (int sl = __ldg(geo.kslice + q * C); sl < __ldg(geo.kslice + q * C + C); ++sl)
-            v += gsum[sl * 2 + c];
+            v += gsum[sl * NQ + c];
         gs[i] = v;
     }
     __syncthreads();
     const int NE = P * (P + 1) / 2;
-    const int NA = NE + P;
-    for (int a = t; a < NA; a += nt) {
+    const int NA = NW * NE + NV * P + NF;
+    for (int a = t; a < NA + NS; a += nt) {
         double s = 0.0;
-        if (a < NE) {
-            for (int e = __ldg(geo.qptr + a); e < __ldg(geo.qptr + a + 1); ++e)
-                s += gs[__ldg(geo.qu + e) * 2] * __ldg(geo.qv + e);
-        } else {
-            const int i = a - NE;
+        if (a < NW * NE) {
+            const int w = a / NE, qq = a - w * NE;
+            for (int e = __ldg(geo.qptr + qq); e < __ldg(geo.qptr + qq + 1); ++e)
+                s += gs[__ldg(geo.qu + e) * NQ + w] * __ldg(geo.qv + e);
+        } else if (a < NW * NE + NV * P) {
+            const int r = a - NW * NE;
+            const int v = r / P, i = r - v * P;
             for (int e = __ldg(geo.vptr + i); e < __ldg(geo.vptr + i + 1); ++e)
-                s += gs[__ldg(geo.vu + e) * 2 + 1] * __ldg(geo.vv + e);
+                s += gs[__ldg(geo.vu + e) * NQ + NW + v] * __ldg(geo.vv + e);
+        } else {
+            const int f = a - NW * NE - NV * P;
+            const int col = a < NA ? NW + NV + f : NWV + (a - NA);
+            for (int u = 0; u < U; ++u) s += gs[u * NQ + col];
         }
-        geo.partW[(int64_t)slot * NA + a] = s;
+        if (a < NA)
+            geo.partW[(int64_t)slot * NA + a] = s;
+        else
+            geo.partS[(int64_t)slot * NS + (a - NA)] = s;
     }
 }
 
-int grp_irls_tile(int64_t hint, int S, int sm_count) {
-    // about six blocks per SM over the whole grid, tiles of 32..1024 genes
-    const int64_t want = (hint * S + (int64_t)sm_count * 6 - 1) / ((int64_t)sm_count * 6);
-    return (int)std::max<int64_t>(32, std::min<int64_t>(1024, want));
+int grp_slices_tile(int64_t hint, int S, int sm_count) {
+    // two resident blocks per SM (registers, the 64 KB slice stage); about
+    // three waves, the tile count chosen so the last wave is nearly full,
+    // tiles of 16..1024 genes
+    const int64_t cap = (int64_t)sm_count * 2;
+    int64_t tiles = std::max<int64_t>(1, (3 * cap + S - 1) / S);
+    double best_eff = 0.0;
+    int64_t best = tiles;
+    for (int64_t tc = tiles; tc <= 2 * tiles; ++tc) {
+        const double waves = (double)tc * S / (double)cap;
+        const double eff = waves / std::ceil(waves);
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = tc;
+        }
+        if (eff >= 0.95) break;
+    }
+    const int64_t tile = (hint + best - 1) / best;
+    return (int)std::max<int64_t>(16, std::min<int64_t>(1024, tile));
 }
 
-cudaError_t launch_grp_irls(const GrpGeom& geo, const PassParamsAny& pa, int val_u16, int max_slots,
-                            int tile, cudaStream_t st) {
-    if (max_slots <= 0) return cudaSuccess;
-    PassIRLS::Params prm{pa.beta, pa.beta_d, pa.k};
+template <class Pass>
+static cudaError_t slices_run(const GrpGeom& geo, typename Pass::Params prm, int val_u16,
+                              int max_slots, int tile, cudaStream_t st) {
+    constexpr int NQ = Pass::NW + Pass::NV + Pass::NF + Pass::NS;
     const size_t smem = (size_t)kSliceCells * sizeof(double);
     dim3 grid((unsigned)geo.S, (unsigned)((max_slots + tile - 1) / tile));
-    cudaError_t e;
-    if (val_u16) {
-        auto k = grp_irls_slices_kernel<uint16_t>;
-        e = raise_dyn_smem(k, smem);
+    auto go = [&](auto kern) -> cudaError_t {
+        cudaError_t e = raise_dyn_smem(kern, smem);
         if (e != cudaSuccess) return e;
-        k<<<grid, kSlNT, smem, st>>>(geo, prm, tile);
-    } else {
-        auto k = grp_irls_slices_kernel<float>;
-        e = raise_dyn_smem(k, smem);
-        if (e != cudaSuccess) return e;
-        k<<<grid, kSlNT, smem, st>>>(geo, prm, tile);
-    }
-    e = cudaGetLastError();
+        kern<<<grid, kSlNT, smem, st>>>(geo, prm, tile);
+        return cudaGetLastError();
+    };
+    cudaError_t e = val_u16 ? go(grp_slices_kernel<Pass, uint16_t>) : go(grp_slices_kernel<Pass, float>);
     if (e != cudaSuccess) return e;
-    grp_assemble_irls_kernel<<<(unsigned)max_slots, 256, (size_t)geo.U * 2 * sizeof(double), st>>>(geo);
+    grp_assemble_kernel<Pass><<<(unsigned)max_slots, 256, (size_t)geo.U * NQ * sizeof(double), st>>>(geo);
     return cudaGetLastError();
+}
+
+int grp_slices_nq(PassKind k) { return pass_nw(k) + pass_nv(k) + pass_nf(k) + pass_ns(k); }
+
+cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& pa,
+                              int val_u16, int max_slots, int tile, cudaStream_t st) {
+    if (max_slots <= 0) return cudaSuccess;
+    if (kind == PASS_IRLS)
+        return slices_run<PassIRLS>(geo, PassIRLS::Params{pa.beta, pa.beta_d, pa.k}, val_u16,
+                                    max_slots, tile, st);
+    if (kind == PASS_MLE)
+        return slices_run<PassMLE>(geo, PassMLE::Params{pa.beta, pa.beta_d, pa.log_theta}, val_u16,
+                                   max_slots, tile, st);
+    return cudaErrorInvalidValue;
 }
 
 // init_beta (R/beta.R:12-24) on a grouped design: X' z with

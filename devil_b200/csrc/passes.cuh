@@ -126,10 +126,10 @@ struct RecAcc {
 };
 
 // 1/x in FP64 for x > 0: the MUFU estimate (rcp.approx.ftz.f64, about 23
-// correct bits) refined by two Newton-Raphson steps r <- r + r (1 - x r),
-// each of which doubles the number of correct bits; the result is within an
-// ulp of the IEEE quotient at a fraction of the cost of the division
-// sequence.  x = +inf gives 0, as the quotient does.
+// correct bits) refined by Newton-Raphson steps r <- r + r (1 - x r), each
+// of which doubles the number of correct bits: two steps give the quotient
+// to within an ulp, one step to ~1e-14 relative (plenty for terms that are
+// summed over cells).  x = +inf gives 0, as the quotient does.
 DEV double rcp_nr(double x) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
@@ -139,11 +139,19 @@ DEV double rcp_nr(double x) {
     r = fma(r, e, r);
     return isinf(x) ? 0.0 : r;
 }
+DEV double rcp_nr1(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    const double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    return isinf(x) ? 0.0 : r;
+}
 
 // reciprocal in the arithmetic of the pass: MUFU estimate in FP32, the
-// Newton-refined estimate in FP64
+// estimate refined by one Newton step in FP64 (the per-cell terms are summed
+// over cells; ~1e-11 relative per term is far below what the sums carry)
 DEV float rcp_r(float x) { return rcp_approx(x); }
-DEV double rcp_r(double x) { return rcp_nr(x); }
+DEV double rcp_r(double x) { return rcp_nr1(x); }
 
 // ---------------------------------------------------------------------
 // pass traits
@@ -323,15 +331,31 @@ DEV void build_psi_tables(int GTn, const double* a, double* tab, double* scratch
     }
     __syncthreads();
 }
+// Without tables (T.d1 null: kernels that visit many genes per block),
+// small integer counts sum the recurrence terms directly.
+constexpr int kPsiDirect = 16;
 DEV void psi_diffs_tab(double y, double a, const PsiTable& T, double& d1, double& d2) {
     if (y < (double)kPsiTab && y == floor(y)) {
         int v = (int)y;
-        d1 = T.d1[v];
-        d2 = T.d2[v];
-    } else {
-        d1 = digamma_d(y + a) - T.pa;
-        d2 = trigamma_d(y + a) - T.ta;
+        if (T.d1) {
+            d1 = T.d1[v];
+            d2 = T.d2[v];
+            return;
+        }
+        if (v <= kPsiDirect) {
+            double s1 = 0.0, s2 = 0.0;
+            for (int j = 0; j < v; ++j) {
+                const double t = 1.0 / (a + j);
+                s1 += t;
+                s2 -= t * t;
+            }
+            d1 = s1;
+            d2 = s2;
+            return;
+        }
     }
+    d1 = digamma_d(y + a) - T.pa;
+    d2 = trigamma_d(y + a) - T.ta;
 }
 
 // One evaluation of the dispersion score and its derivative in log theta
