@@ -670,7 +670,8 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     dbg_mark(ctx, "g.rules");
     // CSR copy ordered by slice within each gene: 4-byte entries (index in
     // the slice, 16-bit count) or 8-byte ones for float counts
-    void* gent = ws<char>(ctx, "grp_ent", (size_t)std::max<int64_t>(dp.nnz, 4) * (dp.val_u16 ? 4 : 8));
+    // (padded to a whole 16-byte group: the pass reads the groups covering a range)
+    void* gent = ws<char>(ctx, "grp_ent", (size_t)(dp.nnz + 4) * (dp.val_u16 ? 4 : 8));
     int64_t* gptr = ws<int64_t>(ctx, "grp_ptr", (size_t)dp.G * (NSL + 1));
     const int S = group_csr_segment(dp.nnz, dp.G, NSL);
     int64_t* segcnt = ws<int64_t>(ctx, "grp_segcnt", dp.G + 1);
@@ -959,9 +960,10 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
         gg.partW = static_cast<double*>(pb.partW);
         gg.partS = pb.partS;
         gg.slot_stride = tiles;
-        if ((kind == PASS_IRLS || kind == PASS_MLE) && !fine && ctx->grp_slices) {
+        if (kind == PASS_IRLS && !fine && ctx->grp_slices) {
             // slice-major pass: per-(gene, slice) sums, then the assembly
             gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * grp_slices_nq(kind));
+            gg.rowexp = ws<double>(ctx, "grp_rowexp", (size_t)tiles * gg.U);
             LAUNCH(launch_grp_slices(kind, gg, prm, dp.val_u16, tiles,
                                      grp_slices_tile(tiles, gg.S, ctx->sm_count), ctx->stream));
         } else {

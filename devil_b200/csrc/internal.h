@@ -125,6 +125,7 @@ struct GrpGeom {
     const int32_t* sl_key;    // [S] its key u * C + c
     const int32_t* kslice;    // [U*C + 1] first slice of every key (slices ordered by key)
     double* gsum;          // slice-major IRLS: [slots][S][NQ] per-(gene, slice) sums
+    double* rowexp;        // slice-major IRLS: [slots][U] exp(x_u . beta)
     const double* rs;      // [rules][kRuleCap] node offsets; rules 0..U-1 coarse, U.. fine
     const double* rw;      // [rules][kRuleCap] node weights
     const int32_t* rm;     // [rules] node counts
@@ -176,10 +177,10 @@ cudaError_t launch_new_od(const NodArgs& a, const double* Xcm, double* xcolsum, 
 
 cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm, int val_u16,
                             int max_slots, cudaStream_t st);
-// the IRLS and MLE passes of the design-group engine, slice-major: a block
-// stages one slice's exp(offset) in shared memory and runs `tile` genes
-// over it, then a block per gene assembles the p x p sums
-// (geo.gsum: slots x S x grp_slices_nq(kind) doubles)
+// the IRLS pass of the design-group engine, slice-major: a block stages one
+// slice's exp(offset) in shared memory and runs `tile` genes over it, then a
+// block per gene assembles the p x p sums (geo.gsum: slots x S x
+// grp_slices_nq(kind) doubles; geo.rowexp: slots x U)
 int grp_slices_tile(int64_t hint, int S, int sm_count);
 int grp_slices_nq(PassKind k);
 cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm,

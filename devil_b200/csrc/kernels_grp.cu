@@ -718,12 +718,13 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
 }
 
 // ---------------------------------------------------------------------
-// IRLS and MLE passes, slice-major.  Block (slice s, tile of active genes):
+// IRLS pass, slice-major.  Block (slice s, tile of active genes):
 // the slice's exp(offset) values are staged in shared memory once, then
-// each warp takes the tile's genes in turn: A = exp(x_u . beta), the rule
-// terms of group u when s is the group's first slice, and the gene's
-// entries of the slice streamed as 16-byte loads (4 entries each for 16-bit
-// counts), exp(offset) read from shared memory.  The per-(gene, slice) sums
+// each warp takes the tile's genes in turn: A = exp(x_u . beta) (computed
+// per gene and group beforehand), the rule terms of group u when s is the
+// group's first slice, and the gene's entries of the slice streamed as
+// 16-byte loads (4 entries each for 16-bit counts), exp(offset) read from
+// shared memory.  The per-(gene, slice) sums
 // go to geo.gsum; grp_assemble_kernel forms the p x p terms per gene.
 // ---------------------------------------------------------------------
 constexpr int kSlNT = 512;
@@ -741,19 +742,19 @@ DEV uint4 ld_stream(const uint4* p) {
 
 template <class Pass, class VT>
 __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typename Pass::Params prm,
-                                                           int tile) {
+                                                              int tile) {
     using Ent = GrpEnt<VT>;
     using ET = typename Ent::T;
     constexpr int NWV = Pass::NW + Pass::NV + Pass::NF, NS = Pass::NS, NQ = NWV + NS;
     constexpr int EPL = sizeof(uint4) / sizeof(ET);  // entries per 16-byte load
+    static_assert(!Pass::TABLES, "per-gene tables are built by the block-per-gene pass");
     if (geo.reset_next && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *geo.reset_next = 0;
     const int nact = *geo.n_act;
     const int j0 = blockIdx.y * tile;
     if (j0 >= nact) return;
     const int j1 = min(nact, j0 + tile);
-    const int s = blockIdx.x, S = geo.S, P = geo.P;
+    const int s = blockIdx.x, S = geo.S, U = geo.U;
     extern __shared__ double Es[];  // [kSliceCells] exp(offset) of the slice's cells
-    __shared__ double bet[kSlNT / 32][32];  // per warp: beta of its current gene
     const int c0 = __ldg(geo.sl_start + s), nc = __ldg(geo.sl_start + s + 1) - c0;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
     for (int i = t; i < nc; i += blockDim.x) Es[i] = __ldg(geo.E + c0 + i);
@@ -761,17 +762,31 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
     const bool first = s == __ldg(geo.kslice + u * geo.C);  // the group's rule goes here
     const int m = first ? __ldg(geo.rm + u) : 0;
     __syncthreads();
-    const ET* __restrict__ gent = static_cast<const ET*>(geo.gent);
-    for (int jj = j0 + warp; jj < j1; jj += nw) {
-        const int g = __ldg(geo.act + jj);
-        if (lane < P) bet[warp][lane] = __ldg(prm.beta_d + (int64_t)g * P + lane);
-        __syncwarp();
-        const double A = exp(row_dot(geo, u, bet[warp], lane));
-        typename Pass::Gene gpar = Pass::load(prm, g);
-        if constexpr (Pass::TABLES) {  // no per-gene tables here: direct sums for small counts
-            gpar.tab.pa = digamma_d(gpar.a);
-            gpar.tab.ta = trigamma_d(gpar.a);
+    const uint4* __restrict__ v4 = static_cast<const uint4*>(geo.gent);
+    // per gene: exp(x_u . beta) (from grp_rowexp_kernel) and the slice's
+    // entry range; the next gene's are loaded while this one runs
+    int jj = j0 + warp;
+    int g = 0;
+    double A = 0.0;
+    int64_t e0 = 0, e1 = 0;
+    if (jj < j1) {
+        g = __ldg(geo.act + jj);
+        A = __ldg(geo.rowexp + (int64_t)jj * U + u);
+        e0 = __ldg(geo.gptr + (int64_t)g * (S + 1) + s);
+        e1 = __ldg(geo.gptr + (int64_t)g * (S + 1) + s + 1);
+    }
+    while (jj < j1) {
+        const int jn = jj + nw;
+        int gn = 0;
+        double An = 0.0;
+        int64_t f0 = 0, f1 = 0;
+        if (jn < j1) {
+            gn = __ldg(geo.act + jn);
+            An = __ldg(geo.rowexp + (int64_t)jn * U + u);
+            f0 = __ldg(geo.gptr + (int64_t)gn * (S + 1) + s);
+            f1 = __ldg(geo.gptr + (int64_t)gn * (S + 1) + s + 1);
         }
+        const typename Pass::Gene gpar = Pass::load(prm, g);
         GrpAcc<NWV, NS> acc;
         acc.zero();
         for (int j = lane; j < m; j += 32) {
@@ -779,40 +794,27 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
             Pass::template dense<double>(gpar, A * __ldg(geo.res + (int64_t)u * kRuleCap + j), acc);
         }
         acc.q = 1.0;
-        const int64_t* gp = geo.gptr + (int64_t)g * (S + 1) + s;
-        const int64_t e0 = __ldg(gp), e1 = __ldg(gp + 1);
-        // entries up to the first 16-byte boundary, whole 16-byte groups,
-        // the rest
-        const int64_t a0 = min(e1, (e0 + EPL - 1) / EPL * EPL);
-        const int64_t a1 = max(a0, e1 / EPL * EPL);
-        if (e0 + lane < a0) {
-            const ET c = gent[e0 + lane];
-            Pass::template sparse<double>(gpar, A * Es[Ent::loc(c)], Ent::y(c), acc);
-        }
-        // whole 16-byte groups, kSlUnr loads in flight per lane before any
-        // is consumed (the segments are short: the latency of each batch
-        // is what the pass waits on)
-        const uint4* vb = reinterpret_cast<const uint4*>(gent) + a0 / EPL;
-        const int nb = (int)(a1 / EPL - a0 / EPL);
-        constexpr int UNR = NS > 0 ? 2 : kSlUnr;  // MLE: fewer, its accumulators need the registers
-        for (int base = lane; base < nb; base += 32 * UNR) {
-            uint4 v[UNR];
+        // the 16-byte groups covering [e0, e1) (the copy is padded to a whole
+        // group), kSlUnr loads in flight per lane before any is consumed;
+        // entries outside the range are masked
+        const int64_t b0 = e0 / EPL;
+        const int nb = (int)((e1 + EPL - 1) / EPL - b0);
+        for (int base = lane; base < nb; base += 32 * kSlUnr) {
+            uint4 v[kSlUnr];
 #pragma unroll
-            for (int q = 0; q < UNR; ++q)
-                if (base + 32 * q < nb) v[q] = ld_stream(vb + base + 32 * q);
+            for (int q = 0; q < kSlUnr; ++q)
+                if (base + 32 * q < nb) v[q] = ld_stream(v4 + b0 + base + 32 * q);
 #pragma unroll
-            for (int q = 0; q < UNR; ++q) {
+            for (int q = 0; q < kSlUnr; ++q) {
+                const int64_t ea = (b0 + base + 32 * q) * EPL;  // first entry of the group
                 if (base + 32 * q < nb) {
                     const ET* c = reinterpret_cast<const ET*>(&v[q]);
 #pragma unroll
                     for (int r = 0; r < EPL; ++r)
-                        Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[r])], Ent::y(c[r]), acc);
+                        if (ea + r >= e0 && ea + r < e1)
+                            Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[r])], Ent::y(c[r]), acc);
                 }
             }
-        }
-        if (a1 + lane < e1) {
-            const ET c = gent[a1 + lane];
-            Pass::template sparse<double>(gpar, A * Es[Ent::loc(c)], Ent::y(c), acc);
         }
         double* o = geo.gsum + ((int64_t)jj * S + s) * NQ;
 #pragma unroll
@@ -825,8 +827,27 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
             const double v = warp_sum(acc.s[i]);
             if (lane == 0) o[NWV + i] = v;
         }
-        __syncwarp();
+        jj = jn;
+        g = gn;
+        A = An;
+        e0 = f0;
+        e1 = f1;
     }
+}
+
+// exp(x_u . beta) for every (active gene, design group): the factor the
+// slice-major pass multiplies each cell's exp(offset) by
+__global__ void grp_rowexp_kernel(GrpGeom geo, const double* beta_d, int64_t max_slots) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int U = geo.U, P = geo.P;
+    const int64_t slot = i / U;
+    if (slot >= *geo.n_act || slot >= max_slots) return;
+    const int u = (int)(i - slot * U);
+    const double* b = beta_d + (int64_t)__ldg(geo.act + slot) * P;
+    double a = 0.0;
+    for (int e = __ldg(geo.rptr + u); e < __ldg(geo.rptr + u + 1); ++e)
+        a += __ldg(geo.rval + e) * __ldg(b + __ldg(geo.rcol + e));
+    geo.rowexp[i] = exp(a);
 }
 
 // Per active gene: group sums over the gene's slices (in slice order) and
@@ -900,6 +921,8 @@ static cudaError_t slices_run(const GrpGeom& geo, typename Pass::Params prm, int
                               int max_slots, int tile, cudaStream_t st) {
     constexpr int NQ = Pass::NW + Pass::NV + Pass::NF + Pass::NS;
     const size_t smem = (size_t)kSliceCells * sizeof(double);
+    const int64_t nrow = (int64_t)max_slots * geo.U;
+    grp_rowexp_kernel<<<nblk(nrow, 256), 256, 0, st>>>(geo, prm.beta_d, max_slots);
     dim3 grid((unsigned)geo.S, (unsigned)((max_slots + tile - 1) / tile));
     auto go = [&](auto kern) -> cudaError_t {
         cudaError_t e = raise_dyn_smem(kern, smem);
@@ -921,9 +944,6 @@ cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParam
     if (kind == PASS_IRLS)
         return slices_run<PassIRLS>(geo, PassIRLS::Params{pa.beta, pa.beta_d, pa.k}, val_u16,
                                     max_slots, tile, st);
-    if (kind == PASS_MLE)
-        return slices_run<PassMLE>(geo, PassMLE::Params{pa.beta, pa.beta_d, pa.log_theta}, val_u16,
-                                   max_slots, tile, st);
     return cudaErrorInvalidValue;
 }
 

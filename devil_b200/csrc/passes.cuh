@@ -331,31 +331,15 @@ DEV void build_psi_tables(int GTn, const double* a, double* tab, double* scratch
     }
     __syncthreads();
 }
-// Without tables (T.d1 null: kernels that visit many genes per block),
-// small integer counts sum the recurrence terms directly.
-constexpr int kPsiDirect = 16;
 DEV void psi_diffs_tab(double y, double a, const PsiTable& T, double& d1, double& d2) {
     if (y < (double)kPsiTab && y == floor(y)) {
         int v = (int)y;
-        if (T.d1) {
-            d1 = T.d1[v];
-            d2 = T.d2[v];
-            return;
-        }
-        if (v <= kPsiDirect) {
-            double s1 = 0.0, s2 = 0.0;
-            for (int j = 0; j < v; ++j) {
-                const double t = 1.0 / (a + j);
-                s1 += t;
-                s2 -= t * t;
-            }
-            d1 = s1;
-            d2 = s2;
-            return;
-        }
+        d1 = T.d1[v];
+        d2 = T.d2[v];
+    } else {
+        d1 = digamma_d(y + a) - T.pa;
+        d2 = trigamma_d(y + a) - T.ta;
     }
-    d1 = digamma_d(y + a) - T.pa;
-    d2 = trigamma_d(y + a) - T.ta;
 }
 
 // One evaluation of the dispersion score and its derivative in log theta
