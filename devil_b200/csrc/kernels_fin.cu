@@ -13,6 +13,7 @@ static inline unsigned nblk(int64_t m, int t) { return (unsigned)((m + t - 1) / 
 template <class T>
 DEV void reduce_partials(const T* part, int nseg, int slot_stride, int slot, int stride, int count,
                          double* sums, int lane) {
+#pragma unroll 4
     for (int a = lane; a < count; a += 32) {
         double s = 0.0;
         for (int seg = 0; seg < nseg; ++seg)
@@ -48,12 +49,11 @@ __global__ void irls_finalize_kernel(const TW* partW, int nseg, int slot_stride,
     extern __shared__ double fsh[];
     const int NE = P * (P + 1) / 2, NA = NE + P, LD = wla_ld(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = NA + P * LD + 2 * P + P;  // sums, H, S, x, perm
+    const int per = NA + P * LD + P;  // sums, H, then perm and step (P ints each)
     double* sums = fsh + warp * per;
     double* H = sums + NA;
-    double* S = H + P * LD;
-    double* xs = S + P;
-    int* perm = reinterpret_cast<int*>(xs + P);
+    int* perm = reinterpret_cast<int*>(H + P * LD);
+    int* step = perm + P;
     const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
     const int nact = *n_act;
     if (slot >= nact) return;
@@ -63,21 +63,24 @@ __global__ void irls_finalize_kernel(const TW* partW, int nseg, int slot_stride,
     // the pass accumulates H / k^2 and -score / k (see PassIRLS)
     const double k = (double)kf[g];
     warp_unpack_sym(P, sums, k * k, 0.0, H, LD);
-    if (lane < P) S[lane] = -k * sums[NE + lane];
-    warp_lu(H, LD, P, perm);
-    if (lane != 0) return;
-    lu_solve_perm(H, LD, P, perm, S, xs);
-    double mx = 0.0;
-    for (int i = 0; i < P; ++i) {
-        double b = beta[(int64_t)g * P + i] + xs[i];
-        beta[(int64_t)g * P + i] = b;
-        beta_f[(int64_t)g * P + i] = (float)b;
-        double a = fabs(xs[i]);
-        if (a > mx) mx = a;  // NaN entries never compare greater
+    const double s_own = lane < P ? -k * sums[NE + lane] : 0.0;
+    warp_lu(H, LD, P, perm, step);
+    const double x_own = warp_lu_solve(H, LD, P, perm, step, s_own);
+    double b = 0.0;
+    if (lane < P) {
+        b = beta[(int64_t)g * P + lane] + x_own;
+        beta[(int64_t)g * P + lane] = b;
+        beta_f[(int64_t)g * P + lane] = (float)b;
     }
+    // max |x| (NaN entries never compare greater) and x_0
+    double mx = lane < P ? fabs(x_own) : 0.0;
+    mx = (mx == mx) ? mx : 0.0;
+    mx = warp_max(mx);
+    const double x0 = __shfl_sync(0xffffffffu, x_own, 0);
+    if (lane != 0) return;
     const int it = iters[g] + 1;
     iters[g] = it;
-    const bool isnan0 = !(xs[0] == xs[0]);
+    const bool isnan0 = !(x0 == x0);
     const bool conv = mx < eps;
     if (isnan0) {
         status[g] = 2;  // DEVIL_GENE_NAN
@@ -98,7 +101,7 @@ cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slo
                                  const float* k, cudaStream_t st) {
     if (max_slots <= 0) return cudaSuccess;
     const int NA = P * (P + 1) / 2 + P;
-    const size_t per = (size_t)(NA + P * wla_ld(P) + 3 * P) * sizeof(double);
+    const size_t per = (size_t)(NA + P * wla_ld(P) + P) * sizeof(double);
     const int w = fin_warps(per);
     const size_t smem = per * w;
     auto go = [&](auto* pw) -> cudaError_t {
