@@ -93,7 +93,9 @@ struct devil_ctx {
     int sm_count = 148;
     int use_tma = 0;
     int use_groups = 1;
-    int grp_slices = 1;  // slice-major IRLS pass of the design-group engine (DEVIL_GRP_SLICES=0: block per gene)
+    // slice-major passes of the design-group engine, a bit mask: 1 IRLS, 2 MLE
+    // (DEVIL_GRP_SLICES; 0: every pass block per gene)
+    int grp_slices = 3;
     int debug = 0;  // DEVIL_DEBUG=1: engine choices on stderr
     // profiling: CUDA events around every pass launch, per pass kind
     int profiling = 0;
@@ -960,10 +962,12 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
         gg.partW = static_cast<double*>(pb.partW);
         gg.partS = pb.partS;
         gg.slot_stride = tiles;
-        if (kind == PASS_IRLS && !fine && ctx->grp_slices) {
+        const int slice_bit = kind == PASS_IRLS ? 1 : (kind == PASS_MLE ? 2 : 0);
+        if ((ctx->grp_slices & slice_bit) && !fine) {
             // slice-major pass: per-(gene, slice) sums, then the assembly
             gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * grp_slices_nq(kind));
             gg.rowexp = ws<double>(ctx, "grp_rowexp", (size_t)tiles * gg.U);
+            if (kind == PASS_MLE) gg.psitab = ws<double>(ctx, "grp_psitab", (size_t)tiles * kGrpTab);
             LAUNCH(launch_grp_slices(kind, gg, prm, dp.val_u16, tiles,
                                      grp_slices_tile(tiles, gg.S, ctx->sm_count), ctx->stream));
         } else {
@@ -1513,7 +1517,7 @@ int devil_ctx_create(int device, devil_ctx** out) {
         const char* ug = getenv("DEVIL_GROUPS");
         ctx->use_groups = (ug && !atoi(ug)) ? 0 : 1;
         const char* gsl = getenv("DEVIL_GRP_SLICES");
-        ctx->grp_slices = (gsl && !atoi(gsl)) ? 0 : 1;
+        ctx->grp_slices = gsl ? (atoi(gsl) & 3) : 3;
         const char* dbg = getenv("DEVIL_DEBUG");
         ctx->debug = (dbg && atoi(dbg)) ? 1 : 0;
         int32_t* err = ws<int32_t>(ctx, "kernel_err", 1);

@@ -91,6 +91,7 @@ constexpr int kMaxGroups = 256;       // distinct design rows
 constexpr int kMaxFine = 4096;        // (design row, cluster) pairs
 constexpr int kMinCellsPerGroup = 32; // grouping pays when groups are larger
 constexpr int kSliceCells = 8192;     // cells per slice (its exp(offset) fits shared memory)
+constexpr int kGrpTab = 2 * kPsiTab + 2;  // per-gene psi tables + psi(a), psi1(a)
 constexpr int kMaxSlices = 12288;     // the CSR copy's per-warp key table stays <= 48 KB
 
 // One entry of the slice-ordered CSR copy of the design-group engine: the
@@ -125,7 +126,8 @@ struct GrpGeom {
     const int32_t* sl_key;    // [S] its key u * C + c
     const int32_t* kslice;    // [U*C + 1] first slice of every key (slices ordered by key)
     double* gsum;          // slice-major IRLS: [slots][S][NQ] per-(gene, slice) sums
-    double* rowexp;        // slice-major IRLS: [slots][U] exp(x_u . beta)
+    double* rowexp;        // slice-major passes: [slots][U] exp(x_u . beta)
+    double* psitab;        // slice-major MLE: [slots][kGrpTab] psi tables, psi(a), psi1(a)
     const double* rs;      // [rules][kRuleCap] node offsets; rules 0..U-1 coarse, U.. fine
     const double* rw;      // [rules][kRuleCap] node weights
     const int32_t* rm;     // [rules] node counts
@@ -177,10 +179,11 @@ cudaError_t launch_new_od(const NodArgs& a, const double* Xcm, double* xcolsum, 
 
 cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm, int val_u16,
                             int max_slots, cudaStream_t st);
-// the IRLS pass of the design-group engine, slice-major: a block stages one
-// slice's exp(offset) in shared memory and runs `tile` genes over it, then a
-// block per gene assembles the p x p sums (geo.gsum: slots x S x
-// grp_slices_nq(kind) doubles; geo.rowexp: slots x U)
+// the IRLS and MLE passes of the design-group engine, slice-major: a block
+// stages one slice's exp(offset) in shared memory and runs `tile` genes over
+// it, then a block per gene assembles the p x p sums (geo.gsum: slots x S x
+// grp_slices_nq(kind) doubles; geo.rowexp: slots x U; geo.psitab, MLE:
+// slots x kGrpTab)
 int grp_slices_tile(int64_t hint, int S, int sm_count);
 int grp_slices_nq(PassKind k);
 cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm,

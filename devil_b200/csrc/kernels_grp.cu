@@ -718,7 +718,7 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
 }
 
 // ---------------------------------------------------------------------
-// IRLS pass, slice-major.  Block (slice s, tile of active genes):
+// IRLS and MLE passes, slice-major.  Block (slice s, tile of active genes):
 // the slice's exp(offset) values are staged in shared memory once, then
 // each warp takes the tile's genes in turn: A = exp(x_u . beta) (computed
 // per gene and group beforehand), the rule terms of group u when s is the
@@ -747,7 +747,6 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
     using ET = typename Ent::T;
     constexpr int NWV = Pass::NW + Pass::NV + Pass::NF, NS = Pass::NS, NQ = NWV + NS;
     constexpr int EPL = sizeof(uint4) / sizeof(ET);  // entries per 16-byte load
-    static_assert(!Pass::TABLES, "per-gene tables are built by the block-per-gene pass");
     if (geo.reset_next && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *geo.reset_next = 0;
     const int nact = *geo.n_act;
     const int j0 = blockIdx.y * tile;
@@ -757,6 +756,8 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
     extern __shared__ double Es[];  // [kSliceCells] exp(offset) of the slice's cells
     const int c0 = __ldg(geo.sl_start + s), nc = __ldg(geo.sl_start + s + 1) - c0;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
+    // per warp: the psi tables of its current gene (passes with TABLES)
+    double* wtab = Es + kSliceCells + warp * kGrpTab;
     for (int i = t; i < nc; i += blockDim.x) Es[i] = __ldg(geo.E + c0 + i);
     const int u = __ldg(geo.sl_key + s) / geo.C;
     const bool first = s == __ldg(geo.kslice + u * geo.C);  // the group's rule goes here
@@ -786,7 +787,17 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
             f0 = __ldg(geo.gptr + (int64_t)gn * (S + 1) + s);
             f1 = __ldg(geo.gptr + (int64_t)gn * (S + 1) + s + 1);
         }
-        const typename Pass::Gene gpar = Pass::load(prm, g);
+        typename Pass::Gene gpar = Pass::load(prm, g);
+        if constexpr (Pass::TABLES) {
+            // the gene's psi tables (grp_psi_tables_kernel) into the warp's slot
+            const double* src = geo.psitab + (int64_t)jj * kGrpTab;
+            for (int i = lane; i < kGrpTab; i += 32) wtab[i] = __ldg(src + i);
+            __syncwarp();
+            gpar.tab.d1 = wtab;
+            gpar.tab.d2 = wtab + kPsiTab;
+            gpar.tab.pa = wtab[2 * kPsiTab];
+            gpar.tab.ta = wtab[2 * kPsiTab + 1];
+        }
         GrpAcc<NWV, NS> acc;
         acc.zero();
         for (int j = lane; j < m; j += 32) {
@@ -795,24 +806,31 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
         }
         acc.q = 1.0;
         // the 16-byte groups covering [e0, e1) (the copy is padded to a whole
-        // group), kSlUnr loads in flight per lane before any is consumed;
+        // group), UNR loads in flight per lane before any is consumed;
         // entries outside the range are masked
+        constexpr int UNR = NS > 0 ? 2 : kSlUnr;  // the MLE's accumulators need the registers
         const int64_t b0 = e0 / EPL;
         const int nb = (int)((e1 + EPL - 1) / EPL - b0);
-        for (int base = lane; base < nb; base += 32 * kSlUnr) {
-            uint4 v[kSlUnr];
+        for (int base = lane; base < nb; base += 32 * UNR) {
+            uint4 v[UNR];
 #pragma unroll
-            for (int q = 0; q < kSlUnr; ++q)
+            for (int q = 0; q < UNR; ++q)
                 if (base + 32 * q < nb) v[q] = ld_stream(v4 + b0 + base + 32 * q);
 #pragma unroll
-            for (int q = 0; q < kSlUnr; ++q) {
+            for (int q = 0; q < UNR; ++q) {
                 const int64_t ea = (b0 + base + 32 * q) * EPL;  // first entry of the group
                 if (base + 32 * q < nb) {
                     const ET* c = reinterpret_cast<const ET*>(&v[q]);
+                    if (ea >= e0 && ea + EPL <= e1) {  // a whole group inside the range
 #pragma unroll
-                    for (int r = 0; r < EPL; ++r)
-                        if (ea + r >= e0 && ea + r < e1)
+                        for (int r = 0; r < EPL; ++r)
                             Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[r])], Ent::y(c[r]), acc);
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < EPL; ++r)
+                            if (ea + r >= e0 && ea + r < e1)
+                                Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[r])], Ent::y(c[r]), acc);
+                    }
                 }
             }
         }
@@ -832,6 +850,30 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
         A = An;
         e0 = f0;
         e1 = f1;
+        if constexpr (Pass::TABLES) __syncwarp();  // the table slot is rewritten next
+    }
+}
+
+// psi(v + a) - psi(a) and psi1(v + a) - psi1(a) (v < kPsiTab), psi(a),
+// psi1(a) for every active gene of an MLE evaluation (a = 1/theta), built
+// as the block-per-gene pass builds them; the slice-major pass copies a
+// gene's tables into shared memory once per (gene, slice)
+__global__ void __launch_bounds__(32) grp_psi_tables_kernel(const int32_t* act, const int32_t* n_act,
+                                                            const double* log_theta, double* tab) {
+    __shared__ double a[1];
+    __shared__ double t[2 * kPsiTab];
+    __shared__ double scr[kPsiTab];
+    const int slot = blockIdx.x;
+    if (slot >= *n_act) return;
+    const double th = exp(log_theta[__ldg(act + slot)]);
+    if (threadIdx.x == 0) a[0] = 1.0 / th;
+    __syncthreads();
+    build_psi_tables(1, a, t, scr);
+    double* o = tab + (int64_t)slot * kGrpTab;
+    for (int i = threadIdx.x; i < 2 * kPsiTab; i += 32) o[i] = t[i];
+    if (threadIdx.x == 0) {
+        o[2 * kPsiTab] = digamma_d(a[0]);
+        o[2 * kPsiTab + 1] = trigamma_d(a[0]);
     }
 }
 
@@ -920,7 +962,11 @@ template <class Pass>
 static cudaError_t slices_run(const GrpGeom& geo, typename Pass::Params prm, int val_u16,
                               int max_slots, int tile, cudaStream_t st) {
     constexpr int NQ = Pass::NW + Pass::NV + Pass::NF + Pass::NS;
-    const size_t smem = (size_t)kSliceCells * sizeof(double);
+    const size_t smem = ((size_t)kSliceCells + (Pass::TABLES ? (kSlNT / 32) * kGrpTab : 0)) *
+                        sizeof(double);
+    if constexpr (Pass::TABLES)
+        grp_psi_tables_kernel<<<(unsigned)max_slots, 32, 0, st>>>(geo.act, geo.n_act, prm.log_theta,
+                                                                 geo.psitab);
     const int64_t nrow = (int64_t)max_slots * geo.U;
     grp_rowexp_kernel<<<nblk(nrow, 256), 256, 0, st>>>(geo, prm.beta_d, max_slots);
     dim3 grid((unsigned)geo.S, (unsigned)((max_slots + tile - 1) / tile));
@@ -944,6 +990,9 @@ cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParam
     if (kind == PASS_IRLS)
         return slices_run<PassIRLS>(geo, PassIRLS::Params{pa.beta, pa.beta_d, pa.k}, val_u16,
                                     max_slots, tile, st);
+    if (kind == PASS_MLE)
+        return slices_run<PassMLE>(geo, PassMLE::Params{pa.beta, pa.beta_d, pa.log_theta}, val_u16,
+                                   max_slots, tile, st);
     return cudaErrorInvalidValue;
 }
 

@@ -125,11 +125,11 @@ struct RecAcc {
     DEV void fscal(R v) { w[NW + NV + K] += v; }
 };
 
-// 1/x in FP64 for x > 0: the MUFU estimate (rcp.approx.ftz.f64, about 23
+// 1/x in FP64 for x > 0: the MUFU estimate (rcp.approx.ftz.f64, about 20
 // correct bits) refined by Newton-Raphson steps r <- r + r (1 - x r), each
 // of which doubles the number of correct bits: two steps give the quotient
-// to within an ulp, one step to ~1e-14 relative (plenty for terms that are
-// summed over cells).  x = +inf gives 0, as the quotient does.
+// to within an ulp, one step to ~1e-12 relative (plenty for terms that are
+// summed over cells).  rcp_nr gives 0 for x = +inf, as the quotient does.
 DEV double rcp_nr(double x) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
@@ -139,12 +139,13 @@ DEV double rcp_nr(double x) {
     r = fma(r, e, r);
     return isinf(x) ? 0.0 : r;
 }
+// (one step, and no special case for x = +inf: there the pass's dense term
+// mu / (mu + k) is already NaN, whatever the reciprocal returns)
 DEV double rcp_nr1(double x) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
     const double e = fma(-x, r, 1.0);
-    r = fma(r, e, r);
-    return isinf(x) ? 0.0 : r;
+    return fma(r, e, r);
 }
 
 // reciprocal in the arithmetic of the pass: MUFU estimate in FP32, the

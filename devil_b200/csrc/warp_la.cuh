@@ -88,7 +88,7 @@ DEV double warp_lu_solve(const double* A, int ld, int P, const int* perm, const 
     const int lane = threadIdx.x & 31;
     // forward: rows in pivot order, unit lower factor; lane r holds the
     // running value of row r, y_k is row perm[k]'s value at step k
-    const int my_step = lane < P ? step[lane] : P;
+    const int my_step = lane < P ? step[lane] : -1;  // lanes without a row take no part
     double c = lane < P ? b_own : 0.0;
     double y_mine = 0.0;  // y_{lane}: lane k keeps y_k
     for (int k = 0; k < P; ++k) {
