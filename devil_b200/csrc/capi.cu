@@ -968,8 +968,10 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
             gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * grp_slices_nq(kind));
             gg.rowexp = ws<double>(ctx, "grp_rowexp", (size_t)tiles * gg.U);
             if (kind == PASS_MLE) gg.psitab = ws<double>(ctx, "grp_psitab", (size_t)tiles * kGrpTab);
+            // (the IRLS step folds the assembly into its finalize)
             LAUNCH(launch_grp_slices(kind, gg, prm, dp.val_u16, tiles,
-                                     grp_slices_tile(tiles, gg.S, ctx->sm_count), ctx->stream));
+                                     grp_slices_tile(tiles, gg.S, ctx->sm_count), kind != PASS_IRLS,
+                                     ctx->stream));
         } else {
             LAUNCH(launch_grp_pass(kind, gg, prm, dp.val_u16, tiles, ctx->stream));
         }
@@ -1064,9 +1066,19 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
                     dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
         ++launched;
         const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC;
-        LAUNCH(launch_irls_finalize(pb.partW, part_f64, nseg, tiles * plan.GT, dp.P, act[cur], cnt + cur,
-                                    (int)hint, act[nxt], cnt + nxt, beta, beta_f, iters, status,
-                                    max_iter, eps, k, st));
+        if (plan.engine == ENGINE_GRP && (ctx->grp_slices & 1)) {
+            // slice-major pass: the assembly is part of the step
+            GrpGeom gg = grp_geom(dp);
+            gg.act = act[cur];
+            gg.n_act = cnt + cur;
+            gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * 2);
+            LAUNCH(launch_grp_irls_finalize(gg, (int)hint, act[nxt], cnt + nxt, beta, beta_f, iters,
+                                            status, max_iter, eps, k, st));
+        } else {
+            LAUNCH(launch_irls_finalize(pb.partW, part_f64, nseg, tiles * plan.GT, dp.P, act[cur],
+                                        cnt + cur, (int)hint, act[nxt], cnt + nxt, beta, beta_f,
+                                        iters, status, max_iter, eps, k, st));
+        }
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
@@ -1391,8 +1403,19 @@ void fit_pipeline(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
         CK(cudaStreamSynchronize(st));
         if (herr) fail(ctx, DEVIL_ERR_SINGULAR, "design matrix is rank deficient");
     }
-    if (dp.grp.active && !o->init_beta_rough)
-        LAUNCH(launch_grp_init_beta(grp_geom(dp), dp.val_u16, ginv, G, fb.beta, fb.beta_f, st));
+    if (dp.grp.active && !o->init_beta_rough) {
+        GrpGeom gg = grp_geom(dp);
+        int32_t* cnt = nullptr;
+        gg.act = all_genes(ctx, dp, &cnt);
+        gg.n_act = cnt;
+        gg.reset_next = nullptr;
+        gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)G * gg.S);
+        gg.rowexp = ws<double>(ctx, "grp_rowexp", (size_t)G * gg.U);
+        double* zb = ws<double>(ctx, "grp_zero_beta", (size_t)G * P);
+        CK(cudaMemsetAsync(zb, 0, (size_t)G * P * sizeof(double), st));
+        LAUNCH(launch_grp_init_beta(gg, dp.val_u16, zb, ginv, G, grp_slices_tile(G, gg.S, ctx->sm_count),
+                                    fb.beta, fb.beta_f, st));
+    }
     else
         LAUNCH(launch_init_beta(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.Xdrm, dp.xs, dp.off,
                                 ws<double>(ctx, "inv_sf", dp.n), ginv, dp.stats, G, dp.n, P,

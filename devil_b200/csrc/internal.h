@@ -92,7 +92,7 @@ constexpr int kMaxFine = 4096;        // (design row, cluster) pairs
 constexpr int kMinCellsPerGroup = 32; // grouping pays when groups are larger
 constexpr int kSliceCells = 8192;     // cells per slice (its exp(offset) fits shared memory)
 constexpr int kGrpTab = 2 * kPsiTab + 2;  // per-gene psi tables + psi(a), psi1(a)
-constexpr int kMaxSlices = 12288;     // the CSR copy's per-warp key table stays <= 48 KB
+constexpr int kMaxSlices = 12288;     // the CSR copy's per-warp key table stays <= 48 KB; keys fit 16 bits
 
 // One entry of the slice-ordered CSR copy of the design-group engine: the
 // cell's index within its slice and the count.
@@ -187,13 +187,16 @@ cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsA
 int grp_slices_tile(int64_t hint, int S, int sm_count);
 int grp_slices_nq(PassKind k);
 cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm,
-                              int val_u16, int max_slots, int tile, cudaStream_t st);
+                              int val_u16, int max_slots, int tile, bool assemble, cudaStream_t st);
 // cells in key order: sl_cell / sl_loc per original cell, E in slice order
 cudaError_t launch_slice_cells(const int32_t* pnew, const int32_t* sl_start, int S, int64_t n,
                                const double* off, int32_t* cslice, int32_t* cloc, double* E,
                                cudaStream_t st);
-cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* ginv, int64_t G,
-                                 double* beta, float* beta_f, cudaStream_t st);
+// beta_0 of a grouped design: geo.act / geo.n_act list every gene, geo.gsum
+// holds G x S doubles, geo.rowexp G x U; zero_beta is G x P zeros
+cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* zero_beta,
+                                 const double* ginv, int64_t G, int tile, double* beta,
+                                 float* beta_f, cudaStream_t st);
 cudaError_t launch_row_hash(const double* X, int64_t n, int P, uint64_t* h, int32_t* idx,
                             cudaStream_t st);
 cudaError_t launch_group_heads(const double* X, int64_t n, int P, const uint64_t* hs,
@@ -285,6 +288,13 @@ cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slo
                                  int32_t* act_next, int32_t* n_next, double* beta, float* beta_f,
                                  int32_t* iters, int32_t* status, int max_iter, double eps,
                                  const float* k, cudaStream_t st);
+// the IRLS step of the design-group engine's slice-major pass, the p x p
+// assembly from geo.gsum folded in (geo.act / geo.n_act: this iteration's
+// active genes)
+cudaError_t launch_grp_irls_finalize(const GrpGeom& geo, int max_slots, int32_t* act_next,
+                                     int32_t* n_next, double* beta, float* beta_f, int32_t* iters,
+                                     int32_t* status, int max_iter, double eps, const float* k,
+                                     cudaStream_t st);
 cudaError_t launch_mom_finalize(const double* partS, int nseg, int slot_stride,
                                 const int32_t* act, const int32_t* n_act, int max_slots,
                                 int64_t n, int P, double* theta, cudaStream_t st);

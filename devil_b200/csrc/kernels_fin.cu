@@ -120,6 +120,106 @@ cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slo
 }
 
 // ------------------------------------------------------------------
+// IRLS step of the design-group engine's slice-major pass, warp per gene,
+// with the assembly folded in: the group sums of the gene's per-slice sums
+// (slice order), H = k^2 sum over (group, pair) lists, score = -k sum over
+// (group, entry) lists -- the same sums in the same order as
+// grp_assemble_kernel + irls_finalize_kernel, without the round trip of the
+// p x p partial sums through global memory -- then the LU, the solve and the
+// update of irls_finalize_kernel.
+// ------------------------------------------------------------------
+__global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t* n_next,
+                                         double* beta, float* beta_f, int32_t* iters,
+                                         int32_t* status, int max_iter, double eps,
+                                         const float* kf) {
+    extern __shared__ double fsh[];
+    const int P = geo.P, U = geo.U, C = geo.C, S = geo.S, LD = wla_ld(P);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = 2 * U + P * LD + P;  // group sums, H, then perm and step (P ints each)
+    double* gs = fsh + warp * per;
+    double* H = gs + 2 * U;
+    int* perm = reinterpret_cast<int*>(H + P * LD);
+    int* step = perm + P;
+    const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (slot >= *geo.n_act) return;
+    const int g = geo.act[slot];
+    const double* gsum = geo.gsum + (int64_t)slot * S * 2;
+    for (int i = lane; i < 2 * U; i += 32) {
+        const int q = i >> 1, c = i & 1;
+        double v = 0.0;
+        for (int sl = __ldg(geo.kslice + q * C); sl < __ldg(geo.kslice + q * C + C); ++sl)
+            v += gsum[sl * 2 + c];
+        gs[i] = v;
+    }
+    __syncwarp();
+    // the pass accumulates H / k^2 and -score / k (see PassIRLS)
+    const double k = (double)kf[g];
+    const double k2 = k * k;
+    const int NE = P * (P + 1) / 2;
+    for (int a = lane; a < NE; a += 32) {
+        double s = 0.0;
+        for (int e = __ldg(geo.qptr + a); e < __ldg(geo.qptr + a + 1); ++e)
+            s += gs[__ldg(geo.qu + e) * 2] * __ldg(geo.qv + e);
+        // packed upper-triangle index a = j (j + 1) / 2 + i, i <= j
+        int j = (int)((sqrtf(8.f * (float)a + 1.f) - 1.f) * 0.5f);
+        while (j * (j + 1) / 2 > a) --j;
+        while ((j + 1) * (j + 2) / 2 <= a) ++j;
+        const int i = a - j * (j + 1) / 2;
+        const double v = s * k2;
+        H[i * LD + j] = v;
+        H[j * LD + i] = v;
+    }
+    double s_own = 0.0;
+    if (lane < P) {
+        double s = 0.0;
+        for (int e = __ldg(geo.vptr + lane); e < __ldg(geo.vptr + lane + 1); ++e)
+            s += gs[__ldg(geo.vu + e) * 2 + 1] * __ldg(geo.vv + e);
+        s_own = -k * s;
+    }
+    __syncwarp();
+    warp_lu(H, LD, P, perm, step);
+    const double x_own = warp_lu_solve(H, LD, P, perm, step, s_own);
+    if (lane < P) {
+        const double b = beta[(int64_t)g * P + lane] + x_own;
+        beta[(int64_t)g * P + lane] = b;
+        beta_f[(int64_t)g * P + lane] = (float)b;
+    }
+    double mx = lane < P ? fabs(x_own) : 0.0;
+    mx = (mx == mx) ? mx : 0.0;  // NaN entries never compare greater
+    mx = warp_max(mx);
+    const double x0 = __shfl_sync(0xffffffffu, x_own, 0);
+    if (lane != 0) return;
+    const int it = iters[g] + 1;
+    iters[g] = it;
+    if (!(x0 == x0)) {
+        status[g] = 2;  // DEVIL_GENE_NAN
+    } else if (mx < eps) {
+        status[g] = 0;
+    } else if (it >= max_iter) {
+        status[g] = 1;
+    } else {
+        act_next[atomicAdd(n_next, 1)] = g;
+    }
+}
+
+cudaError_t launch_grp_irls_finalize(const GrpGeom& geo, int max_slots, int32_t* act_next,
+                                     int32_t* n_next, double* beta, float* beta_f, int32_t* iters,
+                                     int32_t* status, int max_iter, double eps, const float* k,
+                                     cudaStream_t st) {
+    if (max_slots <= 0) return cudaSuccess;
+    const size_t per = (size_t)(2 * geo.U + geo.P * wla_ld(geo.P) + geo.P) * sizeof(double);
+    const int w = fin_warps(per);
+    const size_t smem = per * w;
+    if (smem > 48 * 1024) {
+        cudaError_t e = raise_dyn_smem(grp_irls_finalize_kernel, smem);
+        if (e != cudaSuccess) return e;
+    }
+    grp_irls_finalize_kernel<<<nblk(max_slots, w), 32 * w, smem, st>>>(
+        geo, act_next, n_next, beta, beta_f, iters, status, max_iter, eps, k);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------
 // MOM (src/mom_overdispersion.cpp:47-53)
 // ------------------------------------------------------------------
 __global__ void mom_finalize_kernel(const double* partS, int nseg, int slot_stride,

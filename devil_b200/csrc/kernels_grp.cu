@@ -25,6 +25,8 @@
 // finalize kernels are shared.
 #include <cub/cub.cuh>
 
+#include <type_traits>
+
 #include "internal.h"
 
 namespace devil {
@@ -376,7 +378,8 @@ __global__ void __launch_bounds__(kRuleNT) group_rules_kernel(
 //   2. per gene, turn the counts into the first output position of every
 //      (segment, key) in key-major, segment-minor order (block per gene),
 //   3. scatter every segment's entries from those cursors, in order
-//      (warp per segment; ranks among equal keys from __match_any_sync).
+//      (block per segment: a stable sort by key in shared memory, then
+//      each key's run written to its contiguous range).
 // ---------------------------------------------------------------------
 __global__ void seg_count_kernel(const int64_t* rowptr, int64_t G, int S, int64_t* nseg) {
     int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -444,43 +447,81 @@ __global__ void __launch_bounds__(kOffNT) seg_offsets_kernel(const int64_t* rowp
     if (t == 0) gptr[g * (K + 1) + K] = rowptr[g + 1];
 }
 
+// The scatter with coalesced writes: a block takes one segment in chunks
+// of kSortItems entries, sorts each chunk by key in shared memory (a stable
+// block radix sort, so the original order within a key is kept) and writes
+// every key's run to its contiguous range of the output, so consecutive
+// threads write consecutive entries (a warp-per-segment scatter writes each
+// 4-byte entry to its own 32-byte sector).
+constexpr int kSortNT = 256, kSortIPT = 8, kSortItems = kSortNT * kSortIPT;
+
 template <class VT>
-__global__ void seg_scatter_kernel(const int64_t* rowptr, const int32_t* col, const VT* val,
-                                   int64_t G, const int64_t* segbase, int S, const int32_t* ckey,
-                                   const int32_t* cloc, int K, const int32_t* hist,
-                                   typename GrpEnt<VT>::T* gent) {
-    extern __shared__ int32_t cur_all[];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
-    if (s >= segbase[G]) return;
-    int32_t* cur = cur_all + (int64_t)w * K;
-    for (int k = lane; k < K; k += 32) cur[k] = hist[s * K + k];
-    __syncwarp();
-    const int64_t g = seg_gene(segbase, G, s);
+__global__ void __launch_bounds__(kSortNT) seg_scatter_sorted_kernel(
+    const int64_t* rowptr, const int32_t* col, const VT* val, int64_t G, const int64_t* segbase,
+    int S, const int32_t* ckey, const int32_t* cloc, int K, int kbits, const int32_t* hist,
+    typename GrpEnt<VT>::T* gent) {
+    using ET = typename GrpEnt<VT>::T;
+    using Sort = cub::BlockRadixSort<uint16_t, kSortNT, kSortIPT, ET>;
+    using Scan = cub::BlockScan<int, kSortNT>;
+    __shared__ union {
+        typename Sort::TempStorage sort;
+        typename Scan::TempStorage scan;
+    } tmp;
+    __shared__ uint16_t skey[kSortItems + 1];
+    extern __shared__ int32_t cur[];  // [K] output cursors of this segment
+    const int64_t seg = blockIdx.x;
+    if (seg >= segbase[G]) return;
+    const int t = threadIdx.x;
+    for (int k = t; k < K; k += kSortNT) cur[k] = hist[seg * K + k];
+    const int64_t g = seg_gene(segbase, G, seg);
     const int64_t rs = rowptr[g];
-    const int64_t r0 = rs + (s - segbase[g]) * S;
+    const int64_t r0 = rs + (seg - segbase[g]) * S;
     const int64_t r1 = min(r0 + S, rowptr[g + 1]);
-    const unsigned lt = (1u << lane) - 1u;
-    for (int64_t base = r0; base < r1; base += 32) {
-        const int64_t e = base + lane;
-        const bool valid = e < r1;
-        int c = 0;
-        VT v = VT(0);
-        int k = -1;
-        if (valid) {
-            c = col[e];
-            v = val[e];
-            k = ckey[c];
+    __syncthreads();
+    for (int64_t c0 = r0; c0 < r1; c0 += kSortItems) {
+        uint16_t key[kSortIPT];
+        ET ent[kSortIPT];
+#pragma unroll
+        for (int j = 0; j < kSortIPT; ++j) {
+            const int64_t e = c0 + t * kSortIPT + j;  // blocked: the original order
+            if (e < r1) {
+                const int c = col[e];
+                key[j] = (uint16_t)ckey[c];
+                ent[j] = GrpEnt<VT>::pack(cloc[c], val[e]);
+            } else {
+                key[j] = (uint16_t)K;  // after every real key
+                ent[j] = ET();
+            }
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, k);
-        const int rank = __popc(peers & lt);
-        const int pos = valid ? cur[k] + rank : 0;
-        __syncwarp();
-        if (valid) {
-            gent[rs + pos] = GrpEnt<VT>::pack(cloc[c], v);
-            if (lane == __ffs(peers) - 1) cur[k] += __popc(peers);
+        Sort(tmp.sort).Sort(key, ent, 0, kbits);
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kSortIPT; ++j) skey[t * kSortIPT + j] = key[j];
+        if (t == 0) skey[kSortItems] = (uint16_t)(K + 1);
+        __syncthreads();
+        // start of each item's run of equal keys: inclusive max-scan of the
+        // run heads' positions
+        int head[kSortIPT];
+#pragma unroll
+        for (int j = 0; j < kSortIPT; ++j) {
+            const int i = t * kSortIPT + j;
+            head[j] = (i == 0 || skey[i - 1] != key[j]) ? i : 0;
         }
-        __syncwarp();
+        int start[kSortIPT];
+        Scan(tmp.scan).InclusiveScan(head, start, cub::Max());
+#pragma unroll
+        for (int j = 0; j < kSortIPT; ++j) {
+            const int i = t * kSortIPT + j;
+            if (key[j] < K) gent[rs + cur[key[j]] + (i - start[j])] = ent[j];
+        }
+        __syncthreads();
+        // advance the cursors: the last item of each run adds the run length
+#pragma unroll
+        for (int j = 0; j < kSortIPT; ++j) {
+            const int i = t * kSortIPT + j;
+            if (key[j] < K && skey[i + 1] != key[j]) cur[key[j]] += i - start[j] + 1;
+        }
+        __syncthreads();
     }
 }
 
@@ -761,7 +802,8 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
     for (int i = t; i < nc; i += blockDim.x) Es[i] = __ldg(geo.E + c0 + i);
     const int u = __ldg(geo.sl_key + s) / geo.C;
     const bool first = s == __ldg(geo.kslice + u * geo.C);  // the group's rule goes here
-    const int m = first ? __ldg(geo.rm + u) : 0;
+    constexpr bool kRule = !std::is_same<Pass, PassInitZ>::value;  // zero counts contribute
+    const int m = (kRule && first) ? __ldg(geo.rm + u) : 0;
     __syncthreads();
     const uint4* __restrict__ v4 = static_cast<const uint4*>(geo.gent);
     // per gene: exp(x_u . beta) (from grp_rowexp_kernel) and the slice's
@@ -960,7 +1002,7 @@ int grp_slices_tile(int64_t hint, int S, int sm_count) {
 
 template <class Pass>
 static cudaError_t slices_run(const GrpGeom& geo, typename Pass::Params prm, int val_u16,
-                              int max_slots, int tile, cudaStream_t st) {
+                              int max_slots, int tile, bool assemble, cudaStream_t st) {
     constexpr int NQ = Pass::NW + Pass::NV + Pass::NF + Pass::NS;
     const size_t smem = ((size_t)kSliceCells + (Pass::TABLES ? (kSlNT / 32) * kGrpTab : 0)) *
                         sizeof(double);
@@ -977,7 +1019,7 @@ static cudaError_t slices_run(const GrpGeom& geo, typename Pass::Params prm, int
         return cudaGetLastError();
     };
     cudaError_t e = val_u16 ? go(grp_slices_kernel<Pass, uint16_t>) : go(grp_slices_kernel<Pass, float>);
-    if (e != cudaSuccess) return e;
+    if (e != cudaSuccess || !assemble) return e;
     grp_assemble_kernel<Pass><<<(unsigned)max_slots, 256, (size_t)geo.U * NQ * sizeof(double), st>>>(geo);
     return cudaGetLastError();
 }
@@ -985,50 +1027,41 @@ static cudaError_t slices_run(const GrpGeom& geo, typename Pass::Params prm, int
 int grp_slices_nq(PassKind k) { return pass_nw(k) + pass_nv(k) + pass_nf(k) + pass_ns(k); }
 
 cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& pa,
-                              int val_u16, int max_slots, int tile, cudaStream_t st) {
+                              int val_u16, int max_slots, int tile, bool assemble, cudaStream_t st) {
     if (max_slots <= 0) return cudaSuccess;
     if (kind == PASS_IRLS)
         return slices_run<PassIRLS>(geo, PassIRLS::Params{pa.beta, pa.beta_d, pa.k}, val_u16,
-                                    max_slots, tile, st);
+                                    max_slots, tile, assemble, st);
     if (kind == PASS_MLE)
         return slices_run<PassMLE>(geo, PassMLE::Params{pa.beta, pa.beta_d, pa.log_theta}, val_u16,
-                                   max_slots, tile, st);
+                                   max_slots, tile, assemble, st);
     return cudaErrorInvalidValue;
 }
 
 // init_beta (R/beta.R:12-24) on a grouped design: X' z with
-// z = log1p(y / exp(offset)) (zero where y = 0) is sum_u x_u sum_{i in u,
-// y_i > 0} z_i, so the nonzeros are read once and summed per group;
-// beta_0 = (X'X)^-1 X' z.  Block per gene, warps over groups.
-template <class VT>
-__global__ void grp_init_beta_kernel(GrpGeom geo, const double* ginv, int64_t G, double* beta,
-                                     float* beta_f) {
-    using Ent = GrpEnt<VT>;
-    using ET = typename Ent::T;
-    __shared__ double su[kMaxGroups];
+// z = log1p(y / exp(offset)) (zero where y = 0) is sum_u x_u z_u where z_u
+// sums the group's nonzeros, so the nonzeros are read once
+// (grp_slices_kernel<PassInitZ>, per-(gene, slice) sums) and then, per gene,
+// z_u = the sum over the group's slices, r = X' z = sum_u x_u z_u and
+// beta_0 = (X'X)^-1 r.
+__global__ void grp_init_finish_kernel(GrpGeom geo, const double* ginv, int64_t G, double* beta,
+                                       float* beta_f) {
+    __shared__ double zu[kMaxGroups];
     __shared__ double r[32];
     const int64_t g = blockIdx.x;
     if (g >= G) return;
-    const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
+    const int t = threadIdx.x, nt = blockDim.x;
     const int U = geo.U, C = geo.C, P = geo.P, S = geo.S;
-    const int64_t* gp = geo.gptr + g * (S + 1);
-    const ET* gent = static_cast<const ET*>(geo.gent);
-    for (int u = warp; u < U; u += nw) {
+    const double* gs = geo.gsum + g * S;
+    for (int u = t; u < U; u += nt) {
         double z = 0.0;
-        for (int sl = __ldg(geo.kslice + u * C); sl < __ldg(geo.kslice + u * C + C); ++sl) {
-            const double* Es = geo.E + __ldg(geo.sl_start + sl);
-            for (int64_t e = gp[sl] + lane; e < gp[sl + 1]; e += 32) {
-                const ET c = gent[e];
-                z += log1p((double)Ent::y(c) / Es[Ent::loc(c)]);
-            }
-        }
-        z = warp_sum(z);
-        if (lane == 0) su[u] = z;
+        for (int sl = __ldg(geo.kslice + u * C); sl < __ldg(geo.kslice + u * C + C); ++sl) z += gs[sl];
+        zu[u] = z;
     }
     __syncthreads();
     if (t < P) {
         double v = 0.0;
-        for (int u = 0; u < U; ++u) v += geo.xg[u * P + t] * su[u];
+        for (int u = 0; u < U; ++u) v += geo.xg[u * P + t] * zu[u];
         r[t] = v;
     }
     __syncthreads();
@@ -1040,14 +1073,24 @@ __global__ void grp_init_beta_kernel(GrpGeom geo, const double* ginv, int64_t G,
     }
 }
 
-cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* ginv, int64_t G,
-                                 double* beta, float* beta_f, cudaStream_t st) {
+cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* zero_beta,
+                                 const double* ginv, int64_t G, int tile, double* beta,
+                                 float* beta_f, cudaStream_t st) {
     if (G <= 0) return cudaSuccess;
-    const int nt = 32 * (geo.U < 8 ? (geo.U < 1 ? 1 : geo.U) : 8);
-    if (val_u16)
-        grp_init_beta_kernel<uint16_t><<<(unsigned)G, nt, 0, st>>>(geo, ginv, G, beta, beta_f);
-    else
-        grp_init_beta_kernel<float><<<(unsigned)G, nt, 0, st>>>(geo, ginv, G, beta, beta_f);
+    PassInitZ::Params prm{nullptr, zero_beta};
+    const size_t smem = (size_t)kSliceCells * sizeof(double);
+    const int64_t nrow = G * geo.U;
+    grp_rowexp_kernel<<<nblk(nrow, 256), 256, 0, st>>>(geo, zero_beta, G);  // exp(0) = 1
+    dim3 grid((unsigned)geo.S, (unsigned)((G + tile - 1) / tile));
+    auto go = [&](auto kern) -> cudaError_t {
+        cudaError_t e = raise_dyn_smem(kern, smem);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, kSlNT, smem, st>>>(geo, prm, tile);
+        return cudaGetLastError();
+    };
+    cudaError_t e = val_u16 ? go(grp_slices_kernel<PassInitZ, uint16_t>) : go(grp_slices_kernel<PassInitZ, float>);
+    if (e != cudaSuccess) return e;
+    grp_init_finish_kernel<<<(unsigned)G, 64, 0, st>>>(geo, ginv, G, beta, beta_f);
     return cudaGetLastError();
 }
 
@@ -1196,15 +1239,26 @@ cudaError_t launch_group_csr(const int64_t* rowptr, const int32_t* col, const vo
     const unsigned grid = (unsigned)((nsegs + wpb - 1) / wpb);
     if (grid > 0) seg_hist_kernel<<<grid, 32 * wpb, smem, st>>>(rowptr, col, G, segbase, S, ckey, K, hist);
     seg_offsets_kernel<<<(unsigned)G, kOffNT, 0, st>>>(rowptr, G, segbase, K, hist, gptr);
-    if (grid > 0) {
-        if (val_u16)
-            seg_scatter_kernel<uint16_t><<<grid, 32 * wpb, smem, st>>>(
-                rowptr, col, static_cast<const uint16_t*>(val), G, segbase, S, ckey, cloc, K, hist,
-                static_cast<GrpEnt<uint16_t>::T*>(gent));
-        else
-            seg_scatter_kernel<float><<<grid, 32 * wpb, smem, st>>>(
-                rowptr, col, static_cast<const float*>(val), G, segbase, S, ckey, cloc, K, hist,
-                static_cast<GrpEnt<float>::T*>(gent));
+    if (nsegs > 0) {
+        // block radix sort per chunk, coalesced runs (K <= kMaxSlices: keys fit 16 bits)
+        int kbits = 1;
+        while ((1 << kbits) <= K + 1) ++kbits;
+        const size_t csm = (size_t)K * sizeof(int32_t);
+        if (val_u16) {
+            auto k = seg_scatter_sorted_kernel<uint16_t>;
+            cudaError_t e = raise_dyn_smem(k, csm);
+            if (e != cudaSuccess) return e;
+            k<<<(unsigned)nsegs, kSortNT, csm, st>>>(rowptr, col, static_cast<const uint16_t*>(val), G,
+                                                     segbase, S, ckey, cloc, K, kbits, hist,
+                                                     static_cast<GrpEnt<uint16_t>::T*>(gent));
+        } else {
+            auto k = seg_scatter_sorted_kernel<float>;
+            cudaError_t e = raise_dyn_smem(k, csm);
+            if (e != cudaSuccess) return e;
+            k<<<(unsigned)nsegs, kSortNT, csm, st>>>(rowptr, col, static_cast<const float*>(val), G,
+                                                     segbase, S, ckey, cloc, K, kbits, hist,
+                                                     static_cast<GrpEnt<float>::T*>(gent));
+        }
     }
     return cudaGetLastError();
 }

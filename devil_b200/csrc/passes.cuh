@@ -392,6 +392,28 @@ struct PassMLE {
     }
 };
 
+// init_beta's right-hand side on a grouped design (R/beta.R:12-24): the sum
+// over the gene's nonzeros of log1p(y / exp(offset)) (zero counts give
+// log1p(0) = 0).  Run by the slice-major pass with beta = 0, where mu is
+// exp(offset) itself.
+struct PassInitZ {
+    static constexpr int NF = 0;
+    static constexpr int NW = 0, NV = 0, NS = 1;
+    static constexpr bool F64 = true;
+    static constexpr bool TABLES = false;
+    using AW = double;
+    using AS = double;
+    struct Params { const float* beta; const double* beta_d; };
+    struct Gene { int dummy; };
+    static DEV Gene load(const Params&, int) { return Gene{0}; }
+    template <class R, class A>
+    static DEV void dense(const Gene&, R, A&) {}
+    template <class R, class A>
+    static DEV void sparse(const Gene&, R mu, float y, A& acc) {
+        acc.template scal<0>(log1p((double)y / (double)mu));
+    }
+};
+
 // compute_hessian (src/variance.cpp:22-47) and the per-cluster score sums of
 // compute_clustered_meat_fast (src/variance.cpp:207-217) in one pass:
 //   outer0 = X' diag((y theta + 1) mu / (1 + theta mu)^2) X
