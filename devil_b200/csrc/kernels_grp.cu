@@ -378,8 +378,7 @@ __global__ void __launch_bounds__(kRuleNT) group_rules_kernel(
 //   2. per gene, turn the counts into the first output position of every
 //      (segment, key) in key-major, segment-minor order (block per gene),
 //   3. scatter every segment's entries from those cursors, in order
-//      (block per segment: a stable sort by key in shared memory, then
-//      each key's run written to its contiguous range).
+//      (warp per segment; ranks among equal keys from __match_any_sync).
 // ---------------------------------------------------------------------
 __global__ void seg_count_kernel(const int64_t* rowptr, int64_t G, int S, int64_t* nseg) {
     int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -447,81 +446,43 @@ __global__ void __launch_bounds__(kOffNT) seg_offsets_kernel(const int64_t* rowp
     if (t == 0) gptr[g * (K + 1) + K] = rowptr[g + 1];
 }
 
-// The scatter with coalesced writes: a block takes one segment in chunks
-// of kSortItems entries, sorts each chunk by key in shared memory (a stable
-// block radix sort, so the original order within a key is kept) and writes
-// every key's run to its contiguous range of the output, so consecutive
-// threads write consecutive entries (a warp-per-segment scatter writes each
-// 4-byte entry to its own 32-byte sector).
-constexpr int kSortNT = 256, kSortIPT = 8, kSortItems = kSortNT * kSortIPT;
-
 template <class VT>
-__global__ void __launch_bounds__(kSortNT) seg_scatter_sorted_kernel(
-    const int64_t* rowptr, const int32_t* col, const VT* val, int64_t G, const int64_t* segbase,
-    int S, const int32_t* ckey, const int32_t* cloc, int K, int kbits, const int32_t* hist,
-    typename GrpEnt<VT>::T* gent) {
-    using ET = typename GrpEnt<VT>::T;
-    using Sort = cub::BlockRadixSort<uint16_t, kSortNT, kSortIPT, ET>;
-    using Scan = cub::BlockScan<int, kSortNT>;
-    __shared__ union {
-        typename Sort::TempStorage sort;
-        typename Scan::TempStorage scan;
-    } tmp;
-    __shared__ uint16_t skey[kSortItems + 1];
-    extern __shared__ int32_t cur[];  // [K] output cursors of this segment
-    const int64_t seg = blockIdx.x;
-    if (seg >= segbase[G]) return;
-    const int t = threadIdx.x;
-    for (int k = t; k < K; k += kSortNT) cur[k] = hist[seg * K + k];
-    const int64_t g = seg_gene(segbase, G, seg);
+__global__ void seg_scatter_kernel(const int64_t* rowptr, const int32_t* col, const VT* val,
+                                   int64_t G, const int64_t* segbase, int S, const int32_t* ckey,
+                                   const int32_t* cloc, int K, const int32_t* hist,
+                                   typename GrpEnt<VT>::T* gent) {
+    extern __shared__ int32_t cur_all[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
+    if (s >= segbase[G]) return;
+    int32_t* cur = cur_all + (int64_t)w * K;
+    for (int k = lane; k < K; k += 32) cur[k] = hist[s * K + k];
+    __syncwarp();
+    const int64_t g = seg_gene(segbase, G, s);
     const int64_t rs = rowptr[g];
-    const int64_t r0 = rs + (seg - segbase[g]) * S;
+    const int64_t r0 = rs + (s - segbase[g]) * S;
     const int64_t r1 = min(r0 + S, rowptr[g + 1]);
-    __syncthreads();
-    for (int64_t c0 = r0; c0 < r1; c0 += kSortItems) {
-        uint16_t key[kSortIPT];
-        ET ent[kSortIPT];
-#pragma unroll
-        for (int j = 0; j < kSortIPT; ++j) {
-            const int64_t e = c0 + t * kSortIPT + j;  // blocked: the original order
-            if (e < r1) {
-                const int c = col[e];
-                key[j] = (uint16_t)ckey[c];
-                ent[j] = GrpEnt<VT>::pack(cloc[c], val[e]);
-            } else {
-                key[j] = (uint16_t)K;  // after every real key
-                ent[j] = ET();
-            }
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t base = r0; base < r1; base += 32) {
+        const int64_t e = base + lane;
+        const bool valid = e < r1;
+        int c = 0;
+        VT v = VT(0);
+        int k = -1;
+        if (valid) {
+            c = col[e];
+            v = val[e];
+            k = ckey[c];
         }
-        Sort(tmp.sort).Sort(key, ent, 0, kbits);
-        __syncthreads();
-#pragma unroll
-        for (int j = 0; j < kSortIPT; ++j) skey[t * kSortIPT + j] = key[j];
-        if (t == 0) skey[kSortItems] = (uint16_t)(K + 1);
-        __syncthreads();
-        // start of each item's run of equal keys: inclusive max-scan of the
-        // run heads' positions
-        int head[kSortIPT];
-#pragma unroll
-        for (int j = 0; j < kSortIPT; ++j) {
-            const int i = t * kSortIPT + j;
-            head[j] = (i == 0 || skey[i - 1] != key[j]) ? i : 0;
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        const int rank = __popc(peers & lt);
+        const int pos = valid ? cur[k] + rank : 0;
+        __syncwarp();
+        if (valid) {
+            gent[rs + pos] = GrpEnt<VT>::pack(cloc[c], v);
+            if (lane == __ffs(peers) - 1) cur[k] += __popc(peers);
         }
-        int start[kSortIPT];
-        Scan(tmp.scan).InclusiveScan(head, start, cub::Max());
-#pragma unroll
-        for (int j = 0; j < kSortIPT; ++j) {
-            const int i = t * kSortIPT + j;
-            if (key[j] < K) gent[rs + cur[key[j]] + (i - start[j])] = ent[j];
-        }
-        __syncthreads();
-        // advance the cursors: the last item of each run adds the run length
-#pragma unroll
-        for (int j = 0; j < kSortIPT; ++j) {
-            const int i = t * kSortIPT + j;
-            if (key[j] < K && skey[i + 1] != key[j]) cur[key[j]] += i - start[j] + 1;
-        }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
@@ -808,6 +769,11 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
     const uint4* __restrict__ v4 = static_cast<const uint4*>(geo.gent);
     // per gene: exp(x_u . beta) (from grp_rowexp_kernel) and the slice's
     // entry range; the next gene's are loaded while this one runs
+    // the tile's genes are handed out one at a time (a shared counter), so
+    // warps that drew short genes take more of them
+    __shared__ int next_gene;
+    if (t == 0) next_gene = j0 + nw;
+    __syncthreads();
     int jj = j0 + warp;
     int g = 0;
     double A = 0.0;
@@ -819,7 +785,9 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
         e1 = __ldg(geo.gptr + (int64_t)g * (S + 1) + s + 1);
     }
     while (jj < j1) {
-        const int jn = jj + nw;
+        int jn = 0;
+        if (lane == 0) jn = atomicAdd(&next_gene, 1);
+        jn = __shfl_sync(0xffffffffu, jn, 0);
         int gn = 0;
         double An = 0.0;
         int64_t f0 = 0, f1 = 0;
@@ -1239,26 +1207,15 @@ cudaError_t launch_group_csr(const int64_t* rowptr, const int32_t* col, const vo
     const unsigned grid = (unsigned)((nsegs + wpb - 1) / wpb);
     if (grid > 0) seg_hist_kernel<<<grid, 32 * wpb, smem, st>>>(rowptr, col, G, segbase, S, ckey, K, hist);
     seg_offsets_kernel<<<(unsigned)G, kOffNT, 0, st>>>(rowptr, G, segbase, K, hist, gptr);
-    if (nsegs > 0) {
-        // block radix sort per chunk, coalesced runs (K <= kMaxSlices: keys fit 16 bits)
-        int kbits = 1;
-        while ((1 << kbits) <= K + 1) ++kbits;
-        const size_t csm = (size_t)K * sizeof(int32_t);
-        if (val_u16) {
-            auto k = seg_scatter_sorted_kernel<uint16_t>;
-            cudaError_t e = raise_dyn_smem(k, csm);
-            if (e != cudaSuccess) return e;
-            k<<<(unsigned)nsegs, kSortNT, csm, st>>>(rowptr, col, static_cast<const uint16_t*>(val), G,
-                                                     segbase, S, ckey, cloc, K, kbits, hist,
-                                                     static_cast<GrpEnt<uint16_t>::T*>(gent));
-        } else {
-            auto k = seg_scatter_sorted_kernel<float>;
-            cudaError_t e = raise_dyn_smem(k, csm);
-            if (e != cudaSuccess) return e;
-            k<<<(unsigned)nsegs, kSortNT, csm, st>>>(rowptr, col, static_cast<const float*>(val), G,
-                                                     segbase, S, ckey, cloc, K, kbits, hist,
-                                                     static_cast<GrpEnt<float>::T*>(gent));
-        }
+    if (grid > 0) {
+        if (val_u16)
+            seg_scatter_kernel<uint16_t><<<grid, 32 * wpb, smem, st>>>(
+                rowptr, col, static_cast<const uint16_t*>(val), G, segbase, S, ckey, cloc, K, hist,
+                static_cast<GrpEnt<uint16_t>::T*>(gent));
+        else
+            seg_scatter_kernel<float><<<grid, 32 * wpb, smem, st>>>(
+                rowptr, col, static_cast<const float*>(val), G, segbase, S, ckey, cloc, K, hist,
+                static_cast<GrpEnt<float>::T*>(gent));
     }
     return cudaGetLastError();
 }

@@ -177,33 +177,21 @@ __global__ void gene_stats_kernel(const int64_t* rowptr, const VT* val, int64_t 
     int lane = threadIdx.x & 31;
     if (g >= G) return;
     int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
-    // four entries per lane per round, their loads issued together
     double s = 0.0, sp = 0.0, mx = 0.0;
-    for (int64_t e = e0 + lane; e < e1; e += 128) {
-        double y[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) y[q] = e + 32 * q < e1 ? (double)val[e + 32 * q] : 0.0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {  // absent entries are 0: no contribution
-            s += y[q];
-            sp += (y[q] - 1.0) * y[q];
-            mx = fmax(mx, y[q]);
-        }
+    for (int64_t e = e0 + lane; e < e1; e += 32) {
+        double y = (double)val[e];
+        s += y;
+        sp += (y - 1.0) * y;
+        mx = fmax(mx, y);
     }
     s = warp_sum(s);
     sp = warp_sum(sp);
     mx = warp_max(mx);
     double mean = s / (double)n;
     double ss = 0.0;
-    for (int64_t e = e0 + lane; e < e1; e += 128) {
-        double y[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) y[q] = e + 32 * q < e1 ? (double)val[e + 32 * q] : mean;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const double d = y[q] - mean;
-            ss += d * d;
-        }
+    for (int64_t e = e0 + lane; e < e1; e += 32) {
+        double d = (double)val[e] - mean;
+        ss += d * d;
     }
     ss = warp_sum(ss);
     if (lane == 0) {
@@ -597,21 +585,10 @@ __global__ void validate_csr_kernel(const int64_t* rowptr, const int32_t* col, i
     if (e0 < 0 || e1 < e0 || e1 > nnz) {
         b = 1;
     } else {
-        // four entries per lane per round, their loads issued together
-        for (int64_t e = e0 + lane; e < e1; e += 128) {
-            int c[4], pr[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int64_t ee = e + 32 * q;
-                c[q] = ee < e1 ? col[ee] : 0;
-                pr[q] = (ee < e1 && ee > e0) ? col[ee - 1] : -1;
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (e + 32 * q >= e1) continue;
-                if (c[q] < 0 || c[q] >= n) b = 1;
-                if (pr[q] >= c[q]) b = 1;
-            }
+        for (int64_t e = e0 + lane; e < e1; e += 32) {
+            int c = col[e];
+            if (c < 0 || c >= n) b = 1;
+            if (e > e0 && col[e - 1] >= c) b = 1;
         }
     }
     b = __any_sync(0xffffffffu, b);
