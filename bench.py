@@ -69,6 +69,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--p", type=int, default=None,
+                    help="design columns of a covariates-only config (continuous)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "tc_tf32"],
+                    help="arithmetic of the Hessian contractions (DEVIL_PREC_*)")
     return ap.parse_args()
 
 
@@ -100,7 +104,7 @@ def make_inputs(args, rank, device):
     from devil_b200 import synthetic
 
     return synthetic.make_torch(args.config, seed=args.seed + rank, G=args.genes, n=args.cells,
-                                device=device)
+                                device=device, p=args.p)
 
 
 def normed_sum_offsets(rowptr, col, val, n):
@@ -312,6 +316,16 @@ def read_peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def read_bf16_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 def read_traffic_ratio(name):
     """DRAM bytes per algorithmic byte of a pass kernel, from its committed
     ncu summary (line dram_per_alg_byte=...)."""
@@ -328,8 +342,9 @@ def read_traffic_ratio(name):
 KERNELS = {"register": ("reg_pass_kernel<P={p},{pass},uint16> (register tiles)",
                         "irls_pass_traffic.txt"),
            "tensor": ("tc_irls_kernel<P={p},uint16> (tcgen05 kind::tf32 Hessian)", None),
+           "tensor_wide": ("tcw_irls_kernel<XS,uint16> (tcgen05 kind::tf32 Hessian, p={p})", None),
            "shared": ("gen_pass_kernel<{pass},uint16> (shared-memory tiles, p={p})", None),
-           "groups": ("grp_pass_kernel<{pass},uint16> (design groups, p={p})",
+           "groups": ("grp_slices_kernel<{pass},uint16> (design groups, slice-major, p={p})",
                       "irls_grp_pass_traffic.txt")}
 PASS_NAMES = ["irls", "mom", "mle", "bread_meat"]
 PASS_TRAITS = ["PassIRLS", "PassMOM", "PassMLE", "PassSandwich"]
@@ -477,6 +492,7 @@ def main():
     opts.size_factors = L.SF_NORMED_SUM
     opts.compute_theta_mom = 1
     opts.form = L.FORM_CHOSEN
+    opts.precision = {"fp32": L.PREC_FP32, "tc_tf32": L.PREC_TC_TF32}[args.precision]
     contrast = np.zeros(p)
     contrast[1] = 1.0
     main_fit = Fit(L, lib, ctx, dev, data["rowptr"], data["col"], data["val"], X, p, n, opts,
@@ -524,6 +540,7 @@ def main():
     ms = e0.elapsed_time(e1) / args.steps
     launches = ctx.launches - l0
     prof = {k: ctx.profile(k) for k in range(4)}
+    tc_flops = ctx.profile_tc_flops(0)
     ctx.set_profiling(False)
     clk = clocks.stop()
     if world > 1:
@@ -632,6 +649,20 @@ def main():
                 "launches": n_l, "avg_launch_ms": round(t_ms / n_l, 4),
                 "alg_bytes_per_launch": round(alg_per_launch, 1),
                 "share_of_step": round(t_ms / args.steps / ms, 4)}
+        if eng == "tensor_wide" and tc_flops > 0:
+            # the Hessian MMAs are the kernel's bound: FLOPs issued (3 split
+            # TF32 products, padding included) against the TF32 tensor rate,
+            # half the measured dense BF16 rate
+            bf16, bf16_kind = read_bf16_peak()
+            tf32_peak = bf16 / 2.0
+            achieved_tf = tc_flops / (t_ms / 1e3) / 1e12
+            roof = {"bound": "tensor", "achieved": round(achieved_tf, 1), "peak": round(tf32_peak, 1),
+                    "unit": "TFLOP/s", "frac": round(achieved_tf / tf32_peak, 4), "traffic": None,
+                    "peak_source": f"half the {bf16_kind} bf16_tflops (TF32 MMA rate)",
+                    "kernel": kname, "launches": n_l, "avg_launch_ms": round(t_ms / n_l, 4),
+                    "tc_flops_per_launch": round(tc_flops / n_l, 1),
+                    "hbm_achieved_gbs": round(achieved, 1), "hbm_frac": round(achieved / peak, 4),
+                    "share_of_step": round(t_ms / args.steps / ms, 4)}
         if eng == "groups":
             roof["tensor_note"] = (
                 "no dense contraction left for the tensor cores: the design has few distinct rows, "
@@ -690,7 +721,8 @@ def main():
         "scaling": "weak", "vs_baseline": None,
         # per-cell arithmetic of the IRLS pass: FP32 in the register engine,
         # FP64 in the shared-memory and design-group engines
-        "dtype": "f32" if engines["irls"] in ("register", "tensor") else "f64", "data": "synthetic",
+        "dtype": {"register": "f32", "tensor": "tf32x3", "tensor_wide": "tf32x3"}.get(engines["irls"], "f64"),
+        "data": "synthetic",
         "config": workload_config(args.config, G, n, p, nnz),
         "chosen_vs_plain": None if plain is None else round(plain["chosen_vs_plain"], 2),
         "plain": plain,

@@ -37,7 +37,7 @@ EXPORTS = (
     "devil_compute_clustered_meat", "devil_nb_adjoint", "devil_cluster_blocks",
     "devil_group_order", "devil_ctx_set_profiling", "devil_ctx_profile", "devil_ctx_engine",
     "devil_p_adjust_device_static", "devil_fit_overdispersion_new", "devil_fit_batch",
-    "devil_p_adjust_device",
+    "devil_p_adjust_device", "devil_ctx_profile_tc",
 )
 
 
@@ -129,6 +129,7 @@ def load():
         L.devil_ctx_profile.argtypes = [vp, i, C.POINTER(i64), C.POINTER(dbl), C.POINTER(dbl)]
         L.devil_fit_batch.argtypes = [vp, i, C.POINTER(Problem), C.POINTER(FitOpts),
                                       C.POINTER(FitResult), i]
+        L.devil_ctx_profile_tc.argtypes = [vp, i, C.POINTER(dbl)]
         L.devil_ctx_engine.argtypes = [vp, i]
         L.devil_ctx_engine.restype = i
         L.devil_p_adjust_device_static.argtypes = [i64, vp, i, vp, vp, C.c_char_p, C.c_size_t]
@@ -172,11 +173,18 @@ class Context:
                                             C.byref(b)))
         return n.value, ms.value, b.value
 
+    def profile_tc_flops(self, kind: int) -> float:
+        """Tensor-core FLOPs the profiled launches of a pass kind issued."""
+        f = C.c_double(0)
+        self.check(load().devil_ctx_profile_tc(self.h, int(kind), C.byref(f)))
+        return f.value
+
     def engine(self, kind: int) -> str:
         """Engine of the last launch of pass kind 0 IRLS, 1 MOM, 2 MLE,
-        3 bread/meat: "register", "shared", "groups", "tensor" or "none"."""
+        3 bread/meat: "register", "shared", "groups", "tensor" (p <= 4),
+        "tensor_wide" (IRLS, p = 5..32) or "none"."""
         e = load().devil_ctx_engine(self.h, int(kind))
-        return {0: "register", 1: "shared", 2: "groups", 3: "tensor"}.get(e, "none")
+        return {0: "register", 1: "shared", 2: "groups", 3: "tensor", 4: "tensor_wide"}.get(e, "none")
 
     def synchronize(self):
         self.check(load().devil_ctx_synchronize(self.h))

@@ -66,6 +66,7 @@ int pass_blocks_per_sm(PassKind kind, Engine engine, int P, int GT, int val_u16,
     if (engine == ENGINE_REG) e = launch_reg_pass(L);
     else if (engine == ENGINE_GEN) e = launch_gen_pass(L);
     else if (engine == ENGINE_TC) e = launch_tc_pass(L, nullptr);
+    else if (engine == ENGINE_TCW) e = launch_tcw_pass(L, TcwGeom{});
     if (e != cudaSuccess || occ < 1) {
         cudaGetLastError();  // a failed query leaves no sticky error; use one block per SM
         occ = 1;
@@ -106,6 +107,7 @@ struct devil_ctx {
     int64_t prof_launches[4] = {0, 0, 0, 0};
     double prof_ms[4] = {0, 0, 0, 0};
     double prof_bytes[4] = {0, 0, 0, 0};
+    double prof_tc_flops[4] = {0, 0, 0, 0};  // tensor-core FLOPs issued (MMA shapes, padding included)
     int last_engine[4] = {-1, -1, -1, -1};
     // DEVIL_DEBUG: CUDA events at the phase boundaries of a fit
     std::vector<std::pair<const char*, cudaEvent_t>> marks;
@@ -245,6 +247,11 @@ struct DevProblem {
     // products image of the tensor-core IRLS engine (p <= 4), built by its
     // first launch
     mutable float4* zimg = nullptr;
+    // inputs of the tensor-core IRLS engine for p = 5..32 (dense count
+    // image, feature rows, padded offsets), built by its first launch
+    mutable TcwGeom tcw;
+    mutable bool tcw_ready = false;
+    bool tcw_fits = false;  // the dense count image fits half of the free device memory
     int precision = DEVIL_PREC_FP32;  // DEVIL_PREC_*: tensor-core passes at p <= 4
     double* Xdrm = nullptr;  // row-major FP64 copy for the FP64 passes
     double* sf = nullptr;
@@ -461,6 +468,13 @@ void prepare_design(devil_ctx* ctx, DevProblem& dp, const double* X, int P, bool
     dp.stats = ws<double>(ctx, "stats", (size_t)dp.G * 6);
     LAUNCH(launch_gene_stats(dp.rowptr, dp.val, dp.val_u16, dp.G, dp.n, dp.stats, st));
     CK(cudaStreamSynchronize(st));  // host copies above must stay valid until here
+    if (tcw_supported(P, dp.xs)) {
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        const double need = (double)dp.G * tcw_npad(dp.n) * (dp.val_u16 ? 2.0 : 4.0) +
+                            (double)(dp.xs + 1) * tcw_npad(dp.n) * 4.0;
+        dp.tcw_fits = need <= 0.5 * (double)fr;
+    }
 }
 
 // size factors and offsets (R/main.R:224-230, R/size_factors.R)
@@ -825,12 +839,23 @@ struct PassPlan {
     int plain = 0;  // the plain comparison form
 };
 
+// the tensor-core IRLS engine for p = 5..32 (kernels_tcw.cu): DEVIL_TCW=1
+// selects it wherever it applies, DEVIL_TCW=0 never; otherwise the
+// DEVIL_PREC_TC_TF32 precision selects it
+bool tcw_wanted(const DevProblem& dp) {
+    if (!tcw_supported(dp.P, dp.xs) || !dp.tcw_fits) return false;
+    const char* e = getenv("DEVIL_TCW");
+    if (e && *e) return atoi(e) == 1;
+    return dp.precision == DEVIL_PREC_TC_TF32;
+}
+
 PassPlan plan_engine(PassKind k, const DevProblem& dp, int form) {
     const int P = dp.P;
     // the plain comparison form: every pass on the per-cell shared-memory
     // engine, FP32 per-cell arithmetic for the FP32 passes (IRLS, MLE)
     if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, gen_default_gt(k, P), k, 1};
     if (dp.grp.active) return {ENGINE_GRP, 1};
+    if (k == PASS_IRLS && tcw_wanted(dp)) return {ENGINE_TCW, 128};
     const bool tc = tc_enabled(k) ||
                     (dp.precision == DEVIL_PREC_TC_TF32 && (k == PASS_IRLS || k == PASS_MLE));
     if (P <= tc_max_p() && tc) return {ENGINE_TC, tc_tile_genes(k)};
@@ -872,7 +897,9 @@ int choose_nseg(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, int 
     if (plan.engine == ENGINE_GRP) return 1;
     const int occ = pass_blocks_per_sm(plan.kind, plan.engine, dp.P, plan.GT, dp.val_u16, plan.plain);
     const int64_t cap = (int64_t)ctx->sm_count * std::max(1, occ);
-    const int64_t min_waves = plan.engine == ENGINE_TC ? 4 : 1;
+    const int64_t min_waves = plan.engine == ENGINE_TC ? 4 : (plan.engine == ENGINE_TCW ? 2 : 1);
+    // the wide tensor-core engine has tcw_blocks(p) product blocks per tile
+    if (plan.engine == ENGINE_TCW) tiles *= tcw_blocks(dp.P);
     int want = (int)((min_waves * cap + tiles - 1) / tiles);
     want = std::max(1, std::min(want, dp.nfine));
     const int hi = std::min(dp.nfine, 4 * want);
@@ -983,6 +1010,24 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
             LAUNCH(launch_tc_zimg(dp.Xrm, dp.xs, dp.n, dp.P, dp.zimg, ctx->stream));
         }
         LAUNCH(launch_tc_pass(L, dp.zimg));
+    } else if (plan.engine == ENGINE_TCW) {
+        if (!dp.tcw_ready) {
+            TcwGeom& t = dp.tcw;
+            t.npad = tcw_npad(dp.n);
+            t.ld = t.npad;
+            t.P = dp.P;
+            t.NE = dp.P * (dp.P + 1) / 2;
+            t.NA = t.NE + dp.P;
+            t.nblk = tcw_nblk(dp.P);
+            t.ydense = dp.val_u16 ? (const void*)ws<uint16_t>(ctx, "tcw_y", (size_t)dp.G * t.ld)
+                                  : (const void*)ws<float>(ctx, "tcw_y", (size_t)dp.G * t.ld);
+            t.xt = ws<float>(ctx, "tcw_xt", (size_t)dp.xs * t.npad);
+            t.offp = ws<float>(ctx, "tcw_off", (size_t)t.npad);
+            LAUNCH(launch_tcw_prepare(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.G, dp.n, dp.Xrm, dp.xs,
+                                      dp.off_f, t, ctx->stream));
+            dp.tcw_ready = true;
+        }
+        LAUNCH(launch_tcw_pass(L, dp.tcw));
     } else {
         LAUNCH(launch_gen_pass(L));
     }
@@ -1016,6 +1061,16 @@ void prof_add_bytes(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const i
                                         (double)(dp.grp.U * (dp.grp.C > 1 ? dp.grp.C + 1 : 1)) *
                                             kRuleCap * 16.0
                                   : (double)dp.n * 4.0 * (dp.xs + 1);
+    if (plan.engine == ENGINE_TCW) {
+        // the dense count image: every cell of the gene once per pass; the
+        // MMA work: 3 TF32 products of 128 x nblk x npad per tile and block
+        const double npad = (double)tcw_npad(dp.n);
+        const double rows = npad * (dp.val_u16 ? 2.0 : 4.0);
+        ctx->prof_bytes[kind] += rows * (double)h[1] + per_gene * (double)h[1] +
+                                 (double)launches * npad * 4.0 * (dp.xs + 1);
+        ctx->prof_tc_flops[kind] += 6.0 * npad * tcw_blocks(dp.P) * tcw_nblk(dp.P) * (double)h[1];
+        return;
+    }
     ctx->prof_bytes[kind] += ebytes * (double)h[0] + per_gene * (double)h[1] +
                              (double)launches * per_launch;
 }
@@ -1065,7 +1120,7 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
         launch_pass(ctx, dp, PASS_IRLS, plan, nseg, tiles, dp.fine_bound, dp.fine_ptr,
                     dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
         ++launched;
-        const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC;
+        const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC && plan.engine != ENGINE_TCW;
         if (plan.engine == ENGINE_GRP && (ctx->grp_slices & 1)) {
             // slice-major pass: the assembly is part of the step
             GrpGeom gg = grp_geom(dp);
@@ -1585,6 +1640,7 @@ int devil_ctx_set_profiling(devil_ctx* ctx, int enable) {
             ctx->prof_launches[k] = 0;
             ctx->prof_ms[k] = 0.0;
             ctx->prof_bytes[k] = 0.0;
+            ctx->prof_tc_flops[k] = 0.0;
         }
     });
 }
@@ -1602,6 +1658,13 @@ int devil_ctx_profile(devil_ctx* ctx, int pass_kind, int64_t* launches, double* 
         if (launches) *launches = ctx->prof_launches[pass_kind];
         if (ms) *ms = ctx->prof_ms[pass_kind];
         if (alg_bytes) *alg_bytes = ctx->prof_bytes[pass_kind];
+    });
+}
+
+int devil_ctx_profile_tc(devil_ctx* ctx, int pass_kind, double* tc_flops) {
+    return guarded(ctx, [&] {
+        if (pass_kind < 0 || pass_kind > 3) fail(ctx, DEVIL_ERR_ARG, "pass kind 0..3");
+        if (tc_flops) *tc_flops = ctx->prof_tc_flops[pass_kind];
     });
 }
 

@@ -11,7 +11,7 @@
 namespace devil {
 
 enum PassKind { PASS_IRLS = 0, PASS_MOM = 1, PASS_MLE = 2, PASS_SANDWICH = 3 };
-enum Engine { ENGINE_REG = 0, ENGINE_GEN = 1, ENGINE_GRP = 2, ENGINE_TC = 3 };
+enum Engine { ENGINE_REG = 0, ENGINE_GEN = 1, ENGINE_GRP = 2, ENGINE_TC = 3, ENGINE_TCW = 4 };
 
 inline int pass_nw(PassKind k) { return k == PASS_MLE ? 3 : (k == PASS_MOM ? 0 : 1); }
 inline int pass_nv(PassKind k) { return (k == PASS_IRLS || k == PASS_SANDWICH) ? 1 : 0; }
@@ -81,6 +81,29 @@ int64_t tc_zimg_float4s(int64_t n);  // its size in float4
 cudaError_t launch_tc_zimg(const float* Xrm, int xs, int64_t n, int P, float4* zimg, cudaStream_t st);
 cudaError_t launch_tc_pass(const PassLaunch& L, const float4* zimg);
 cudaError_t launch_gen_pass(const PassLaunch& L);
+
+// ---- tensor-core IRLS engine for p = 5..32 (kernels_tcw.cu) ----
+// Inputs built once per fit by launch_tcw_prepare: the counts as a dense
+// image (gene rows of ld = npad cells, uint16 or float, zero where the CSR
+// has no entry), the design's feature rows xt [xs][npad] and the offsets
+// offp [npad] (zero past n).
+struct TcwGeom {
+    const float* xt = nullptr;
+    const float* offp = nullptr;
+    const void* ydense = nullptr;
+    int64_t ld = 0;
+    int64_t npad = 0;
+    int P = 0, NE = 0, NA = 0;
+    int nblk = 0;  // product columns per block (tcw_nblk(P))
+};
+int tcw_blocks(int P);          // product blocks (grid.z)
+int tcw_nblk(int P);
+int64_t tcw_npad(int64_t n);
+bool tcw_supported(int P, int xs);
+cudaError_t launch_tcw_prepare(const int64_t* rowptr, const int32_t* col, const void* val, int val_u16,
+                               int64_t G, int64_t n, const float* Xrm, int xs, const float* off,
+                               const TcwGeom& tw, cudaStream_t st);
+cudaError_t launch_tcw_pass(const PassLaunch& L, const TcwGeom& tw);
 
 // ---- design-group engine (kernels_grp.cu) ----
 constexpr int kBinNodes = 10;         // Gauss nodes per offset bin

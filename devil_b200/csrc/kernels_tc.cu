@@ -29,7 +29,7 @@
 // it (mbarrier, bounded wait).  All waits are bounded: on expiry the block
 // records an error, skips its output, drains and frees its tensor memory.
 #include "internal.h"
-#include "tma_pass.cuh"
+#include "tc_common.cuh"
 
 #include <cstdlib>
 
@@ -64,73 +64,11 @@ constexpr uint32_t kTcCols = 2 * kTcRegion;    // 128 columns allocated
 static_assert(kTcN * kTcKC / 4 == kTcNT, "one 16-byte piece of Z per thread and chunk");
 static_assert(kTcKC / 4 == kTcNT / 32, "one quad of cells per warp and chunk");
 
-// shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8
-// rows x 16 bytes; lbo = bytes between the two K-halves of an MMA (K = 8
-// TF32 = 2 x 16 bytes), sbo = bytes between groups of 8 rows
-DEV uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
-    return d;
-}
-
-// instruction descriptor of kind::tf32: D FP32, A and B TF32, both K-major
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
-                            ((uint32_t)(kTcM >> 4) << 24);
-
-// byte offset of element (row, k) in a K-major stage with R rows: the 16
-// bytes of cells 4q..4q+3 of every row follow each other, row by row
-__host__ __device__ constexpr int stage_off(int row, int q, int R) { return (q * R + row) * 16; }
-
-DEV float to_tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
-}
-
-// per-thread asynchronous global -> shared copy of 16 bytes (completion
-// tracked in this thread's commit groups)
-template <int BYTES>
-DEV void cp_async(void* dst, const void* src) {
-    static_assert(BYTES == 16, "16-byte pieces");
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-// the first `bytes` (0..16) bytes from src, zeros after them; bytes = 0
-// reads nothing
-DEV void cp_async_zfill(void* dst, const void* src, uint32_t bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(bytes)
-                 : "memory");
-}
-DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+constexpr uint32_t kIdesc = tf32_idesc(kTcM, kTcN);
 
 DEV void tc_mma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t accumulate) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
-        "l"(ad), "l"(bd), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+    tc_mma_n(tmem, ad, bd, accumulate, kIdesc);
 }
-
-DEV void tc_mma_n(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t accumulate, uint32_t idesc) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(tmem),
-        "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
-}
-
-DEV void tc_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_u32(bar))
-                 : "memory");
-}
-
-// 16 consecutive FP32 columns of the 32 lanes this warp may access
-DEV void tc_ld16(uint32_t taddr, float* v);
 
 // add two of the four 16-column parts of one region (rows of this warp's
 // lanes): parts 0, 1 (R_hi against Z_hi, Z_lo) or parts 2, 3 (R_lo)
@@ -142,20 +80,6 @@ DEV void tc_drain(uint32_t taddr, float* h) {
 #pragma unroll
         for (int a = 0; a < 16; ++a) h[a] += t[a];
     }
-}
-
-DEV void tc_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-        "[%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
 template <int P, class VT>
@@ -490,8 +414,7 @@ __global__ void __launch_bounds__(kTcNT) tc_irls_kernel(PassGeom geo, PassIRLS::
 constexpr int kMleG = 32;                    // genes per tile
 constexpr uint32_t kMleRegion = kTcN;        // 32 columns per run region
 constexpr uint32_t kMleCols = 2 * kMleRegion;
-constexpr uint32_t kIdesc16 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcZ >> 3) << 17) |
-                              ((uint32_t)(kTcM >> 4) << 24);
+constexpr uint32_t kIdesc16 = tf32_idesc(kTcM, kTcZ);
 
 struct ScalAcc {
     double s[4] = {0.0, 0.0, 0.0, 0.0};

@@ -22,6 +22,10 @@ shapes, sparsity and value distributions of the benchmark workloads:
 * ``binary``       -- G=20,000 x n=1,000,000, p=2 (intercept + binary
   condition, 50/50), the model of ``plain_small`` with beta0 ~ N(-3, 1.5):
   about 10% nonzeros, CSR uint16.
+* ``continuous``   -- G=20,000 x n=100,000, p=16 (intercept, condition and
+  p - 2 N(0, 1) covariates with gene effects N(0, 0.2)), beta0 ~ N(-2, 1),
+  CSR uint16: a design without few distinct rows.  ``p`` (3..32) overrides
+  the number of columns.
 
 Counts are NB with Var = mu + theta * mu^2 (theta is the dispersion devil
 returns), drawn as a Gamma-Poisson mixture: lambda ~ Gamma(shape=1/theta,
@@ -51,7 +55,21 @@ CONFIGS = {
                  types=31, patients=1, dense=False),
     "binary": dict(G=20000, n=1000000, p=2, b0_loc=-3.0, b0_sd=1.5, covariates=0, types=0,
                    patients=1, dense=False),
+    "continuous": dict(G=20000, n=100000, p=16, b0_loc=-2.0, b0_sd=1.0, covariates=14, types=0,
+                       patients=1, dense=False),
 }
+
+
+def config_params(name: str, p: int | None = None) -> dict:
+    """The config's parameters; ``p`` sets the column count of a config of
+    intercept, condition and covariates only."""
+    cfg = dict(CONFIGS[name])
+    if p is not None and int(p) != cfg["p"]:
+        if cfg["types"] or not 3 <= int(p) <= 32:
+            raise ValueError(f"config {name!r} has no p = {p}")
+        cfg["p"] = int(p)
+        cfg["covariates"] = int(p) - 2
+    return cfg
 
 
 @dataclass
@@ -120,10 +138,11 @@ def patient_sizes(n: int, k: int, rng: np.random.Generator):
 
 
 def make(config: str = "plain_small", seed: int = 0, G: int | None = None, n: int | None = None,
-         chunk_cells: int = 1 << 24, mean_loc: float | None = None) -> Problem:
+         chunk_cells: int = 1 << 24, mean_loc: float | None = None, p: int | None = None) -> Problem:
     """Draw one problem with numpy (PCG64).  G / n override the config sizes;
-    mean_loc the location of the gene means (configs that draw them)."""
-    cfg = dict(CONFIGS[config])
+    mean_loc the location of the gene means (configs that draw them); p the
+    column count of a covariates-only config."""
+    cfg = config_params(config, p)
     if mean_loc is not None:
         cfg["mean_loc"] = float(mean_loc)
     G = cfg["G"] if G is None else int(G)
@@ -180,7 +199,7 @@ def make(config: str = "plain_small", seed: int = 0, G: int | None = None, n: in
 
 def make_torch(config: str = "plain_sparse", seed: int = 0, G: int | None = None,
                n: int | None = None, device="cuda", chunk_cells: int = 1 << 27,
-               mean_loc: float | None = None):
+               mean_loc: float | None = None, p: int | None = None):
     """Draw the same model on a torch device (full-size benchmark inputs).
 
     Returns a dict of device tensors: rowptr (int64), col (int32), val
@@ -188,7 +207,7 @@ def make_torch(config: str = "plain_sparse", seed: int = 0, G: int | None = None
     copies of the truth and the design."""
     import torch
 
-    cfg = dict(CONFIGS[config])
+    cfg = config_params(config, p)
     if mean_loc is not None:
         cfg["mean_loc"] = float(mean_loc)
     G = cfg["G"] if G is None else int(G)

@@ -94,8 +94,10 @@ typedef struct devil_counts {
 /* arithmetic of the per-cell Hessian contractions (IRLS and MLE passes) */
 #define DEVIL_PREC_FP32      0   /* FP32 FMAs on the CUDA cores (default)   */
 #define DEVIL_PREC_TC_TF32   1   /* tcgen05 MMAs on split TF32 (hi + lo)    */
-                                 /* operands, FP32 accumulation; p <= 4,    */
-                                 /* other p fall back to DEVIL_PREC_FP32    */
+                                 /* operands, FP32 accumulation: IRLS and   */
+                                 /* MLE at p <= 4, IRLS at p = 5..32        */
+                                 /* (designs without few distinct rows);    */
+                                 /* other passes as DEVIL_PREC_FP32         */
 #define DEVIL_PREC_TC_BF16X3 2   /* not provided (DEVIL_ERR_UNSUPPORTED):   */
                                  /* the split-TF32 path already reaches     */
                                  /* FP32 accuracy                           */
@@ -152,10 +154,15 @@ DEVIL_API int64_t devil_ctx_launch_count(const devil_ctx *ctx);
 DEVIL_API int devil_ctx_set_profiling(devil_ctx *ctx, int enable);
 DEVIL_API int devil_ctx_profile(devil_ctx *ctx, int pass_kind, int64_t *launches, double *ms,
                                 double *alg_bytes);
+/* Tensor-core FLOPs the profiled launches of a pass kind issued (MMA
+ * shapes, padding included; no counterpart in the reference).  Counted for
+ * the tensor-core IRLS engine of p = 5..32 (engine 4); 0 otherwise. */
+DEVIL_API int devil_ctx_profile_tc(devil_ctx *ctx, int pass_kind, double *tc_flops);
 /* Engine of the last launch of a pass kind on this context (no counterpart
  * in the reference): 0 register tiles (p <= 8), 1 shared-memory tiles,
  * 2 design groups (few distinct design rows), 3 tensor cores (IRLS pass,
- * p <= 4), -1 none yet. */
+ * p <= 4), 4 tensor cores (IRLS pass, p = 5..32: the Hessian as split-TF32
+ * MMAs over a dense count image), -1 none yet. */
 DEVIL_API int devil_ctx_engine(const devil_ctx *ctx, int pass_kind);
 
 /* ---- full pipeline --------------------------------------------------- */

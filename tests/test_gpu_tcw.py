@@ -1,0 +1,72 @@
+"""The tensor-core IRLS engine for designs of p = 5..32 columns without few
+distinct rows (continuous covariates): the per-gene Hessian as split-TF32
+tcgen05 MMAs over a dense count image, the score on the CUDA cores in FP32
+(devil_b200/csrc/kernels_tcw.cu).  It replaces the per-cell contraction of
+beta_fit (src/beta.cpp:35-42); the bars are the path's: |d beta| <= 1e-5
+absolute on genes that converge in both with equal iteration counts, MOM /
+MLE theta 1e-4 relative, bread 1e-4 of the diagonal scale."""
+import numpy as np
+import pytest
+
+from devil_b200 import synthetic
+from test_gpu_parity import _theta_mask, check_beta, check_mats, check_rel, gpu_fit, oracle_fit
+
+pytestmark = pytest.mark.gpu
+
+
+def _agree(a, b, tol=1e-5):
+    """Two GPU fits of one problem: equal iteration counts on >= 97 % of the
+    genes, |d beta| <= tol on the genes converged in both with equal counts."""
+    ia, ib = a["iterations"]["beta_iters"], b["iterations"]["beta_iters"]
+    same = ia == ib
+    assert same.mean() >= 0.97, same.mean()
+    both = same & (ia < 200)
+    d = np.abs(a["beta"] - b["beta"])[both]
+    assert d.size == 0 or d.max() <= tol, d.max()
+
+
+@pytest.mark.parametrize("p,n", [(8, 4000), (16, 4001), (32, 3001)])
+def test_tcw_irls_matches_oracle(dv, orc, p, n):
+    """p = 8, 16, 32 with continuous covariates; n not a multiple of the
+    32-cell chunk (zero padding), 300 genes (a partial last tile), several
+    cell segments and, at p = 32, three product blocks."""
+    P = synthetic.make("continuous", seed=40 + p, G=300, n=n, p=p)
+    ref = oracle_fit(orc, P, orc.OD_MOM)
+    ctx = dv.context()
+    ctx.set_profiling(True)
+    fit = gpu_fit(dv, P, "MOM", precision="tc_tf32")
+    assert ctx.engine(0) == "tensor_wide"
+    assert ctx.profile_tc_flops(0) > 0
+    ctx.set_profiling(False)
+    same = check_beta(fit, ref)
+    check_rel(fit["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta MOM")
+    check_mats(fit["beta_sandwiches_null"], ref["bread"], same & (ref["theta"] < 1e3), 1e-4, "bread")
+    # the CUDA-core engine of the default precision on the same problem
+    base = gpu_fit(dv, P, "MOM")
+    assert ctx.engine(0) in ("register", "shared")
+    _agree(fit, base)
+
+
+def test_tcw_float_counts_and_mle(dv, orc):
+    """Float counts (the dense image holds FP32 values) and the MLE theta
+    that follows the IRLS."""
+    P = synthetic.make("continuous", seed=77, G=200, n=2500, p=12)
+    ref = oracle_fit(orc, P, orc.OD_MLE)
+    fit = dv.fit_devil((P.rowptr, P.col, P.val.astype(np.float64), P.n), P.X, overdispersion="MLE",
+                       size_factors="normed_sum", compute_theta_mom=True, precision="tc_tf32")
+    assert dv.context().engine(0) == "tensor_wide"
+    same = check_beta(fit, ref)
+    check_rel(fit["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta MLE")
+
+
+def test_tcw_switch(dv, monkeypatch):
+    """DEVIL_TCW=1 selects the engine at the default precision; DEVIL_TCW=0
+    keeps it off even for precision="tc_tf32"; fits through both agree."""
+    P = synthetic.make("continuous", seed=5, G=150, n=2000, p=10)
+    monkeypatch.setenv("DEVIL_TCW", "1")
+    on = gpu_fit(dv, P, "MOM")
+    assert dv.context().engine(0) == "tensor_wide"
+    monkeypatch.setenv("DEVIL_TCW", "0")
+    off = gpu_fit(dv, P, "MOM", precision="tc_tf32")
+    assert dv.context().engine(0) == "shared"
+    _agree(on, off)
