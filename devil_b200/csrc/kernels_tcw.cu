@@ -25,8 +25,10 @@
 //
 // Accumulation: D accumulates a run of 8 chunks (256 cells) in tensor
 // memory; the run is then added in FP32 on the CUDA cores into a running
-// total (tensor-memory columns 256.., tcgen05.ld / add / tcgen05.st), so no
-// tensor-core accumulation spans more than 256 terms.
+// total (tensor-memory columns T.., T = 128 or 256, tcgen05.ld / add /
+// tcgen05.st), so no tensor-core accumulation spans more than 256 terms.
+// A block allocates 2 T columns: two blocks of a small product count
+// (T = 128) can share an SM's 512 columns.
 //
 // Pipeline: cp.async brings the chunk's design rows (transposed: feature
 // rows of 32 cells), offsets and count rows two chunks ahead (ring of 3);
@@ -50,8 +52,6 @@ constexpr int kWKC = 32;                  // cells per chunk (4 K-steps of 8 TF3
 constexpr int kWNT = 256;                 // threads per block
 constexpr int kWNmax = 176;               // product columns per block at most
 constexpr int kWRun = 8;                  // chunks per tensor-memory run (256 cells)
-constexpr uint32_t kWTotal = 256;         // tensor-memory column of the running total
-constexpr uint32_t kWCols = 512;          // columns allocated
 constexpr int kWA = kWM * kWKC * 4;       // one of HW_hi, HW_lo: 16 KB
 constexpr int kWRing = 3;                 // input ring depth
 
@@ -92,17 +92,18 @@ DEV void load_counts(const float* ys, int q, int gr, float* y) {
 }
 
 // add the run (columns [c0, c1) of this warp's 32 lanes) into the total
-DEV void tcw_drain(uint32_t tmem, uint32_t lanes, int c0, int c1, bool first) {
+// at column offset tot
+DEV void tcw_drain(uint32_t tmem, uint32_t lanes, uint32_t tot, int c0, int c1, bool first) {
     for (int c = c0; c < c1; c += 8) {
         float v[8];
         tc_ld8(tmem + lanes + (uint32_t)c, v);
         if (!first) {
             float t[8];
-            tc_ld8(tmem + lanes + kWTotal + (uint32_t)c, t);
+            tc_ld8(tmem + lanes + tot + (uint32_t)c, t);
 #pragma unroll
             for (int u = 0; u < 8; ++u) v[u] += t[u];
         }
-        tc_st8(tmem + lanes + kWTotal + (uint32_t)c, v);
+        tc_st8(tmem + lanes + tot + (uint32_t)c, v);
     }
     tc_wait_st();
 }
@@ -123,6 +124,8 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
     const int seg = blockIdx.x;
     const int zb = blockIdx.z;
     const int nblk = tw.nblk;
+    const uint32_t tot = nblk <= 128 ? 128u : 256u;  // column of the running total
+    const uint32_t ncols = 2 * tot;                  // columns allocated
     const int tid = threadIdx.x, warp = tid >> 5;
     const int gr = tid & (kWM - 1);  // this thread's gene row (= its tensor-memory lane)
     const int hh = tid >> 7;         // its half of the chunk's cells (and of the drained columns)
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tslot)),
-                     "r"(kWCols)
+                     "r"(ncols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -303,7 +306,7 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
             okd = __all_sync(0xffffffffu, okd);
             if (okd) {
                 tc_fence_after();
-                tcw_drain(tmem, lanes, dc0, dc1, drained == 0);
+                tcw_drain(tmem, lanes, tot, dc0, dc1, drained == 0);
             } else {
                 atomicExch(&abort_flag, 1);
             }
@@ -341,7 +344,7 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
     tc_fence_after();
     __syncthreads();  // abort_flag is final from here on
     const bool good = !abort_flag;
-    if (good && issued > 0) tcw_drain(tmem, lanes, dc0, dc1, drained == 0);  // the last run
+    if (good && issued > 0) tcw_drain(tmem, lanes, tot, dc0, dc1, drained == 0);  // the last run
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -352,7 +355,7 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
     for (int c = dc0; c < dc1; c += 8) {
         float v[8];
         if (issued > 0) {
-            tc_ld8(tmem + lanes + kWTotal + (uint32_t)c, v);
+            tc_ld8(tmem + lanes + tot + (uint32_t)c, v);
         } else {
 #pragma unroll
             for (int u = 0; u < 8; ++u) v[u] = 0.f;
@@ -381,7 +384,7 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kWCols)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols)
                      : "memory");
     if (abort_flag && tid == 0) atomicExch(geo.err, 1);
 }
