@@ -840,13 +840,15 @@ struct PassPlan {
 };
 
 // the tensor-core IRLS engine for p = 5..32 (kernels_tcw.cu): DEVIL_TCW=1
-// selects it wherever it applies, DEVIL_TCW=0 never; otherwise the
-// DEVIL_PREC_TC_TF32 precision selects it
+// selects it wherever it applies, DEVIL_TCW=0 never; otherwise it runs for
+// the DEVIL_PREC_TC_TF32 precision and, by default, from p = 9 on, where
+// the alternative is the FP64 shared-memory engine (about 20x slower per
+// IRLS pass at p = 16 and 32 on the 20,000 x 100,000 continuous workload)
 bool tcw_wanted(const DevProblem& dp) {
     if (!tcw_supported(dp.P, dp.xs) || !dp.tcw_fits) return false;
     const char* e = getenv("DEVIL_TCW");
     if (e && *e) return atoi(e) == 1;
-    return dp.precision == DEVIL_PREC_TC_TF32;
+    return dp.precision == DEVIL_PREC_TC_TF32 || dp.P > reg_max_p();
 }
 
 PassPlan plan_engine(PassKind k, const DevProblem& dp, int form) {

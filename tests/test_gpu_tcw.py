@@ -26,7 +26,7 @@ def _agree(a, b, tol=1e-5):
 
 
 @pytest.mark.parametrize("p,n", [(8, 4000), (16, 4001), (32, 3001)])
-def test_tcw_irls_matches_oracle(dv, orc, p, n):
+def test_tcw_irls_matches_oracle(dv, orc, monkeypatch, p, n):
     """p = 8, 16, 32 with continuous covariates; n not a multiple of the
     32-cell chunk (zero padding), 300 genes (a partial last tile), several
     cell segments and, at p = 32, three product blocks."""
@@ -41,10 +41,16 @@ def test_tcw_irls_matches_oracle(dv, orc, p, n):
     same = check_beta(fit, ref)
     check_rel(fit["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta MOM")
     check_mats(fit["beta_sandwiches_null"], ref["bread"], same & (ref["theta"] < 1e3), 1e-4, "bread")
-    # the CUDA-core engine of the default precision on the same problem
+    # the CUDA-core engine on the same problem (FP32 register tiles at
+    # p <= 8, FP64 shared-memory tiles above)
+    monkeypatch.setenv("DEVIL_TCW", "0")
     base = gpu_fit(dv, P, "MOM")
+    monkeypatch.delenv("DEVIL_TCW")
     assert ctx.engine(0) in ("register", "shared")
     _agree(fit, base)
+    # the default precision: the tensor-core engine from p = 9 on
+    gpu_fit(dv, P, "MOM")
+    assert ctx.engine(0) == ("register" if p <= 8 else "tensor_wide")
 
 
 def test_tcw_float_counts_and_mle(dv, orc):
