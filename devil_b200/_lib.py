@@ -37,7 +37,7 @@ EXPORTS = (
     "devil_compute_clustered_meat", "devil_nb_adjoint", "devil_cluster_blocks",
     "devil_group_order", "devil_ctx_set_profiling", "devil_ctx_profile", "devil_ctx_engine",
     "devil_p_adjust_device_static", "devil_fit_overdispersion_new", "devil_fit_batch",
-    "devil_p_adjust_device", "devil_ctx_profile_tc",
+    "devil_p_adjust_device", "devil_ctx_profile_tc", "devil_ctx_irls_rescued",
 )
 
 
@@ -130,6 +130,8 @@ def load():
         L.devil_fit_batch.argtypes = [vp, i, C.POINTER(Problem), C.POINTER(FitOpts),
                                       C.POINTER(FitResult), i]
         L.devil_ctx_profile_tc.argtypes = [vp, i, C.POINTER(dbl)]
+        L.devil_ctx_irls_rescued.argtypes = [vp]
+        L.devil_ctx_irls_rescued.restype = i64
         L.devil_ctx_engine.argtypes = [vp, i]
         L.devil_ctx_engine.restype = i
         L.devil_p_adjust_device_static.argtypes = [i64, vp, i, vp, vp, C.c_char_p, C.c_size_t]
@@ -172,6 +174,12 @@ class Context:
         self.check(load().devil_ctx_profile(self.h, int(kind), C.byref(n), C.byref(ms),
                                             C.byref(b)))
         return n.value, ms.value, b.value
+
+    @property
+    def irls_rescued(self) -> int:
+        """Genes of the last fit refitted on the CUDA-core engine after too
+        many IRLS steps on the tensor-core engine of p = 5..32."""
+        return int(load().devil_ctx_irls_rescued(self.h))
 
     def profile_tc_flops(self, kind: int) -> float:
         """Tensor-core FLOPs the profiled launches of a pass kind issued."""

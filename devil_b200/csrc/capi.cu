@@ -108,6 +108,7 @@ struct devil_ctx {
     double prof_ms[4] = {0, 0, 0, 0};
     double prof_bytes[4] = {0, 0, 0, 0};
     double prof_tc_flops[4] = {0, 0, 0, 0};  // tensor-core FLOPs issued (MMA shapes, padding included)
+    int64_t irls_rescued = 0;                 // genes the last fit refitted on the CUDA-core engine
     int last_engine[4] = {-1, -1, -1, -1};
     // DEVIL_DEBUG: CUDA events at the phase boundaries of a fit
     std::vector<std::pair<const char*, cudaEvent_t>> marks;
@@ -851,13 +852,13 @@ bool tcw_wanted(const DevProblem& dp) {
     return dp.precision == DEVIL_PREC_TC_TF32 || dp.P > reg_max_p();
 }
 
-PassPlan plan_engine(PassKind k, const DevProblem& dp, int form) {
+PassPlan plan_engine(PassKind k, const DevProblem& dp, int form, bool allow_tcw = true) {
     const int P = dp.P;
     // the plain comparison form: every pass on the per-cell shared-memory
     // engine, FP32 per-cell arithmetic for the FP32 passes (IRLS, MLE)
     if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, gen_default_gt(k, P), k, 1};
     if (dp.grp.active) return {ENGINE_GRP, 1};
-    if (k == PASS_IRLS && tcw_wanted(dp)) return {ENGINE_TCW, 128};
+    if (k == PASS_IRLS && allow_tcw && tcw_wanted(dp)) return {ENGINE_TCW, 128};
     const bool tc = tc_enabled(k) ||
                     (dp.precision == DEVIL_PREC_TC_TF32 && (k == PASS_IRLS || k == PASS_MLE));
     if (P <= tc_max_p() && tc) return {ENGINE_TC, tc_tile_genes(k)};
@@ -882,8 +883,8 @@ PassPlan plan_engine(PassKind k, const DevProblem& dp, int form) {
     return {ENGINE_GEN, gen_default_gt(k, P)};
 }
 
-PassPlan plan_for(PassKind k, const DevProblem& dp, int form) {
-    PassPlan p = plan_engine(k, dp, form);
+PassPlan plan_for(PassKind k, const DevProblem& dp, int form, bool allow_tcw = true) {
+    PassPlan p = plan_engine(k, dp, form, allow_tcw);
     p.kind = k;
     return p;
 }
@@ -1090,24 +1091,21 @@ const int32_t* all_genes(devil_ctx* ctx, const DevProblem& dp, int32_t** count_o
 // ------------------------------------------------------------------
 // IRLS loop (src/beta.cpp:25-51) with active-gene compaction
 // ------------------------------------------------------------------
-void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f, const float* k,
-              int32_t* iters, int32_t* status, int max_iter, double eps, int form) {
+// One IRLS loop over the n0 genes listed in the "act0" workspace (their
+// iteration counts and status start at 0); returns the pass launches.
+int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, double* beta, float* beta_f,
+                  const float* k, int32_t* iters, int32_t* status, int max_iter, double eps, int form,
+                  int64_t n0) {
     cudaStream_t st = ctx->stream;
     const int64_t G = dp.G;
-    CK(cudaMemsetAsync(iters, 0, G * sizeof(int32_t), st));
-    CK(cudaMemsetAsync(status, 0, G * sizeof(int32_t), st));
-    if (G == 0 || max_iter <= 0) return;
-    const PassPlan plan = plan_for(PASS_IRLS, dp, form);
-    if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported", dp.P);
     int32_t* act[2] = {ws<int32_t>(ctx, "act0", G), ws<int32_t>(ctx, "act1", G)};
     int32_t* cnt = ws<int32_t>(ctx, "cnt", 4);
-    LAUNCH(launch_iota(act[0], G, st));
-    LAUNCH(launch_set_i32(cnt, (int32_t)G, st));
+    LAUNCH(launch_set_i32(cnt, (int32_t)n0, st));
     LAUNCH(launch_set_i32(cnt + 1, 0, st));
     PassBuffers pb = pass_buffers(ctx, PASS_IRLS, dp.P, max_slot_segs(ctx, dp, plan, form));
     // copies of an earlier loop still in flight would overwrite the mirror
     CK(cudaStreamSynchronize(st));
-    *ctx->mapped_host = (int32_t)G;
+    *ctx->mapped_host = (int32_t)n0;
     const int LAG = 2;
     PassParamsAny prm{beta_f, beta, k, nullptr, nullptr};
     int64_t launched = 0;
@@ -1115,7 +1113,7 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
         const int cur = t & 1, nxt = cur ^ 1;
         // active-gene count of LAG iterations ago (an upper bound: blocks
         // beyond the current count exit at once)
-        const int64_t hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
+        const int64_t hint = t == 0 ? n0 : *(volatile int32_t*)ctx->mapped_host;
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
@@ -1140,9 +1138,64 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
     }
+    return launched;
+}
+
+// beta_fit for every gene (src/beta.cpp:25-51).  On the tensor-core engine
+// of p = 5..32 (FP32-level Hessian and score), genes whose IRLS takes more
+// than tcw_rescue_steps() steps are fitted again from beta_0 on the
+// CUDA-core engine (FP64 per cell above p = 8): a slowly converging gene is
+// ill-conditioned, and along its many steps FP32-level rounding moves the
+// iterate where the FP64 path would not (|d beta| up to ~1e-4 at 180 steps
+// against < 1e-7 at a few dozen).
+int tcw_rescue_steps() {
+    const char* e = getenv("DEVIL_TCW_RESCUE");
+    return (e && *e) ? atoi(e) : 40;
+}
+
+void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f, const float* k,
+              int32_t* iters, int32_t* status, int max_iter, double eps, int form) {
+    cudaStream_t st = ctx->stream;
+    const int64_t G = dp.G;
+    CK(cudaMemsetAsync(iters, 0, G * sizeof(int32_t), st));
+    CK(cudaMemsetAsync(status, 0, G * sizeof(int32_t), st));
+    if (G == 0 || max_iter <= 0) return;
+    const PassPlan plan = plan_for(PASS_IRLS, dp, form);
+    if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported", dp.P);
+    const int limit = tcw_rescue_steps();
+    const bool rescue = plan.engine == ENGINE_TCW && limit < max_iter;
+    double* beta0 = nullptr;
+    if (rescue) {
+        beta0 = ws<double>(ctx, "irls_beta0", (size_t)G * dp.P);
+        CK(cudaMemcpyAsync(beta0, beta, (size_t)G * dp.P * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    }
+    LAUNCH(launch_iota(ws<int32_t>(ctx, "act0", G), G, st));
+    const int64_t launched = irls_loop(ctx, dp, plan, beta, beta_f, k, iters, status, max_iter, eps, form, G);
     if (ctx->profiling) {
         prof_collect(ctx);
         prof_add_bytes(ctx, dp, PASS_IRLS, iters, launched, plan);
+    }
+    ctx->irls_rescued = 0;
+    if (!rescue) return;
+    int32_t* act0 = ws<int32_t>(ctx, "act0", G);
+    int32_t* flag = ws<int32_t>(ctx, "irls_rescue_flag", G);
+    int32_t* cnt = ws<int32_t>(ctx, "cnt", 4);
+    LAUNCH(launch_set_i32(cnt + 2, 0, st));
+    LAUNCH(launch_irls_rescue_select(iters, G, limit, beta0, dp.P, beta, beta_f, iters, status, act0,
+                                     cnt + 2, flag, st));
+    int32_t nr = 0;
+    CK(cudaMemcpyAsync(&nr, cnt + 2, sizeof nr, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    ctx->irls_rescued = nr;
+    if (nr == 0) return;
+    const PassPlan p2 = plan_for(PASS_IRLS, dp, form, false);
+    const int64_t l2 = irls_loop(ctx, dp, p2, beta, beta_f, k, iters, status, max_iter, eps, form, nr);
+    if (ctx->profiling) {
+        // the rescue loop's passes: the rescued genes' iteration counts
+        int32_t* passes = ws<int32_t>(ctx, "irls_rescue_passes", G);
+        LAUNCH(launch_mask_i32(iters, flag, G, passes, st));
+        prof_collect(ctx);
+        prof_add_bytes(ctx, dp, PASS_IRLS, passes, l2, p2);
     }
 }
 
@@ -1662,6 +1715,8 @@ int devil_ctx_profile(devil_ctx* ctx, int pass_kind, int64_t* launches, double* 
         if (alg_bytes) *alg_bytes = ctx->prof_bytes[pass_kind];
     });
 }
+
+int64_t devil_ctx_irls_rescued(const devil_ctx* ctx) { return ctx ? ctx->irls_rescued : -1; }
 
 int devil_ctx_profile_tc(devil_ctx* ctx, int pass_kind, double* tc_flops) {
     return guarded(ctx, [&] {

@@ -76,3 +76,26 @@ def test_tcw_switch(dv, monkeypatch):
     off = gpu_fit(dv, P, "MOM", precision="tc_tf32")
     assert dv.context().engine(0) == "shared"
     _agree(on, off)
+
+
+def test_tcw_rescue_of_slow_genes(dv, orc, monkeypatch):
+    """Genes whose IRLS takes more than DEVIL_TCW_RESCUE steps on the
+    tensor-core engine are fitted again from beta_0 on the CUDA-core engine
+    (FP64 per cell at p = 12): with the limit at 3 steps most genes are
+    rescued, and they must equal the CUDA-core fit of the same genes."""
+    P = synthetic.make("continuous", seed=9, G=256, n=3000, p=12)
+    ref = oracle_fit(orc, P, orc.OD_MOM)
+    ctx = dv.context()
+    monkeypatch.setenv("DEVIL_TCW_RESCUE", "3")
+    fit = gpu_fit(dv, P, "MOM")
+    nr = ctx.irls_rescued
+    slow = fit["iterations"]["beta_iters"] > 3
+    assert nr == int(slow.sum()) and nr > P.G // 2
+    check_beta(fit, ref)
+    monkeypatch.setenv("DEVIL_TCW", "0")
+    base = gpu_fit(dv, P, "MOM")
+    assert ctx.irls_rescued == 0
+    np.testing.assert_array_equal(fit["iterations"]["beta_iters"][slow],
+                                  base["iterations"]["beta_iters"][slow])
+    d = np.abs(fit["beta"][slow] - base["beta"][slow]) / np.maximum(1.0, np.abs(base["beta"][slow]))
+    assert d.max() <= 1e-9, d.max()
