@@ -541,6 +541,7 @@ def main():
     launches = ctx.launches - l0
     prof = {k: ctx.profile(k) for k in range(4)}
     tc_flops = ctx.profile_tc_flops(0)
+    rescued = ctx.irls_rescued
     ctx.set_profiling(False)
     clk = clocks.stop()
     if world > 1:
@@ -729,6 +730,7 @@ def main():
         "roofline": roof, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "clocks": clk,
         "gpu_launches": int(launches),
         "breakdown": {"form": "chosen", "engines": engines, "passes": passes,
+                      "irls_rescued_genes": rescued,
                       "parallelism": f"genes sharded over {world} rank(s), no exchange during "
                                      f"the fit; p-values all-gathered for BH",
                       "saturated_counts": int(data.get("saturated", 0)),

@@ -177,8 +177,9 @@ class Context:
 
     @property
     def irls_rescued(self) -> int:
-        """Genes of the last fit refitted on the CUDA-core engine after too
-        many IRLS steps on the tensor-core engine of p = 5..32."""
+        """Genes of the last fit that the tensor-core engine of p = 5..32
+        handed back to the CUDA-core engine (a coefficient beyond +-8, or
+        more steps than DEVIL_TCW_RESCUE)."""
         return int(load().devil_ctx_irls_rescued(self.h))
 
     def profile_tc_flops(self, kind: int) -> float:

@@ -1142,15 +1142,23 @@ int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, do
 }
 
 // beta_fit for every gene (src/beta.cpp:25-51).  On the tensor-core engine
-// of p = 5..32 (FP32-level Hessian and score), genes whose IRLS takes more
-// than tcw_rescue_steps() steps are fitted again from beta_0 on the
-// CUDA-core engine (FP64 per cell above p = 8): a slowly converging gene is
-// ill-conditioned, and along its many steps FP32-level rounding moves the
-// iterate where the FP64 path would not (|d beta| up to ~1e-4 at 180 steps
-// against < 1e-7 at a few dozen).
-int tcw_rescue_steps() {
+// of p = 5..32 (FP32-level Hessian and score) a gene whose fit ends with a
+// coefficient beyond +-8 is fitted again from beta_0 on the CUDA-core engine
+// (FP64 per cell above p = 8): such a gene has a group of cells without
+// counts, its intercept and group coefficients drift apart step after step
+// along a nearly flat direction of the likelihood, and along that path
+// FP32-level rounding moves the iterate where the FP64 path would not
+// (|d beta| 2e-4 after 183 steps at |beta| ~ 15).  On continuous designs the
+// engine stays within 2e-6 of the FP64 oracle at every iteration count up
+// to max_iter.  DEVIL_TCW_RESCUE_BETA sets the coefficient bound;
+// DEVIL_TCW_RESCUE=s also refits every gene that took more than s steps.
+int tcw_rescue_steps(int max_iter) {
     const char* e = getenv("DEVIL_TCW_RESCUE");
-    return (e && *e) ? atoi(e) : 40;
+    return (e && *e) ? atoi(e) : max_iter;
+}
+double tcw_rescue_beta() {
+    const char* e = getenv("DEVIL_TCW_RESCUE_BETA");
+    return (e && *e) ? atof(e) : 8.0;
 }
 
 void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f, const float* k,
@@ -1162,8 +1170,8 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
     if (G == 0 || max_iter <= 0) return;
     const PassPlan plan = plan_for(PASS_IRLS, dp, form);
     if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported", dp.P);
-    const int limit = tcw_rescue_steps();
-    const bool rescue = plan.engine == ENGINE_TCW && limit < max_iter;
+    const int limit = tcw_rescue_steps(max_iter);
+    const bool rescue = plan.engine == ENGINE_TCW;
     double* beta0 = nullptr;
     if (rescue) {
         beta0 = ws<double>(ctx, "irls_beta0", (size_t)G * dp.P);
@@ -1181,8 +1189,8 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
     int32_t* flag = ws<int32_t>(ctx, "irls_rescue_flag", G);
     int32_t* cnt = ws<int32_t>(ctx, "cnt", 4);
     LAUNCH(launch_set_i32(cnt + 2, 0, st));
-    LAUNCH(launch_irls_rescue_select(iters, G, limit, beta0, dp.P, beta, beta_f, iters, status, act0,
-                                     cnt + 2, flag, st));
+    LAUNCH(launch_irls_rescue_select(iters, G, limit, tcw_rescue_beta(), beta0, dp.P, beta, beta_f, iters,
+                                     status, act0, cnt + 2, flag, st));
     int32_t nr = 0;
     CK(cudaMemcpyAsync(&nr, cnt + 2, sizeof nr, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -1190,6 +1198,7 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
     if (nr == 0) return;
     const PassPlan p2 = plan_for(PASS_IRLS, dp, form, false);
     const int64_t l2 = irls_loop(ctx, dp, p2, beta, beta_f, k, iters, status, max_iter, eps, form, nr);
+    ctx->last_engine[PASS_IRLS] = (int)plan.engine;  // the fit's engine (the rescue is counted apart)
     if (ctx->profiling) {
         // the rescue loop's passes: the rescued genes' iteration counts
         int32_t* passes = ws<int32_t>(ctx, "irls_rescue_passes", G);

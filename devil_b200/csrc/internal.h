@@ -104,12 +104,13 @@ cudaError_t launch_tcw_prepare(const int64_t* rowptr, const int32_t* col, const 
                                int64_t G, int64_t n, const float* Xrm, int xs, const float* off,
                                const TcwGeom& tw, cudaStream_t st);
 cudaError_t launch_tcw_pass(const PassLaunch& L, const TcwGeom& tw);
-// genes with more than `limit` IRLS steps: listed in act (count in *cnt,
-// which starts at 0), flag[g] = 1, beta / beta_f reset to beta0, iteration
-// count and status cleared; flag[g] = 0 for the others
-cudaError_t launch_irls_rescue_select(const int32_t* iters_in, int64_t G, int limit, const double* beta0, int P,
-                                      double* beta, float* beta_f, int32_t* iters, int32_t* status,
-                                      int32_t* act, int32_t* cnt, int32_t* flag, cudaStream_t st);
+// genes with more than `limit` IRLS steps or a coefficient beyond
+// +-beta_limit (or NaN): listed in act (count in *cnt, which starts at 0),
+// flag[g] = 1, beta / beta_f reset to beta0, iteration count and status
+// cleared; flag[g] = 0 for the others
+cudaError_t launch_irls_rescue_select(const int32_t* iters_in, int64_t G, int limit, double beta_limit,
+                                      const double* beta0, int P, double* beta, float* beta_f, int32_t* iters,
+                                      int32_t* status, int32_t* act, int32_t* cnt, int32_t* flag, cudaStream_t st);
 // out[g] = flag[g] ? v[g] : 0
 cudaError_t launch_mask_i32(const int32_t* v, const int32_t* flag, int64_t G, int32_t* out, cudaStream_t st);
 

@@ -441,11 +441,13 @@ __global__ void tcw_xt_kernel(const float* __restrict__ Xrm, int xs, int64_t n, 
     }
 }
 
-__global__ void irls_rescue_kernel(const int32_t* iters_in, int64_t G, int limit, const double* __restrict__ beta0,
-                                   int P, double* beta, float* beta_f, int32_t* iters, int32_t* status,
-                                   int32_t* act, int32_t* cnt, int32_t* flag) {
+__global__ void irls_rescue_kernel(const int32_t* iters_in, int64_t G, int limit, double beta_limit,
+                                   const double* __restrict__ beta0, int P, double* beta, float* beta_f,
+                                   int32_t* iters, int32_t* status, int32_t* act, int32_t* cnt, int32_t* flag) {
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < G; g += (int64_t)gridDim.x * blockDim.x) {
-        const bool slow = iters_in[g] > limit;
+        double bmax = 0.0;
+        for (int i = 0; i < P; ++i) bmax = fmax(bmax, fabs(beta[g * P + i]));
+        const bool slow = iters_in[g] > limit || !(bmax <= beta_limit);
         flag[g] = slow ? 1 : 0;
         if (!slow) continue;
         act[atomicAdd(cnt, 1)] = (int32_t)g;
@@ -466,12 +468,12 @@ __global__ void mask_i32_kernel(const int32_t* v, const int32_t* flag, int64_t G
 
 }  // namespace
 
-cudaError_t launch_irls_rescue_select(const int32_t* iters_in, int64_t G, int limit, const double* beta0, int P,
-                                      double* beta, float* beta_f, int32_t* iters, int32_t* status,
-                                      int32_t* act, int32_t* cnt, int32_t* flag, cudaStream_t st) {
+cudaError_t launch_irls_rescue_select(const int32_t* iters_in, int64_t G, int limit, double beta_limit,
+                                      const double* beta0, int P, double* beta, float* beta_f, int32_t* iters,
+                                      int32_t* status, int32_t* act, int32_t* cnt, int32_t* flag, cudaStream_t st) {
     if (G == 0) return cudaSuccess;
     irls_rescue_kernel<<<(unsigned)std::min<int64_t>((G + 255) / 256, 1024), 256, 0, st>>>(
-        iters_in, G, limit, beta0, P, beta, beta_f, iters, status, act, cnt, flag);
+        iters_in, G, limit, beta_limit, beta0, P, beta, beta_f, iters, status, act, cnt, flag);
     return cudaGetLastError();
 }
 

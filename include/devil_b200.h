@@ -158,10 +158,11 @@ DEVIL_API int devil_ctx_profile(devil_ctx *ctx, int pass_kind, int64_t *launches
  * shapes, padding included; no counterpart in the reference).  Counted for
  * the tensor-core IRLS engine of p = 5..32 (engine 4); 0 otherwise. */
 DEVIL_API int devil_ctx_profile_tc(devil_ctx *ctx, int pass_kind, double *tc_flops);
-/* Genes of the last fit on this context whose IRLS ran more steps than
- * DEVIL_TCW_RESCUE (default 40) on the tensor-core engine of p = 5..32 and
- * were fitted again from beta_0 on the CUDA-core engine (no counterpart in
- * the reference); 0 when that engine did not run. */
+/* Genes of the last fit on this context that the tensor-core engine of
+ * p = 5..32 handed back to the CUDA-core engine, which fitted them again
+ * from beta_0: a coefficient beyond +-8 (DEVIL_TCW_RESCUE_BETA) or more
+ * IRLS steps than DEVIL_TCW_RESCUE (default: none) (no counterpart in the
+ * reference); 0 when that engine did not run. */
 DEVIL_API int64_t devil_ctx_irls_rescued(const devil_ctx *ctx);
 /* Engine of the last launch of a pass kind on this context (no counterpart
  * in the reference): 0 register tiles (p <= 8), 1 shared-memory tiles,

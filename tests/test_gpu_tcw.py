@@ -79,10 +79,10 @@ def test_tcw_switch(dv, monkeypatch):
 
 
 def test_tcw_rescue_of_slow_genes(dv, orc, monkeypatch):
-    """Genes whose IRLS takes more than DEVIL_TCW_RESCUE steps on the
-    tensor-core engine are fitted again from beta_0 on the CUDA-core engine
-    (FP64 per cell at p = 12): with the limit at 3 steps most genes are
-    rescued, and they must equal the CUDA-core fit of the same genes."""
+    """Genes the tensor-core engine hands back (here every gene with more
+    than DEVIL_TCW_RESCUE = 3 steps; by default a coefficient beyond +-8)
+    are fitted again from beta_0 on the CUDA-core engine (FP64 per cell at
+    p = 12) and must equal the CUDA-core fit of the same genes."""
     P = synthetic.make("continuous", seed=9, G=256, n=3000, p=12)
     ref = oracle_fit(orc, P, orc.OD_MOM)
     ctx = dv.context()
@@ -90,7 +90,8 @@ def test_tcw_rescue_of_slow_genes(dv, orc, monkeypatch):
     fit = gpu_fit(dv, P, "MOM")
     nr = ctx.irls_rescued
     slow = fit["iterations"]["beta_iters"] > 3
-    assert nr == int(slow.sum()) and nr > P.G // 2
+    assert nr >= int(slow.sum()) and nr > P.G // 2
+    assert ctx.engine(0) == "tensor_wide"
     check_beta(fit, ref)
     monkeypatch.setenv("DEVIL_TCW", "0")
     base = gpu_fit(dv, P, "MOM")
