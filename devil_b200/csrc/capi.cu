@@ -851,6 +851,14 @@ bool tcw_wanted(const DevProblem& dp) {
     if (e && *e) return atoi(e) == 1;
     return dp.precision == DEVIL_PREC_TC_TF32 || dp.P > reg_max_p();
 }
+// its dispersion (MLE) pass: DEVIL_TCW_MLE=1 / 0; otherwise the
+// DEVIL_PREC_TC_TF32 precision selects it
+bool tcw_mle_wanted(const DevProblem& dp) {
+    if (!tcw_supported(dp.P, dp.xs) || !dp.tcw_fits) return false;
+    const char* e = getenv("DEVIL_TCW_MLE");
+    if (e && *e) return atoi(e) == 1;
+    return dp.precision == DEVIL_PREC_TC_TF32;
+}
 
 PassPlan plan_engine(PassKind k, const DevProblem& dp, int form, bool allow_tcw = true) {
     const int P = dp.P;
@@ -858,7 +866,8 @@ PassPlan plan_engine(PassKind k, const DevProblem& dp, int form, bool allow_tcw 
     // engine, FP32 per-cell arithmetic for the FP32 passes (IRLS, MLE)
     if (form == DEVIL_FORM_PLAIN) return {ENGINE_GEN, gen_default_gt(k, P), k, 1};
     if (dp.grp.active) return {ENGINE_GRP, 1};
-    if (k == PASS_IRLS && allow_tcw && tcw_wanted(dp)) return {ENGINE_TCW, 128};
+    if (k == PASS_IRLS && allow_tcw && tcw_wanted(dp)) return {ENGINE_TCW, tcw_tile_genes(k)};
+    if (k == PASS_MLE && allow_tcw && tcw_mle_wanted(dp)) return {ENGINE_TCW, tcw_tile_genes(k)};
     const bool tc = tc_enabled(k) ||
                     (dp.precision == DEVIL_PREC_TC_TF32 && (k == PASS_IRLS || k == PASS_MLE));
     if (P <= tc_max_p() && tc) return {ENGINE_TC, tc_tile_genes(k)};
@@ -1071,7 +1080,10 @@ void prof_add_bytes(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const i
         const double rows = npad * (dp.val_u16 ? 2.0 : 4.0);
         ctx->prof_bytes[kind] += rows * (double)h[1] + per_gene * (double)h[1] +
                                  (double)launches * npad * 4.0 * (dp.xs + 1);
-        ctx->prof_tc_flops[kind] += 6.0 * npad * tcw_blocks(dp.P) * tcw_nblk(dp.P) * (double)h[1];
+        // (an MMA covers 128 rows: 128 genes in the IRLS pass, 32 genes x 4
+        // weights in the MLE pass)
+        ctx->prof_tc_flops[kind] += 6.0 * npad * tcw_blocks(dp.P) * tcw_nblk(dp.P) * (double)h[1] *
+                                    (128.0 / tcw_tile_genes(kind));
         return;
     }
     ctx->prof_bytes[kind] += ebytes * (double)h[0] + per_gene * (double)h[1] +
@@ -1272,7 +1284,7 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
         launch_pass(ctx, dp, PASS_MLE, plan, nseg, tiles, dp.fine_bound,
                     dp.fine_ptr, dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
         ++launched;
-        const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC;
+        const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC && plan.engine != ENGINE_TCW;
         LAUNCH(launch_mle_finalize(pb.partW, part_f64, pb.partS, nseg, tiles * plan.GT, dp.P, dp.stats, dp.n,
                                    act[cur], cnt + cur, (int)hint, act[nxt], cnt + nxt, s, max_iter,
                                    cox_reid, nullptr, st));

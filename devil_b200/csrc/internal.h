@@ -97,6 +97,7 @@ struct TcwGeom {
     int nblk = 0;  // product columns per block (tcw_nblk(P))
 };
 int tcw_blocks(int P);          // product blocks (grid.z)
+int tcw_tile_genes(PassKind k); // genes per tile: 128 (IRLS), 32 (MLE)
 int tcw_nblk(int P);
 int64_t tcw_npad(int64_t n);
 bool tcw_supported(int P, int xs);

@@ -1,6 +1,8 @@
-// IRLS pass with the per-gene Hessian on the tensor cores (sm_100a tcgen05,
-// kind::tf32) for designs of p = 5..32 columns that do not collapse to a
-// few distinct rows (continuous covariates).
+// IRLS and dispersion (MLE) passes with the per-gene p x p contractions on
+// the tensor cores (sm_100a tcgen05, kind::tf32) for designs of p = 5..32
+// columns that do not collapse to a few distinct rows (continuous
+// covariates).  The IRLS form is described here; the MLE form (the Cox-Reid
+// matrices) is described at tcw_pass_kernel.
 //
 // beta_fit (src/beta.cpp:35-42) needs per gene g and IRLS step
 //     H_g = sum_c hw_gc z_c,   z_c = the products x_ci x_cj (i <= j),
@@ -56,12 +58,17 @@ constexpr int kWA = kWM * kWKC * 4;       // one of HW_hi, HW_lo: 16 KB
 constexpr int kWRing = 3;                 // input ring depth
 
 constexpr int op_bytes(int nblk) { return 2 * kWA + 2 * nblk * kWKC * 4; }
-template <class VT>
-constexpr int in_bytes(int XS) { return XS * kWKC * 4 + kWKC * 4 + kWM * kWKC * (int)sizeof(VT); }
-template <class VT>
-constexpr int tcw_smem(int XS, int nblk) { return 2 * op_bytes(nblk) + kWRing * in_bytes<VT>(XS); }
+template <class VT, int GTn>
+constexpr int in_bytes(int XS) { return XS * kWKC * 4 + kWKC * 4 + GTn * kWKC * (int)sizeof(VT); }
+constexpr int kMleG = 32;                             // genes per tile of the MLE pass
+constexpr int kPsiBytes = kMleG * 2 * kPsiTab * 8;    // their psi tables
+template <class VT, bool MLE>
+constexpr int tcw_smem(int XS, int nblk) {
+    return 2 * op_bytes(nblk) + kWRing * in_bytes<VT, MLE ? kMleG : kWM>(XS) + (MLE ? kPsiBytes : 0);
+}
 
-static_assert(tcw_smem<float>(32, kWNmax) <= 227 * 1024, "stages fit the shared memory of one block");
+static_assert(tcw_smem<float, false>(32, kWNmax) <= 227 * 1024, "stages fit the shared memory of one block");
+static_assert(tcw_smem<float, true>(32, kWNmax) <= 227 * 1024, "stages fit the shared memory of one block");
 
 // (a0, a1) += (b0, b1) * (c0, c1) as one packed FP32x2 FMA
 DEV void fma2(float& a0, float& a1, float b0, float b1, float c0, float c1) {
@@ -73,18 +80,21 @@ DEV void fma2(float& a0, float& a1, float b0, float b1, float c0, float c1) {
     asm("mov.b64 {%0, %1}, %2;" : "=f"(a0), "=f"(a1) : "l"(acc));
 }
 
+// counts of cells 4q..4q+3 of gene row gr in a count stage of R rows
+template <int R>
 DEV void load_counts(const uint16_t* ys, int q, int gr, float* y) {
-    // piece (gene, 8 cells) at ((q >> 1) * 128 + gene) * 16; this quad is its half q & 1
+    // piece (gene, 8 cells) at ((q >> 1) * R + gene) * 16; this quad is its half q & 1
     const uint2 h = *reinterpret_cast<const uint2*>(
-        reinterpret_cast<const unsigned char*>(ys) + (((q >> 1) * kWM + gr) * 16 + (q & 1) * 8));
+        reinterpret_cast<const unsigned char*>(ys) + (((q >> 1) * R + gr) * 16 + (q & 1) * 8));
     y[0] = (float)(h.x & 0xFFFFu);
     y[1] = (float)(h.x >> 16);
     y[2] = (float)(h.y & 0xFFFFu);
     y[3] = (float)(h.y >> 16);
 }
+template <int R>
 DEV void load_counts(const float* ys, int q, int gr, float* y) {
     const float4 v = *reinterpret_cast<const float4*>(
-        reinterpret_cast<const unsigned char*>(ys) + (q * kWM + gr) * 16);
+        reinterpret_cast<const unsigned char*>(ys) + (q * R + gr) * 16);
     y[0] = v.x;
     y[1] = v.y;
     y[2] = v.z;
@@ -108,37 +118,65 @@ DEV void tcw_drain(uint32_t tmem, uint32_t lanes, uint32_t tot, int c0, int c1, 
     tc_wait_st();
 }
 
-template <int XS, class VT>
-__global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRLS::Params prm, TcwGeom tw) {
+DEV void store_split(unsigned char* sA, int row, int q, const float* v) {
+    float hi[4], lo[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) tf32_split(v[c], hi[c], lo[c]);
+    *reinterpret_cast<float4*>(sA + stage_off(row, q, kWM)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<float4*>(sA + kWA + stage_off(row, q, kWM)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+}
+
+// The IRLS pass (MLE = false): 128 genes per tile, A row = gene, weight
+// r (1 + y / k); thread = (gene row tid % 128, cells of quads 4 h .. 4 h + 3
+// with h = tid / 128), the score in registers.
+// The dispersion pass (MLE = true; PassMLE in passes.cuh,
+// src/overdispersion.cpp:95-242): 32 genes per tile, A rows 32 b + gene
+// carry the Cox-Reid weights w, -w^2, 2 w^3 (b = 0, 1, 2; rows 96..127
+// zero); thread = (gene tid % 32, quad tid / 32); the two FP32 scalar sums
+// and, at the gene's nonzeros, the four FP64 sums with per-gene psi tables,
+// all in block z = 0.
+template <int XS, class VT, bool MLE>
+__global__ void __launch_bounds__(kWNT, 1) tcw_pass_kernel(PassGeom geo, PassParamsAny prm, TcwGeom tw) {
+    constexpr int GTn = MLE ? kMleG : kWM;
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ uint32_t tslot;
     __shared__ int abort_flag;
     __shared__ int16_t ptab[kWNmax];  // product row -> i | j << 8 (-1: padding)
+    __shared__ double psia[MLE ? kMleG : 1];
 
     if (geo.reset_next && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0)
         *geo.reset_next = 0;
     const int nact = *geo.n_act;
     const int tile = blockIdx.y;
-    if (tile * kWM >= nact) return;
+    if (tile * GTn >= nact) return;
     const int seg = blockIdx.x;
     const int zb = blockIdx.z;
     const int nblk = tw.nblk;
     const uint32_t tot = nblk <= 128 ? 128u : 256u;  // column of the running total
     const uint32_t ncols = 2 * tot;                  // columns allocated
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int gr = tid & (kWM - 1);  // this thread's gene row (= its tensor-memory lane)
-    const int hh = tid >> 7;         // its half of the chunk's cells (and of the drained columns)
-    const bool score = zb == 0;
+    const int gi = tid & (GTn - 1);  // this thread's gene within the tile
+    const int hh = tid >> 7;         // IRLS: half of the chunk's cells (and of the drained columns)
+    const bool extra = zb == 0;      // block z = 0 adds the score / scalar sums
 
-    int slot = tile * kWM + gr;
+    int slot = tile * GTn + gi;
     const bool valid_slot = slot < nact;
-    if (!valid_slot) slot = tile * kWM;  // duplicate a valid gene; not written
+    if (!valid_slot) slot = tile * GTn;  // duplicate a valid gene; not written
     const int g = __ldg(geo.act + slot);
     float bt[XS];
 #pragma unroll
     for (int i = 0; i < XS; ++i) bt[i] = i < tw.P ? __ldg(prm.beta + (int64_t)g * tw.P + i) * kLog2e : 0.f;
-    const float kk = __ldg(prm.k + g), rk = 1.f / kk;
+    float kk = 0.f, rk = 0.f, thf = 0.f;
+    double theta = 0.0, aa = 0.0;
+    if constexpr (MLE) {
+        theta = exp(prm.log_theta[g]);
+        aa = 1.0 / theta;
+        thf = (float)theta;
+    } else {
+        kk = __ldg(prm.k + g);
+        rk = 1.f / kk;
+    }
 
     for (int r = tid; r < nblk; r += kWNT) {
         const int gp = zb * nblk + r;
@@ -162,10 +200,30 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
     const int nchunk = (int)(k1 - k0);
 
     const int OPB = op_bytes(nblk);
-    constexpr int INB = in_bytes<VT>(XS);
+    constexpr int INB = in_bytes<VT, GTn>(XS);
     auto op = [&](int s) { return smem + s * OPB; };
     auto in_slot = [&](int s) { return smem + 2 * OPB + s * INB; };
     const VT* __restrict__ yrow = static_cast<const VT*>(tw.ydense) + (int64_t)g * tw.ld;
+
+    // MLE: the tile's psi tables (scratch in the first operand stage), then
+    // the zero rows 96..127 of both A stages
+    PsiTable tab{nullptr, nullptr, 0.0, 0.0};
+    if constexpr (MLE) {
+        double* psitab = reinterpret_cast<double*>(smem + 2 * OPB + kWRing * INB);
+        if (tid < kMleG) psia[tid] = aa;
+        __syncthreads();
+        build_psi_tables(kMleG, psia, psitab, reinterpret_cast<double*>(smem));
+        tab.d1 = psitab + (gi * 2 + 0) * kPsiTab;
+        tab.d2 = psitab + (gi * 2 + 1) * kPsiTab;
+        if (extra) {
+            tab.pa = digamma_d(aa);
+            tab.ta = trigamma_d(aa);
+        }
+        for (int t = tid; t < 2 * 2 * 32 * 8; t += kWNT) {
+            const int s = t >> 9, hl = (t >> 8) & 1, row = 96 + ((t >> 3) & 31), q = t & 7;
+            *reinterpret_cast<float4*>(op(s) + hl * kWA + stage_off(row, q, kWM)) = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
 
     auto fetch = [&](int kc) {
         unsigned char* ib = in_slot(kc % kWRing);
@@ -182,10 +240,18 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
         unsigned char* yb = ib + XS * kWKC * 4 + kWKC * 4;
         constexpr int CPP = 16 / (int)sizeof(VT);  // cells per piece
         constexpr int NPG = kWKC / CPP;            // pieces per gene row
+        if constexpr (MLE) {
+            // piece (gene tid % 32, p = tid / 32)
+            if (tid < kMleG * NPG) {
+                const int p = tid >> 5;
+                cp_async<16>(yb + (p * kMleG + gi) * 16, yrow + cs + p * CPP);
+            }
+        } else {
 #pragma unroll
-        for (int u = 0; u < NPG / 2; ++u) {
-            const int p = hh + 2 * u;  // piece index within the row
-            cp_async<16>(yb + (p * kWM + gr) * 16, yrow + cs + p * CPP);
+            for (int u = 0; u < NPG / 2; ++u) {
+                const int p = hh + 2 * u;  // piece index within the row
+                cp_async<16>(yb + (p * kWM + gi) * 16, yrow + cs + p * CPP);
+            }
         }
     };
 
@@ -215,9 +281,15 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
     const int dc0 = hh * (nblk / 2), dc1 = dc0 + nblk / 2;  // this warp's drained columns
     const uint32_t idesc = tf32_idesc(kWM, nblk);
 
-    float va[XS], vb[XS];  // score: cells (0, 1) and (2, 3) of each quad
+    // IRLS score: cells (0, 1) and (2, 3) of each quad; MLE: the FP32 and
+    // FP64 scalar sums
+    float va[MLE ? 1 : XS], vb[MLE ? 1 : XS];
+    float fs[2] = {0.f, 0.f};
+    double sc[4] = {0.0, 0.0, 0.0, 0.0};
+    if constexpr (!MLE) {
 #pragma unroll
-    for (int i = 0; i < XS; ++i) va[i] = vb[i] = 0.f;
+        for (int i = 0; i < XS; ++i) va[i] = vb[i] = 0.f;
+    }
 
     int issued = 0;   // chunks whose MMAs were committed (uniform)
     int drained = 0;  // runs added into the total (uniform)
@@ -238,10 +310,10 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
         const float4* o4 = reinterpret_cast<const float4*>(ib + XS * kWKC * 4);
         const VT* ys = reinterpret_cast<const VT*>(ib + XS * kWKC * 4 + kWKC * 4);
         unsigned char* sA = op(st);
-        // weights of this thread's gene at cells 16 hh .. 16 hh + 15
+        // the weights of this thread's gene at its cells
 #pragma unroll
-        for (int qi = 0; qi < 4; ++qi) {
-            const int q = 4 * hh + qi;
+        for (int qi = 0; qi < (MLE ? 1 : 4); ++qi) {
+            const int q = MLE ? warp : 4 * hh + qi;
             const float4 o = o4[q];
             float e0 = o.x * kLog2e, e1 = o.y * kLog2e, e2 = o.z * kLog2e, e3 = o.w * kLog2e;
 #pragma unroll
@@ -251,26 +323,57 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
                 fma_x2(e2, e3, bt[i], x.z, x.w);
             }
             float y[4];
-            load_counts(ys, q, gr, y);
+            load_counts<GTn>(ys, q, gi, y);
             const float e[4] = {e0, e1, e2, e3};
-            float hi[4], lo[4], sw[4];
+            if constexpr (MLE) {
+                float w1[4], w2[4], w3[4];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const float mu = ex2_approx(e[c]);
-                const float r = rcp_approx(mu + kk);
-                const float yr = y[c] * r;
-                tf32_split(fmaf(yr, rk, r), hi[c], lo[c]);  // r + y r / k
-                sw[c] = fmaf(mu, r, -yr);                   // (mu - y) r
-            }
-            *reinterpret_cast<float4*>(sA + stage_off(gr, q, kWM)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-            *reinterpret_cast<float4*>(sA + kWA + stage_off(gr, q, kWM)) =
-                make_float4(lo[0], lo[1], lo[2], lo[3]);
-            if (score) {
+                for (int c = 0; c < 4; ++c) {
+                    const float mu = ex2_approx(e[c]);
+                    const float xx = mu * thf;
+                    const float r = rcp_r(1.f + xx);
+                    const float w = mu * r;
+                    w1[c] = w;
+                    w2[c] = -w * w;
+                    w3[c] = 2.f * w * w * w;
+                    if (extra) {
+                        fs[0] += nb_ll_term<float>(xx, r);
+                        fs[1] += w * xx * r;
+                        if (y[c] > 0.f) {
+                            const double m = mu, yy = y[c];
+                            const double den = 1.0 + m * theta;
+                            double rr = (double)rcp_approx((float)den);
+                            rr = rr + rr * (1.0 - den * rr);
+                            sc[0] += yy * theta * rr;
+                            sc[1] += yy * rr * rr;
+                            double d1, d2;
+                            psi_diffs_tab(yy, aa, tab, d1, d2);
+                            sc[2] += d1;
+                            sc[3] += d2;
+                        }
+                    }
+                }
+                store_split(sA, gi, q, w1);
+                store_split(sA, 32 + gi, q, w2);
+                store_split(sA, 64 + gi, q, w3);
+            } else {
+                float hw[4], sw[4];
 #pragma unroll
-                for (int i = 0; i < XS; ++i) {
-                    const float4 x = x4[q * XS + i];
-                    fma2(va[i], vb[i], sw[0], sw[2], x.x, x.z);
-                    fma2(va[i], vb[i], sw[1], sw[3], x.y, x.w);
+                for (int c = 0; c < 4; ++c) {
+                    const float mu = ex2_approx(e[c]);
+                    const float r = rcp_approx(mu + kk);
+                    const float yr = y[c] * r;
+                    hw[c] = fmaf(yr, rk, r);    // r + y r / k
+                    sw[c] = fmaf(mu, r, -yr);   // (mu - y) r
+                }
+                store_split(sA, gi, q, hw);
+                if (extra) {
+#pragma unroll
+                    for (int i = 0; i < XS; ++i) {
+                        const float4 x = x4[q * XS + i];
+                        fma2(va[i], vb[i], sw[0], sw[2], x.x, x.z);
+                        fma2(va[i], vb[i], sw[1], sw[3], x.y, x.w);
+                    }
                 }
             }
         }
@@ -349,36 +452,70 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
     __syncthreads();
     tc_fence_after();
 
-    float* out = static_cast<float*>(geo.partW) + ((int64_t)seg * geo.slot_stride + tile * kWM + gr) * tw.NA;
-    const bool write = good && valid_slot;
-    // Hessian columns of this warp's half
-    for (int c = dc0; c < dc1; c += 8) {
-        float v[8];
-        if (issued > 0) {
-            tc_ld8(tmem + lanes + tot + (uint32_t)c, v);
-        } else {
+    // the Hessian-like columns of this warp's lanes: IRLS rows = genes;
+    // MLE rows 32 b + gene (b = warp % 4 < 3)
+    {
+        const int b = MLE ? (warp & 3) : 0;
+        const int lg = MLE ? (tid & 31) : gi;  // gene of this thread's tensor-memory lane
+        const bool write = good && tile * GTn + lg < nact && (!MLE || b < 3);
+        float* out = static_cast<float*>(geo.partW) + ((int64_t)seg * geo.slot_stride + tile * GTn + lg) * tw.NA +
+                     b * tw.NE;
+        for (int c = dc0; c < dc1; c += 8) {
+            float v[8];
+            if (issued > 0) {
+                tc_ld8(tmem + lanes + tot + (uint32_t)c, v);
+            } else {
 #pragma unroll
-            for (int u = 0; u < 8; ++u) v[u] = 0.f;
-        }
+                for (int u = 0; u < 8; ++u) v[u] = 0.f;
+            }
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const int gp = zb * nblk + c + u;
-            if (write && c + u < nblk && gp < tw.NE) out[gp] = v[u];
+            for (int u = 0; u < 8; ++u) {
+                const int gp = zb * nblk + c + u;
+                if (write && c + u < nblk && gp < tw.NE) out[gp] = v[u];
+            }
         }
     }
-    if (score) {
-        // the two halves of the cells: half 1 hands its sums to half 0
-        // through the (idle) first operand stage
-        float* red = reinterpret_cast<float*>(smem);  // [128 genes][XS]
-        if (hh == 1) {
+    if (extra) {
+        const bool write = good && valid_slot;
+        float* out = static_cast<float*>(geo.partW) + ((int64_t)seg * geo.slot_stride + tile * GTn + gi) * tw.NA;
+        if constexpr (MLE) {
+            // the 8 quads' sums of each gene, added in quad order
+            float* fred = reinterpret_cast<float*>(smem);                  // [8][32][2]
+            double* dred = reinterpret_cast<double*>(smem + 8 * 32 * 2 * 4);  // [8][32][4]
+            fred[(warp * 32 + gi) * 2 + 0] = fs[0];
+            fred[(warp * 32 + gi) * 2 + 1] = fs[1];
 #pragma unroll
-            for (int i = 0; i < XS; ++i) red[gr * XS + i] = va[i] + vb[i];
-        }
-        __syncthreads();
-        if (hh == 0 && write) {
+            for (int j = 0; j < 4; ++j) dred[(warp * 32 + gi) * 4 + j] = sc[j];
+            __syncthreads();
+            if (warp == 0 && write) {
+                float f0 = 0.f, f1 = 0.f;
+                double d[4] = {0.0, 0.0, 0.0, 0.0};
+                for (int w = 0; w < 8; ++w) {
+                    f0 += fred[(w * 32 + gi) * 2 + 0];
+                    f1 += fred[(w * 32 + gi) * 2 + 1];
 #pragma unroll
-            for (int i = 0; i < XS; ++i)
-                if (i < tw.P) out[tw.NE + i] = va[i] + vb[i] + red[gr * XS + i];
+                    for (int j = 0; j < 4; ++j) d[j] += dred[(w * 32 + gi) * 4 + j];
+                }
+                out[3 * tw.NE + 0] = f0;
+                out[3 * tw.NE + 1] = f1;
+                double* os = geo.partS + ((int64_t)seg * geo.slot_stride + tile * GTn + gi) * 4;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) os[j] = d[j];
+            }
+        } else {
+            // the two halves of the cells: half 1 hands its sums to half 0
+            // through the (idle) first operand stage
+            float* red = reinterpret_cast<float*>(smem);  // [128 genes][XS]
+            if (hh == 1) {
+#pragma unroll
+                for (int i = 0; i < XS; ++i) red[gi * XS + i] = va[i] + vb[i];
+            }
+            __syncthreads();
+            if (hh == 0 && write) {
+#pragma unroll
+                for (int i = 0; i < XS; ++i)
+                    if (i < tw.P) out[tw.NE + i] = va[i] + vb[i] + red[gi * XS + i];
+            }
         }
     }
     tc_fence_before();
@@ -389,29 +526,28 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_irls_kernel(PassGeom geo, PassIRL
     if (abort_flag && tid == 0) atomicExch(geo.err, 1);
 }
 
-template <int XS, class VT>
+template <int XS, class VT, bool MLE>
 cudaError_t run_tcw(const PassLaunch& L, const TcwGeom& tw) {
-    auto k = tcw_irls_kernel<XS, VT>;
-    const int smem = tcw_smem<VT>(XS, tw.nblk);
+    auto k = tcw_pass_kernel<XS, VT, MLE>;
+    const int smem = tcw_smem<VT, MLE>(XS, tw.nblk);
     cudaError_t e = raise_dyn_smem(k, smem);
     if (e != cudaSuccess) return e;
     if (L.occ_out) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(L.occ_out, k, kWNT, smem);
     dim3 grid(L.nseg, L.ntiles, tcw_blocks(L.P));
-    PassIRLS::Params prm{L.prm.beta, L.prm.beta_d, L.prm.k};
-    k<<<grid, kWNT, smem, L.stream>>>(L.geo, prm, tw);
+    k<<<grid, kWNT, smem, L.stream>>>(L.geo, L.prm, tw);
     return cudaGetLastError();
 }
 
-template <class VT>
+template <class VT, bool MLE>
 cudaError_t run_tcw_xs(const PassLaunch& L, const TcwGeom& tw) {
     switch (L.xs_pad) {
-        case 8: return run_tcw<8, VT>(L, tw);
-        case 12: return run_tcw<12, VT>(L, tw);
-        case 16: return run_tcw<16, VT>(L, tw);
-        case 20: return run_tcw<20, VT>(L, tw);
-        case 24: return run_tcw<24, VT>(L, tw);
-        case 28: return run_tcw<28, VT>(L, tw);
-        case 32: return run_tcw<32, VT>(L, tw);
+        case 8: return run_tcw<8, VT, MLE>(L, tw);
+        case 12: return run_tcw<12, VT, MLE>(L, tw);
+        case 16: return run_tcw<16, VT, MLE>(L, tw);
+        case 20: return run_tcw<20, VT, MLE>(L, tw);
+        case 24: return run_tcw<24, VT, MLE>(L, tw);
+        case 28: return run_tcw<28, VT, MLE>(L, tw);
+        case 32: return run_tcw<32, VT, MLE>(L, tw);
     }
     return cudaErrorInvalidValue;
 }
@@ -517,14 +653,21 @@ cudaError_t launch_tcw_prepare(const int64_t* rowptr, const int32_t* col, const 
     return cudaGetLastError();
 }
 
-// L.GT = 128 genes per tile; grid (L.nseg, L.ntiles, tcw_blocks(P))
+int tcw_tile_genes(PassKind k) { return k == PASS_MLE ? kMleG : kWM; }
+
+// L.GT = tcw_tile_genes(L.kind) genes per tile; grid (L.nseg, L.ntiles, tcw_blocks(P))
 cudaError_t launch_tcw_pass(const PassLaunch& L, const TcwGeom& tw) {
-    if (L.kind != PASS_IRLS || L.GT != kWM || !tcw_supported(L.P, L.xs_pad)) return cudaErrorInvalidValue;
-    if (!L.occ_out && (tw.nblk != tcw_nblk(L.P) || tw.NE != L.P * (L.P + 1) / 2 || tw.P != L.P))
+    if ((L.kind != PASS_IRLS && L.kind != PASS_MLE) || L.GT != tcw_tile_genes(L.kind) ||
+        !tcw_supported(L.P, L.xs_pad))
         return cudaErrorInvalidValue;
     TcwGeom t = tw;
+    t.NA = pass_na(L.kind, L.P);
     if (L.occ_out) t.nblk = tcw_nblk(L.P);
-    return L.val_u16 ? run_tcw_xs<uint16_t>(L, t) : run_tcw_xs<float>(L, t);
+    else if (tw.nblk != tcw_nblk(L.P) || tw.NE != L.P * (L.P + 1) / 2 || tw.P != L.P)
+        return cudaErrorInvalidValue;
+    if (L.kind == PASS_MLE)
+        return L.val_u16 ? run_tcw_xs<uint16_t, true>(L, t) : run_tcw_xs<float, true>(L, t);
+    return L.val_u16 ? run_tcw_xs<uint16_t, false>(L, t) : run_tcw_xs<float, false>(L, t);
 }
 
 }  // namespace devil

@@ -60,9 +60,29 @@ def test_tcw_float_counts_and_mle(dv, orc):
     ref = oracle_fit(orc, P, orc.OD_MLE)
     fit = dv.fit_devil((P.rowptr, P.col, P.val.astype(np.float64), P.n), P.X, overdispersion="MLE",
                        size_factors="normed_sum", compute_theta_mom=True, precision="tc_tf32")
-    assert dv.context().engine(0) == "tensor_wide"
+    assert [dv.context().engine(k) for k in (0, 2)] == ["tensor_wide", "tensor_wide"]
     same = check_beta(fit, ref)
     check_rel(fit["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta MLE")
+
+
+@pytest.mark.parametrize("p,n", [(9, 3000), (20, 2501), (32, 2000)])
+def test_tcw_mle_matches_oracle(dv, orc, monkeypatch, p, n):
+    """The dispersion pass on the tensor cores (precision "tc_tf32"): the
+    Cox-Reid matrices b, db, d2b as split-TF32 MMAs (32 genes x 3 weights
+    per tile), the scalar sums on the CUDA cores (FP64 at the nonzeros).
+    MLE theta 1e-4 relative against the oracle, and the CUDA-core pass
+    (FP64 per cell above p = 8) agrees to 1e-5."""
+    P = synthetic.make("continuous", seed=60 + p, G=160, n=n, p=p)
+    ref = oracle_fit(orc, P, orc.OD_MLE)
+    fit = gpu_fit(dv, P, "MLE", precision="tc_tf32")
+    assert dv.context().engine(2) == "tensor_wide"
+    same = check_beta(fit, ref)
+    check_rel(fit["overdispersion"], ref["theta"], _theta_mask(ref["theta"], same), 1e-4, "theta MLE")
+    monkeypatch.setenv("DEVIL_TCW_MLE", "0")
+    base = gpu_fit(dv, P, "MLE", precision="tc_tf32")
+    assert dv.context().engine(2) == "shared"
+    check_rel(fit["overdispersion"], base["overdispersion"], _theta_mask(base["overdispersion"], same),
+              1e-5, "theta MLE vs the CUDA-core pass")
 
 
 def test_tcw_switch(dv, monkeypatch):
