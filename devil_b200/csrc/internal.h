@@ -85,8 +85,8 @@ cudaError_t launch_gen_pass(const PassLaunch& L);
 // ---- tensor-core IRLS engine for p = 5..32 (kernels_tcw.cu) ----
 // Inputs built once per fit by launch_tcw_prepare: the counts as a dense
 // image (gene rows of ld = npad cells, uint16 or float, zero where the CSR
-// has no entry), the design's feature rows xt [xs][npad] and the offsets
-// offp [npad] (zero past n).
+// has no entry), the design's feature rows xt [xs][npad] (zero past n) and
+// the offsets offp [npad] (-1e30 past n: mu = 0 in the padding).
 struct TcwGeom {
     const float* xt = nullptr;
     const float* offp = nullptr;

@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kWNT, 1) tcw_pass_kernel(PassGeom geo, PassPar
     }
 
     // this block's cells: fine segments [b0, b1) (multiples of 32 cells up
-    // to n; chunks past n read the zero padding of the images)
+    // to n; the last chunk reads the padding of the images past n)
     const int nfs = geo.nbound - 1;
     const int b0 = (int)(((int64_t)seg * nfs) / geo.nseg);
     const int b1 = (int)(((int64_t)(seg + 1) * nfs) / geo.nseg);
@@ -564,8 +564,10 @@ __global__ void tcw_dense_kernel(const int64_t* __restrict__ rowptr, const int32
     }
 }
 
-// feature rows of the design (zero past n and past p) and the offsets
-// (zero past n)
+// feature rows of the design (zero past n and past p) and the offsets:
+// -1e30 past n, so that mu = 0 there and the padding cells of the last
+// chunk add nothing to any sum (the products and the score vanish with
+// x = 0 as well, the dispersion pass's scalar sums only with mu = 0)
 __global__ void tcw_xt_kernel(const float* __restrict__ Xrm, int xs, int64_t n, int64_t npad,
                               const float* __restrict__ off, float* __restrict__ xt, float* __restrict__ offp) {
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < (int64_t)(xs + 1) * npad;
@@ -573,7 +575,7 @@ __global__ void tcw_xt_kernel(const float* __restrict__ Xrm, int xs, int64_t n, 
         const int i = (int)(t / npad);
         const int64_t c = t - (int64_t)i * npad;
         if (i < xs) xt[t] = c < n ? Xrm[c * xs + i] : 0.f;
-        else offp[c] = c < n ? off[c] : 0.f;
+        else offp[c] = c < n ? off[c] : -1e30f;
     }
 }
 
