@@ -851,13 +851,14 @@ bool tcw_wanted(const DevProblem& dp) {
     if (e && *e) return atoi(e) == 1;
     return dp.precision == DEVIL_PREC_TC_TF32 || dp.P > reg_max_p();
 }
-// its dispersion (MLE) pass: DEVIL_TCW_MLE=1 / 0; otherwise the
-// DEVIL_PREC_TC_TF32 precision selects it
+// its dispersion (MLE) pass: DEVIL_TCW_MLE=1 / 0; otherwise as the IRLS
+// pass (the FP64 shared-memory pass it replaces from p = 9 on is about 13x
+// slower on the 20,000 x 100,000 continuous workload at p = 16 and 32)
 bool tcw_mle_wanted(const DevProblem& dp) {
     if (!tcw_supported(dp.P, dp.xs) || !dp.tcw_fits) return false;
     const char* e = getenv("DEVIL_TCW_MLE");
     if (e && *e) return atoi(e) == 1;
-    return dp.precision == DEVIL_PREC_TC_TF32;
+    return dp.precision == DEVIL_PREC_TC_TF32 || dp.P > reg_max_p();
 }
 
 PassPlan plan_engine(PassKind k, const DevProblem& dp, int form, bool allow_tcw = true) {

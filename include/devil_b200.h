@@ -95,8 +95,9 @@ typedef struct devil_counts {
 #define DEVIL_PREC_FP32      0   /* FP32 FMAs on the CUDA cores (default)   */
 #define DEVIL_PREC_TC_TF32   1   /* tcgen05 MMAs on split TF32 (hi + lo)    */
                                  /* operands, FP32 accumulation: IRLS and   */
-                                 /* MLE at p <= 4, IRLS at p = 5..32        */
-                                 /* (designs without few distinct rows);    */
+                                 /* MLE passes at every p (designs without  */
+                                 /* few distinct rows; from p = 9 on this   */
+                                 /* is also what DEVIL_PREC_FP32 runs);     */
                                  /* other passes as DEVIL_PREC_FP32         */
 #define DEVIL_PREC_TC_BF16X3 2   /* not provided (DEVIL_ERR_UNSUPPORTED):   */
                                  /* the split-TF32 path already reaches     */
@@ -166,9 +167,10 @@ DEVIL_API int devil_ctx_profile_tc(devil_ctx *ctx, int pass_kind, double *tc_flo
 DEVIL_API int64_t devil_ctx_irls_rescued(const devil_ctx *ctx);
 /* Engine of the last launch of a pass kind on this context (no counterpart
  * in the reference): 0 register tiles (p <= 8), 1 shared-memory tiles,
- * 2 design groups (few distinct design rows), 3 tensor cores (IRLS pass,
- * p <= 4), 4 tensor cores (IRLS pass, p = 5..32: the Hessian as split-TF32
- * MMAs over a dense count image), -1 none yet. */
+ * 2 design groups (few distinct design rows), 3 tensor cores (IRLS and MLE
+ * passes, p <= 4), 4 tensor cores (IRLS and MLE passes, p = 5..32: the
+ * p x p contractions as split-TF32 MMAs over a dense count image), -1 none
+ * yet. */
 DEVIL_API int devil_ctx_engine(const devil_ctx *ctx, int pass_kind);
 
 /* ---- full pipeline --------------------------------------------------- */

@@ -48,9 +48,10 @@ def test_tcw_irls_matches_oracle(dv, orc, monkeypatch, p, n):
     monkeypatch.delenv("DEVIL_TCW")
     assert ctx.engine(0) in ("register", "shared")
     _agree(fit, base)
-    # the default precision: the tensor-core engine from p = 9 on
-    gpu_fit(dv, P, "MOM")
-    assert ctx.engine(0) == ("register" if p <= 8 else "tensor_wide")
+    # the default precision: the tensor-core engines from p = 9 on
+    gpu_fit(dv, P, "MLE")
+    want = "register" if p <= 8 else "tensor_wide"
+    assert [ctx.engine(k) for k in (0, 2)] == [want, want]
 
 
 def test_tcw_float_counts_and_mle(dv, orc):
