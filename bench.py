@@ -73,6 +73,9 @@ def parse():
                     help="design columns of a covariates-only config (continuous)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "tc_tf32"],
                     help="arithmetic of the Hessian contractions (DEVIL_PREC_*)")
+    ap.add_argument("--problems", type=int, default=40,
+                    help="--config many: the first K problems of the seeded 500-problem draw")
+    ap.add_argument("--workers", type=int, default=4, help="--config many: concurrent streams")
     return ap.parse_args()
 
 
@@ -455,8 +458,114 @@ def time_plain(args, L, lib, ctx, dev, ext, data, X, p, n, sf_dev, opts_chosen, 
     return res, fitted
 
 
+def run_many(args):
+    """Many uneven problems (one fit_devil per problem in the reference,
+    R/main.R:164-273): the first K problems of the seeded 500-problem draw
+    (n ~ LogUniform(200, 5e4), G ~ U{5000..20000}, p ~ U{2..16}, continuous
+    designs, per-problem dispersion scale), fitted through the host-buffer
+    C ABI (H2D copies of the counts and design, D2H of the results inside the
+    timed region) as (a) one devil_fit_batch call on --workers concurrent
+    streams and (b) one devil_fit call per problem.  Both are synchronous
+    calls timed by the host clock (the batch spreads over several streams).
+    fit + MOM and MLE theta + bread per problem."""
+    import torch
+
+    import devil_b200 as dv
+    from devil_b200 import _lib as L
+    from devil_b200 import synthetic
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    shapes = synthetic.many_problems_shapes(500, seed=args.seed)[: args.problems]
+    dev = torch.device("cuda:0")
+    keep, probs = [], (L.Problem * len(shapes))()
+    res = (L.FitResult * len(shapes))()
+    genes = cells = nnz_tot = 0
+    for i, (G, n, p, sc) in enumerate(shapes):
+        d = synthetic.make_torch("continuous", seed=args.seed + 1000 + i, G=G, n=n, p=p,
+                                 theta_scale=sc, device=dev)
+        rp = d["rowptr"].cpu().numpy()
+        cl = d["col"].cpu().numpy()
+        vl = d["val"].cpu().numpy().view(np.uint16)
+        X = np.asfortranarray(d["X"]).ravel(order="F").astype(np.float64)
+        out = {k: np.empty(sz, dt) for k, sz, dt in [
+            ("beta", G * p, np.float64), ("theta", G, np.float64), ("iters", G, np.int32),
+            ("bread", G * p * p, np.float64), ("theta_mom", G, np.float64), ("status", G, np.int32)]}
+        keep.append((rp, cl, vl, X, out))
+        c = probs[i].counts
+        c.format = L.COUNTS_CSR_U16
+        c.n_genes, c.n_cells, c.nnz = G, n, int(rp[-1])
+        c.values, c.ptr, c.idx = vl.ctypes.data, rp.ctypes.data, cl.ctypes.data
+        probs[i].X = X.ctypes.data
+        probs[i].p = p
+        probs[i].cluster_ends = None
+        probs[i].n_clusters = 0
+        res[i] = L.FitResult(out["beta"].ctypes.data, out["theta"].ctypes.data, out["iters"].ctypes.data,
+                             None, out["bread"].ctypes.data, None, out["theta_mom"].ctypes.data,
+                             out["status"].ctypes.data, None, None, None)
+        genes += G
+        cells += n
+        nnz_tot += int(rp[-1])
+        del d
+    torch.cuda.empty_cache()
+    ctx = dv.context(0)
+    lib = L.load()
+    opts = L.FitOpts()
+    lib.devil_fit_opts_default(C.byref(opts))
+    opts.overdispersion = L.OD_MLE
+    opts.size_factors = L.SF_NORMED_SUM
+    opts.compute_theta_mom = 1
+    opts.precision = {"fp32": L.PREC_FP32, "tc_tf32": L.PREC_TC_TF32}[args.precision]
+    K = len(shapes)
+
+    def batch():
+        ctx.check(lib.devil_fit_batch(ctx.h, K, probs, C.byref(opts), res, int(args.workers)))
+
+    def loop():
+        for i in range(K):
+            ctx.check(lib.devil_fit(ctx.h, C.byref(probs[i].counts), C.c_void_p(probs[i].X), probs[i].p,
+                                    None, 0, C.byref(opts), C.byref(res[i])))
+
+    for _ in range(max(1, args.warmup)):
+        batch()
+    loop()
+    clocks = Clocks(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        batch()
+    tb = (time.perf_counter() - t0) / args.steps
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        loop()
+    tl = (time.perf_counter() - t0) / args.steps
+    clk = clocks.stop()
+    conv = float(np.mean(np.concatenate([k[4]["status"] for k in keep]) == L.GENE_CONVERGED))
+    line = {
+        "metric": METRIC, "value": genes / tb, "unit": "genes/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": max(1, args.warmup), "ms_per_step": tb * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32/tf32x3", "data": "synthetic",
+        "config": {"workload": f"many uneven problems: the first {K} of a seeded draw of 500 "
+                               f"(n ~ LogUniform(200, 5e4), G ~ U{{5000..20000}}, p ~ U{{2..16}}, "
+                               f"continuous designs, per-problem dispersion scale), CSR uint16; "
+                               f"normed_sum size factors, IRLS, MOM + MLE theta, bread per problem",
+                   "problems": K, "genes": genes, "cells": cells, "nnz": nnz_tot,
+                   "timing": "host clock around synchronous host-buffer calls (copies included)"},
+        "many": {"batch": {"workers": args.workers, "ms": tb * 1e3, "problems_per_s": K / tb,
+                           "genes_per_s": genes / tb},
+                 "one_call_per_problem": {"ms": tl * 1e3, "problems_per_s": K / tl, "genes_per_s": genes / tl},
+                 "batch_vs_loop": tl / tb, "converged_frac": round(conv, 4)},
+        "clocks": clk, "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.config == "many":
+        run_many(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return

@@ -13,6 +13,7 @@
 #include <atomic>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <thread>
 #include <string>
 #include <unordered_map>
@@ -838,6 +839,8 @@ struct PassPlan {
     int GT;
     PassKind kind = PASS_IRLS;
     int plain = 0;  // the plain comparison form
+    int waves = 0;  // design groups: waves of a slice-major step; wide tensor cores: minimum waves
+                    // (0: the engine's default)
 };
 
 // the tensor-core IRLS engine for p = 5..32 (kernels_tcw.cu): DEVIL_TCW=1
@@ -910,7 +913,8 @@ int choose_nseg(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, int 
     if (plan.engine == ENGINE_GRP) return 1;
     const int occ = pass_blocks_per_sm(plan.kind, plan.engine, dp.P, plan.GT, dp.val_u16, plan.plain);
     const int64_t cap = (int64_t)ctx->sm_count * std::max(1, occ);
-    const int64_t min_waves = plan.engine == ENGINE_TC ? 4 : (plan.engine == ENGINE_TCW ? 2 : 1);
+    const int64_t min_waves =
+        plan.engine == ENGINE_TC ? 4 : (plan.engine == ENGINE_TCW ? (plan.waves > 0 ? plan.waves : 2) : 1);
     // the wide tensor-core engine has tcw_blocks(p) product blocks per tile
     if (plan.engine == ENGINE_TCW) tiles *= tcw_blocks(dp.P);
     int want = (int)((min_waves * cap + tiles - 1) / tiles);
@@ -1010,7 +1014,8 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
             if (kind == PASS_MLE) gg.psitab = ws<double>(ctx, "grp_psitab", (size_t)tiles * kGrpTab);
             // (the IRLS step folds the assembly into its finalize)
             LAUNCH(launch_grp_slices(kind, gg, prm, dp.val_u16, tiles,
-                                     grp_slices_tile(tiles, gg.S, ctx->sm_count), kind != PASS_IRLS,
+                                     grp_slices_tile(tiles, gg.S, ctx->sm_count, plan.waves > 0 ? plan.waves : 3),
+                                     kind != PASS_IRLS,
                                      ctx->stream));
         } else {
             LAUNCH(launch_grp_pass(kind, gg, prm, dp.val_u16, tiles, ctx->stream));
@@ -1104,9 +1109,116 @@ const int32_t* all_genes(devil_ctx* ctx, const DevProblem& dp, int32_t** count_o
 // ------------------------------------------------------------------
 // IRLS loop (src/beta.cpp:25-51) with active-gene compaction
 // ------------------------------------------------------------------
+// ------------------------------------------------------------------
+// tile autotuner
+// ------------------------------------------------------------------
+// Each engine has a tile knob whose best value depends on the shape: genes
+// per thread of the register engine (GT), the waves a slice-major step of
+// the design-group engine is spread over (its gene tile), the minimum
+// waves of the wide tensor-core pass (its cell segments).  On the first
+// loop of a shape bucket (pass kind, engine, p, count type, log2 n,
+// log2 G, half-octaves of the density) in this process, each candidate
+// plan runs the loop's first pass once untimed and once timed (CUDA events
+// on the context stream, all genes active); the fastest is kept for the
+// bucket.  The candidates leave every gene's result unchanged except for
+// the register and wide engines, whose FP32 segment sums can round
+// differently (well inside the parity bars).  DEVIL_AUTOTUNE=0 keeps the
+// heuristic defaults.
+struct TuneKey {
+    int kind, engine, P, u16, nb, gb, db;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(kind, engine, P, u16, nb, gb, db) < std::tie(o.kind, o.engine, o.P, o.u16, o.nb, o.gb, o.db);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, PassPlan> g_tune;
+
+bool autotune_enabled() {
+    const char* e = getenv("DEVIL_AUTOTUNE");
+    return !(e && *e && atoi(e) == 0);
+}
+
+std::vector<PassPlan> tune_candidates(devil_ctx* ctx, const DevProblem& dp, const PassPlan& base) {
+    std::vector<PassPlan> c{base};
+    if (base.plain) return c;
+    if (base.engine == ENGINE_REG && (base.kind == PASS_IRLS || base.kind == PASS_MLE)) {
+        if (getenv(base.kind == PASS_IRLS ? "DEVIL_IRLS_GT" : "DEVIL_MLE_GT")) return c;  // set by hand
+        for (int gt : {base.GT / 2, base.GT * 2}) {
+            if (gt < 1 || !reg_gt_supported(base.kind, dp.P, gt)) continue;
+            PassPlan p = base;
+            p.GT = gt;
+            c.push_back(p);
+        }
+    } else if (base.engine == ENGINE_GRP) {
+        const int bit = base.kind == PASS_IRLS ? 1 : (base.kind == PASS_MLE ? 2 : 0);
+        if (ctx->grp_slices & bit) {
+            for (int w : {2, 6}) {
+                PassPlan p = base;
+                p.waves = w;
+                c.push_back(p);
+            }
+        }
+    } else if (base.engine == ENGINE_TCW) {
+        PassPlan p = base;
+        p.waves = 4;
+        c.push_back(p);
+    }
+    return c;
+}
+
+// the plan for a loop's passes; act / n_act list the n0 genes of its first pass
+PassPlan autotune(devil_ctx* ctx, const DevProblem& dp, const PassPlan& base, const int32_t* act,
+                  const int32_t* n_act, int64_t n0, const PassParamsAny& prm, int form) {
+    if (!autotune_enabled() || n0 < 256) return base;
+    const double dens = dp.nnz > 0 ? (double)dp.nnz / ((double)dp.G * (double)dp.n) : 1e-9;
+    const TuneKey key{(int)base.kind, (int)base.engine, dp.P, dp.val_u16,
+                      (int)std::floor(std::log2((double)dp.n)), (int)std::floor(std::log2((double)dp.G)),
+                      (int)std::floor(-2.0 * std::log2(dens))};
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second;
+    const std::vector<PassPlan> cands = tune_candidates(ctx, dp, base);
+    PassPlan best = base;
+    if (cands.size() > 1) {
+        const int was_profiling = ctx->profiling;
+        ctx->profiling = 0;
+        cudaEvent_t t0, t1;
+        CK(cudaEventCreate(&t0));
+        CK(cudaEventCreate(&t1));
+        double best_ms = 0.0;
+        for (size_t i = 0; i < cands.size(); ++i) {
+            const PassPlan& pl = cands[i];
+            const int tiles = (int)((n0 + pl.GT - 1) / pl.GT);
+            const int nseg = choose_nseg(ctx, dp, pl, tiles, form);
+            const PassBuffers pb = pass_buffers(ctx, pl.kind, dp.P, (size_t)nseg * tiles * pl.GT);
+            float ms = 0.f;
+            for (int rep = 0; rep < 2; ++rep) {
+                CK(cudaEventRecord(t0, ctx->stream));
+                launch_pass(ctx, dp, pl.kind, pl, nseg, tiles, dp.fine_bound, dp.fine_ptr, dp.nfine + 1, act,
+                            n_act, nullptr, pb, prm);
+                CK(cudaEventRecord(t1, ctx->stream));
+                CK(cudaEventSynchronize(t1));
+                CK(cudaEventElapsedTime(&ms, t0, t1));
+            }
+            // a candidate replaces the default only when clearly faster
+            if (i == 0 || ms < 0.97 * best_ms) {
+                best = pl;
+                best_ms = ms;
+            }
+            if (ctx->debug) fprintf(stderr, "[devil] tune kind %d engine %d GT %d waves %d: %.3f ms\n",
+                                    (int)pl.kind, (int)pl.engine, pl.GT, pl.waves, ms);
+        }
+        CK(cudaEventDestroy(t0));
+        CK(cudaEventDestroy(t1));
+        ctx->profiling = was_profiling;
+    }
+    g_tune[key] = best;
+    return best;
+}
+
 // One IRLS loop over the n0 genes listed in the "act0" workspace (their
 // iteration counts and status start at 0); returns the pass launches.
-int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, double* beta, float* beta_f,
+int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan0, double* beta, float* beta_f,
                   const float* k, int32_t* iters, int32_t* status, int max_iter, double eps, int form,
                   int64_t n0) {
     cudaStream_t st = ctx->stream;
@@ -1115,12 +1227,13 @@ int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan, do
     int32_t* cnt = ws<int32_t>(ctx, "cnt", 4);
     LAUNCH(launch_set_i32(cnt, (int32_t)n0, st));
     LAUNCH(launch_set_i32(cnt + 1, 0, st));
+    PassParamsAny prm{beta_f, beta, k, nullptr, nullptr};
+    const PassPlan plan = autotune(ctx, dp, plan0, act[0], cnt, n0, prm, form);
     PassBuffers pb = pass_buffers(ctx, PASS_IRLS, dp.P, max_slot_segs(ctx, dp, plan, form));
     // copies of an earlier loop still in flight would overwrite the mirror
     CK(cudaStreamSynchronize(st));
     *ctx->mapped_host = (int32_t)n0;
     const int LAG = 2;
-    PassParamsAny prm{beta_f, beta, k, nullptr, nullptr};
     int64_t launched = 0;
     for (int t = 0; t < max_iter; ++t) {
         const int cur = t & 1, nxt = cur ^ 1;
@@ -1251,7 +1364,7 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     cudaStream_t st = ctx->stream;
     const int64_t G = dp.G;
     if (G == 0) return;
-    const PassPlan plan = plan_for(PASS_MLE, dp, form);
+    PassPlan plan = plan_for(PASS_MLE, dp, form);
     if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported for MLE", dp.P);
     MleState s;
     s.x = ws<double>(ctx, "mle_x", G);
@@ -1268,12 +1381,13 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     LAUNCH(launch_set_i32(cnt, 0, st));
     LAUNCH(launch_set_i32(cnt + 1, 0, st));
     LAUNCH(launch_mle_init(dp.stats, G, dp.n, s, act[0], cnt, st));
+    PassParamsAny prm{beta_f, beta_d, nullptr, s.x, nullptr};
+    plan = autotune(ctx, dp, plan, act[0], cnt, G, prm, form);
     PassBuffers pb = pass_buffers(ctx, PASS_MLE, dp.P, max_slot_segs(ctx, dp, plan, form));
     // copies of an earlier loop still in flight would overwrite the mirror
     CK(cudaStreamSynchronize(st));
     *ctx->mapped_host = (int32_t)G;
     const int LAG = 2;
-    PassParamsAny prm{beta_f, beta_d, nullptr, s.x, nullptr};
     int64_t launched = 0;
     // one far-left evaluation plus at most max_iter Newton evaluations
     for (int t = 0; t <= max_iter; ++t) {

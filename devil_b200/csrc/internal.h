@@ -217,7 +217,7 @@ cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsA
 // it, then a block per gene assembles the p x p sums (geo.gsum: slots x S x
 // grp_slices_nq(kind) doubles; geo.rowexp: slots x U; geo.psitab, MLE:
 // slots x kGrpTab)
-int grp_slices_tile(int64_t hint, int S, int sm_count);
+int grp_slices_tile(int64_t hint, int S, int sm_count, int waves = 3);
 int grp_slices_nq(PassKind k);
 cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm,
                               int val_u16, int max_slots, int tile, bool assemble, cudaStream_t st);

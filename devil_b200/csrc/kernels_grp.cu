@@ -947,12 +947,12 @@ __global__ void __launch_bounds__(256) grp_assemble_kernel(GrpGeom geo) {
     }
 }
 
-int grp_slices_tile(int64_t hint, int S, int sm_count) {
+int grp_slices_tile(int64_t hint, int S, int sm_count, int waves) {
     // two resident blocks per SM (registers, the 64 KB slice stage); about
-    // three waves, the tile count chosen so the last wave is nearly full,
-    // tiles of 16..1024 genes
+    // `waves` waves (3 unless tuned), the tile count chosen so the last
+    // wave is nearly full, tiles of 16..1024 genes
     const int64_t cap = (int64_t)sm_count * 2;
-    int64_t tiles = std::max<int64_t>(1, (3 * cap + S - 1) / S);
+    int64_t tiles = std::max<int64_t>(1, ((int64_t)std::max(1, waves) * cap + S - 1) / S);
     double best_eff = 0.0;
     int64_t best = tiles;
     for (int64_t tc = tiles; tc <= 2 * tiles; ++tc) {

@@ -24,8 +24,12 @@ shapes, sparsity and value distributions of the benchmark workloads:
   about 10% nonzeros, CSR uint16.
 * ``continuous``   -- G=20,000 x n=100,000, p=16 (intercept, condition and
   p - 2 N(0, 1) covariates with gene effects N(0, 0.2)), beta0 ~ N(-2, 1),
-  CSR uint16: a design without few distinct rows.  ``p`` (3..32) overrides
+  CSR uint16: a design without few distinct rows.  ``p`` (2..32) overrides
   the number of columns.
+* ``many_problems_shapes`` -- the many-uneven-problems workload: per
+  problem n ~ LogUniform(200, 50,000) cells, G ~ U{5,000..20,000} genes,
+  p ~ U{2..16} (the ``continuous`` design) and a per-problem dispersion
+  scale s ~ LogUniform(0.1, 10) (theta_g ~ LogNormal(log s, 1)).
 
 Counts are NB with Var = mu + theta * mu^2 (theta is the dispersion devil
 returns), drawn as a Gamma-Poisson mixture: lambda ~ Gamma(shape=1/theta,
@@ -65,7 +69,7 @@ def config_params(name: str, p: int | None = None) -> dict:
     intercept, condition and covariates only."""
     cfg = dict(CONFIGS[name])
     if p is not None and int(p) != cfg["p"]:
-        if cfg["types"] or not 3 <= int(p) <= 32:
+        if cfg["types"] or not 2 <= int(p) <= 32:
             raise ValueError(f"config {name!r} has no p = {p}")
         cfg["p"] = int(p)
         cfg["covariates"] = int(p) - 2
@@ -197,9 +201,23 @@ def make(config: str = "plain_small", seed: int = 0, G: int | None = None, n: in
                    dict(config=config, seed=seed, dense=cfg["dense"], saturated=sat))
 
 
+def many_problems_shapes(n_problems: int = 500, seed: int = 0):
+    """(G, n, p, theta scale) of each problem of the many-uneven-problems
+    workload (seeded)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(int(n_problems)):
+        n = int(round(np.exp(rng.uniform(np.log(200.0), np.log(50000.0)))))
+        G = int(rng.integers(5000, 20001))
+        p = int(rng.integers(2, 17))
+        scale = float(np.exp(rng.uniform(np.log(0.1), np.log(10.0))))
+        out.append((G, n, p, scale))
+    return out
+
+
 def make_torch(config: str = "plain_sparse", seed: int = 0, G: int | None = None,
                n: int | None = None, device="cuda", chunk_cells: int = 1 << 27,
-               mean_loc: float | None = None, p: int | None = None):
+               mean_loc: float | None = None, p: int | None = None, theta_scale: float = 1.0):
     """Draw the same model on a torch device (full-size benchmark inputs).
 
     Returns a dict of device tensors: rowptr (int64), col (int32), val
@@ -216,7 +234,7 @@ def make_torch(config: str = "plain_sparse", seed: int = 0, G: int | None = None
     rng = np.random.default_rng(seed)
     X = design(cfg, n, rng)
     sf = rng.lognormal(0.0, 0.3, n)
-    theta = rng.lognormal(0.0, 1.0, G)
+    theta = rng.lognormal(0.0, 1.0, G) * float(theta_scale)
     beta = np.zeros((G, p))
     if cfg["b0_loc"] is None:
         beta[:, 0] = np.log(rng.lognormal(cfg["mean_loc"], 2.0, G))
