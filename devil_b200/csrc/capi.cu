@@ -253,7 +253,7 @@ struct DevProblem {
     // image, feature rows, padded offsets), built by its first launch
     mutable TcwGeom tcw;
     mutable bool tcw_ready = false;
-    bool tcw_fits = false;  // the dense count image fits half of the free device memory
+    mutable int tcw_fits = -1;  // the dense count image fits half of the free device memory (-1: not asked)
     int precision = DEVIL_PREC_FP32;  // DEVIL_PREC_*: tensor-core passes at p <= 4
     double* Xdrm = nullptr;  // row-major FP64 copy for the FP64 passes
     double* sf = nullptr;
@@ -280,6 +280,8 @@ struct DevProblem {
         // sparse design rows and the assembly's (group, weight) lists
         int32_t *rptr = nullptr, *rcol = nullptr, *qptr = nullptr, *qu = nullptr, *vptr = nullptr,
                 *vu = nullptr;
+        int nA = 0;  // exclusive-column structure (GrpGeom)
+        int32_t *colA = nullptr, *colD = nullptr, *colpos = nullptr;
         double *rval = nullptr, *qv = nullptr, *vv = nullptr;
     } grp;
 };
@@ -470,13 +472,20 @@ void prepare_design(devil_ctx* ctx, DevProblem& dp, const double* X, int P, bool
     dp.stats = ws<double>(ctx, "stats", (size_t)dp.G * 6);
     LAUNCH(launch_gene_stats(dp.rowptr, dp.val, dp.val_u16, dp.G, dp.n, dp.stats, st));
     CK(cudaStreamSynchronize(st));  // host copies above must stay valid until here
-    if (tcw_supported(P, dp.xs)) {
+}
+
+// whether the wide tensor-core engine's dense count image fits half of the
+// free device memory (asked once per fit, and only where that engine could
+// run: the query costs milliseconds on a busy device)
+bool tcw_fits(const DevProblem& dp) {
+    if (dp.tcw_fits < 0) {
         size_t fr = 0, tot = 0;
-        CK(cudaMemGetInfo(&fr, &tot));
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
         const double need = (double)dp.G * tcw_npad(dp.n) * (dp.val_u16 ? 2.0 : 4.0) +
                             (double)(dp.xs + 1) * tcw_npad(dp.n) * 4.0;
-        dp.tcw_fits = need <= 0.5 * (double)fr;
+        dp.tcw_fits = need <= 0.5 * (double)fr ? 1 : 0;
     }
+    return dp.tcw_fits == 1;
 }
 
 // size factors and offsets (R/main.R:224-230, R/size_factors.R)
@@ -763,6 +772,42 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
             }
         vptr[i + 1] = (int32_t)vu.size();
     }
+    // exclusive columns (no design row with two of them nonzero), chosen
+    // greedily in order of fewest collisions: the one-hot cell-type
+    // indicators of a design; the rest stay dense.  Used when at least four
+    // columns are exclusive and at most eight are dense.
+    std::vector<int32_t> colA, colD, colpos(P, 0);
+    {
+        std::vector<int> coll(P, 0);
+        auto collide = [&](int i, int j) {
+            for (int u = 0; u < U; ++u)
+                if (hx[(size_t)u * P + i] != 0.0 && hx[(size_t)u * P + j] != 0.0) return true;
+            return false;
+        };
+        for (int i = 0; i < P; ++i)
+            for (int j = 0; j < P; ++j)
+                if (i != j && collide(i, j)) ++coll[i];
+        std::vector<int> order(P);
+        for (int i = 0; i < P; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return coll[a] < coll[b]; });
+        std::vector<char> inD(P, 0);
+        for (int c : order) {
+            bool ok = true;
+            for (int d = 0; d < P && ok; ++d)
+                if (inD[d] && collide(c, d)) ok = false;
+            if (ok) inD[c] = 1;
+        }
+        for (int c = 0; c < P; ++c) {
+            if (inD[c]) {
+                colpos[c] = -1 - (int32_t)colD.size();
+                colD.push_back(c);
+            } else {
+                colpos[c] = (int32_t)colA.size();
+                colA.push_back(c);
+            }
+        }
+        if (colD.size() < 4 || colA.size() > 8 || colA.empty()) colA.clear();
+    }
     auto up_i = [&](const char* nm, const std::vector<int32_t>& v) {
         int32_t* d = ws<int32_t>(ctx, nm, std::max<size_t>(v.size(), 1));
         h2d(ctx, d, v.data(), v.size());
@@ -783,6 +828,12 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
     g.vptr = up_i("grp_vptr", vptr);
     g.vu = up_i("grp_vu", vu);
     g.vv = up_d("grp_vv", vv);
+    g.nA = (int)colA.size();
+    if (g.nA > 0) {
+        g.colA = up_i("grp_colA", colA);
+        g.colD = up_i("grp_colD", colD);
+        g.colpos = up_i("grp_colpos", colpos);
+    }
     g.res = res;
     CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
     g.active = true;
@@ -826,6 +877,10 @@ GrpGeom grp_geom(const DevProblem& dp) {
     gg.qu = gr.qu;
     gg.qv = gr.qv;
     gg.vptr = gr.vptr;
+    gg.nA = gr.nA;
+    gg.colA = gr.colA;
+    gg.colD = gr.colD;
+    gg.colpos = gr.colpos;
     gg.vu = gr.vu;
     gg.vv = gr.vv;
     return gg;
@@ -849,7 +904,7 @@ struct PassPlan {
 // the alternative is the FP64 shared-memory engine (about 20x slower per
 // IRLS pass at p = 16 and 32 on the 20,000 x 100,000 continuous workload)
 bool tcw_wanted(const DevProblem& dp) {
-    if (!tcw_supported(dp.P, dp.xs) || !dp.tcw_fits) return false;
+    if (!tcw_supported(dp.P, dp.xs) || !tcw_fits(dp)) return false;
     const char* e = getenv("DEVIL_TCW");
     if (e && *e) return atoi(e) == 1;
     return dp.precision == DEVIL_PREC_TC_TF32 || dp.P > reg_max_p();
@@ -858,7 +913,7 @@ bool tcw_wanted(const DevProblem& dp) {
 // pass (the FP64 shared-memory pass it replaces from p = 9 on is about 13x
 // slower on the 20,000 x 100,000 continuous workload at p = 16 and 32)
 bool tcw_mle_wanted(const DevProblem& dp) {
-    if (!tcw_supported(dp.P, dp.xs) || !dp.tcw_fits) return false;
+    if (!tcw_supported(dp.P, dp.xs) || !tcw_fits(dp)) return false;
     const char* e = getenv("DEVIL_TCW_MLE");
     if (e && *e) return atoi(e) == 1;
     return dp.precision == DEVIL_PREC_TC_TF32 || dp.P > reg_max_p();

@@ -179,6 +179,14 @@ struct GrpGeom {
     const int32_t* vptr;   // [P + 1]
     const int32_t* vu;
     const double* vv;
+    // exclusive columns: no design row has two of them nonzero (one-hot
+    // cell types), so the p x p Hessian restricted to them is diagonal and
+    // a Newton step needs only the Schur complement on the nA other
+    // columns.  nA = 0: no such structure (dense solve).
+    int nA;
+    const int32_t* colA;   // [nA] the dense columns
+    const int32_t* colD;   // [P - nA] the exclusive columns
+    const int32_t* colpos; // [P] position in colA (>= 0) or -1 - position in colD
     const int32_t* act;
     const int32_t* n_act;
     int32_t* reset_next;

@@ -128,6 +128,61 @@ cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slo
 // p x p partial sums through global memory -- then the LU, the solve and the
 // update of irls_finalize_kernel.
 // ------------------------------------------------------------------
+// Newton step of the SPD system H x = s when the exclusive columns D
+// (geo.colD, m = P - nA of them) form a diagonal block of H:
+//   S = H_AA - H_AD diag(H_DD)^-1 H_DA        (Schur complement, nA x nA)
+//   S x_A = s_A - H_AD diag(H_DD)^-1 s_D,      x_D = diag(H_DD)^-1 (s_D - H_DA x_A)
+// Lane t < m handles exclusive column colD[t]; the sums over t are warp
+// sums in lane order.  Exact in exact arithmetic, like the LU of H (the
+// arrowhead H of a one-hot design costs O(p) instead of O(p^3)).  Returns
+// the step of column `lane` (lanes < P).
+DEV double schur_step(const GrpGeom& geo, const double* H, int LD, int P, double* Sm, int* perm, int* step,
+                      double s_own, int lane) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int k = geo.nA, m = P - k;
+    const int LDk = wla_ld(k);
+    const int c = lane < m ? __ldg(geo.colD + lane) : 0;
+    const double sc = __shfl_sync(FULL, s_own, c);
+    double r = 0.0, hA[8];
+    if (lane < m) r = 1.0 / H[c * LD + c];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) hA[a] = (a < k && lane < m) ? H[__ldg(geo.colA + a) * LD + c] : 0.0;
+    double rhs_own = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        if (a >= k) break;
+        const int ca = __ldg(geo.colA + a);
+        const double ta = warp_sum(lane < m ? hA[a] * sc * r : 0.0);
+        const double sa = __shfl_sync(FULL, s_own, ca);
+        if (lane == a) rhs_own = sa - ta;
+#pragma unroll
+        for (int b = 0; b <= a; ++b) {
+            const double tab = warp_sum(hA[a] * hA[b] * r);
+            if (lane == 0) {
+                const double v = H[ca * LD + __ldg(geo.colA + b)] - tab;
+                Sm[a * LDk + b] = v;
+                Sm[b * LDk + a] = v;
+            }
+        }
+    }
+    __syncwarp();
+    warp_lu(Sm, LDk, k, perm, step);
+    const double xa = warp_lu_solve(Sm, LDk, k, perm, step, rhs_own);  // lanes < k
+    double dot = 0.0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        if (a >= k) break;
+        dot += hA[a] * __shfl_sync(FULL, xa, a);
+    }
+    const double xd = (sc - dot) * r;  // lanes < m
+    const int pc = lane < P ? __ldg(geo.colpos + lane) : 0;
+    const double fromA = __shfl_sync(FULL, xa, pc >= 0 ? pc : 0);
+    const double fromD = __shfl_sync(FULL, xd, pc < 0 ? -1 - pc : 0);
+    return pc >= 0 ? fromA : fromD;
+}
+
+constexpr int kSchurScratch = 8 * wla_ld(8);  // doubles: the Schur complement of at most 8 dense columns
+
 __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t* n_next,
                                          double* beta, float* beta_f, int32_t* iters,
                                          int32_t* status, int max_iter, double eps,
@@ -135,10 +190,12 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
     extern __shared__ double fsh[];
     const int P = geo.P, U = geo.U, C = geo.C, S = geo.S, LD = wla_ld(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = 2 * U + P * LD + P;  // group sums, H, then perm and step (P ints each)
+    // group sums, H, the Schur scratch, then perm and step (P ints each)
+    const int per = 2 * U + P * LD + kSchurScratch + P;
     double* gs = fsh + warp * per;
     double* H = gs + 2 * U;
-    int* perm = reinterpret_cast<int*>(H + P * LD);
+    double* Sm = H + P * LD;
+    int* perm = reinterpret_cast<int*>(Sm + kSchurScratch);
     int* step = perm + P;
     const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
     if (slot >= *geo.n_act) return;
@@ -177,8 +234,13 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
         s_own = -k * s;
     }
     __syncwarp();
-    warp_lu(H, LD, P, perm, step);
-    const double x_own = warp_lu_solve(H, LD, P, perm, step, s_own);
+    double x_own;
+    if (geo.nA > 0) {
+        x_own = schur_step(geo, H, LD, P, Sm, perm, step, s_own, lane);
+    } else {
+        warp_lu(H, LD, P, perm, step);
+        x_own = warp_lu_solve(H, LD, P, perm, step, s_own);
+    }
     if (lane < P) {
         const double b = beta[(int64_t)g * P + lane] + x_own;
         beta[(int64_t)g * P + lane] = b;
@@ -207,7 +269,7 @@ cudaError_t launch_grp_irls_finalize(const GrpGeom& geo, int max_slots, int32_t*
                                      int32_t* status, int max_iter, double eps, const float* k,
                                      cudaStream_t st) {
     if (max_slots <= 0) return cudaSuccess;
-    const size_t per = (size_t)(2 * geo.U + geo.P * wla_ld(geo.P) + geo.P) * sizeof(double);
+    const size_t per = (size_t)(2 * geo.U + geo.P * wla_ld(geo.P) + kSchurScratch + geo.P) * sizeof(double);
     const int w = fin_warps(per);
     const size_t smem = per * w;
     if (smem > 48 * 1024) {
