@@ -1455,9 +1455,13 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
                     dp.fine_ptr, dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
         ++launched;
         const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC && plan.engine != ENGINE_TCW;
+        // the exclusive-column (one-hot) structure of a grouped design
+        // shortens the Cox-Reid terms
+        const bool structured = plan.engine == ENGINE_GRP && dp.grp.nA > 0;
         LAUNCH(launch_mle_finalize(pb.partW, part_f64, pb.partS, nseg, tiles * plan.GT, dp.P, dp.stats, dp.n,
                                    act[cur], cnt + cur, (int)hint, act[nxt], cnt + nxt, s, max_iter,
-                                   cox_reid, nullptr, st));
+                                   cox_reid, nullptr, st, structured ? dp.grp.nA : 0,
+                                   structured ? dp.grp.colA : nullptr, structured ? dp.grp.colD : nullptr));
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));

@@ -356,7 +356,8 @@ cudaError_t launch_mle_finalize(const void* partW, bool wide, const double* part
                                 int slot_stride, int P, const double* stats, int64_t n,
                                 const int32_t* act, const int32_t* n_act, int max_slots,
                                 int32_t* act_next, int32_t* n_next, MleState s, int max_iter,
-                                int cox_reid, volatile int32_t* mirror, cudaStream_t st);
+                                int cox_reid, volatile int32_t* mirror, cudaStream_t st, int nA = 0,
+                                const int32_t* colA = nullptr, const int32_t* colD = nullptr);
 cudaError_t launch_sandwich_finalize(const double* partW, int nseg, int slot_stride, int P,
                                      const int32_t* seg_cluster, int n_clusters, int64_t n,
                                      const int32_t* act, const int32_t* n_act, int max_slots,

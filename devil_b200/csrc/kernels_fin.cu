@@ -345,16 +345,139 @@ cudaError_t launch_mle_init(const double* stats, int64_t G, int64_t n, MleState 
     return cudaGetLastError();
 }
 
+// The Cox-Reid terms tr(B^-1 db), tr((B^-1 db)^2), tr(B^-1 d2b) (B = b + 1e-6 I)
+// when the exclusive columns D (colD, m of them) make b, db and d2b diagonal
+// on D x D.  With Q = B_AD, delta = diag(B_DD) and S = B_AA - Q delta^-1 Q^T
+// (the Schur complement on the nA dense columns A):
+//   B^-1 = Y + V S^-1 V^T,  Y = [0 0; 0 delta^-1],  V = [I; -delta^-1 Q^T],
+// so for E = db (e = diag(E_DD)):
+//   tr(B^-1 E)     = sum e/delta + tr(S^-1 G),            G = V^T E V
+//   tr((B^-1 E)^2) = sum (e/delta)^2 + 2 tr(S^-1 K) + tr((S^-1 G)^2),
+//                    K = sum_t w_t w_t^T / delta_t,  w_t = E_A,t - Q_t e_t / delta_t
+// and likewise tr(B^-1 d2b).  Lane t < m holds column colD[t]; the sums over
+// t are warp sums; the nA x nA algebra runs on lane 0.  O(p nA^2) per gene
+// instead of the O(p^3) factorisation, inverse and product.
+DEV void mle_cr_structured(const double* sums, int P, int NE, int k, const int32_t* colA,
+                           const int32_t* colD, double* Wk, double& ddetb, double& trmm, double& trbd2) {
+    const int lane = threadIdx.x & 31, m = P - k;
+    auto pk = [&](int base, int i, int j) { return i <= j ? sums[base + tri_index(i, j)] : sums[base + tri_index(j, i)]; };
+    const int c = lane < m ? __ldg(colD + lane) : 0;
+    double rd = 0.0, e = 0.0, e2 = 0.0;
+    double q[8], w1[8], w2[8];
+    if (lane < m) {
+        rd = 1.0 / (pk(0, c, c) + 1e-6);
+        e = pk(NE, c, c);
+        e2 = pk(2 * NE, c, c);
+    }
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        q[a] = w1[a] = w2[a] = 0.0;
+        if (a < k && lane < m) {
+            const int ca = __ldg(colA + a);
+            q[a] = pk(0, ca, c);
+            w1[a] = pk(NE, ca, c) - q[a] * e * rd;
+            w2[a] = pk(2 * NE, ca, c) - q[a] * e2 * rd;
+        }
+    }
+    const double se = warp_sum(e * rd), see = warp_sum(e * rd * e * rd), se2 = warp_sum(e2 * rd);
+    // k x k blocks on lane 0: S, G, K, G2, then two scratch blocks
+    const int kk = k * k;
+    double* Sm = Wk;
+    double* Gm = Wk + kk;
+    double* Km = Wk + 2 * kk;
+    double* G2 = Wk + 3 * kk;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        if (a >= k) break;
+        const int ca = __ldg(colA + a);
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            if (b >= k) break;
+            const int cb = __ldg(colA + b);
+            // V^T E V = E_AA - Q d^-1 E_DA - W1_D d^-1 Q^T with W1_D = E_AD - Q d^-1 diag(e)
+            const double qq = warp_sum(q[a] * q[b] * rd);
+            const double qe = warp_sum(q[a] * (w1[b] + q[b] * e * rd) * rd);
+            const double wq = warp_sum(w1[a] * q[b] * rd);
+            const double ww = warp_sum(w1[a] * w1[b] * rd);
+            const double qe2 = warp_sum(q[a] * (w2[b] + q[b] * e2 * rd) * rd);
+            const double w2q = warp_sum(w2[a] * q[b] * rd);
+            if (lane == 0) {
+                Sm[a * k + b] = pk(0, ca, cb) + (a == b ? 1e-6 : 0.0) - qq;
+                Gm[a * k + b] = pk(NE, ca, cb) - qe - wq;
+                Km[a * k + b] = ww;
+                G2[a * k + b] = pk(2 * NE, ca, cb) - qe2 - w2q;
+            }
+        }
+    }
+    __syncwarp();
+    if (lane != 0) return;
+    // S^-1 by Gauss-Jordan with partial pivoting (S is SPD), into Si
+    double* Si = Wk + 4 * kk;
+    double* T = Wk + 5 * kk;
+    for (int i = 0; i < kk; ++i) {
+        T[i] = Sm[i];
+        Si[i] = (i / k == i % k) ? 1.0 : 0.0;
+    }
+    for (int col = 0; col < k; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < k; ++r)
+            if (fabs(T[r * k + col]) > fabs(T[piv * k + col])) piv = r;
+        if (piv != col)
+            for (int j = 0; j < k; ++j) {
+                double t0 = T[col * k + j];
+                T[col * k + j] = T[piv * k + j];
+                T[piv * k + j] = t0;
+                t0 = Si[col * k + j];
+                Si[col * k + j] = Si[piv * k + j];
+                Si[piv * k + j] = t0;
+            }
+        const double inv = 1.0 / T[col * k + col];
+        for (int j = 0; j < k; ++j) {
+            T[col * k + j] *= inv;
+            Si[col * k + j] *= inv;
+        }
+        for (int r = 0; r < k; ++r) {
+            if (r == col) continue;
+            const double f = T[r * k + col];
+            for (int j = 0; j < k; ++j) {
+                T[r * k + j] -= f * T[col * k + j];
+                Si[r * k + j] -= f * Si[col * k + j];
+            }
+        }
+    }
+    // traces; T = S^-1 G
+    double t1 = 0.0, tk = 0.0, t2 = 0.0;
+    for (int a = 0; a < k; ++a)
+        for (int b = 0; b < k; ++b) {
+            t1 += Si[a * k + b] * Gm[b * k + a];
+            tk += Si[a * k + b] * Km[b * k + a];
+            t2 += Si[a * k + b] * G2[b * k + a];
+        }
+    for (int a = 0; a < k; ++a)
+        for (int b = 0; b < k; ++b) {
+            double v = 0.0;
+            for (int j = 0; j < k; ++j) v += Si[a * k + j] * Gm[j * k + b];
+            T[a * k + b] = v;
+        }
+    double tgg = 0.0;
+    for (int a = 0; a < k; ++a)
+        for (int b = 0; b < k; ++b) tgg += T[a * k + b] * T[b * k + a];
+    ddetb = se + t1;
+    trmm = see + 2.0 * tk + tgg;
+    trbd2 = se2 + t2;
+}
+
 template <class TW>
 __global__ void mle_finalize_kernel(const TW* partW, const double* partS, int nseg,
                                     int slot_stride, int P, const double* stats, int64_t n,
                                     const int32_t* act, const int32_t* n_act, int32_t* act_next,
-                                    int32_t* n_next, MleState st, int max_iter, int cox_reid) {
+                                    int32_t* n_next, MleState st, int max_iter, int cox_reid,
+                                    int nA, const int32_t* colA, const int32_t* colD) {
     extern __shared__ double fsh[];
     const int NE = P * (P + 1) / 2, NA = 3 * NE + 2;  // b, db, d2b, two FP32 scalars
     const int LD = wla_ld(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = NA + 6 + 4 * P * LD + P;
+    const int per = NA + 6 + (nA > 0 ? 6 * nA * nA : 4 * P * LD) + P;
     double* sums = fsh + warp * per;
     double* ss = sums + NA;
     double* B = ss + 6;
@@ -370,7 +493,14 @@ __global__ void mle_finalize_kernel(const TW* partW, const double* partS, int ns
     __syncwarp();
     // Cox-Reid terms (warp-parallel): B = b + 1e-6 I (inv_sympd), M = B^-1 db
     double cr_s = 0.0, cr_d = 0.0, cr_d2 = 0.0;
-    if (cox_reid) {
+    if (cox_reid && nA > 0) {
+        double ddetb = 0.0, trmm = 0.0, trbd2 = 0.0;
+        mle_cr_structured(sums, P, NE, nA, colA, colD, B, ddetb, trmm, trbd2);
+        const double d2detb = ddetb * ddetb - trmm + trbd2;
+        cr_s = -0.5 * ddetb * kCrFactor;
+        cr_d = (0.5 * ddetb * ddetb - 0.5 * d2detb) * kCrFactor;
+        cr_d2 = -0.5 * ddetb * kCrFactor;
+    } else if (cox_reid) {
         warp_unpack_sym(P, sums, 1.0, 1e-6, B, LD);
         warp_lu(B, LD, P, perm);
         warp_lu_inverse(B, LD, P, perm, Bi, LD);
@@ -485,11 +615,12 @@ cudaError_t launch_mle_finalize(const void* partW, bool wide, const double* part
                                 int slot_stride, int P, const double* stats, int64_t n,
                                 const int32_t* act, const int32_t* n_act, int max_slots,
                                 int32_t* act_next, int32_t* n_next, MleState s, int max_iter,
-                                int cox_reid, volatile int32_t* mirror, cudaStream_t st) {
+                                int cox_reid, volatile int32_t* mirror, cudaStream_t st, int nA,
+                                const int32_t* colA, const int32_t* colD) {
     (void)mirror;
     if (max_slots <= 0) return cudaSuccess;
     const int NA = 3 * (P * (P + 1) / 2) + 2;
-    const size_t per = (size_t)(NA + 6 + 4 * P * wla_ld(P) + P) * sizeof(double);
+    const size_t per = (size_t)(NA + 6 + (nA > 0 ? 6 * nA * nA : 4 * P * wla_ld(P)) + P) * sizeof(double);
     const int w = fin_warps(per);
     const size_t smem = per * w;
     auto go = [&](auto* pw) -> cudaError_t {
@@ -500,7 +631,7 @@ cudaError_t launch_mle_finalize(const void* partW, bool wide, const double* part
         }
         mle_finalize_kernel<TW><<<nblk(max_slots, w), 32 * w, smem, st>>>(
             pw, partS, nseg, slot_stride, P, stats, n, act, n_act, act_next, n_next, s, max_iter,
-            cox_reid);
+            cox_reid, nA, colA, colD);
         return cudaGetLastError();
     };
     return wide ? go(static_cast<const double*>(partW)) : go(static_cast<const float*>(partW));
