@@ -410,7 +410,18 @@ __global__ void seg_hist_kernel(const int64_t* rowptr, const int32_t* col, int64
     const int64_t g = seg_gene(segbase, G, s);
     const int64_t r0 = rowptr[g] + (s - segbase[g]) * S;
     const int64_t r1 = min(r0 + S, rowptr[g + 1]);
-    for (int64_t e = r0 + lane; e < r1; e += 32) atomicAdd(&cnt[ckey[col[e]]], 1);
+    constexpr int U = 4;  // loads in flight per lane
+    for (int64_t base = r0 + lane; base < r1; base += 32 * U) {
+        int c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) c[u] = base + 32 * u < r1 ? __ldg(col + base + 32 * u) : -1;
+        int k[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) k[u] = c[u] >= 0 ? __ldg(ckey + c[u]) : -1;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k[u] >= 0) atomicAdd(&cnt[k[u]], 1);
+    }
     __syncwarp();
     int32_t* h = hist + s * K;
     for (int k = lane; k < K; k += 32) h[k] = cnt[k];
@@ -463,26 +474,37 @@ __global__ void seg_scatter_kernel(const int64_t* rowptr, const int32_t* col, co
     const int64_t r0 = rs + (s - segbase[g]) * S;
     const int64_t r1 = min(r0 + S, rowptr[g + 1]);
     const unsigned lt = (1u << lane) - 1u;
-    for (int64_t base = r0; base < r1; base += 32) {
-        const int64_t e = base + lane;
-        const bool valid = e < r1;
-        int c = 0;
-        VT v = VT(0);
-        int k = -1;
-        if (valid) {
-            c = col[e];
-            v = val[e];
-            k = ckey[c];
+    // U rounds of 32 entries: every load and key lookup of the rounds is
+    // issued first, then the rounds are placed in order (the same positions
+    // as one round at a time)
+    constexpr int U = 4;
+    for (int64_t base = r0; base < r1; base += 32 * U) {
+        int c[U], k[U], lc[U];
+        VT v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t e = base + 32 * u + lane;
+            c[u] = e < r1 ? __ldg(col + e) : -1;
+            v[u] = e < r1 ? val[e] : VT(0);
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, k);
-        const int rank = __popc(peers & lt);
-        const int pos = valid ? cur[k] + rank : 0;
-        __syncwarp();
-        if (valid) {
-            gent[rs + pos] = GrpEnt<VT>::pack(cloc[c], v);
-            if (lane == __ffs(peers) - 1) cur[k] += __popc(peers);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            k[u] = c[u] >= 0 ? __ldg(ckey + c[u]) : -1;
+            lc[u] = c[u] >= 0 ? __ldg(cloc + c[u]) : 0;
         }
-        __syncwarp();
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const bool valid = c[u] >= 0;
+            const unsigned peers = __match_any_sync(0xffffffffu, k[u]);
+            const int rank = __popc(peers & lt);
+            const int pos = valid ? cur[k[u]] + rank : 0;
+            __syncwarp();
+            if (valid) {
+                gent[rs + pos] = GrpEnt<VT>::pack(lc[u], v[u]);
+                if (lane == __ffs(peers) - 1) cur[k[u]] += __popc(peers);
+            }
+            __syncwarp();
+        }
     }
 }
 
