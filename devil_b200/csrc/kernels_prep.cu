@@ -170,73 +170,41 @@ cudaError_t launch_x_rowmajor_d(const double* Xcm, int64_t n, int P, int xs, dou
 // stats[g*6 + 0..5] = mean, sample variance (n-1), sum y,
 //                     sum (y-1) y, max y, nnz
 // ------------------------------------------------------------------
-// uint16 counts: one pass with exact integer sums (sum y, sum y^2 < 2^64 for
-// any int32 cell count), the variance from the exact numerator
-// n sum y^2 - (sum y)^2 (128-bit); four loads in flight per lane
-__global__ void gene_stats_u16_kernel(const int64_t* rowptr, const uint16_t* val, int64_t G, int64_t n,
-                                      double* stats) {
-    int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    int lane = threadIdx.x & 31;
-    if (g >= G) return;
-    const int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
-    unsigned long long s1 = 0, s2 = 0;
-    unsigned mx = 0;
-    constexpr int U = 4;
-    for (int64_t base = e0 + lane; base < e1; base += 32 * U) {
-        unsigned y[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int64_t e = base + 32 * u;
-            y[u] = e < e1 ? (unsigned)__ldg(val + e) : 0u;
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            s1 += y[u];
-            s2 += (unsigned long long)y[u] * y[u];
-            mx = max(mx, y[u]);
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    }
-    if (lane == 0) {
-        const double mean = (double)s1 / (double)n;
-        const __int128 num = (__int128)n * (__int128)s2 - (__int128)s1 * (__int128)s1;
-        double* o = stats + g * 6;
-        o[0] = mean;
-        o[1] = (double)num / ((double)n * (double)(n - 1));
-        o[2] = (double)s1;
-        o[3] = (double)(s2 - s1);
-        o[4] = (double)mx;
-        o[5] = (double)(e1 - e0);
-    }
-}
-
 template <class VT>
 __global__ void gene_stats_kernel(const int64_t* rowptr, const VT* val, int64_t G, int64_t n,
                                   double* stats) {
     int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (g >= G) return;
-    int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
+    const int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
+    // two passes (mean, then squared deviations), four loads in flight per
+    // lane; the same order for every count type, so uint16 and float copies
+    // of the same counts give the same statistics
+    constexpr int U = 4;
     double s = 0.0, sp = 0.0, mx = 0.0;
-    for (int64_t e = e0 + lane; e < e1; e += 32) {
-        double y = (double)val[e];
-        s += y;
-        sp += (y - 1.0) * y;
-        mx = fmax(mx, y);
+    for (int64_t base = e0 + lane; base < e1; base += 32 * U) {
+        double y[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) y[u] = base + 32 * u < e1 ? (double)__ldg(val + base + 32 * u) : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            s += y[u];
+            sp += (y[u] - 1.0) * y[u];
+            mx = fmax(mx, y[u]);
+        }
     }
     s = warp_sum(s);
     sp = warp_sum(sp);
     mx = warp_max(mx);
     double mean = s / (double)n;
     double ss = 0.0;
-    for (int64_t e = e0 + lane; e < e1; e += 32) {
-        double d = (double)val[e] - mean;
-        ss += d * d;
+    for (int64_t base = e0 + lane; base < e1; base += 32 * U) {
+        double d[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            d[u] = base + 32 * u < e1 ? (double)__ldg(val + base + 32 * u) - mean : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) ss += d[u] * d[u];
     }
     ss = warp_sum(ss);
     if (lane == 0) {
@@ -254,7 +222,7 @@ cudaError_t launch_gene_stats(const int64_t* rowptr, const void* val, int val_u1
                               int64_t n, double* stats, cudaStream_t st) {
     if (G == 0) return cudaSuccess;
     if (val_u16)
-        gene_stats_u16_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, (const uint16_t*)val, G, n, stats);
+        gene_stats_kernel<uint16_t><<<nblk(G, 8), 256, 0, st>>>(rowptr, (const uint16_t*)val, G, n, stats);
     else
         gene_stats_kernel<float><<<nblk(G, 8), 256, 0, st>>>(rowptr, (const float*)val, G, n, stats);
     return cudaGetLastError();
@@ -630,29 +598,10 @@ __global__ void validate_csr_kernel(const int64_t* rowptr, const int32_t* col, i
     if (e0 < 0 || e1 < e0 || e1 > nnz) {
         b = 1;
     } else {
-        // four loads in flight per lane; each entry is compared with the one
-        // before it (from the neighbouring lane, or the previous round)
-        constexpr int U = 4;
-        int carry = -1;  // the last index of the previous round
-        for (int64_t base = e0; base < e1; base += 32 * U) {
-            int c[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int64_t e = base + 32 * u + lane;
-                c[u] = e < e1 ? __ldg(col + e) : 0;
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int64_t e = base + 32 * u + lane;
-                const int up = __shfl_up_sync(0xffffffffu, c[u], 1);
-                const int last = __shfl_sync(0xffffffffu, c[u], 31);
-                const int prev = lane > 0 ? up : carry;
-                if (e < e1) {
-                    if (c[u] < 0 || c[u] >= n) b = 1;
-                    if (e > e0 && prev >= c[u]) b = 1;
-                }
-                carry = last;
-            }
+        for (int64_t e = e0 + lane; e < e1; e += 32) {
+            int c = col[e];
+            if (c < 0 || c >= n) b = 1;
+            if (e > e0 && col[e - 1] >= c) b = 1;
         }
     }
     b = __any_sync(0xffffffffu, b);
