@@ -4,6 +4,8 @@
 // and the CSR offsets of every cell segment.
 #include "internal.h"
 
+#include <type_traits>
+
 namespace devil {
 
 static inline unsigned nblk(int64_t m, int t) { return (unsigned)((m + t - 1) / t); }
@@ -177,39 +179,70 @@ __global__ void gene_stats_kernel(const int64_t* rowptr, const VT* val, int64_t 
     int lane = threadIdx.x & 31;
     if (g >= G) return;
     const int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
-    // two passes (mean, then squared deviations), four loads in flight per
-    // lane; the same order for every count type, so uint16 and float copies
-    // of the same counts give the same statistics
-    constexpr int U = 4;
-    double s = 0.0, sp = 0.0, mx = 0.0;
-    for (int64_t base = e0 + lane; base < e1; base += 32 * U) {
-        double y[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) y[u] = base + 32 * u < e1 ? (double)__ldg(val + base + 32 * u) : 0.0;
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            s += y[u];
-            sp += (y[u] - 1.0) * y[u];
-            mx = fmax(mx, y[u]);
+    // Counts that are whole numbers (always for uint16; checked for float):
+    // one pass with exact integer sums of y and y^2 (below 2^64 for any int32
+    // cell count and counts below 2^16) and the variance from the exact
+    // numerator n sum y^2 - (sum y)^2 in 128 bits, so a uint16 and a float
+    // copy of the same counts give the same statistics.  Other float counts:
+    // a second pass over the squared deviations in FP64.
+    unsigned long long s1 = 0, s2 = 0;
+    double s = 0.0, mx = 0.0;
+    bool whole = true;
+    for (int64_t e = e0 + lane; e < e1; e += 32) {
+        const double y = (double)val[e];
+        s += y;
+        mx = fmax(mx, y);
+        if constexpr (std::is_same<VT, uint16_t>::value) {
+            const unsigned long long v = (unsigned long long)val[e];
+            s1 += v;
+            s2 += v * v;
+        } else {
+            const bool w = y >= 0.0 && y < 65536.0 && y == floor(y);
+            whole = whole && w;
+            if (w) {
+                const unsigned long long v = (unsigned long long)y;
+                s1 += v;
+                s2 += v * v;
+            }
         }
+    }
+    whole = __all_sync(0xffffffffu, whole);
+    double* o = stats + g * 6;
+    if (whole) {
+#pragma unroll
+        for (int sh = 16; sh > 0; sh >>= 1) {
+            s1 += __shfl_xor_sync(0xffffffffu, s1, sh);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, sh);
+        }
+        mx = warp_max(mx);
+        if (lane == 0) {
+            const __int128 num = (__int128)n * (__int128)s2 - (__int128)s1 * (__int128)s1;
+            o[0] = (double)s1 / (double)n;
+            o[1] = (double)num / ((double)n * (double)(n - 1));
+            o[2] = (double)s1;
+            o[3] = (double)(s2 - s1);
+            o[4] = mx;
+            o[5] = (double)(e1 - e0);
+        }
+        return;
+    }
+    double sp = 0.0;
+    for (int64_t e = e0 + lane; e < e1; e += 32) {
+        const double y = (double)val[e];
+        sp += (y - 1.0) * y;
     }
     s = warp_sum(s);
     sp = warp_sum(sp);
     mx = warp_max(mx);
-    double mean = s / (double)n;
+    const double mean = s / (double)n;
     double ss = 0.0;
-    for (int64_t base = e0 + lane; base < e1; base += 32 * U) {
-        double d[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-            d[u] = base + 32 * u < e1 ? (double)__ldg(val + base + 32 * u) - mean : 0.0;
-#pragma unroll
-        for (int u = 0; u < U; ++u) ss += d[u] * d[u];
+    for (int64_t e = e0 + lane; e < e1; e += 32) {
+        const double d = (double)val[e] - mean;
+        ss += d * d;
     }
     ss = warp_sum(ss);
     if (lane == 0) {
         ss += (double)(n - (e1 - e0)) * mean * mean;
-        double* o = stats + g * 6;
         o[0] = mean;
         o[1] = ss / (double)(n - 1);
         o[2] = s;
