@@ -188,21 +188,28 @@ __global__ void gene_stats_kernel(const int64_t* rowptr, const VT* val, int64_t 
     unsigned long long s1 = 0, s2 = 0;
     double s = 0.0, mx = 0.0;
     bool whole = true;
-    for (int64_t e = e0 + lane; e < e1; e += 32) {
-        const double y = (double)val[e];
-        s += y;
-        mx = fmax(mx, y);
-        if constexpr (std::is_same<VT, uint16_t>::value) {
-            const unsigned long long v = (unsigned long long)val[e];
-            s1 += v;
-            s2 += v * v;
-        } else {
-            const bool w = y >= 0.0 && y < 65536.0 && y == floor(y);
-            whole = whole && w;
-            if (w) {
-                const unsigned long long v = (unsigned long long)y;
+    constexpr int U = 4;  // loads in flight per lane
+    for (int64_t base = e0 + lane; base < e1; base += 32 * U) {
+        VT raw[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) raw[u] = base + 32 * u < e1 ? __ldg(val + base + 32 * u) : VT(0);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const double y = (double)raw[u];
+            s += y;
+            mx = fmax(mx, y);
+            if constexpr (std::is_same<VT, uint16_t>::value) {
+                const unsigned long long v = (unsigned long long)raw[u];
                 s1 += v;
                 s2 += v * v;
+            } else {
+                const bool w = y >= 0.0 && y < 65536.0 && y == floor(y);
+                whole = whole && w;
+                if (w) {
+                    const unsigned long long v = (unsigned long long)y;
+                    s1 += v;
+                    s2 += v * v;
+                }
             }
         }
     }
@@ -268,6 +275,25 @@ cudaError_t launch_gene_stats(const int64_t* rowptr, const void* val, int val_u1
 template <class VT>
 __global__ void colstats_kernel(const int32_t* col, const VT* val, int64_t nnz, double* colsum,
                                 double* collog, int32_t* colcnt, int32_t* colmin_bits) {
+    if (!collog) {
+        // normed_sum: column sums only; four entries' loads in flight per thread
+        constexpr int U = 4;
+        const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+        for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < nnz; e0 += stride * U) {
+            int c[U];
+            float v[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int64_t e = e0 + stride * u;
+                c[u] = e < nnz ? __ldg(col + e) : -1;
+                v[u] = e < nnz ? (float)val[e] : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                if (c[u] >= 0) atomicAdd(colsum + c[u], (double)v[u]);
+        }
+        return;
+    }
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
          e += (int64_t)gridDim.x * blockDim.x) {
         int c = col[e];
