@@ -852,7 +852,9 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
             // underflowing exp(x_u beta)) takes the direct form.
             if (A > 1e-200) {
                 const double iA = 1.0 / A, kA = (double)gpar.k * iA;
-                double sy = 0.0;
+                double sy4[EPL];  // one chain per entry of a group: independent adds
+#pragma unroll
+                for (int r = 0; r < EPL; ++r) sy4[r] = 0.0;
                 for (int base = lane; base < nb; base += 32 * UNR) {
                     uint4 v[UNR];
 #pragma unroll
@@ -866,16 +868,19 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
                             if (ea >= e0 && ea + EPL <= e1) {
 #pragma unroll
                                 for (int r = 0; r < EPL; ++r)
-                                    sy += (double)Ent::y(c[r]) * rcp_r(Es[Ent::loc(c[r])] + kA);
+                                    sy4[r] += (double)Ent::y(c[r]) * rcp_r(Es[Ent::loc(c[r])] + kA);
                             } else {
 #pragma unroll
                                 for (int r = 0; r < EPL; ++r)
                                     if (ea + r >= e0 && ea + r < e1)
-                                        sy += (double)Ent::y(c[r]) * rcp_r(Es[Ent::loc(c[r])] + kA);
+                                        sy4[r] += (double)Ent::y(c[r]) * rcp_r(Es[Ent::loc(c[r])] + kA);
                             }
                         }
                     }
                 }
+                double sy = 0.0;
+#pragma unroll
+                for (int r = 0; r < EPL; ++r) sy += sy4[r];
                 acc.w[0] += (double)gpar.rk * iA * sy;
                 acc.w[1] -= iA * sy;
                 goto slice_done;
