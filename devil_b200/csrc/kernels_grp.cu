@@ -843,49 +843,6 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
         constexpr int UNR = NS > 0 ? 2 : kSlUnr;  // the MLE's accumulators need the registers
         const int64_t b0 = e0 / EPL;
         const int nb = (int)((e1 + EPL - 1) / EPL - b0);
-        if constexpr (std::is_same<Pass, PassIRLS>::value) {
-            // Both IRLS sums of a nonzero are multiples of y r = y / (A E + k)
-            // (PassIRLS::sparse: rk y r to the Hessian weight, -y r to the
-            // score), so one sum S = sum y / (E + k / A) is accumulated and
-            // folded in with the factors rk / A and -1 / A: three FP64
-            // operations per entry instead of seven.  A below 1e-200 (an
-            // underflowing exp(x_u beta)) takes the direct form.
-            if (A > 1e-200) {
-                const double iA = 1.0 / A, kA = (double)gpar.k * iA;
-                double sy4[EPL];  // one chain per entry of a group: independent adds
-#pragma unroll
-                for (int r = 0; r < EPL; ++r) sy4[r] = 0.0;
-                for (int base = lane; base < nb; base += 32 * UNR) {
-                    uint4 v[UNR];
-#pragma unroll
-                    for (int q = 0; q < UNR; ++q)
-                        if (base + 32 * q < nb) v[q] = ld_stream(v4 + b0 + base + 32 * q);
-#pragma unroll
-                    for (int q = 0; q < UNR; ++q) {
-                        const int64_t ea = (b0 + base + 32 * q) * EPL;
-                        if (base + 32 * q < nb) {
-                            const ET* c = reinterpret_cast<const ET*>(&v[q]);
-                            if (ea >= e0 && ea + EPL <= e1) {
-#pragma unroll
-                                for (int r = 0; r < EPL; ++r)
-                                    sy4[r] += (double)Ent::y(c[r]) * rcp_r(Es[Ent::loc(c[r])] + kA);
-                            } else {
-#pragma unroll
-                                for (int r = 0; r < EPL; ++r)
-                                    if (ea + r >= e0 && ea + r < e1)
-                                        sy4[r] += (double)Ent::y(c[r]) * rcp_r(Es[Ent::loc(c[r])] + kA);
-                            }
-                        }
-                    }
-                }
-                double sy = 0.0;
-#pragma unroll
-                for (int r = 0; r < EPL; ++r) sy += sy4[r];
-                acc.w[0] += (double)gpar.rk * iA * sy;
-                acc.w[1] -= iA * sy;
-                goto slice_done;
-            }
-        }
         for (int base = lane; base < nb; base += 32 * UNR) {
             uint4 v[UNR];
 #pragma unroll
@@ -909,7 +866,6 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
                 }
             }
         }
-    slice_done:
         double* o = geo.gsum + ((int64_t)jj * S + s) * NQ;
 #pragma unroll
         for (int i = 0; i < NWV; ++i) {
