@@ -214,9 +214,16 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
     const double k2 = k * k;
     const int NE = P * (P + 1) / 2;
     for (int a = lane; a < NE; a += 32) {
-        double s = 0.0;
-        for (int e = __ldg(geo.qptr + a); e < __ldg(geo.qptr + a + 1); ++e)
-            s += gs[__ldg(geo.qu + e) * 2] * __ldg(geo.qv + e);
+        // four partial sums: the intercept's lists run over every group
+        const int q0 = __ldg(geo.qptr + a), q1 = __ldg(geo.qptr + a + 1);
+        double s4[4] = {0.0, 0.0, 0.0, 0.0};
+        int e = q0;
+        for (; e + 4 <= q1; e += 4) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) s4[r] += gs[__ldg(geo.qu + e + r) * 2] * __ldg(geo.qv + e + r);
+        }
+        for (; e < q1; ++e) s4[0] += gs[__ldg(geo.qu + e) * 2] * __ldg(geo.qv + e);
+        const double s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
         // packed upper-triangle index a = j (j + 1) / 2 + i, i <= j
         int j = (int)((sqrtf(8.f * (float)a + 1.f) - 1.f) * 0.5f);
         while (j * (j + 1) / 2 > a) --j;
@@ -228,10 +235,15 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
     }
     double s_own = 0.0;
     if (lane < P) {
-        double s = 0.0;
-        for (int e = __ldg(geo.vptr + lane); e < __ldg(geo.vptr + lane + 1); ++e)
-            s += gs[__ldg(geo.vu + e) * 2 + 1] * __ldg(geo.vv + e);
-        s_own = -k * s;
+        const int v0 = __ldg(geo.vptr + lane), v1 = __ldg(geo.vptr + lane + 1);
+        double s4[4] = {0.0, 0.0, 0.0, 0.0};
+        int e = v0;
+        for (; e + 4 <= v1; e += 4) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) s4[r] += gs[__ldg(geo.vu + e + r) * 2 + 1] * __ldg(geo.vv + e + r);
+        }
+        for (; e < v1; ++e) s4[0] += gs[__ldg(geo.vu + e) * 2 + 1] * __ldg(geo.vv + e);
+        s_own = -k * ((s4[0] + s4[1]) + (s4[2] + s4[3]));
     }
     __syncwarp();
     double x_own;
