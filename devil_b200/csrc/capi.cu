@@ -282,6 +282,8 @@ struct DevProblem {
                 *vu = nullptr;
         int nA = 0;  // exclusive-column structure (GrpGeom)
         int32_t *colA = nullptr, *colD = nullptr, *colpos = nullptr;
+        int n_need = 0;
+        int32_t *need_q = nullptr, *need_d = nullptr;
         double *rval = nullptr, *qv = nullptr, *vv = nullptr;
     } grp;
 };
@@ -808,6 +810,24 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
         }
         if (colD.size() < 4 || colA.size() > 8 || colA.empty()) colA.clear();
     }
+    // the Hessian entries the Schur step reads: for every packed output
+    // (i <= j) with i or j dense, or i == j, its places in the compact store
+    // (rows of the dense columns [nA][P], then the diagonal [P])
+    std::vector<int32_t> need_q, need_d;
+    if (!colA.empty()) {
+        const int k = (int)colA.size();
+        for (int j = 0; j < P; ++j)
+            for (int i = 0; i <= j; ++i) {
+                const int pi = colpos[i], pj = colpos[j];
+                int d[3] = {-1, -1, -1}, nd = 0;
+                if (pi >= 0) d[nd++] = pi * P + j;
+                if (pj >= 0 && i != j) d[nd++] = pj * P + i;
+                if (i == j) d[nd++] = k * P + i;
+                if (nd == 0) continue;
+                need_q.push_back(j * (j + 1) / 2 + i);
+                for (int t = 0; t < 3; ++t) need_d.push_back(d[t]);
+            }
+    }
     auto up_i = [&](const char* nm, const std::vector<int32_t>& v) {
         int32_t* d = ws<int32_t>(ctx, nm, std::max<size_t>(v.size(), 1));
         h2d(ctx, d, v.data(), v.size());
@@ -833,6 +853,9 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
         g.colA = up_i("grp_colA", colA);
         g.colD = up_i("grp_colD", colD);
         g.colpos = up_i("grp_colpos", colpos);
+        g.n_need = (int)need_q.size();
+        g.need_q = up_i("grp_need_q", need_q);
+        g.need_d = up_i("grp_need_d", need_d);
     }
     g.res = res;
     CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
@@ -881,6 +904,9 @@ GrpGeom grp_geom(const DevProblem& dp) {
     gg.colA = gr.colA;
     gg.colD = gr.colD;
     gg.colpos = gr.colpos;
+    gg.n_need = gr.n_need;
+    gg.need_q = gr.need_q;
+    gg.need_d = gr.need_d;
     gg.vu = gr.vu;
     gg.vv = gr.vv;
     return gg;

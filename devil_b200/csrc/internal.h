@@ -187,6 +187,12 @@ struct GrpGeom {
     const int32_t* colA;   // [nA] the dense columns
     const int32_t* colD;   // [P - nA] the exclusive columns
     const int32_t* colpos; // [P] position in colA (>= 0) or -1 - position in colD
+    // the Hessian entries that step needs (rows of the dense columns and the
+    // diagonal): packed output index and up to three destinations in the
+    // compact store [nA][P] rows then [P] diagonal (-1: none)
+    int n_need;
+    const int32_t* need_q;
+    const int32_t* need_d;  // [n_need][3]
     const int32_t* act;
     const int32_t* n_act;
     int32_t* reset_next;

@@ -136,30 +136,32 @@ cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slo
 // sums in lane order.  Exact in exact arithmetic, like the LU of H (the
 // arrowhead H of a one-hot design costs O(p) instead of O(p^3)).  Returns
 // the step of column `lane` (lanes < P).
-DEV double schur_step(const GrpGeom& geo, const double* H, int LD, int P, double* Sm, int* perm, int* step,
-                      double s_own, int lane) {
+// HA: the rows of the dense columns ([nA][P]), Hd: the diagonal ([P])
+DEV double schur_step(const GrpGeom& geo, const double* HA, const double* Hd, int P, double* Sm, int* perm,
+                      int* step, double s_own, int lane) {
     constexpr unsigned FULL = 0xffffffffu;
     const int k = geo.nA, m = P - k;
     const int LDk = wla_ld(k);
     const int c = lane < m ? __ldg(geo.colD + lane) : 0;
     const double sc = __shfl_sync(FULL, s_own, c);
     double r = 0.0, hA[8];
-    if (lane < m) r = 1.0 / H[c * LD + c];
+    if (lane < m) r = 1.0 / Hd[c];
 #pragma unroll
-    for (int a = 0; a < 8; ++a) hA[a] = (a < k && lane < m) ? H[__ldg(geo.colA + a) * LD + c] : 0.0;
+    for (int a = 0; a < 8; ++a) hA[a] = (a < k && lane < m) ? HA[a * P + c] : 0.0;
     double rhs_own = 0.0;
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
         if (a >= k) break;
         const int ca = __ldg(geo.colA + a);
         const double ta = warp_sum(lane < m ? hA[a] * sc * r : 0.0);
+        (void)ca;
         const double sa = __shfl_sync(FULL, s_own, ca);
         if (lane == a) rhs_own = sa - ta;
 #pragma unroll
         for (int b = 0; b <= a; ++b) {
             const double tab = warp_sum(hA[a] * hA[b] * r);
             if (lane == 0) {
-                const double v = H[ca * LD + __ldg(geo.colA + b)] - tab;
+                const double v = HA[a * P + __ldg(geo.colA + b)] - tab;
                 Sm[a * LDk + b] = v;
                 Sm[b * LDk + a] = v;
             }
@@ -190,12 +192,15 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
     extern __shared__ double fsh[];
     const int P = geo.P, U = geo.U, C = geo.C, S = geo.S, LD = wla_ld(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // group sums, H, the Schur scratch, then perm and step (P ints each)
-    const int per = 2 * U + P * LD + kSchurScratch + P;
+    // group sums, then H (P x LD) for the LU step, or the compact store of
+    // the Schur step (rows of the dense columns, the diagonal) and its
+    // scratch; then perm and step (P ints each)
+    const int k_a = geo.nA;
+    const int per = k_a > 0 ? 2 * U + k_a * P + P + kSchurScratch + P : 2 * U + P * LD + P;
     double* gs = fsh + warp * per;
     double* H = gs + 2 * U;
-    double* Sm = H + P * LD;
-    int* perm = reinterpret_cast<int*>(Sm + kSchurScratch);
+    double* Sm = H + (k_a > 0 ? k_a * P + P : P * LD);
+    int* perm = reinterpret_cast<int*>(k_a > 0 ? Sm + kSchurScratch : H + P * LD);
     int* step = perm + P;
     const int slot = blockIdx.x * (blockDim.x >> 5) + warp;
     if (slot >= *geo.n_act) return;
@@ -213,7 +218,9 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
     const double k = (double)kf[g];
     const double k2 = k * k;
     const int NE = P * (P + 1) / 2;
-    for (int a = lane; a < NE; a += 32) {
+    const int nout = k_a > 0 ? geo.n_need : NE;
+    for (int o = lane; o < nout; o += 32) {
+        const int a = k_a > 0 ? __ldg(geo.need_q + o) : o;
         // four partial sums: the intercept's lists run over every group
         const int q0 = __ldg(geo.qptr + a), q1 = __ldg(geo.qptr + a + 1);
         double s4[4] = {0.0, 0.0, 0.0, 0.0};
@@ -224,14 +231,22 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
         }
         for (; e < q1; ++e) s4[0] += gs[__ldg(geo.qu + e) * 2] * __ldg(geo.qv + e);
         const double s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
-        // packed upper-triangle index a = j (j + 1) / 2 + i, i <= j
-        int j = (int)((sqrtf(8.f * (float)a + 1.f) - 1.f) * 0.5f);
-        while (j * (j + 1) / 2 > a) --j;
-        while ((j + 1) * (j + 2) / 2 <= a) ++j;
-        const int i = a - j * (j + 1) / 2;
         const double v = s * k2;
-        H[i * LD + j] = v;
-        H[j * LD + i] = v;
+        if (k_a > 0) {
+#pragma unroll
+            for (int t = 0; t < 3; ++t) {
+                const int d = __ldg(geo.need_d + 3 * o + t);
+                if (d >= 0) H[d] = v;
+            }
+        } else {
+            // packed upper-triangle index a = j (j + 1) / 2 + i, i <= j
+            int j = (int)((sqrtf(8.f * (float)a + 1.f) - 1.f) * 0.5f);
+            while (j * (j + 1) / 2 > a) --j;
+            while ((j + 1) * (j + 2) / 2 <= a) ++j;
+            const int i = a - j * (j + 1) / 2;
+            H[i * LD + j] = v;
+            H[j * LD + i] = v;
+        }
     }
     double s_own = 0.0;
     if (lane < P) {
@@ -248,7 +263,7 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
     __syncwarp();
     double x_own;
     if (geo.nA > 0) {
-        x_own = schur_step(geo, H, LD, P, Sm, perm, step, s_own, lane);
+        x_own = schur_step(geo, H, H + k_a * P, P, Sm, perm, step, s_own, lane);
     } else {
         warp_lu(H, LD, P, perm, step);
         x_own = warp_lu_solve(H, LD, P, perm, step, s_own);
@@ -281,7 +296,10 @@ cudaError_t launch_grp_irls_finalize(const GrpGeom& geo, int max_slots, int32_t*
                                      int32_t* status, int max_iter, double eps, const float* k,
                                      cudaStream_t st) {
     if (max_slots <= 0) return cudaSuccess;
-    const size_t per = (size_t)(2 * geo.U + geo.P * wla_ld(geo.P) + kSchurScratch + geo.P) * sizeof(double);
+    const int P = geo.P, na = geo.nA;
+    const size_t per =
+        (size_t)(na > 0 ? 2 * geo.U + na * P + P + kSchurScratch + P : 2 * geo.U + P * wla_ld(P) + P) *
+        sizeof(double);
     const int w = fin_warps(per);
     const size_t smem = per * w;
     if (smem > 48 * 1024) {
