@@ -764,8 +764,11 @@ DEV uint4 ld_stream(const uint4* p) {
     return v;
 }
 
+template <class Pass>
+constexpr int sl_min_blocks() { return std::is_same<Pass, PassIRLS>::value ? 1 : 2; }
+
 template <class Pass, class VT>
-__global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typename Pass::Params prm,
+__global__ void __launch_bounds__(kSlNT, sl_min_blocks<Pass>()) grp_slices_kernel(GrpGeom geo, typename Pass::Params prm,
                                                               int tile) {
     using Ent = GrpEnt<VT>;
     using ET = typename Ent::T;
@@ -843,22 +846,6 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
         constexpr int UNR = NS > 0 ? 2 : kSlUnr;  // the MLE's accumulators need the registers
         const int64_t b0 = e0 / EPL;
         const int nb = (int)((e1 + EPL - 1) / EPL - b0);
-        // IRLS: both sums of a nonzero are multiples of y / (A E + k)
-        // (PassIRLS::sparse: rk y r to the Hessian weight, -y r to the
-        // score): one sum of y / (E + k/A), folded in with rk/A and -1/A
-        // (A held above 1e-200: an underflowing A leaves y / k either way)
-        constexpr bool kFold = std::is_same<Pass, PassIRLS>::value;
-        double iA = 0.0, kA = 0.0, sy = 0.0;
-        if constexpr (kFold) {
-            iA = 1.0 / fmax(A, 1e-200);
-            kA = (double)gpar.k * iA;
-        }
-        auto term = [&](ET cr) {
-            if constexpr (kFold)
-                sy += (double)Ent::y(cr) * rcp_r(Es[Ent::loc(cr)] + kA);
-            else
-                Pass::template sparse<double>(gpar, A * Es[Ent::loc(cr)], Ent::y(cr), acc);
-        };
         for (int base = lane; base < nb; base += 32 * UNR) {
             uint4 v[UNR];
 #pragma unroll
@@ -871,18 +858,16 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
                     const ET* c = reinterpret_cast<const ET*>(&v[q]);
                     if (ea >= e0 && ea + EPL <= e1) {  // a whole group inside the range
 #pragma unroll
-                        for (int r = 0; r < EPL; ++r) term(c[r]);
+                        for (int r = 0; r < EPL; ++r)
+                            Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[r])], Ent::y(c[r]), acc);
                     } else {
 #pragma unroll
                         for (int r = 0; r < EPL; ++r)
-                            if (ea + r >= e0 && ea + r < e1) term(c[r]);
+                            if (ea + r >= e0 && ea + r < e1)
+                                Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[r])], Ent::y(c[r]), acc);
                     }
                 }
             }
-        }
-        if constexpr (kFold) {
-            acc.w[0] += (double)gpar.rk * iA * sy;
-            acc.w[1] -= iA * sy;
         }
         double* o = geo.gsum + ((int64_t)jj * S + s) * NQ;
 #pragma unroll
