@@ -764,11 +764,8 @@ DEV uint4 ld_stream(const uint4* p) {
     return v;
 }
 
-template <class Pass>
-constexpr int sl_min_blocks() { return std::is_same<Pass, PassIRLS>::value ? 1 : 2; }
-
 template <class Pass, class VT>
-__global__ void __launch_bounds__(kSlNT, sl_min_blocks<Pass>()) grp_slices_kernel(GrpGeom geo, typename Pass::Params prm,
+__global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typename Pass::Params prm,
                                                               int tile) {
     using Ent = GrpEnt<VT>;
     using ET = typename Ent::T;
