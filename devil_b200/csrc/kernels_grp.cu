@@ -840,7 +840,7 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
         // the 16-byte groups covering [e0, e1) (the copy is padded to a whole
         // group), UNR loads in flight per lane before any is consumed;
         // entries outside the range are masked
-        constexpr int UNR = NS > 0 ? 2 : kSlUnr;  // the MLE's accumulators need the registers
+        constexpr int UNR = NS > 0 ? 2 : 3;  // the MLE's accumulators need the registers
         const int64_t b0 = e0 / EPL;
         const int nb = (int)((e1 + EPL - 1) / EPL - b0);
         for (int base = lane; base < nb; base += 32 * UNR) {
