@@ -837,10 +837,22 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
             Pass::template dense<double>(gpar, A * __ldg(geo.res + (int64_t)u * kRuleCap + j), acc);
         }
         acc.q = 1.0;
+        double* o = geo.gsum + ((int64_t)jj * S + s) * NQ;
+        if constexpr (NS > 0) {
+            // the nonzeros add only FP64 scalars (PassMLE): the weight sums are
+            // final here, and their registers free for the loads below
+#pragma unroll
+            for (int i = 0; i < NWV; ++i) {
+                const double v = warp_sum(acc.w[i]);
+                if (lane == 0) o[i] = v;
+            }
+        }
         // the 16-byte groups covering [e0, e1) (the copy is padded to a whole
         // group), UNR loads in flight per lane before any is consumed;
         // entries outside the range are masked
-        constexpr int UNR = NS > 0 ? 2 : 3;  // the MLE's accumulators need the registers
+        // 16-byte loads in flight per lane: as many as the 64-register budget
+        // holds without spilling (the MLE's accumulators need more registers)
+        constexpr int UNR = NS > 0 ? 2 : 3;
         const int64_t b0 = e0 / EPL;
         const int nb = (int)((e1 + EPL - 1) / EPL - b0);
         for (int base = lane; base < nb; base += 32 * UNR) {
@@ -866,11 +878,12 @@ __global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typen
                 }
             }
         }
-        double* o = geo.gsum + ((int64_t)jj * S + s) * NQ;
+        if constexpr (NS == 0) {
 #pragma unroll
-        for (int i = 0; i < NWV; ++i) {
-            const double v = warp_sum(acc.w[i]);
-            if (lane == 0) o[i] = v;
+            for (int i = 0; i < NWV; ++i) {
+                const double v = warp_sum(acc.w[i]);
+                if (lane == 0) o[i] = v;
+            }
         }
 #pragma unroll
         for (int i = 0; i < NS; ++i) {
