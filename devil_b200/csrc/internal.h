@@ -123,7 +123,7 @@ constexpr int kRuleCap = kMaxBins * kBinNodes;  // node capacity of one rule
 constexpr int kMaxGroups = 256;       // distinct design rows
 constexpr int kMaxFine = 4096;        // (design row, cluster) pairs
 constexpr int kMinCellsPerGroup = 32; // grouping pays when groups are larger
-constexpr int kSliceCells = 8192;     // cells per slice (its exp(offset) fits shared memory)
+constexpr int kSliceCells = 16384;    // cells per slice (its FP64 exp(offset), 128 KB, fits shared memory)
 constexpr int kGrpTab = 2 * kPsiTab + 2;  // per-gene psi tables + psi(a), psi1(a)
 constexpr int kMaxSlices = 12288;     // the CSR copy's per-warp key table stays <= 48 KB; keys fit 16 bits
 

@@ -751,7 +751,7 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
 // shared memory.  The per-(gene, slice) sums
 // go to geo.gsum; grp_assemble_kernel forms the p x p terms per gene.
 // ---------------------------------------------------------------------
-constexpr int kSlNT = 512;
+constexpr int kSlNT = 1024;  // one block per SM: 32 warps, 64 registers each, the 128 KB slice stage
 constexpr int kSlUnr = 4;  // 16-byte loads in flight per lane
 
 // streaming 16-byte load that does not allocate in L1 (each entry is read
@@ -765,7 +765,7 @@ DEV uint4 ld_stream(const uint4* p) {
 }
 
 template <class Pass, class VT>
-__global__ void __launch_bounds__(kSlNT, 2) grp_slices_kernel(GrpGeom geo, typename Pass::Params prm,
+__global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typename Pass::Params prm,
                                                               int tile) {
     using Ent = GrpEnt<VT>;
     using ET = typename Ent::T;
@@ -983,10 +983,10 @@ __global__ void __launch_bounds__(256) grp_assemble_kernel(GrpGeom geo) {
 }
 
 int grp_slices_tile(int64_t hint, int S, int sm_count, int waves) {
-    // two resident blocks per SM (registers, the 64 KB slice stage); about
-    // `waves` waves (3 unless tuned), the tile count chosen so the last
-    // wave is nearly full, tiles of 16..1024 genes
-    const int64_t cap = (int64_t)sm_count * 2;
+    // one resident block per SM (1,024 threads at 64 registers, the 128 KB
+    // slice stage); about `waves` waves (3 unless tuned), the tile count
+    // chosen so the last wave is nearly full, tiles of 16..1024 genes
+    const int64_t cap = (int64_t)sm_count;
     int64_t tiles = std::max<int64_t>(1, ((int64_t)std::max(1, waves) * cap + S - 1) / S);
     double best_eff = 0.0;
     int64_t best = tiles;
