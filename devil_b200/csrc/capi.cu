@@ -285,6 +285,9 @@ struct DevProblem {
         int n_need = 0;
         int32_t *need_q = nullptr, *need_d = nullptr;
         double *rval = nullptr, *qv = nullptr, *vv = nullptr;
+        int32_t* order = nullptr;  // genes by decreasing entry count (the passes' work order)
+        int32_t* wkey = nullptr;   // [G] entries of every gene
+        int32_t* skey = nullptr;   // [G] the same in the work order (descending)
     } grp;
 };
 
@@ -858,6 +861,22 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
         g.need_d = up_i("grp_need_d", need_d);
     }
     g.res = res;
+    {
+        // the work order of the slice-major passes: genes by decreasing entries
+        const int64_t G = dp.G;
+        int32_t* key = ws<int32_t>(ctx, "grp_ord_key", G);
+        int32_t* key2 = ws<int32_t>(ctx, "grp_ord_key2", G);
+        int32_t* idx = ws<int32_t>(ctx, "grp_ord_idx", G);
+        g.order = ws<int32_t>(ctx, "grp_order", G);
+        LAUNCH(launch_gene_entries(dp.rowptr, G, key, idx, st));
+        size_t ob = 0;
+        cub::DeviceRadixSort::SortPairsDescending(nullptr, ob, key, key2, idx, g.order, (int)G);
+        CK(cub::DeviceRadixSort::SortPairsDescending(ws<char>(ctx, "grp_ord_tmp", ob), ob, key, key2, idx,
+                                                     g.order, (int)G, 0, 32, st));
+        ctx->launches++;
+        g.wkey = key;
+        g.skey = key2;
+    }
     CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
     g.active = true;
     g.U = U;
@@ -1043,7 +1062,8 @@ PassBuffers pass_buffers(devil_ctx* ctx, PassKind k, int P, size_t slots_x_segs)
 void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const PassPlan& plan,
                  int nseg, int tiles, const int32_t* bound, const int64_t* segptr,
                  int nbound, const int32_t* act, const int32_t* n_act, int32_t* reset_next,
-                 const PassBuffers& pb, const PassParamsAny& prm, int fine = 0) {
+                 const PassBuffers& pb, const PassParamsAny& prm, int fine = 0,
+                 const int32_t* n_heavy = nullptr) {
     PassLaunch L;
     L.kind = kind;
     L.engine = plan.engine;
@@ -1083,6 +1103,7 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
         gg.fine = fine;
         gg.act = act;
         gg.n_act = n_act;
+        gg.n_heavy = n_heavy;
         gg.reset_next = reset_next;
         gg.partW = static_cast<double*>(pb.partW);
         gg.partS = pb.partS;
@@ -1311,6 +1332,13 @@ int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan0, d
     PassParamsAny prm{beta_f, beta, k, nullptr, nullptr};
     const PassPlan plan = autotune(ctx, dp, plan0, act[0], cnt, n0, prm, form);
     PassBuffers pb = pass_buffers(ctx, PASS_IRLS, dp.P, max_slot_segs(ctx, dp, plan, form));
+    // slice-major passes over the genes in decreasing order of entries
+    // (act0 = dp.grp.order): the genes below kLightEntries entries per slice
+    // on average take eight lanes each
+    const bool sliced = plan.engine == ENGINE_GRP && (ctx->grp_slices & 1);
+    int32_t* nheavy = ws<int32_t>(ctx, "cnt_heavy", 2);
+    const int32_t thr = (int32_t)std::min<int64_t>((int64_t)kLightEntries * dp.grp.S, INT32_MAX);
+    if (sliced) LAUNCH(launch_count_at_least(dp.grp.skey, n0, thr, nheavy, st));
     // copies of an earlier loop still in flight would overwrite the mirror
     CK(cudaStreamSynchronize(st));
     *ctx->mapped_host = (int32_t)n0;
@@ -1325,17 +1353,22 @@ int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan0, d
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
         launch_pass(ctx, dp, PASS_IRLS, plan, nseg, tiles, dp.fine_bound, dp.fine_ptr,
-                    dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
+                    dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm, 0, sliced ? nheavy + cur : nullptr);
         ++launched;
         const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC && plan.engine != ENGINE_TCW;
-        if (plan.engine == ENGINE_GRP && (ctx->grp_slices & 1)) {
+        if (sliced) {
             // slice-major pass: the assembly is part of the step
             GrpGeom gg = grp_geom(dp);
             gg.act = act[cur];
             gg.n_act = cnt + cur;
             gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * 2);
+            // the genes that go on keep the order of the list (decreasing
+            // entries: the pass's work order)
+            int8_t* keep = ws<int8_t>(ctx, "keep", G);
             LAUNCH(launch_grp_irls_finalize(gg, (int)hint, act[nxt], cnt + nxt, beta, beta_f, iters,
-                                            status, max_iter, eps, k, st));
+                                            status, max_iter, eps, k, st, keep));
+            LAUNCH(launch_compact_kept(act[cur], cnt + cur, 0, keep, act[nxt], cnt + nxt, st, dp.grp.wkey, thr,
+                                       nheavy + nxt));
         } else {
             LAUNCH(launch_irls_finalize(pb.partW, part_f64, nseg, tiles * plan.GT, dp.P, act[cur],
                                         cnt + cur, (int)hint, act[nxt], cnt + nxt, beta, beta_f,
@@ -1384,7 +1417,11 @@ void run_irls(devil_ctx* ctx, const DevProblem& dp, double* beta, float* beta_f,
         beta0 = ws<double>(ctx, "irls_beta0", (size_t)G * dp.P);
         CK(cudaMemcpyAsync(beta0, beta, (size_t)G * dp.P * sizeof(double), cudaMemcpyDeviceToDevice, st));
     }
-    LAUNCH(launch_iota(ws<int32_t>(ctx, "act0", G), G, st));
+    if (plan.engine == ENGINE_GRP && (ctx->grp_slices & 1))
+        CK(cudaMemcpyAsync(ws<int32_t>(ctx, "act0", G), dp.grp.order, G * sizeof(int32_t),
+                           cudaMemcpyDeviceToDevice, st));  // decreasing entries
+    else
+        LAUNCH(launch_iota(ws<int32_t>(ctx, "act0", G), G, st));
     const int64_t launched = irls_loop(ctx, dp, plan, beta, beta_f, k, iters, status, max_iter, eps, form, G);
     if (ctx->profiling) {
         prof_collect(ctx);
@@ -1461,7 +1498,11 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     int32_t* cnt = ws<int32_t>(ctx, "cnt", 4);
     LAUNCH(launch_set_i32(cnt, 0, st));
     LAUNCH(launch_set_i32(cnt + 1, 0, st));
+    // slice-major passes: the active genes stay in decreasing order of entries
+    const bool ordered = plan.engine == ENGINE_GRP && (ctx->grp_slices & 2);
+    if (ordered) s.keep = ws<int8_t>(ctx, "keep", G);
     LAUNCH(launch_mle_init(dp.stats, G, dp.n, s, act[0], cnt, st));
+    if (ordered) LAUNCH(launch_compact_kept(dp.grp.order, nullptr, G, s.keep, act[0], cnt, st));
     PassParamsAny prm{beta_f, beta_d, nullptr, s.x, nullptr};
     plan = autotune(ctx, dp, plan, act[0], cnt, G, prm, form);
     PassBuffers pb = pass_buffers(ctx, PASS_MLE, dp.P, max_slot_segs(ctx, dp, plan, form));
@@ -1488,6 +1529,7 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
                                    act[cur], cnt + cur, (int)hint, act[nxt], cnt + nxt, s, max_iter,
                                    cox_reid, nullptr, st, structured ? dp.grp.nA : 0,
                                    structured ? dp.grp.colA : nullptr, structured ? dp.grp.colD : nullptr));
+        if (ordered) LAUNCH(launch_compact_kept(act[cur], cnt + cur, 0, s.keep, act[nxt], cnt + nxt, st));
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));

@@ -123,6 +123,8 @@ constexpr int kRuleCap = kMaxBins * kBinNodes;  // node capacity of one rule
 constexpr int kMaxGroups = 256;       // distinct design rows
 constexpr int kMaxFine = 4096;        // (design row, cluster) pairs
 constexpr int kMinCellsPerGroup = 32; // grouping pays when groups are larger
+constexpr int kLightEntries = 96;     // slice-major passes: genes below this many entries per slice on
+                                      // average take eight lanes (one round of three 16-byte loads)
 constexpr int kSliceCells = 16384;    // cells per slice (its FP64 exp(offset), 128 KB, fits shared memory)
 constexpr int kGrpTab = 2 * kPsiTab + 2;  // per-gene psi tables + psi(a), psi1(a)
 constexpr int kMaxSlices = 12288;     // the CSR copy's per-warp key table stays <= 48 KB; keys fit 16 bits
@@ -195,6 +197,10 @@ struct GrpGeom {
     const int32_t* need_d;  // [n_need][3]
     const int32_t* act;
     const int32_t* n_act;
+    // slice-major passes: the first *n_heavy active genes (the list is in
+    // decreasing order of entries) take a warp each, the others eight lanes
+    // each; null: a warp each
+    const int32_t* n_heavy;
     int32_t* reset_next;
     double* partW;         // FP64 partial sums, layout of the other engines
     double* partS;
@@ -232,6 +238,10 @@ cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsA
 // grp_slices_nq(kind) doubles; geo.rowexp: slots x U; geo.psitab, MLE:
 // slots x kGrpTab)
 int grp_slices_tile(int64_t hint, int S, int sm_count, int waves = 3);
+// key[g] = entries of gene g, idx[g] = g (sorted descending into the work
+// order of the slice-major passes)
+cudaError_t launch_gene_entries(const int64_t* rowptr, int64_t G, int32_t* key, int32_t* idx,
+                                cudaStream_t st);
 int grp_slices_nq(PassKind k);
 cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm,
                               int val_u16, int max_slots, int tile, bool assemble, cudaStream_t st);
@@ -325,6 +335,14 @@ cudaError_t launch_fill_i32(int32_t* a, int32_t v, int64_t m, cudaStream_t st);
 cudaError_t launch_mle_passes(const int32_t* it, const int32_t* phase, const double* stats,
                               int64_t G, int32_t* out, cudaStream_t st);
 cudaError_t launch_set_i32(int32_t* a, int32_t v, cudaStream_t st);
+// act_next = the genes g of act[0, n) (n = *n_act, or n_fixed when n_act is
+// null) with keep[g] != 0, in order; *n_next = their count
+// (wkey non-null: *n_heavy_next = the kept genes with wkey[g] >= thr)
+cudaError_t launch_compact_kept(const int32_t* act, const int32_t* n_act, int64_t n_fixed, const int8_t* keep,
+                                int32_t* act_next, int32_t* n_next, cudaStream_t st,
+                                const int32_t* wkey = nullptr, int32_t thr = 0, int32_t* n_heavy_next = nullptr);
+// *out = the number of leading entries of key (in descending order) >= thr
+cudaError_t launch_count_at_least(const int32_t* key, int64_t n, int32_t thr, int32_t* out, cudaStream_t st);
 cudaError_t launch_copy_i32_to_host_mapped(const int32_t* src, volatile int32_t* dst,
                                            cudaStream_t st);
 
@@ -338,10 +356,12 @@ cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slo
 // the IRLS step of the design-group engine's slice-major pass, the p x p
 // assembly from geo.gsum folded in (geo.act / geo.n_act: this iteration's
 // active genes)
+// (keep non-null: keep[g] = 1 for the genes that go on, 0 for the others,
+// and act_next / n_next untouched: launch_compact_kept lists them in order)
 cudaError_t launch_grp_irls_finalize(const GrpGeom& geo, int max_slots, int32_t* act_next,
                                      int32_t* n_next, double* beta, float* beta_f, int32_t* iters,
                                      int32_t* status, int max_iter, double eps, const float* k,
-                                     cudaStream_t st);
+                                     cudaStream_t st, int8_t* keep = nullptr);
 cudaError_t launch_mom_finalize(const double* partS, int nseg, int slot_stride,
                                 const int32_t* act, const int32_t* n_act, int max_slots,
                                 int64_t n, int P, double* theta, cudaStream_t st);
@@ -355,6 +375,8 @@ struct MleState {
     double* dx;      // last step and the one before (bisection safeguard)
     double* dxold;
     const double* start_hint;  // optional per-gene start (MOM theta), may be null
+    int8_t* keep = nullptr;    // non-null: keep[g] marks the genes that go on (launch_compact_kept
+                               // lists them in order); null: appended to the next list
 };
 cudaError_t launch_mle_init(const double* stats, int64_t G, int64_t n, MleState s,
                             int32_t* act, int32_t* n_act, cudaStream_t st);

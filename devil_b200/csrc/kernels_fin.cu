@@ -188,7 +188,7 @@ constexpr int kSchurScratch = 8 * wla_ld(8);  // doubles: the Schur complement o
 __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t* n_next,
                                          double* beta, float* beta_f, int32_t* iters,
                                          int32_t* status, int max_iter, double eps,
-                                         const float* kf) {
+                                         const float* kf, int8_t* keep) {
     extern __shared__ double fsh[];
     const int P = geo.P, U = geo.U, C = geo.C, S = geo.S, LD = wla_ld(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -280,6 +280,7 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
     if (lane != 0) return;
     const int it = iters[g] + 1;
     iters[g] = it;
+    bool more = false;
     if (!(x0 == x0)) {
         status[g] = 2;  // DEVIL_GENE_NAN
     } else if (mx < eps) {
@@ -287,14 +288,16 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
     } else if (it >= max_iter) {
         status[g] = 1;
     } else {
-        act_next[atomicAdd(n_next, 1)] = g;
+        more = true;
     }
+    if (keep) keep[g] = more ? 1 : 0;
+    else if (more) act_next[atomicAdd(n_next, 1)] = g;
 }
 
 cudaError_t launch_grp_irls_finalize(const GrpGeom& geo, int max_slots, int32_t* act_next,
                                      int32_t* n_next, double* beta, float* beta_f, int32_t* iters,
                                      int32_t* status, int max_iter, double eps, const float* k,
-                                     cudaStream_t st) {
+                                     cudaStream_t st, int8_t* keep) {
     if (max_slots <= 0) return cudaSuccess;
     const int P = geo.P, na = geo.nA;
     const size_t per =
@@ -307,7 +310,7 @@ cudaError_t launch_grp_irls_finalize(const GrpGeom& geo, int max_slots, int32_t*
         if (e != cudaSuccess) return e;
     }
     grp_irls_finalize_kernel<<<nblk(max_slots, w), 32 * w, smem, st>>>(
-        geo, act_next, n_next, beta, beta_f, iters, status, max_iter, eps, k);
+        geo, act_next, n_next, beta, beta_f, iters, status, max_iter, eps, k, keep);
     return cudaGetLastError();
 }
 
@@ -361,9 +364,9 @@ __global__ void mle_init_kernel(const double* stats, int64_t G, MleState s, int3
         } else {
             s.phase[g] = 0;
             s.x[g] = log(1e-8);
-            int pos = atomicAdd(n_act, 1);
-            act[pos] = (int32_t)g;
+            if (!s.keep) act[atomicAdd(n_act, 1)] = (int32_t)g;
         }
+        if (s.keep) s.keep[g] = s.phase[g] == 0 ? 1 : 0;
     }
 }
 cudaError_t launch_mle_init(const double* stats, int64_t G, int64_t n, MleState s, int32_t* act,
@@ -578,6 +581,7 @@ __global__ void mle_finalize_kernel(const TW* partW, const double* partS, int ns
         if (score < 0.0) {
             st.theta[g] = 0.0;
             st.phase[g] = 2;
+            if (st.keep) st.keep[g] = 0;
             return;
         }
         const double mean = gs[0], var = gs[1];
@@ -636,10 +640,10 @@ __global__ void mle_finalize_kernel(const TW* partW, const double* partS, int ns
     if (done) {
         st.theta[g] = exp(xn);
         st.phase[g] = 2;
-    } else {
-        int pos = atomicAdd(n_next, 1);
-        act_next[pos] = g;
+    } else if (!st.keep) {
+        act_next[atomicAdd(n_next, 1)] = g;
     }
+    if (st.keep) st.keep[g] = done ? 0 : 1;
 }
 cudaError_t launch_mle_finalize(const void* partW, bool wide, const double* partS, int nseg,
                                 int slot_stride, int P, const double* stats, int64_t n,

@@ -742,17 +742,30 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
 }
 
 // ---------------------------------------------------------------------
-// IRLS and MLE passes, slice-major.  Block (slice s, tile of active genes):
-// the slice's exp(offset) values are staged in shared memory once, then
-// each warp takes the tile's genes in turn: A = exp(x_u . beta) (computed
-// per gene and group beforehand), the rule terms of group u when s is the
-// group's first slice, and the gene's entries of the slice streamed as
-// 16-byte loads (4 entries each for 16-bit counts), exp(offset) read from
-// shared memory.  The per-(gene, slice) sums
-// go to geo.gsum; grp_assemble_kernel forms the p x p terms per gene.
+// IRLS and MLE passes, slice-major.  Block (slice s, share of the active
+// genes): the slice's exp(offset) values are staged in shared memory once,
+// then each warp takes the block's genes in turn: A = exp(x_u . beta)
+// (computed per gene and group beforehand), the rule terms of group u when
+// s is the group's first slice, and the gene's entries of the slice as
+// 16-byte streaming loads (UNR in flight per lane), mu = A E[cell] with E
+// from shared memory.  The active genes are listed in decreasing order of
+// entries; those with fewer than kLightEntries per slice on average (the
+// tail of the list) take eight lanes each, four to a warp, so that the
+// per-(gene, slice) bookkeeping (hand-out, ranges, sums, stores) is shared
+// by four genes.  The per-(gene, slice) sums go to geo.gsum;
+// grp_assemble_kernel / the IRLS step form the p x p terms per gene.
 // ---------------------------------------------------------------------
 constexpr int kSlNT = 1024;  // one block per SM: 32 warps, 64 registers each, the 128 KB slice stage
-constexpr int kSlUnr = 4;  // 16-byte loads in flight per lane
+
+// 16-byte loads in flight per lane: as many as 64 registers hold (the
+// MLE's accumulators take more registers)
+template <class Pass>
+constexpr int sl_unr() { return Pass::TABLES ? 2 : 3; }
+
+template <class Pass>
+constexpr size_t sl_smem_bytes() {
+    return (size_t)kSliceCells * sizeof(double) + (Pass::TABLES ? (size_t)(kSlNT / 32) * kGrpTab * sizeof(double) : 0);
+}
 
 // streaming 16-byte load that does not allocate in L1 (each entry is read
 // once per pass)
@@ -764,18 +777,35 @@ DEV uint4 ld_stream(const uint4* p) {
     return v;
 }
 
+// one gene of a slice-major block: its list slot, index, exp(x_u . beta)
+// and the range of its entries in the slice
+struct SlItem {
+    int j, g;
+    double A;
+    int64_t e0, e1;
+};
+
 template <class Pass, class VT>
 __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typename Pass::Params prm,
                                                               int tile) {
     using Ent = GrpEnt<VT>;
     using ET = typename Ent::T;
+    using Acc = GrpAcc<Pass::NW + Pass::NV + Pass::NF, Pass::NS>;
     constexpr int NWV = Pass::NW + Pass::NV + Pass::NF, NS = Pass::NS, NQ = NWV + NS;
-    constexpr int EPL = sizeof(uint4) / sizeof(ET);  // entries per 16-byte load
+    constexpr int EPL = sizeof(uint4) / sizeof(ET);  // entries per 16-byte piece
+    constexpr int UNR = sl_unr<Pass>();
+    constexpr int RW = 32 * UNR;                      // 16-byte pieces per round
     if (geo.reset_next && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *geo.reset_next = 0;
+    (void)tile;
     const int nact = *geo.n_act;
-    const int j0 = blockIdx.y * tile;
-    if (j0 >= nact) return;
-    const int j1 = min(nact, j0 + tile);
+    // genes [0, nheavy) of the list take a warp each, the rest eight lanes each
+    const int nheavy = geo.n_heavy ? min(nact, *geo.n_heavy) : nact;
+    // block y takes the slots y, y + T, y + 2T, ... (T = gridDim.y) of each
+    // part: with the active genes listed in decreasing order of entries,
+    // every block gets a like share of the work and hands its largest genes
+    // out first, so the block's last warps finish together
+    const int T = gridDim.y, y = blockIdx.y;
+    if (y >= nact) return;
     const int s = blockIdx.x, S = geo.S, U = geo.U;
     extern __shared__ double Es[];  // [kSliceCells] exp(offset) of the slice's cells
     const int c0 = __ldg(geo.sl_start + s), nc = __ldg(geo.sl_start + s + 1) - c0;
@@ -787,42 +817,37 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
     const bool first = s == __ldg(geo.kslice + u * geo.C);  // the group's rule goes here
     constexpr bool kRule = !std::is_same<Pass, PassInitZ>::value;  // zero counts contribute
     const int m = (kRule && first) ? __ldg(geo.rm + u) : 0;
-    __syncthreads();
     const uint4* __restrict__ v4 = static_cast<const uint4*>(geo.gent);
-    // per gene: exp(x_u . beta) (from grp_rowexp_kernel) and the slice's
-    // entry range; the next gene's are loaded while this one runs
-    // the tile's genes are handed out one at a time (a shared counter), so
+    // the block's genes are handed out one at a time (a shared counter), so
     // warps that drew short genes take more of them
-    __shared__ int next_gene;
-    if (t == 0) next_gene = j0 + nw;
-    __syncthreads();
-    int jj = j0 + warp;
-    int g = 0;
-    double A = 0.0;
-    int64_t e0 = 0, e1 = 0;
-    if (jj < j1) {
-        g = __ldg(geo.act + jj);
-        A = __ldg(geo.rowexp + (int64_t)jj * U + u);
-        e0 = __ldg(geo.gptr + (int64_t)g * (S + 1) + s);
-        e1 = __ldg(geo.gptr + (int64_t)g * (S + 1) + s + 1);
+    __shared__ int next_k, next_l;
+    if (t == 0) {
+        next_k = 0;
+        next_l = 0;
     }
-    while (jj < j1) {
-        int jn = 0;
-        if (lane == 0) jn = atomicAdd(&next_gene, 1);
-        jn = __shfl_sync(0xffffffffu, jn, 0);
-        int gn = 0;
-        double An = 0.0;
-        int64_t f0 = 0, f1 = 0;
-        if (jn < j1) {
-            gn = __ldg(geo.act + jn);
-            An = __ldg(geo.rowexp + (int64_t)jn * U + u);
-            f0 = __ldg(geo.gptr + (int64_t)gn * (S + 1) + s);
-            f1 = __ldg(geo.gptr + (int64_t)gn * (S + 1) + s + 1);
+    __syncthreads();
+    auto take = [&]() -> SlItem {
+        int k = 0;
+        if (lane == 0) k = atomicAdd(&next_k, 1);
+        SlItem it{y + __shfl_sync(0xffffffffu, k, 0) * T, 0, 0.0, 0, 0};
+        if (it.j >= nheavy) it.j = nact;  // past the heavy part
+        if (it.j < nact) {
+            it.g = __ldg(geo.act + it.j);
+            it.A = __ldg(geo.rowexp + (int64_t)it.j * U + u);
+            it.e0 = __ldg(geo.gptr + (int64_t)it.g * (S + 1) + s);
+            it.e1 = __ldg(geo.gptr + (int64_t)it.g * (S + 1) + s + 1);
         }
-        typename Pass::Gene gpar = Pass::load(prm, g);
+        return it;
+    };
+    // a heavy gene's parameters, psi tables and rule terms (lanes over the
+    // rule's nodes); the MLE's weight sums are final after the rule and
+    // stored at once (the nonzeros add only FP64 scalars), freeing their
+    // registers for the entries
+    auto gene_start = [&](const SlItem& it, typename Pass::Gene& gpar, Acc& acc, double*& o) {
+        gpar = Pass::load(prm, it.g);
         if constexpr (Pass::TABLES) {
             // the gene's psi tables (grp_psi_tables_kernel) into the warp's slot
-            const double* src = geo.psitab + (int64_t)jj * kGrpTab;
+            const double* src = geo.psitab + (int64_t)it.j * kGrpTab;
             for (int i = lane; i < kGrpTab; i += 32) wtab[i] = __ldg(src + i);
             __syncwarp();
             gpar.tab.d1 = wtab;
@@ -830,54 +855,22 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
             gpar.tab.pa = wtab[2 * kPsiTab];
             gpar.tab.ta = wtab[2 * kPsiTab + 1];
         }
-        GrpAcc<NWV, NS> acc;
         acc.zero();
         for (int j = lane; j < m; j += 32) {
             acc.q = __ldg(geo.rw + (int64_t)u * kRuleCap + j);
-            Pass::template dense<double>(gpar, A * __ldg(geo.res + (int64_t)u * kRuleCap + j), acc);
+            Pass::template dense<double>(gpar, it.A * __ldg(geo.res + (int64_t)u * kRuleCap + j), acc);
         }
         acc.q = 1.0;
-        double* o = geo.gsum + ((int64_t)jj * S + s) * NQ;
+        o = geo.gsum + ((int64_t)it.j * S + s) * NQ;
         if constexpr (NS > 0) {
-            // the nonzeros add only FP64 scalars (PassMLE): the weight sums are
-            // final here, and their registers free for the loads below
 #pragma unroll
             for (int i = 0; i < NWV; ++i) {
                 const double v = warp_sum(acc.w[i]);
                 if (lane == 0) o[i] = v;
             }
         }
-        // the 16-byte groups covering [e0, e1) (the copy is padded to a whole
-        // group), UNR loads in flight per lane before any is consumed;
-        // entries outside the range are masked
-        // 16-byte loads in flight per lane: as many as the 64-register budget
-        // holds without spilling (the MLE's accumulators need more registers)
-        constexpr int UNR = NS > 0 ? 2 : 3;
-        const int64_t b0 = e0 / EPL;
-        const int nb = (int)((e1 + EPL - 1) / EPL - b0);
-        for (int base = lane; base < nb; base += 32 * UNR) {
-            uint4 v[UNR];
-#pragma unroll
-            for (int q = 0; q < UNR; ++q)
-                if (base + 32 * q < nb) v[q] = ld_stream(v4 + b0 + base + 32 * q);
-#pragma unroll
-            for (int q = 0; q < UNR; ++q) {
-                const int64_t ea = (b0 + base + 32 * q) * EPL;  // first entry of the group
-                if (base + 32 * q < nb) {
-                    const ET* c = reinterpret_cast<const ET*>(&v[q]);
-                    if (ea >= e0 && ea + EPL <= e1) {  // a whole group inside the range
-#pragma unroll
-                        for (int r = 0; r < EPL; ++r)
-                            Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[r])], Ent::y(c[r]), acc);
-                    } else {
-#pragma unroll
-                        for (int r = 0; r < EPL; ++r)
-                            if (ea + r >= e0 && ea + r < e1)
-                                Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[r])], Ent::y(c[r]), acc);
-                    }
-                }
-            }
-        }
+    };
+    auto gene_end = [&](Acc& acc, double* o) {
         if constexpr (NS == 0) {
 #pragma unroll
             for (int i = 0; i < NWV; ++i) {
@@ -890,12 +883,106 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
             const double v = warp_sum(acc.s[i]);
             if (lane == 0) o[NWV + i] = v;
         }
-        jj = jn;
-        g = gn;
-        A = An;
-        e0 = f0;
-        e1 = f1;
-        if constexpr (Pass::TABLES) __syncwarp();  // the table slot is rewritten next
+    };
+    // the entries of one 16-byte piece (first entry ea) inside [e0, e1)
+    auto piece = [&](const uint4& v, int64_t ea, int64_t e0, int64_t e1, const typename Pass::Gene& gpar,
+                     double A, Acc& acc) {
+        const ET* c = reinterpret_cast<const ET*>(&v);
+        if (ea >= e0 && ea + EPL <= e1) {  // a whole piece inside the range
+#pragma unroll
+            for (int rr = 0; rr < EPL; ++rr)
+                Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[rr])], Ent::y(c[rr]), acc);
+        } else {
+#pragma unroll
+            for (int rr = 0; rr < EPL; ++rr)
+                if (ea + rr >= e0 && ea + rr < e1)
+                    Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[rr])], Ent::y(c[rr]), acc);
+        }
+    };
+    {
+        // entries loaded to registers, UNR pieces per lane in flight; the
+        // next gene's range is loaded while this one runs
+        SlItem cur = take();
+        while (cur.j < nact) {
+            const SlItem nx = take();
+            typename Pass::Gene gpar;
+            Acc acc;
+            double* o;
+            gene_start(cur, gpar, acc, o);
+            const int64_t b0 = cur.e0 / EPL;
+            const int nb = (int)((cur.e1 + EPL - 1) / EPL - b0);
+            for (int base = lane; base < nb; base += RW) {
+                uint4 v[UNR];
+#pragma unroll
+                for (int q = 0; q < UNR; ++q)
+                    if (base + 32 * q < nb) v[q] = ld_stream(v4 + b0 + base + 32 * q);
+#pragma unroll
+                for (int q = 0; q < UNR; ++q)
+                    if (base + 32 * q < nb) piece(v[q], (b0 + base + 32 * q) * EPL, cur.e0, cur.e1, gpar, cur.A, acc);
+            }
+            gene_end(acc, o);
+            cur = nx;
+            if constexpr (Pass::TABLES) __syncwarp();  // the table slot is rewritten next
+        }
+    }
+    if constexpr (!Pass::TABLES) {
+        // the light genes: four per warp, eight lanes each (the per-gene
+        // bookkeeping is shared by four genes), loads straight to registers
+        constexpr int LW = 8, LUNR = 3, LRW = LW * LUNR;
+        const int sub = lane / LW, sl = lane % LW;
+        const int nlight = nact - nheavy;
+        while (true) {
+            int k0 = 0;
+            if (lane == 0) k0 = atomicAdd(&next_l, 32 / LW);
+            k0 = __shfl_sync(0xffffffffu, k0, 0);
+            if (y + k0 * T >= nlight) break;  // (warp-uniform)
+            const int jl = y + (k0 + sub) * T;
+            const bool valid = jl < nlight;
+            const int j = nheavy + (valid ? jl : 0);
+            Acc acc;
+            acc.zero();
+            if (valid) {
+                const int g = __ldg(geo.act + j);
+                const double A = __ldg(geo.rowexp + (int64_t)j * U + u);
+                const int64_t e0 = __ldg(geo.gptr + (int64_t)g * (S + 1) + s);
+                const int64_t e1 = __ldg(geo.gptr + (int64_t)g * (S + 1) + s + 1);
+                const typename Pass::Gene gpar = Pass::load(prm, g);
+                for (int jr = sl; jr < m; jr += LW) {
+                    acc.q = __ldg(geo.rw + (int64_t)u * kRuleCap + jr);
+                    Pass::template dense<double>(gpar, A * __ldg(geo.res + (int64_t)u * kRuleCap + jr), acc);
+                }
+                acc.q = 1.0;
+                const int64_t b0 = e0 / EPL;
+                const int nb = (int)((e1 + EPL - 1) / EPL - b0);
+                for (int base = sl; base < nb; base += LRW) {
+                    uint4 v[LUNR];
+#pragma unroll
+                    for (int q = 0; q < LUNR; ++q)
+                        if (base + LW * q < nb) v[q] = ld_stream(v4 + b0 + base + LW * q);
+#pragma unroll
+                    for (int q = 0; q < LUNR; ++q)
+                        if (base + LW * q < nb) piece(v[q], (b0 + base + LW * q) * EPL, e0, e1, gpar, A, acc);
+                }
+            }
+            // sums over each gene's eight lanes
+#pragma unroll
+            for (int i = 0; i < NWV; ++i) {
+#pragma unroll
+                for (int o = LW / 2; o > 0; o >>= 1) acc.w[i] += __shfl_xor_sync(0xffffffffu, acc.w[i], o);
+            }
+#pragma unroll
+            for (int i = 0; i < NS; ++i) {
+#pragma unroll
+                for (int o = LW / 2; o > 0; o >>= 1) acc.s[i] += __shfl_xor_sync(0xffffffffu, acc.s[i], o);
+            }
+            if (valid && sl == 0) {
+                double* o = geo.gsum + ((int64_t)j * S + s) * NQ;
+#pragma unroll
+                for (int i = 0; i < NWV; ++i) o[i] = acc.w[i];
+#pragma unroll
+                for (int i = 0; i < NS; ++i) o[NWV + i] = acc.s[i];
+            }
+        }
     }
 }
 
@@ -982,6 +1069,23 @@ __global__ void __launch_bounds__(256) grp_assemble_kernel(GrpGeom geo) {
     }
 }
 
+// the sort keys of the work order of the slice-major passes: the gene's
+// entries (the sort is descending) and its index
+__global__ void gene_entries_kernel(const int64_t* rowptr, int64_t G, int32_t* key, int32_t* idx) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < G;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = rowptr[g + 1] - rowptr[g];
+        key[g] = (int32_t)(e < INT32_MAX ? e : INT32_MAX);
+        idx[g] = (int32_t)g;
+    }
+}
+cudaError_t launch_gene_entries(const int64_t* rowptr, int64_t G, int32_t* key, int32_t* idx,
+                                cudaStream_t st) {
+    if (G <= 0) return cudaSuccess;
+    gene_entries_kernel<<<(unsigned)std::min<int64_t>(nblk(G, 256), 1024), 256, 0, st>>>(rowptr, G, key, idx);
+    return cudaGetLastError();
+}
+
 int grp_slices_tile(int64_t hint, int S, int sm_count, int waves) {
     // one resident block per SM (1,024 threads at 64 registers, the 128 KB
     // slice stage); about `waves` waves (3 unless tuned), the tile count
@@ -1007,8 +1111,7 @@ template <class Pass>
 static cudaError_t slices_run(const GrpGeom& geo, typename Pass::Params prm, int val_u16,
                               int max_slots, int tile, bool assemble, cudaStream_t st) {
     constexpr int NQ = Pass::NW + Pass::NV + Pass::NF + Pass::NS;
-    const size_t smem = ((size_t)kSliceCells + (Pass::TABLES ? (kSlNT / 32) * kGrpTab : 0)) *
-                        sizeof(double);
+    const size_t smem = sl_smem_bytes<Pass>();
     if constexpr (Pass::TABLES)
         grp_psi_tables_kernel<<<(unsigned)max_slots, 32, 0, st>>>(geo.act, geo.n_act, prm.log_theta,
                                                                  geo.psitab);
@@ -1081,7 +1184,7 @@ cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* 
                                  float* beta_f, cudaStream_t st) {
     if (G <= 0) return cudaSuccess;
     PassInitZ::Params prm{nullptr, zero_beta};
-    const size_t smem = (size_t)kSliceCells * sizeof(double);
+    const size_t smem = sl_smem_bytes<PassInitZ>();
     const int64_t nrow = G * geo.U;
     grp_rowexp_kernel<<<nblk(nrow, 256), 256, 0, st>>>(geo, zero_beta, G);  // exp(0) = 1
     dim3 grid((unsigned)geo.S, (unsigned)((G + tile - 1) / tile));

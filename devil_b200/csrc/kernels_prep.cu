@@ -733,6 +733,79 @@ cudaError_t launch_iota(int32_t* a, int64_t m, cudaStream_t st) {
     iota_kernel<<<(unsigned)std::min<int64_t>(nblk(m, 256), 1024), 256, 0, st>>>(a, m);
     return cudaGetLastError();
 }
+// act_next = the genes of act[0, n) with keep[g] != 0, in their order in
+// act (one block: a thread scans a contiguous run, a block scan places the
+// runs); *n_next = their count.  Keeping the order keeps a list sorted by
+// work sorted from one iteration to the next.
+__global__ void __launch_bounds__(1024) compact_kept_kernel(const int32_t* act, const int32_t* n_act,
+                                                            int64_t n_fixed, const int8_t* keep,
+                                                            int32_t* act_next, int32_t* n_next,
+                                                            const int32_t* wkey, int32_t thr,
+                                                            int32_t* n_heavy_next) {
+    __shared__ int wsum[32];
+    __shared__ int nheavy;
+    if (threadIdx.x == 0) nheavy = 0;
+    const int64_t n = n_act ? (int64_t)*n_act : n_fixed;
+    const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, w = t >> 5;
+    const int64_t per = (n + nt - 1) / nt;
+    const int64_t a = min(n, (int64_t)t * per), b = min(n, a + per);
+    int c = 0;
+    for (int64_t i = a; i < b; ++i) c += keep[act[i]] != 0;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        const int v = lane < (nt >> 5) ? wsum[lane] : 0;
+        int iv = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, iv, o);
+            if (lane >= o) iv += u;
+        }
+        wsum[lane] = iv - v;
+    }
+    __syncthreads();
+    int pos = wsum[w] + incl - c;
+    int heavy = 0;
+    for (int64_t i = a; i < b; ++i) {
+        const int32_t g = act[i];
+        if (keep[g]) {
+            act_next[pos++] = g;
+            if (wkey) heavy += wkey[g] >= thr;
+        }
+    }
+    if (t == nt - 1) *n_next = pos;
+    if (wkey) {
+        if (heavy) atomicAdd(&nheavy, heavy);
+        __syncthreads();
+        if (t == 0) *n_heavy_next = nheavy;
+    }
+}
+cudaError_t launch_compact_kept(const int32_t* act, const int32_t* n_act, int64_t n_fixed, const int8_t* keep,
+                                int32_t* act_next, int32_t* n_next, cudaStream_t st, const int32_t* wkey,
+                                int32_t thr, int32_t* n_heavy_next) {
+    compact_kept_kernel<<<1, 1024, 0, st>>>(act, n_act, n_fixed, keep, act_next, n_next, wkey, thr,
+                                            n_heavy_next);
+    return cudaGetLastError();
+}
+// *out = the number of leading entries of key (descending) that are >= thr
+__global__ void count_at_least_kernel(const int32_t* key, int64_t n, int32_t thr, int32_t* out) {
+    int64_t lo = 0, hi = n;  // key[0, lo) >= thr, key[hi, n) < thr
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) / 2;
+        if (key[mid] >= thr) lo = mid + 1; else hi = mid;
+    }
+    *out = (int32_t)lo;
+}
+cudaError_t launch_count_at_least(const int32_t* key, int64_t n, int32_t thr, int32_t* out, cudaStream_t st) {
+    count_at_least_kernel<<<1, 1, 0, st>>>(key, n, thr, out);
+    return cudaGetLastError();
+}
 __global__ void set_i32_kernel(int32_t* a, int32_t v) { *a = v; }
 cudaError_t launch_set_i32(int32_t* a, int32_t v, cudaStream_t st) {
     set_i32_kernel<<<1, 1, 0, st>>>(a, v);
