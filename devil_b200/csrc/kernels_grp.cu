@@ -812,7 +812,12 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
     // per warp: the psi tables of its current gene (passes with TABLES)
     double* wtab = Es + kSliceCells + warp * kGrpTab;
-    for (int i = t; i < nc; i += blockDim.x) Es[i] = __ldg(geo.E + c0 + i);
+    // (beta_0's pass takes 1/exp(offset): a product per entry, not a quotient)
+    constexpr bool kRecip = std::is_same<Pass, PassInitZ>::value;
+    for (int i = t; i < nc; i += blockDim.x) {
+        const double e = __ldg(geo.E + c0 + i);
+        Es[i] = kRecip ? 1.0 / e : e;
+    }
     const int u = __ldg(geo.sl_key + s) / geo.C;
     const bool first = s == __ldg(geo.kslice + u * geo.C);  // the group's rule goes here
     constexpr bool kRule = !std::is_same<Pass, PassInitZ>::value;  // zero counts contribute

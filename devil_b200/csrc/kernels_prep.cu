@@ -734,63 +734,85 @@ cudaError_t launch_iota(int32_t* a, int64_t m, cudaStream_t st) {
     return cudaGetLastError();
 }
 // act_next = the genes of act[0, n) with keep[g] != 0, in their order in
-// act (one block: a thread scans a contiguous run, a block scan places the
-// runs); *n_next = their count.  Keeping the order keeps a list sorted by
-// work sorted from one iteration to the next.
-__global__ void __launch_bounds__(1024) compact_kept_kernel(const int32_t* act, const int32_t* n_act,
-                                                            int64_t n_fixed, const int8_t* keep,
-                                                            int32_t* act_next, int32_t* n_next,
-                                                            const int32_t* wkey, int32_t thr,
-                                                            int32_t* n_heavy_next) {
-    __shared__ int wsum[32];
-    __shared__ int nheavy;
-    if (threadIdx.x == 0) nheavy = 0;
+// act; *n_next = their count.  Keeping the order keeps a list sorted by work
+// sorted from one iteration to the next.  One block; per batch every thread
+// loads kCompactR elements strided by the block size (coalesced, all loads
+// in flight), the kept ones are placed by warp ballots and one scan of the
+// (round, warp) totals.
+constexpr int kCompactNT = 1024, kCompactR = 16;
+__global__ void __launch_bounds__(kCompactNT) compact_kept_kernel(const int32_t* act, const int32_t* n_act,
+                                                                  int64_t n_fixed, const int8_t* keep,
+                                                                  int32_t* act_next, int32_t* n_next,
+                                                                  const int32_t* wkey, int32_t thr,
+                                                                  int32_t* n_heavy_next) {
+    __shared__ int wtot[kCompactR][32];
+    __shared__ int batch_total;
     const int64_t n = n_act ? (int64_t)*n_act : n_fixed;
-    const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, w = t >> 5;
-    const int64_t per = (n + nt - 1) / nt;
-    const int64_t a = min(n, (int64_t)t * per), b = min(n, a + per);
-    int c = 0;
-    for (int64_t i = a; i < b; ++i) c += keep[act[i]] != 0;
-    int incl = c;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    int base = 0, heavy = 0;
+    for (int64_t c0 = 0; c0 < n; c0 += (int64_t)kCompactNT * kCompactR) {
+        int32_t g[kCompactR];
+        unsigned bal[kCompactR];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    if (lane == 31) wsum[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-        const int v = lane < (nt >> 5) ? wsum[lane] : 0;
-        int iv = v;
+        for (int r = 0; r < kCompactR; ++r) {
+            const int64_t i = c0 + (int64_t)r * kCompactNT + t;
+            g[r] = i < n ? act[i] : -1;
+        }
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, iv, o);
-            if (lane >= o) iv += u;
+        for (int r = 0; r < kCompactR; ++r) {
+            const bool f = g[r] >= 0 && keep[g[r]] != 0;
+            bal[r] = __ballot_sync(0xffffffffu, f);
+            if (f && wkey) heavy += wkey[g[r]] >= thr;
+            if (lane == 0) wtot[r][w] = __popc(bal[r]);
         }
-        wsum[lane] = iv - v;
-    }
-    __syncthreads();
-    int pos = wsum[w] + incl - c;
-    int heavy = 0;
-    for (int64_t i = a; i < b; ++i) {
-        const int32_t g = act[i];
-        if (keep[g]) {
-            act_next[pos++] = g;
-            if (wkey) heavy += wkey[g] >= thr;
-        }
-    }
-    if (t == nt - 1) *n_next = pos;
-    if (wkey) {
-        if (heavy) atomicAdd(&nheavy, heavy);
         __syncthreads();
-        if (t == 0) *n_heavy_next = nheavy;
+        if (w == 0) {
+            // lane r: the exclusive offsets of round r's warps, after the
+            // rounds before it
+            int v = 0;
+            if (lane < kCompactR)
+                for (int q = 0; q < 32; ++q) v += wtot[lane][q];
+            int incl = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int x = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += x;
+            }
+            if (lane < kCompactR) {
+                int run = incl - v;
+                for (int q = 0; q < 32; ++q) {
+                    const int c = wtot[lane][q];
+                    wtot[lane][q] = run;
+                    run += c;
+                }
+            }
+            if (lane == 31) batch_total = incl;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kCompactR; ++r)
+            if (bal[r] >> lane & 1u) act_next[base + wtot[r][w] + __popc(bal[r] & lt)] = g[r];
+        base += batch_total;
+        __syncthreads();  // wtot and batch_total are rewritten by the next batch
+    }
+    if (t == 0) *n_next = base;
+    if (wkey) {
+        heavy = __reduce_add_sync(0xffffffffu, heavy);
+        if (lane == 0) wtot[0][w] = heavy;
+        __syncthreads();
+        if (t == 0) {
+            int h = 0;
+            for (int q = 0; q < kCompactNT / 32; ++q) h += wtot[0][q];
+            *n_heavy_next = h;
+        }
     }
 }
 cudaError_t launch_compact_kept(const int32_t* act, const int32_t* n_act, int64_t n_fixed, const int8_t* keep,
                                 int32_t* act_next, int32_t* n_next, cudaStream_t st, const int32_t* wkey,
                                 int32_t thr, int32_t* n_heavy_next) {
-    compact_kept_kernel<<<1, 1024, 0, st>>>(act, n_act, n_fixed, keep, act_next, n_next, wkey, thr,
-                                            n_heavy_next);
+    compact_kept_kernel<<<1, kCompactNT, 0, st>>>(act, n_act, n_fixed, keep, act_next, n_next, wkey, thr,
+                                                  n_heavy_next);
     return cudaGetLastError();
 }
 // *out = the number of leading entries of key (descending) that are >= thr
