@@ -936,21 +936,37 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
         constexpr int LW = 8, LUNR = 3, LRW = LW * LUNR;
         const int sub = lane / LW, sl = lane % LW;
         const int nlight = nact - nheavy;
-        while (true) {
+        // a batch of four: each eight lanes' gene (j = -1: none); `any`: the
+        // batch has one (warp-uniform).  The next batch's loads are in flight
+        // while this one runs.
+        auto ltake = [&](bool& any) -> SlItem {
             int k0 = 0;
             if (lane == 0) k0 = atomicAdd(&next_l, 32 / LW);
             k0 = __shfl_sync(0xffffffffu, k0, 0);
-            if (y + k0 * T >= nlight) break;  // (warp-uniform)
+            any = y + k0 * T < nlight;
             const int jl = y + (k0 + sub) * T;
-            const bool valid = jl < nlight;
-            const int j = nheavy + (valid ? jl : 0);
+            SlItem it{jl < nlight ? nheavy + jl : -1, 0, 0.0, 0, 0};
+            if (it.j >= 0) {
+                it.g = __ldg(geo.act + it.j);
+                it.A = __ldg(geo.rowexp + (int64_t)it.j * U + u);
+                it.e0 = __ldg(geo.gptr + (int64_t)it.g * (S + 1) + s);
+                it.e1 = __ldg(geo.gptr + (int64_t)it.g * (S + 1) + s + 1);
+            }
+            return it;
+        };
+        bool any = false;
+        SlItem cur = ltake(any);
+        while (any) {
+            bool any_nx = false;
+            const SlItem nx = ltake(any_nx);
+            const bool valid = cur.j >= 0;
+            const int j = cur.j;
             Acc acc;
             acc.zero();
             if (valid) {
-                const int g = __ldg(geo.act + j);
-                const double A = __ldg(geo.rowexp + (int64_t)j * U + u);
-                const int64_t e0 = __ldg(geo.gptr + (int64_t)g * (S + 1) + s);
-                const int64_t e1 = __ldg(geo.gptr + (int64_t)g * (S + 1) + s + 1);
+                const int g = cur.g;
+                const double A = cur.A;
+                const int64_t e0 = cur.e0, e1 = cur.e1;
                 const typename Pass::Gene gpar = Pass::load(prm, g);
                 for (int jr = sl; jr < m; jr += LW) {
                     acc.q = __ldg(geo.rw + (int64_t)u * kRuleCap + jr);
@@ -987,6 +1003,8 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
 #pragma unroll
                 for (int i = 0; i < NS; ++i) o[NWV + i] = acc.s[i];
             }
+            cur = nx;
+            any = any_nx;
         }
     }
 }

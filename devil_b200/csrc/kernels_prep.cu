@@ -258,10 +258,82 @@ __global__ void gene_stats_kernel(const int64_t* rowptr, const VT* val, int64_t 
         o[5] = (double)(e1 - e0);
     }
 }
+// The same statistics for uint16 counts whose array starts on a 16-byte
+// boundary: warp per gene, the row read as 16-byte pieces of eight counts
+// (four pieces in flight per lane), pieces that straddle the row's ends
+// masked, the last piece of the array (which may end past nnz) read count
+// by count.  Exact integer sums, as above.
+__global__ void gene_stats_u16v_kernel(const int64_t* rowptr, const uint16_t* val, int64_t G, int64_t n,
+                                       double* stats) {
+    const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (g >= G) return;
+    const int64_t e0 = rowptr[g], e1 = rowptr[g + 1], nnz = rowptr[G];
+    const int64_t p0 = e0 >> 3, p1 = (e1 + 7) >> 3, pfull = nnz >> 3;
+    const uint4* v4 = reinterpret_cast<const uint4*>(val);
+    unsigned long long s1 = 0, s2 = 0;
+    unsigned mx = 0;
+    constexpr int U = 4;
+    for (int64_t base = p0 + lane; base < p1; base += 32 * U) {
+        uint4 pc[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t pp = base + 32 * u;
+            pc[u] = make_uint4(0, 0, 0, 0);
+            if (pp < p1) {
+                if (pp < pfull) {
+                    pc[u] = __ldg(v4 + pp);
+                } else {
+                    uint16_t h[8];
+#pragma unroll
+                    for (int r = 0; r < 8; ++r) h[r] = pp * 8 + r < nnz ? val[pp * 8 + r] : (uint16_t)0;
+                    pc[u] = make_uint4(h[0] | (unsigned)h[1] << 16, h[2] | (unsigned)h[3] << 16,
+                                       h[4] | (unsigned)h[5] << 16, h[6] | (unsigned)h[7] << 16);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t pp = base + 32 * u;
+            if (pp >= p1) continue;
+            const int64_t ea = pp * 8;
+            const unsigned w[4] = {pc[u].x, pc[u].y, pc[u].z, pc[u].w};
+            const bool whole = ea >= e0 && ea + 8 <= e1;
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const unsigned y = (w[r >> 1] >> (16 * (r & 1))) & 0xffffu;
+                if (whole || (ea + r >= e0 && ea + r < e1)) {
+                    s1 += y;
+                    s2 += (unsigned long long)(y * y);
+                    mx = max(mx, y);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) {
+        s1 += __shfl_xor_sync(0xffffffffu, s1, sh);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, sh);
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, sh));
+    }
+    if (lane == 0) {
+        double* o = stats + g * 6;
+        const __int128 num = (__int128)n * (__int128)s2 - (__int128)s1 * (__int128)s1;
+        o[0] = (double)s1 / (double)n;
+        o[1] = (double)num / ((double)n * (double)(n - 1));
+        o[2] = (double)s1;
+        o[3] = (double)(s2 - s1);
+        o[4] = (double)mx;
+        o[5] = (double)(e1 - e0);
+    }
+}
+
 cudaError_t launch_gene_stats(const int64_t* rowptr, const void* val, int val_u16, int64_t G,
                               int64_t n, double* stats, cudaStream_t st) {
     if (G == 0) return cudaSuccess;
-    if (val_u16)
+    if (val_u16 && (reinterpret_cast<uintptr_t>(val) & 15) == 0)
+        gene_stats_u16v_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, (const uint16_t*)val, G, n, stats);
+    else if (val_u16)
         gene_stats_kernel<uint16_t><<<nblk(G, 8), 256, 0, st>>>(rowptr, (const uint16_t*)val, G, n, stats);
     else
         gene_stats_kernel<float><<<nblk(G, 8), 256, 0, st>>>(rowptr, (const float*)val, G, n, stats);
@@ -667,10 +739,78 @@ __global__ void validate_csr_kernel(const int64_t* rowptr, const int32_t* col, i
     if (lane == 0 && b) atomicOr(bad, 1);
     if (g == G - 1 && lane == 0 && e1 != nnz) atomicOr(bad, 1);
 }
+// The same checks for a cell-index array that starts on a 16-byte boundary:
+// the row read as 16-byte pieces of four indices (four in flight per lane),
+// each index compared with the one before it in the row (the previous
+// piece's last index comes from the lane before, or from the previous
+// round's last lane); the array's last piece, which may end past nnz, is
+// read index by index.
+__global__ void validate_csr_v_kernel(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
+                                      int64_t nnz, int32_t* bad) {
+    const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (g >= G) return;
+    const int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
+    int b = 0;
+    if (e0 < 0 || e1 < e0 || e1 > nnz) {
+        b = 1;
+    } else {
+        const int64_t p0 = e0 >> 2, p1 = (e1 + 3) >> 2, pfull = nnz >> 2;
+        const int4* c4 = reinterpret_cast<const int4*>(col);
+        constexpr int U = 4;
+        int carry = -1;  // the last index of the previous round (-1: none; indices are >= 0)
+        for (int64_t base = p0; base < p1; base += 32 * U) {
+            int4 pc[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int64_t pp = base + 32 * u + lane;
+                pc[u] = make_int4(-1, -1, -1, -1);
+                if (pp < p1) {
+                    if (pp < pfull) {
+                        pc[u] = __ldg(c4 + pp);
+                    } else {
+                        int h[4];
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) h[r] = pp * 4 + r < nnz ? col[pp * 4 + r] : -1;
+                        pc[u] = make_int4(h[0], h[1], h[2], h[3]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int64_t pp = base + 32 * u + lane;
+                // the index before this piece: the previous lane's last, or
+                // (lane 0) the last of round u - 1, or of the previous round
+                int before = __shfl_up_sync(0xffffffffu, pc[u].w, 1);
+                const int last_prev = u > 0 ? __shfl_sync(0xffffffffu, pc[u > 0 ? u - 1 : 0].w, 31) : carry;
+                if (lane == 0) before = last_prev;
+                if (pp < p1) {
+                    const int c[4] = {pc[u].x, pc[u].y, pc[u].z, pc[u].w};
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const int64_t e = pp * 4 + r;
+                        if (e >= e0 && e < e1) {
+                            if (c[r] < 0 || c[r] >= n) b = 1;
+                            const int prv = r == 0 ? before : c[r - 1];
+                            if (e > e0 && prv >= c[r]) b = 1;
+                        }
+                    }
+                }
+            }
+            carry = __shfl_sync(0xffffffffu, pc[U - 1].w, 31);
+        }
+    }
+    b = __any_sync(0xffffffffu, b);
+    if (lane == 0 && b) atomicOr(bad, 1);
+    if (g == G - 1 && lane == 0 && e1 != nnz) atomicOr(bad, 1);
+}
 cudaError_t launch_validate_csr(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
                                 int64_t nnz, int32_t* bad, cudaStream_t st) {
     if (G == 0) return cudaSuccess;
-    validate_csr_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, col, G, n, nnz, bad);
+    if ((reinterpret_cast<uintptr_t>(col) & 15) == 0)
+        validate_csr_v_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, col, G, n, nnz, bad);
+    else
+        validate_csr_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, col, G, n, nnz, bad);
     return cudaGetLastError();
 }
 
