@@ -1500,9 +1500,13 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     LAUNCH(launch_set_i32(cnt + 1, 0, st));
     // slice-major passes: the active genes stay in decreasing order of entries
     const bool ordered = plan.engine == ENGINE_GRP && (ctx->grp_slices & 2);
+    // (and those below kLightEntries entries per slice take eight lanes each)
+    int32_t* nheavy = ws<int32_t>(ctx, "cnt_heavy", 2);
+    const int32_t thr = ordered ? (int32_t)std::min<int64_t>((int64_t)kLightEntries * dp.grp.S, INT32_MAX) : 0;
     if (ordered) s.keep = ws<int8_t>(ctx, "keep", G);
     LAUNCH(launch_mle_init(dp.stats, G, dp.n, s, act[0], cnt, st));
-    if (ordered) LAUNCH(launch_compact_kept(dp.grp.order, nullptr, G, s.keep, act[0], cnt, st));
+    if (ordered)
+        LAUNCH(launch_compact_kept(dp.grp.order, nullptr, G, s.keep, act[0], cnt, st, dp.grp.wkey, thr, nheavy));
     PassParamsAny prm{beta_f, beta_d, nullptr, s.x, nullptr};
     plan = autotune(ctx, dp, plan, act[0], cnt, G, prm, form);
     PassBuffers pb = pass_buffers(ctx, PASS_MLE, dp.P, max_slot_segs(ctx, dp, plan, form));
@@ -1519,7 +1523,8 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
         launch_pass(ctx, dp, PASS_MLE, plan, nseg, tiles, dp.fine_bound,
-                    dp.fine_ptr, dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm);
+                    dp.fine_ptr, dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm, 0,
+                    ordered ? nheavy + cur : nullptr);
         ++launched;
         const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC && plan.engine != ENGINE_TCW;
         // the exclusive-column (one-hot) structure of a grouped design
@@ -1529,7 +1534,9 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
                                    act[cur], cnt + cur, (int)hint, act[nxt], cnt + nxt, s, max_iter,
                                    cox_reid, nullptr, st, structured ? dp.grp.nA : 0,
                                    structured ? dp.grp.colA : nullptr, structured ? dp.grp.colD : nullptr));
-        if (ordered) LAUNCH(launch_compact_kept(act[cur], cnt + cur, 0, s.keep, act[nxt], cnt + nxt, st));
+        if (ordered)
+            LAUNCH(launch_compact_kept(act[cur], cnt + cur, 0, s.keep, act[nxt], cnt + nxt, st, dp.grp.wkey, thr,
+                                       nheavy + nxt));
         LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));

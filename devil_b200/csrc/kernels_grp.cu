@@ -812,11 +812,13 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
     // per warp: the psi tables of its current gene (passes with TABLES)
     double* wtab = Es + kSliceCells + warp * kGrpTab;
-    // (beta_0's pass takes 1/exp(offset): a product per entry, not a quotient)
-    constexpr bool kRecip = std::is_same<Pass, PassInitZ>::value;
+    // beta_0's pass stages log1p(1 / exp(offset)) instead: its term for a
+    // count of 1 (two thirds of the nonzeros of sparse single-cell counts),
+    // the same expression as PassInitZ::sparse
+    constexpr bool kInitZ = std::is_same<Pass, PassInitZ>::value;
     for (int i = t; i < nc; i += blockDim.x) {
         const double e = __ldg(geo.E + c0 + i);
-        Es[i] = kRecip ? 1.0 / e : e;
+        Es[i] = kInitZ ? log1p(1.0 / e) : e;
     }
     const int u = __ldg(geo.sl_key + s) / geo.C;
     const bool first = s == __ldg(geo.kslice + u * geo.C);  // the group's rule goes here
@@ -889,19 +891,28 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
             if (lane == 0) o[NWV + i] = v;
         }
     };
+    // one entry: the pass's nonzero term (beta_0: the staged term for y = 1,
+    // else log1p(y / exp(offset)) with exp(offset) from L2)
+    auto entry = [&](const ET c, const typename Pass::Gene& gpar, double A, Acc& acc) {
+        if constexpr (kInitZ) {
+            const float y = Ent::y(c);
+            const int loc = Ent::loc(c);
+            acc.s[0] += y == 1.f ? Es[loc] : log1p((double)y / __ldg(geo.E + c0 + loc));
+        } else {
+            Pass::template sparse<double>(gpar, A * Es[Ent::loc(c)], Ent::y(c), acc);
+        }
+    };
     // the entries of one 16-byte piece (first entry ea) inside [e0, e1)
     auto piece = [&](const uint4& v, int64_t ea, int64_t e0, int64_t e1, const typename Pass::Gene& gpar,
                      double A, Acc& acc) {
         const ET* c = reinterpret_cast<const ET*>(&v);
         if (ea >= e0 && ea + EPL <= e1) {  // a whole piece inside the range
 #pragma unroll
-            for (int rr = 0; rr < EPL; ++rr)
-                Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[rr])], Ent::y(c[rr]), acc);
+            for (int rr = 0; rr < EPL; ++rr) entry(c[rr], gpar, A, acc);
         } else {
 #pragma unroll
             for (int rr = 0; rr < EPL; ++rr)
-                if (ea + rr >= e0 && ea + rr < e1)
-                    Pass::template sparse<double>(gpar, A * Es[Ent::loc(c[rr])], Ent::y(c[rr]), acc);
+                if (ea + rr >= e0 && ea + rr < e1) entry(c[rr], gpar, A, acc);
         }
     };
     {
@@ -930,10 +941,11 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
             if constexpr (Pass::TABLES) __syncwarp();  // the table slot is rewritten next
         }
     }
-    if constexpr (!Pass::TABLES) {
+    {
         // the light genes: four per warp, eight lanes each (the per-gene
-        // bookkeeping is shared by four genes), loads straight to registers
-        constexpr int LW = 8, LUNR = 3, LRW = LW * LUNR;
+        // bookkeeping is shared by four genes), loads straight to registers;
+        // their psi tables (passes with TABLES) are read from L2
+        constexpr int LW = 8, LUNR = Pass::TABLES ? 1 : UNR, LRW = LW * LUNR;
         const int sub = lane / LW, sl = lane % LW;
         const int nlight = nact - nheavy;
         // a batch of four: each eight lanes' gene (j = -1: none); `any`: the
@@ -967,7 +979,14 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
                 const int g = cur.g;
                 const double A = cur.A;
                 const int64_t e0 = cur.e0, e1 = cur.e1;
-                const typename Pass::Gene gpar = Pass::load(prm, g);
+                typename Pass::Gene gpar = Pass::load(prm, g);
+                if constexpr (Pass::TABLES) {
+                    const double* src = geo.psitab + (int64_t)j * kGrpTab;
+                    gpar.tab.d1 = src;
+                    gpar.tab.d2 = src + kPsiTab;
+                    gpar.tab.pa = __ldg(src + 2 * kPsiTab);
+                    gpar.tab.ta = __ldg(src + 2 * kPsiTab + 1);
+                }
                 for (int jr = sl; jr < m; jr += LW) {
                     acc.q = __ldg(geo.rw + (int64_t)u * kRuleCap + jr);
                     Pass::template dense<double>(gpar, A * __ldg(geo.res + (int64_t)u * kRuleCap + jr), acc);

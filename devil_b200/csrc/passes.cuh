@@ -408,12 +408,9 @@ struct PassInitZ {
     static DEV Gene load(const Params&, int) { return Gene{0}; }
     template <class R, class A>
     static DEV void dense(const Gene&, R, A&) {}
-    // (the slice-major pass stages 1/exp(offset) for this pass: its "mu"
-    // argument is 1/mu, and y/mu a product; one rounding more than the
-    // quotient, 2 ulp at most in the argument of log1p)
     template <class R, class A>
-    static DEV void sparse(const Gene&, R rmu, float y, A& acc) {
-        acc.template scal<0>(log1p((double)y * (double)rmu));
+    static DEV void sparse(const Gene&, R mu, float y, A& acc) {
+        acc.template scal<0>(log1p((double)y / (double)mu));
     }
 };
 
