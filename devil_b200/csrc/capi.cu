@@ -89,8 +89,9 @@ struct devil_ctx {
     std::string err;
     int64_t launches = 0;
     std::map<std::string, DevBuf> bufs;
-    int32_t* mapped_host = nullptr;   // pinned, mapped: active-gene count mirror
-    int32_t* mapped_dev = nullptr;
+    int32_t* mapped_host = nullptr;   // pinned, mapped: active-gene count mirrors, one slot per
+    int32_t* mapped_dev = nullptr;    // loop iteration mod 4
+    int64_t mapped_host_at(int t) const { return *(volatile int32_t*)(mapped_host + (t & 3)); }
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int sm_count = 148;
     int use_tma = 0;
@@ -1341,14 +1342,16 @@ int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan0, d
     if (sliced) LAUNCH(launch_count_at_least(dp.grp.skey, n0, thr, nheavy, st));
     // copies of an earlier loop still in flight would overwrite the mirror
     CK(cudaStreamSynchronize(st));
-    *ctx->mapped_host = (int32_t)n0;
     const int LAG = 2;
     int64_t launched = 0;
     for (int t = 0; t < max_iter; ++t) {
         const int cur = t & 1, nxt = cur ^ 1;
-        // active-gene count of LAG iterations ago (an upper bound: blocks
-        // beyond the current count exit at once)
-        const int64_t hint = t == 0 ? n0 : *(volatile int32_t*)ctx->mapped_host;
+        // active-gene count after iteration t - 1 - LAG, the last one the
+        // host has waited for (an upper bound: blocks beyond the current
+        // count exit at once).  Each iteration mirrors its count into its own
+        // slot, so the grid sizes -- and the segment sums they set -- do not
+        // depend on how far the device has run ahead.
+        const int64_t hint = t <= LAG ? n0 : ctx->mapped_host_at(t - 1 - LAG);
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
@@ -1374,7 +1377,7 @@ int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan0, d
                                         cnt + cur, (int)hint, act[nxt], cnt + nxt, beta, beta_f,
                                         iters, status, max_iter, eps, k, st));
         }
-        LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
+        LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev + (t & 3), st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
     }
@@ -1512,13 +1515,13 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     PassBuffers pb = pass_buffers(ctx, PASS_MLE, dp.P, max_slot_segs(ctx, dp, plan, form));
     // copies of an earlier loop still in flight would overwrite the mirror
     CK(cudaStreamSynchronize(st));
-    *ctx->mapped_host = (int32_t)G;
     const int LAG = 2;
     int64_t launched = 0;
     // one far-left evaluation plus at most max_iter Newton evaluations
     for (int t = 0; t <= max_iter; ++t) {
         const int cur = t & 1, nxt = cur ^ 1;
-        const int64_t hint = t == 0 ? G : *(volatile int32_t*)ctx->mapped_host;
+        // (the count after iteration t - 1 - LAG, as in irls_loop)
+        const int64_t hint = t <= LAG ? G : ctx->mapped_host_at(t - 1 - LAG);
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
@@ -1537,7 +1540,7 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
         if (ordered)
             LAUNCH(launch_compact_kept(act[cur], cnt + cur, 0, s.keep, act[nxt], cnt + nxt, st, dp.grp.wkey, thr,
                                        nheavy + nxt));
-        LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev, st));
+        LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev + (t & 3), st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
     }

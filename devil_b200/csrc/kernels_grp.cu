@@ -756,6 +756,7 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
 // grp_assemble_kernel / the IRLS step form the p x p terms per gene.
 // ---------------------------------------------------------------------
 constexpr int kSlNT = 1024;  // one block per SM: 32 warps, 64 registers each, the 128 KB slice stage
+static_assert(kSliceCells % kSlNT == 0, "a slice is staged in whole rounds of the block");
 
 // 16-byte loads in flight per lane: as many as 64 registers hold (the
 // MLE's accumulators take more registers)
@@ -816,9 +817,21 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
     // count of 1 (two thirds of the nonzeros of sparse single-cell counts),
     // the same expression as PassInitZ::sparse
     constexpr bool kInitZ = std::is_same<Pass, PassInitZ>::value;
-    for (int i = t; i < nc; i += blockDim.x) {
-        const double e = __ldg(geo.E + c0 + i);
-        Es[i] = kInitZ ? log1p(1.0 / e) : e;
+    {
+        // every thread's kSliceCells / kSlNT loads in flight at once (a loop
+        // of dependent L2 round trips would hold the block for microseconds)
+        constexpr int K = kSliceCells / kSlNT;
+        double e[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int i = t + k * kSlNT;
+            e[k] = i < nc ? __ldg(geo.E + c0 + i) : 1.0;
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int i = t + k * kSlNT;
+            if (i < nc) Es[i] = kInitZ ? log1p(1.0 / e[k]) : e[k];
+        }
     }
     const int u = __ldg(geo.sl_key + s) / geo.C;
     const bool first = s == __ldg(geo.kslice + u * geo.C);  // the group's rule goes here
