@@ -765,7 +765,8 @@ constexpr int sl_unr() { return Pass::TABLES ? 2 : 3; }
 
 template <class Pass>
 constexpr size_t sl_smem_bytes() {
-    return (size_t)kSliceCells * sizeof(double) + (Pass::TABLES ? (size_t)(kSlNT / 32) * kGrpTab * sizeof(double) : 0);
+    return (size_t)kSliceCells * sizeof(double) + (Pass::TABLES ? (size_t)(kSlNT / 32) * kGrpTab * sizeof(double) : 0) +
+           (size_t)2 * kRuleCap * sizeof(double);
 }
 
 // streaming 16-byte load that does not allocate in L1 (each entry is read
@@ -837,6 +838,13 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
     const bool first = s == __ldg(geo.kslice + u * geo.C);  // the group's rule goes here
     constexpr bool kRule = !std::is_same<Pass, PassInitZ>::value;  // zero counts contribute
     const int m = (kRule && first) ? __ldg(geo.rm + u) : 0;
+    // the group's rule (node weights, exp(node offsets)) in shared memory:
+    // every gene of the block evaluates it
+    double* rule = Es + kSliceCells + (Pass::TABLES ? nw * kGrpTab : 0);
+    for (int j = t; j < m; j += blockDim.x) {
+        rule[j] = __ldg(geo.rw + (int64_t)u * kRuleCap + j);
+        rule[kRuleCap + j] = __ldg(geo.res + (int64_t)u * kRuleCap + j);
+    }
     const uint4* __restrict__ v4 = static_cast<const uint4*>(geo.gent);
     // the block's genes are handed out one at a time (a shared counter), so
     // warps that drew short genes take more of them
@@ -877,8 +885,8 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
         }
         acc.zero();
         for (int j = lane; j < m; j += 32) {
-            acc.q = __ldg(geo.rw + (int64_t)u * kRuleCap + j);
-            Pass::template dense<double>(gpar, it.A * __ldg(geo.res + (int64_t)u * kRuleCap + j), acc);
+            acc.q = rule[j];
+            Pass::template dense<double>(gpar, it.A * rule[kRuleCap + j], acc);
         }
         acc.q = 1.0;
         o = geo.gsum + ((int64_t)it.j * S + s) * NQ;
@@ -1001,8 +1009,8 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
                     gpar.tab.ta = __ldg(src + 2 * kPsiTab + 1);
                 }
                 for (int jr = sl; jr < m; jr += LW) {
-                    acc.q = __ldg(geo.rw + (int64_t)u * kRuleCap + jr);
-                    Pass::template dense<double>(gpar, A * __ldg(geo.res + (int64_t)u * kRuleCap + jr), acc);
+                    acc.q = rule[jr];
+                    Pass::template dense<double>(gpar, A * rule[kRuleCap + jr], acc);
                 }
                 acc.q = 1.0;
                 const int64_t b0 = e0 / EPL;
