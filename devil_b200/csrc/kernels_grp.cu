@@ -919,21 +919,26 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
             const float y = Ent::y(c);
             const int loc = Ent::loc(c);
             acc.s[0] += y == 1.f ? Es[loc] : log1p((double)y / __ldg(geo.E + c0 + loc));
+        } else if constexpr (std::is_same<VT, uint16_t>::value) {
+            // (a 16-bit count converts to FP64 exactly, in one step)
+            Pass::template sparse<double>(gpar, A * Es[Ent::loc(c)], (double)(c >> 16), acc);
         } else {
             Pass::template sparse<double>(gpar, A * Es[Ent::loc(c)], Ent::y(c), acc);
         }
     };
-    // the entries of one 16-byte piece (first entry ea) inside [e0, e1)
-    auto piece = [&](const uint4& v, int64_t ea, int64_t e0, int64_t e1, const typename Pass::Gene& gpar,
-                     double A, Acc& acc) {
+    // the entries of one 16-byte piece inside the gene's range; positions
+    // relative to the first entry of the gene's first piece: the piece
+    // starts at ea, the range is [lo, hi)
+    auto piece = [&](const uint4& v, int ea, int lo, int hi, const typename Pass::Gene& gpar, double A,
+                     Acc& acc) {
         const ET* c = reinterpret_cast<const ET*>(&v);
-        if (ea >= e0 && ea + EPL <= e1) {  // a whole piece inside the range
+        if (ea >= lo && ea + EPL <= hi) {  // a whole piece inside the range
 #pragma unroll
             for (int rr = 0; rr < EPL; ++rr) entry(c[rr], gpar, A, acc);
         } else {
 #pragma unroll
             for (int rr = 0; rr < EPL; ++rr)
-                if (ea + rr >= e0 && ea + rr < e1) entry(c[rr], gpar, A, acc);
+                if (ea + rr >= lo && ea + rr < hi) entry(c[rr], gpar, A, acc);
         }
     };
     {
@@ -948,6 +953,7 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
             gene_start(cur, gpar, acc, o);
             const int64_t b0 = cur.e0 / EPL;
             const int nb = (int)((cur.e1 + EPL - 1) / EPL - b0);
+            const int lo = (int)(cur.e0 - b0 * EPL), hi = (int)(cur.e1 - b0 * EPL);
             for (int base = lane; base < nb; base += RW) {
                 uint4 v[UNR];
 #pragma unroll
@@ -955,7 +961,7 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
                     if (base + 32 * q < nb) v[q] = ld_stream(v4 + b0 + base + 32 * q);
 #pragma unroll
                 for (int q = 0; q < UNR; ++q)
-                    if (base + 32 * q < nb) piece(v[q], (b0 + base + 32 * q) * EPL, cur.e0, cur.e1, gpar, cur.A, acc);
+                    if (base + 32 * q < nb) piece(v[q], (base + 32 * q) * EPL, lo, hi, gpar, cur.A, acc);
             }
             gene_end(acc, o);
             cur = nx;
@@ -1015,6 +1021,7 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
                 acc.q = 1.0;
                 const int64_t b0 = e0 / EPL;
                 const int nb = (int)((e1 + EPL - 1) / EPL - b0);
+                const int lo = (int)(e0 - b0 * EPL), hi = (int)(e1 - b0 * EPL);
                 for (int base = sl; base < nb; base += LRW) {
                     uint4 v[LUNR];
 #pragma unroll
@@ -1022,7 +1029,7 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
                         if (base + LW * q < nb) v[q] = ld_stream(v4 + b0 + base + LW * q);
 #pragma unroll
                     for (int q = 0; q < LUNR; ++q)
-                        if (base + LW * q < nb) piece(v[q], (b0 + base + LW * q) * EPL, e0, e1, gpar, A, acc);
+                        if (base + LW * q < nb) piece(v[q], (base + LW * q) * EPL, lo, hi, gpar, A, acc);
                 }
             }
             // sums over each gene's eight lanes

@@ -186,8 +186,9 @@ struct PassIRLS {
         acc.template outer<0>(r);
         acc.template vec<0, NW>(mu * r);
     }
-    template <class R, class A>
-    static DEV void sparse(const Gene& G, R mu, float y, A& acc) {
+    // (y: the count, float or -- from integer counts -- converted straight to R)
+    template <class R, class A, class Y>
+    static DEV void sparse(const Gene& G, R mu, Y y, A& acc) {
         R r = rcp_r(mu + (R)G.k);
         R yr = (R)y * r;
         acc.template outer<0>(yr * (R)G.rk);  // rk scales H only, not the score
@@ -376,8 +377,8 @@ struct PassMLE {
         acc.template fscal<0, NW, NV>(nb_ll_term<R>(x, r));
         acc.template fscal<1, NW, NV>(w * x * r);
     }
-    template <class R, class A>
-    static DEV void sparse(const Gene& G, R mu, float y, A& acc) {
+    template <class R, class A, class Y>
+    static DEV void sparse(const Gene& G, R mu, Y y, A& acc) {
         double m = mu, yy = y;
         double den = 1.0 + m * G.theta;
         // reciprocal: MUFU estimate refined by one FP64 Newton step
