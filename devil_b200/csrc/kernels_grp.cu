@@ -763,10 +763,15 @@ static_assert(kSliceCells % kSlNT == 0, "a slice is staged in whole rounds of th
 template <class Pass>
 constexpr int sl_unr() { return Pass::TABLES ? 2 : 3; }
 
+// beta_0's pass: per warp, a queue of the entries with counts above 1 (one
+// round adds at most 32 x 3 x 4 entries to fewer than 32 left over)
+constexpr int kInitQ = 416;
+
 template <class Pass>
 constexpr size_t sl_smem_bytes() {
     return (size_t)kSliceCells * sizeof(double) + (Pass::TABLES ? (size_t)(kSlNT / 32) * kGrpTab * sizeof(double) : 0) +
-           (size_t)2 * kRuleCap * sizeof(double);
+           (size_t)2 * kRuleCap * sizeof(double) +
+           (std::is_same<Pass, PassInitZ>::value ? (size_t)(kSlNT / 32) * kInitQ * sizeof(uint32_t) : 0);
 }
 
 // streaming 16-byte load that does not allocate in L1 (each entry is read
@@ -945,6 +950,65 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
         // entries loaded to registers, UNR pieces per lane in flight; the
         // next gene's range is loaded while this one runs
         SlItem cur = take();
+        if constexpr (kInitZ && std::is_same<VT, uint16_t>::value) {
+            // beta_0 on 16-bit counts: a count of 1 takes the staged term; the
+            // others are queued (warp ballots, in entry order) and evaluated
+            // 32 at a time, every lane on a log1p, instead of a divergent
+            // log1p path in nearly every entry position
+            static_assert(RW * EPL <= kInitQ - 32, "queue holds a round and a partial batch");
+            uint32_t* qbuf = reinterpret_cast<uint32_t*>(rule + 2 * kRuleCap) + warp * kInitQ;
+            const unsigned lt = (1u << lane) - 1u;
+            while (cur.j < nact) {
+                const SlItem nx = take();
+                typename Pass::Gene gpar;
+                Acc acc;
+                double* o;
+                gene_start(cur, gpar, acc, o);
+                const int64_t b0 = cur.e0 / EPL;
+                const int nb = (int)((cur.e1 + EPL - 1) / EPL - b0);
+                const int lo = (int)(cur.e0 - b0 * EPL), hi = (int)(cur.e1 - b0 * EPL);
+                int qn = 0;  // queued entries (warp-uniform)
+                auto drain = [&](bool all) {
+                    __syncwarp();
+                    while (qn >= 32 || (all && qn > 0)) {
+                        const int k = qn - 32 + lane;  // the newest 32, or all that are left
+                        if (k >= 0) {
+                            const uint32_t c = qbuf[k];
+                            acc.s[0] += log1p((double)(c >> 16) / __ldg(geo.E + c0 + (int)(c & 0xffffu)));
+                        }
+                        qn = qn > 32 ? qn - 32 : 0;
+                    }
+                    __syncwarp();
+                };
+                for (int b = 0; b < nb; b += RW) {
+                    const int base = b + lane;
+                    uint4 v[UNR];
+#pragma unroll
+                    for (int q = 0; q < UNR; ++q)
+                        v[q] = base + 32 * q < nb ? ld_stream(v4 + b0 + base + 32 * q) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+                    for (int q = 0; q < UNR; ++q) {
+                        const uint32_t* c = reinterpret_cast<const uint32_t*>(&v[q]);
+                        const int ea = (base + 32 * q) * EPL;
+                        const bool inb = base + 32 * q < nb;
+#pragma unroll
+                        for (int rr = 0; rr < EPL; ++rr) {
+                            const bool valid = inb && ea + rr >= lo && ea + rr < hi;
+                            const uint32_t y = c[rr] >> 16;
+                            if (valid && y == 1u) acc.s[0] += Es[c[rr] & 0xffffu];
+                            const bool slow = valid && y != 1u;
+                            const unsigned bal = __ballot_sync(0xffffffffu, slow);
+                            if (slow) qbuf[qn + __popc(bal & lt)] = c[rr];
+                            qn += __popc(bal);
+                        }
+                    }
+                    drain(false);
+                }
+                drain(true);
+                gene_end(acc, o);
+                cur = nx;
+            }
+        }
         while (cur.j < nact) {
             const SlItem nx = take();
             typename Pass::Gene gpar;
