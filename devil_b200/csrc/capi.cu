@@ -261,6 +261,13 @@ struct DevProblem {
     double* off = nullptr;
     float* off_f = nullptr;
     double* stats = nullptr;
+    // genes by decreasing entry count (sorted once per fit, right after the
+    // counts arrive): the order in which warp-per-gene kernels take the
+    // genes (the largest first, so they do not set the kernel's length) and
+    // the work order of the slice-major passes
+    int32_t* gorder = nullptr;
+    int32_t* gwkey = nullptr;  // [G] entries of every gene
+    int32_t* gskey = nullptr;  // [G] the same in gorder (descending)
     int nfine = 1;
     int32_t* fine_bound = nullptr;
     int64_t* fine_ptr = nullptr;
@@ -308,10 +315,30 @@ void check_counts(devil_ctx* ctx, const devil_counts* c) {
 }
 
 // every kernel indexes the design with CSR cell indices: check them first
-void validate_csr(devil_ctx* ctx, const DevProblem& dp) {
+void gene_order(devil_ctx* ctx, DevProblem& dp) {
+    cudaStream_t st = ctx->stream;
+    const int64_t G = dp.G;
+    dp.gorder = dp.gwkey = dp.gskey = nullptr;
+    if (G <= 0) return;
+    int32_t* idx = ws<int32_t>(ctx, "ord_idx", G);
+    dp.gwkey = ws<int32_t>(ctx, "ord_key", G);
+    dp.gskey = ws<int32_t>(ctx, "ord_key_sorted", G);
+    dp.gorder = ws<int32_t>(ctx, "ord_genes", G);
+    // (row lengths clamped to [0, INT32_MAX]: a malformed row pointer gives a
+    // meaningless order, and the check below rejects the call)
+    LAUNCH(launch_gene_entries(dp.rowptr, G, dp.gwkey, idx, st));
+    size_t ob = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, ob, dp.gwkey, dp.gskey, idx, dp.gorder, (int)G);
+    CK(cub::DeviceRadixSort::SortPairsDescending(ws<char>(ctx, "ord_tmp", ob), ob, dp.gwkey, dp.gskey, idx,
+                                                 dp.gorder, (int)G, 0, 32, st));
+    ctx->launches++;
+}
+
+void validate_csr(devil_ctx* ctx, DevProblem& dp) {
+    gene_order(ctx, dp);
     int32_t* bad = ws<int32_t>(ctx, "csr_bad", 1);
     CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), ctx->stream));
-    LAUNCH(launch_validate_csr(dp.rowptr, dp.col, dp.G, dp.n, dp.nnz, bad, ctx->stream));
+    LAUNCH(launch_validate_csr(dp.rowptr, dp.col, dp.G, dp.n, dp.nnz, bad, ctx->stream, dp.gorder));
     int32_t h = 0;
     CK(cudaMemcpyAsync(&h, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -476,7 +503,7 @@ void prepare_design(devil_ctx* ctx, DevProblem& dp, const double* X, int P, bool
     dp.fine_ptr = ws<int64_t>(ctx, "fine_ptr", (size_t)dp.G * (nf + 1));
     LAUNCH(launch_segptr(dp.rowptr, dp.col, dp.G, dp.fine_bound, nf + 1, dp.fine_ptr, st));
     dp.stats = ws<double>(ctx, "stats", (size_t)dp.G * 6);
-    LAUNCH(launch_gene_stats(dp.rowptr, dp.val, dp.val_u16, dp.G, dp.n, dp.stats, st));
+    LAUNCH(launch_gene_stats(dp.rowptr, dp.val, dp.val_u16, dp.G, dp.n, dp.stats, st, dp.gorder));
     CK(cudaStreamSynchronize(st));  // host copies above must stay valid until here
 }
 
@@ -862,22 +889,13 @@ void build_groups(devil_ctx* ctx, DevProblem& dp, const int32_t* ends_host, int 
         g.need_d = up_i("grp_need_d", need_d);
     }
     g.res = res;
-    {
-        // the work order of the slice-major passes: genes by decreasing entries
-        const int64_t G = dp.G;
-        int32_t* key = ws<int32_t>(ctx, "grp_ord_key", G);
-        int32_t* key2 = ws<int32_t>(ctx, "grp_ord_key2", G);
-        int32_t* idx = ws<int32_t>(ctx, "grp_ord_idx", G);
-        g.order = ws<int32_t>(ctx, "grp_order", G);
-        LAUNCH(launch_gene_entries(dp.rowptr, G, key, idx, st));
-        size_t ob = 0;
-        cub::DeviceRadixSort::SortPairsDescending(nullptr, ob, key, key2, idx, g.order, (int)G);
-        CK(cub::DeviceRadixSort::SortPairsDescending(ws<char>(ctx, "grp_ord_tmp", ob), ob, key, key2, idx,
-                                                     g.order, (int)G, 0, 32, st));
-        ctx->launches++;
-        g.wkey = key;
-        g.skey = key2;
-    }
+    // the work order of the slice-major passes: genes by decreasing entries
+    // (sorted with the CSR check; counts converted from dense or CSC input
+    // are sorted here)
+    if (!dp.gorder) gene_order(ctx, dp);
+    g.order = dp.gorder;
+    g.wkey = dp.gwkey;
+    g.skey = dp.gskey;
     CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
     g.active = true;
     g.U = U;

@@ -301,8 +301,11 @@ cudaError_t launch_x_rowmajor(const double* Xcm, int64_t n, int P, int xs, float
 cudaError_t launch_x_rowmajor_d(const double* Xcm, int64_t n, int P, int xs, double* Xrm,
                                 cudaStream_t st);
 cudaError_t launch_double_to_float(const double* in, float* out, int64_t m, cudaStream_t st);
+// (order: the genes in the order the warps take them, largest first; null:
+// gene order)
 cudaError_t launch_gene_stats(const int64_t* rowptr, const void* val, int val_u16, int64_t G,
-                              int64_t n, double* stats /* G x 6 */, cudaStream_t st);
+                              int64_t n, double* stats /* G x 6 */, cudaStream_t st,
+                              const int32_t* order = nullptr);
 cudaError_t launch_colstats(const int64_t* rowptr, const int32_t* col, const void* val,
                             int val_u16, int64_t G, int64_t nnz, double* colsum,
                             double* collog, int32_t* colcnt, int32_t* colmin_bits,
@@ -327,7 +330,7 @@ cudaError_t launch_init_beta(const int64_t* rowptr, const int32_t* col, const vo
 cudaError_t launch_segptr(const int64_t* rowptr, const int32_t* col, int64_t G,
                           const int32_t* bound, int nbound, int64_t* segptr, cudaStream_t st);
 cudaError_t launch_validate_csr(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
-                                int64_t nnz, int32_t* bad, cudaStream_t st);
+                                int64_t nnz, int32_t* bad, cudaStream_t st, const int32_t* order = nullptr);
 cudaError_t launch_iota(int32_t* a, int64_t m, cudaStream_t st);
 cudaError_t launch_pass_volume(const int64_t* rowptr, const int32_t* passes, int64_t G,
                                int64_t* acc, cudaStream_t st);

@@ -174,10 +174,11 @@ cudaError_t launch_x_rowmajor_d(const double* Xcm, int64_t n, int P, int xs, dou
 // ------------------------------------------------------------------
 template <class VT>
 __global__ void gene_stats_kernel(const int64_t* rowptr, const VT* val, int64_t G, int64_t n,
-                                  double* stats) {
+                                  double* stats, const int32_t* order) {
     int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (g >= G) return;
+    if (order) g = order[g];
     const int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
     // Counts that are whole numbers (always for uint16; checked for float):
     // one pass with exact integer sums of y and y^2 (below 2^64 for any int32
@@ -264,10 +265,11 @@ __global__ void gene_stats_kernel(const int64_t* rowptr, const VT* val, int64_t 
 // masked, the last piece of the array (which may end past nnz) read count
 // by count.  Exact integer sums, as above.
 __global__ void gene_stats_u16v_kernel(const int64_t* rowptr, const uint16_t* val, int64_t G, int64_t n,
-                                       double* stats) {
-    const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+                                       double* stats, const int32_t* order) {
+    int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (g >= G) return;
+    if (order) g = order[g];
     const int64_t e0 = rowptr[g], e1 = rowptr[g + 1], nnz = rowptr[G];
     const int64_t p0 = e0 >> 3, p1 = (e1 + 7) >> 3, pfull = nnz >> 3;
     const uint4* v4 = reinterpret_cast<const uint4*>(val);
@@ -329,14 +331,14 @@ __global__ void gene_stats_u16v_kernel(const int64_t* rowptr, const uint16_t* va
 }
 
 cudaError_t launch_gene_stats(const int64_t* rowptr, const void* val, int val_u16, int64_t G,
-                              int64_t n, double* stats, cudaStream_t st) {
+                              int64_t n, double* stats, cudaStream_t st, const int32_t* order) {
     if (G == 0) return cudaSuccess;
     if (val_u16 && (reinterpret_cast<uintptr_t>(val) & 15) == 0)
-        gene_stats_u16v_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, (const uint16_t*)val, G, n, stats);
+        gene_stats_u16v_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, (const uint16_t*)val, G, n, stats, order);
     else if (val_u16)
-        gene_stats_kernel<uint16_t><<<nblk(G, 8), 256, 0, st>>>(rowptr, (const uint16_t*)val, G, n, stats);
+        gene_stats_kernel<uint16_t><<<nblk(G, 8), 256, 0, st>>>(rowptr, (const uint16_t*)val, G, n, stats, order);
     else
-        gene_stats_kernel<float><<<nblk(G, 8), 256, 0, st>>>(rowptr, (const float*)val, G, n, stats);
+        gene_stats_kernel<float><<<nblk(G, 8), 256, 0, st>>>(rowptr, (const float*)val, G, n, stats, order);
     return cudaGetLastError();
 }
 
@@ -720,10 +722,11 @@ cudaError_t launch_segptr(const int64_t* rowptr, const int32_t* col, int64_t G,
 // CSR sanity (warp per gene): rowptr non-decreasing, cell indices in
 // [0, n) and strictly increasing within each row.  bad[0] != 0 on failure.
 __global__ void validate_csr_kernel(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
-                                    int64_t nnz, int32_t* bad) {
+                                    int64_t nnz, int32_t* bad, const int32_t* order) {
     int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (g >= G) return;
+    if (order) g = order[g];
     const int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
     int b = 0;
     if (e0 < 0 || e1 < e0 || e1 > nnz) {
@@ -746,10 +749,11 @@ __global__ void validate_csr_kernel(const int64_t* rowptr, const int32_t* col, i
 // round's last lane); the array's last piece, which may end past nnz, is
 // read index by index.
 __global__ void validate_csr_v_kernel(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
-                                      int64_t nnz, int32_t* bad) {
-    const int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+                                      int64_t nnz, int32_t* bad, const int32_t* order) {
+    int64_t g = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (g >= G) return;
+    if (order) g = order[g];
     const int64_t e0 = rowptr[g], e1 = rowptr[g + 1];
     int b = 0;
     if (e0 < 0 || e1 < e0 || e1 > nnz) {
@@ -805,12 +809,12 @@ __global__ void validate_csr_v_kernel(const int64_t* rowptr, const int32_t* col,
     if (g == G - 1 && lane == 0 && e1 != nnz) atomicOr(bad, 1);
 }
 cudaError_t launch_validate_csr(const int64_t* rowptr, const int32_t* col, int64_t G, int64_t n,
-                                int64_t nnz, int32_t* bad, cudaStream_t st) {
+                                int64_t nnz, int32_t* bad, cudaStream_t st, const int32_t* order) {
     if (G == 0) return cudaSuccess;
     if ((reinterpret_cast<uintptr_t>(col) & 15) == 0)
-        validate_csr_v_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, col, G, n, nnz, bad);
+        validate_csr_v_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, col, G, n, nnz, bad, order);
     else
-        validate_csr_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, col, G, n, nnz, bad);
+        validate_csr_kernel<<<nblk(G, 8), 256, 0, st>>>(rowptr, col, G, n, nnz, bad, order);
     return cudaGetLastError();
 }
 
