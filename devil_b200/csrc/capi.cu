@@ -96,9 +96,9 @@ struct devil_ctx {
     int sm_count = 148;
     int use_tma = 0;
     int use_groups = 1;
-    // slice-major passes of the design-group engine, a bit mask: 1 IRLS, 2 MLE
-    // (DEVIL_GRP_SLICES; 0: every pass block per gene)
-    int grp_slices = 3;
+    // slice-major passes of the design-group engine, a bit mask: 1 IRLS, 2 MLE,
+    // 4 MOM, 8 bread (unclustered) (DEVIL_GRP_SLICES; 0: every pass block per gene)
+    int grp_slices = 15;
     int debug = 0;  // DEVIL_DEBUG=1: engine choices on stderr
     // profiling: CUDA events around every pass launch, per pass kind
     int profiling = 0;
@@ -1127,7 +1127,8 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
         gg.partW = static_cast<double*>(pb.partW);
         gg.partS = pb.partS;
         gg.slot_stride = tiles;
-        const int slice_bit = kind == PASS_IRLS ? 1 : (kind == PASS_MLE ? 2 : 0);
+        const int slice_bit =
+            kind == PASS_IRLS ? 1 : (kind == PASS_MLE ? 2 : (kind == PASS_MOM ? 4 : (kind == PASS_SANDWICH ? 8 : 0)));
         if ((ctx->grp_slices & slice_bit) && !fine) {
             // slice-major pass: per-(gene, slice) sums, then the assembly
             gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * grp_slices_nq(kind));
@@ -1218,10 +1219,16 @@ void prof_add_bytes(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const i
 }
 
 // all-genes list (for one-shot passes)
-const int32_t* all_genes(devil_ctx* ctx, const DevProblem& dp, int32_t** count_out) {
+// (ordered: in decreasing order of entries when the counts were sorted, the
+// work order of the slice-major passes, for passes whose finalize maps list
+// slots to genes; otherwise slot g is gene g)
+const int32_t* all_genes(devil_ctx* ctx, const DevProblem& dp, int32_t** count_out, bool ordered = false) {
     int32_t* a = ws<int32_t>(ctx, "all_genes", dp.G);
     int32_t* c = ws<int32_t>(ctx, "all_count", 4);
-    LAUNCH(launch_iota(a, dp.G, ctx->stream));
+    if (ordered && dp.gorder)
+        CK(cudaMemcpyAsync(a, dp.gorder, dp.G * sizeof(int32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+    else
+        LAUNCH(launch_iota(a, dp.G, ctx->stream));
     LAUNCH(launch_set_i32(c, (int32_t)dp.G, ctx->stream));
     *count_out = c;
     return a;
@@ -1479,7 +1486,7 @@ void run_mom(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     if (dp.G == 0) return;
     const PassPlan plan = plan_for(PASS_MOM, dp, form);
     int32_t* cnt = nullptr;
-    const int32_t* act = all_genes(ctx, dp, &cnt);
+    const int32_t* act = all_genes(ctx, dp, &cnt, plan.engine == ENGINE_GRP);  // (mom_finalize maps slots)
     const int tiles = (int)((dp.G + plan.GT - 1) / plan.GT);
     const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
     PassBuffers pb = pass_buffers(ctx, PASS_MOM, dp.P, (size_t)nseg * tiles * plan.GT);
@@ -1587,7 +1594,8 @@ void run_sandwich(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, con
     }
     if (plan.GT <= 0) fail(ctx, DEVIL_ERR_UNSUPPORTED, "p = %d unsupported", dp.P);
     int32_t* cnt = nullptr;
-    const int32_t* act = all_genes(ctx, dp, &cnt);
+    // (sandwich_finalize maps slots to genes)
+    const int32_t* act = all_genes(ctx, dp, &cnt, plan.engine == ENGINE_GRP && n_clusters <= 0);
     const int tiles = (int)((dp.G + plan.GT - 1) / plan.GT);
     PassParamsAny prm{beta_f, beta_d, nullptr, nullptr, theta};
     if (plan.engine == ENGINE_GRP && n_clusters > 0) {
@@ -1941,7 +1949,7 @@ int devil_ctx_create(int device, devil_ctx** out) {
         const char* ug = getenv("DEVIL_GROUPS");
         ctx->use_groups = (ug && !atoi(ug)) ? 0 : 1;
         const char* gsl = getenv("DEVIL_GRP_SLICES");
-        ctx->grp_slices = gsl ? (atoi(gsl) & 3) : 3;
+        ctx->grp_slices = gsl ? (atoi(gsl) & 15) : 15;
         const char* dbg = getenv("DEVIL_DEBUG");
         ctx->debug = (dbg && atoi(dbg)) ? 1 : 0;
         int32_t* err = ws<int32_t>(ctx, "kernel_err", 1);

@@ -1275,6 +1275,12 @@ cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParam
     if (kind == PASS_MLE)
         return slices_run<PassMLE>(geo, PassMLE::Params{pa.beta, pa.beta_d, pa.log_theta}, val_u16,
                                    max_slots, tile, assemble, st);
+    if (kind == PASS_MOM)
+        return slices_run<PassMOM>(geo, PassMOM::Params{pa.beta, pa.beta_d}, val_u16, max_slots, tile,
+                                   assemble, st);
+    if (kind == PASS_SANDWICH)
+        return slices_run<PassSandwich>(geo, PassSandwich::Params{pa.beta, pa.beta_d, pa.theta}, val_u16,
+                                        max_slots, tile, assemble, st);
     return cudaErrorInvalidValue;
 }
 
