@@ -1344,6 +1344,22 @@ PassPlan autotune(devil_ctx* ctx, const DevProblem& dp, const PassPlan& base, co
     return best;
 }
 
+// entries per slice below which a gene of a slice-major pass takes eight
+// lanes instead of a warp: IRLS (DEVIL_LIGHT_ENTRIES overrides
+// kLightEntries) and MLE (DEVIL_LIGHT_ENTRIES_MLE, kLightEntriesMle)
+int light_entries(bool mle = false) {
+    static const int v[2] = {
+        [] {
+            const char* e = getenv("DEVIL_LIGHT_ENTRIES");
+            return (e && *e) ? std::max(0, atoi(e)) : kLightEntries;
+        }(),
+        [] {
+            const char* e = getenv("DEVIL_LIGHT_ENTRIES_MLE");
+            return (e && *e) ? std::max(0, atoi(e)) : kLightEntriesMle;
+        }()};
+    return v[mle ? 1 : 0];
+}
+
 // One IRLS loop over the n0 genes listed in the "act0" workspace (their
 // iteration counts and status start at 0); returns the pass launches.
 int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan0, double* beta, float* beta_f,
@@ -1363,7 +1379,7 @@ int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan0, d
     // on average take eight lanes each
     const bool sliced = plan.engine == ENGINE_GRP && (ctx->grp_slices & 1);
     int32_t* nheavy = ws<int32_t>(ctx, "cnt_heavy", 2);
-    const int32_t thr = (int32_t)std::min<int64_t>((int64_t)kLightEntries * dp.grp.S, INT32_MAX);
+    const int32_t thr = (int32_t)std::min<int64_t>((int64_t)light_entries() * dp.grp.S, INT32_MAX);
     if (sliced) LAUNCH(launch_count_at_least(dp.grp.skey, n0, thr, nheavy, st));
     // copies of an earlier loop still in flight would overwrite the mirror
     CK(cudaStreamSynchronize(st));
@@ -1528,9 +1544,9 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
     LAUNCH(launch_set_i32(cnt + 1, 0, st));
     // slice-major passes: the active genes stay in decreasing order of entries
     const bool ordered = plan.engine == ENGINE_GRP && (ctx->grp_slices & 2);
-    // (and those below kLightEntries entries per slice take eight lanes each)
+    // (and those below kLightEntriesMle entries per slice take eight lanes each)
     int32_t* nheavy = ws<int32_t>(ctx, "cnt_heavy", 2);
-    const int32_t thr = ordered ? (int32_t)std::min<int64_t>((int64_t)kLightEntries * dp.grp.S, INT32_MAX) : 0;
+    const int32_t thr = ordered ? (int32_t)std::min<int64_t>((int64_t)light_entries(true) * dp.grp.S, INT32_MAX) : 0;
     if (ordered) s.keep = ws<int8_t>(ctx, "keep", G);
     LAUNCH(launch_mle_init(dp.stats, G, dp.n, s, act[0], cnt, st));
     if (ordered)

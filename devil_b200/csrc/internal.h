@@ -123,8 +123,13 @@ constexpr int kRuleCap = kMaxBins * kBinNodes;  // node capacity of one rule
 constexpr int kMaxGroups = 256;       // distinct design rows
 constexpr int kMaxFine = 4096;        // (design row, cluster) pairs
 constexpr int kMinCellsPerGroup = 32; // grouping pays when groups are larger
-constexpr int kLightEntries = 96;     // slice-major passes: genes below this many entries per slice on
-                                      // average take eight lanes (one round of three 16-byte loads)
+// slice-major passes: genes below this many entries per slice on average
+// take eight lanes instead of a warp (IRLS; the MLE pass, whose light genes
+// load one 16-byte piece per lane at a time, switches lower).  Measured on
+// the headline: IRLS 96 / 192 / 384 / 768 / 1536 -> 103.9 / 99.5 / 98.0 /
+// 99.7 / 106.9 ms per step; MLE 96 / 192 / 384 -> 29.2 / 29.5 / 30.2 ms.
+constexpr int kLightEntries = 384;
+constexpr int kLightEntriesMle = 96;
 constexpr int kSliceCells = 16384;    // cells per slice (its FP64 exp(offset), 128 KB, fits shared memory)
 constexpr int kGrpTab = 2 * kPsiTab + 2;  // per-gene psi tables + psi(a), psi1(a)
 constexpr int kMaxSlices = 12288;     // the CSR copy's per-warp key table stays <= 48 KB; keys fit 16 bits

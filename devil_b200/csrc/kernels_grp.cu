@@ -749,8 +749,9 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
 // s is the group's first slice, and the gene's entries of the slice as
 // 16-byte streaming loads (UNR in flight per lane), mu = A E[cell] with E
 // from shared memory.  The active genes are listed in decreasing order of
-// entries; those with fewer than kLightEntries per slice on average (the
-// tail of the list) take eight lanes each, four to a warp, so that the
+// entries; those with fewer than kLightEntries (MLE: kLightEntriesMle) per
+// slice on average (the tail of the list) take eight lanes each, four to a
+// warp, so that the
 // per-(gene, slice) bookkeeping (hand-out, ranges, sums, stores) is shared
 // by four genes.  The per-(gene, slice) sums go to geo.gsum;
 // grp_assemble_kernel / the IRLS step form the p x p terms per gene.
