@@ -759,10 +759,11 @@ __global__ void __launch_bounds__(256) grp_pass_kernel(GrpGeom geo, typename Pas
 constexpr int kSlNT = 1024;  // one block per SM: 32 warps, 64 registers each, the 128 KB slice stage
 static_assert(kSliceCells % kSlNT == 0, "a slice is staged in whole rounds of the block");
 
-// 16-byte loads in flight per lane: as many as 64 registers hold (the
-// MLE's accumulators take more registers)
+// 16-byte loads in flight per lane: as many as 64 registers hold without
+// spilling (the MLE's accumulators take more registers; beta_0's per-warp
+// queue is sized for three)
 template <class Pass>
-constexpr int sl_unr() { return Pass::TABLES ? 2 : 3; }
+constexpr int sl_unr() { return Pass::TABLES ? 2 : (std::is_same<Pass, PassInitZ>::value ? 3 : 4); }
 
 // beta_0's pass: per warp, a queue of the entries with counts above 1 (one
 // round adds at most 32 x 3 x 4 entries to fewer than 32 left over)
