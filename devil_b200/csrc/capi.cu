@@ -559,8 +559,13 @@ void compute_offsets(devil_ctx* ctx, DevProblem& dp, int method, const double* s
         CK(cudaMemsetAsync(colcnt, 0, n * sizeof(int32_t), st));
         CK(cudaMemsetAsync(colmin, 0x7f, n * sizeof(int32_t), st));  // ~ +3.4e38
     }
+    uint32_t* colsum_u32 = nullptr;
+    if (method == DEVIL_SF_NORMED_SUM && dp.val_u16 && dp.G <= 65537) {
+        colsum_u32 = ws<uint32_t>(ctx, "colsum_u32", n);
+        CK(cudaMemsetAsync(colsum_u32, 0, n * sizeof(uint32_t), st));
+    }
     LAUNCH(launch_colstats(dp.rowptr, dp.col, dp.val, dp.val_u16, dp.G, dp.nnz, colsum, collog,
-                           colcnt, colmin, st));
+                           colcnt, colmin, st, colsum_u32, n));
     int32_t* err = ws<int32_t>(ctx, "sf_err", 1);
     LAUNCH(launch_sf_finalize(method == DEVIL_SF_NORMED_SUM ? 1 : 2, dp.G, n, colsum, collog, colcnt,
                               colmin, offset, dp.sf, dp.off, dp.off_f, err, st));

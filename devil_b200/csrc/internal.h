@@ -311,10 +311,13 @@ cudaError_t launch_double_to_float(const double* in, float* out, int64_t m, cuda
 cudaError_t launch_gene_stats(const int64_t* rowptr, const void* val, int val_u16, int64_t G,
                               int64_t n, double* stats /* G x 6 */, cudaStream_t st,
                               const int32_t* order = nullptr);
+// (colsum_u32, n: zeroed scratch of n cells; normed_sum of 16-bit counts
+// then sums with 32-bit integer atomics)
 cudaError_t launch_colstats(const int64_t* rowptr, const int32_t* col, const void* val,
                             int val_u16, int64_t G, int64_t nnz, double* colsum,
                             double* collog, int32_t* colcnt, int32_t* colmin_bits,
-                            cudaStream_t st);
+                            cudaStream_t st,
+                            uint32_t* colsum_u32 = nullptr, int64_t n = 0);
 cudaError_t launch_sf_finalize(int method, int64_t G, int64_t n, const double* colsum,
                                const double* collog, const int32_t* colcnt,
                                const int32_t* colmin_bits, double offset, double* sf,

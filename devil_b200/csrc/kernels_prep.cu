@@ -383,13 +383,45 @@ __global__ void colstats_kernel(const int32_t* col, const VT* val, int64_t nnz, 
         }
     }
 }
+// normed_sum column sums of 16-bit counts as 32-bit integer atomics (a
+// column sum is at most G x 65535, below 2^32 for G <= 65537), four entries'
+// loads in flight per thread; colsum_from_u32_kernel turns them into FP64
+// (the same exact integers the FP64 atomics give)
+__global__ void colsum_u32_kernel(const int32_t* col, const uint16_t* val, int64_t nnz, uint32_t* colsum) {
+    constexpr int U = 4;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < nnz; e0 += stride * U) {
+        int c[U];
+        uint32_t v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t e = e0 + stride * u;
+            c[u] = e < nnz ? __ldg(col + e) : -1;
+            v[u] = e < nnz ? (uint32_t)__ldg(val + e) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (c[u] >= 0 && v[u]) atomicAdd(colsum + c[u], v[u]);
+    }
+}
+__global__ void colsum_from_u32_kernel(const uint32_t* in, int64_t n, double* out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (double)in[i];
+}
+
 cudaError_t launch_colstats(const int64_t* rowptr, const int32_t* col, const void* val,
                             int val_u16, int64_t G, int64_t nnz, double* colsum,
                             double* collog, int32_t* colcnt, int32_t* colmin_bits,
-                            cudaStream_t st) {
-    (void)rowptr; (void)G;
+                            cudaStream_t st, uint32_t* colsum_u32, int64_t n) {
+    (void)rowptr;
     if (nnz == 0) return cudaSuccess;
     unsigned b = (unsigned)std::min<int64_t>(nblk(nnz, 256), 148 * 32);
+    if (colsum_u32 && val_u16 && !collog && G <= 65537) {
+        colsum_u32_kernel<<<b, 256, 0, st>>>(col, (const uint16_t*)val, nnz, colsum_u32);
+        colsum_from_u32_kernel<<<(unsigned)std::min<int64_t>(nblk(n, 256), 1024), 256, 0, st>>>(colsum_u32, n,
+                                                                                               colsum);
+        return cudaGetLastError();
+    }
     if (val_u16)
         colstats_kernel<uint16_t><<<b, 256, 0, st>>>(col, (const uint16_t*)val, nnz, colsum, collog, colcnt, colmin_bits);
     else
