@@ -122,8 +122,8 @@ cudaError_t launch_irls_finalize(const void* partW, bool wide, int nseg, int slo
 // ------------------------------------------------------------------
 // IRLS step of the design-group engine's slice-major pass, warp per gene,
 // with the assembly folded in: the group sums of the gene's per-slice sums
-// (slice order), H = k^2 sum over (group, pair) lists, score = -k sum over
-// (group, entry) lists -- the same sums in the same order as
+// (a segmented warp scan over the slices), H = k^2 sum over (group, pair)
+// lists, score = -k sum over (group, entry) lists -- the sums of
 // grp_assemble_kernel + irls_finalize_kernel, without the round trip of the
 // p x p partial sums through global memory -- then the LU, the solve and the
 // update of irls_finalize_kernel.
@@ -206,14 +206,32 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
     if (slot >= *geo.n_act) return;
     const int g = geo.act[slot];
     const double* gsum = geo.gsum + (int64_t)slot * S * 2;
-    for (int i = lane; i < 2 * U; i += 32) {
-        const int q = i >> 1, c = i & 1;
-        double v = 0.0;
-        for (int sl = __ldg(geo.kslice + q * C); sl < __ldg(geo.kslice + q * C + C); ++sl)
-            v += gsum[sl * 2 + c];
-        gs[i] = v;
-    }
+    // group sums: lanes over slices (one coalesced load each), then a
+    // segmented warp scan over each run of slices of one group (a group's
+    // slices are contiguous, keyed u * C + c); the run's last lane adds it in
+    for (int i = lane; i < 2 * U; i += 32) gs[i] = 0.0;
     __syncwarp();
+    for (int b = 0; b < S; b += 32) {
+        const int sl = b + lane;
+        const bool ok = sl < S;
+        double v0 = ok ? gsum[sl * 2] : 0.0, v1 = ok ? gsum[sl * 2 + 1] : 0.0;
+        const int q = ok ? __ldg(geo.sl_key + sl) / C : -1 - lane;  // past S: runs of their own
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double t0 = __shfl_up_sync(0xffffffffu, v0, o), t1 = __shfl_up_sync(0xffffffffu, v1, o);
+            const int qo = __shfl_up_sync(0xffffffffu, q, o);
+            if (lane >= o && qo == q) {
+                v0 += t0;
+                v1 += t1;
+            }
+        }
+        const int qn = __shfl_down_sync(0xffffffffu, q, 1);
+        if (ok && (lane == 31 || qn != q)) {
+            gs[2 * q] += v0;
+            gs[2 * q + 1] += v1;
+        }
+        __syncwarp();
+    }
     // the pass accumulates H / k^2 and -score / k (see PassIRLS)
     const double k = (double)kf[g];
     const double k2 = k * k;

@@ -477,7 +477,7 @@ __global__ void seg_scatter_kernel(const int64_t* rowptr, const int32_t* col, co
     // U rounds of 32 entries: every load and key lookup of the rounds is
     // issued first, then the rounds are placed in order (the same positions
     // as one round at a time)
-    constexpr int U = 4;
+    constexpr int U = 8;
     for (int64_t base = r0; base < r1; base += 32 * U) {
         int c[U], k[U], lc[U];
         VT v[U];
