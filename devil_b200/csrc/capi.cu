@@ -1087,7 +1087,7 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
                  int nseg, int tiles, const int32_t* bound, const int64_t* segptr,
                  int nbound, const int32_t* act, const int32_t* n_act, int32_t* reset_next,
                  const PassBuffers& pb, const PassParamsAny& prm, int fine = 0,
-                 const int32_t* n_heavy = nullptr) {
+                 const int32_t* n_heavy = nullptr, bool rowexp_fresh = false) {
     PassLaunch L;
     L.kind = kind;
     L.engine = plan.engine;
@@ -1137,13 +1137,13 @@ void launch_pass(devil_ctx* ctx, const DevProblem& dp, PassKind kind, const Pass
         if ((ctx->grp_slices & slice_bit) && !fine) {
             // slice-major pass: per-(gene, slice) sums, then the assembly
             gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * grp_slices_nq(kind));
-            gg.rowexp = ws<double>(ctx, "grp_rowexp", (size_t)tiles * gg.U);
+            gg.rowexp = ws<double>(ctx, "grp_rowexp", (size_t)dp.G * gg.U);
             if (kind == PASS_MLE) gg.psitab = ws<double>(ctx, "grp_psitab", (size_t)tiles * kGrpTab);
             // (the IRLS step folds the assembly into its finalize)
             LAUNCH(launch_grp_slices(kind, gg, prm, dp.val_u16, tiles,
                                      grp_slices_tile(tiles, gg.S, ctx->sm_count, plan.waves > 0 ? plan.waves : 3),
                                      kind != PASS_IRLS,
-                                     ctx->stream));
+                                     ctx->stream, rowexp_fresh));
         } else {
             LAUNCH(launch_grp_pass(kind, gg, prm, dp.val_u16, tiles, ctx->stream));
         }
@@ -1401,8 +1401,10 @@ int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan0, d
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
+        // (after the first pass the step kernel keeps the genes' exp(x_u . beta))
         launch_pass(ctx, dp, PASS_IRLS, plan, nseg, tiles, dp.fine_bound, dp.fine_ptr,
-                    dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm, 0, sliced ? nheavy + cur : nullptr);
+                    dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm, 0, sliced ? nheavy + cur : nullptr,
+                    sliced && t > 0);
         ++launched;
         const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC && plan.engine != ENGINE_TCW;
         if (sliced) {
@@ -1411,19 +1413,20 @@ int64_t irls_loop(devil_ctx* ctx, const DevProblem& dp, const PassPlan& plan0, d
             gg.act = act[cur];
             gg.n_act = cnt + cur;
             gg.gsum = ws<double>(ctx, "grp_gsum", (size_t)tiles * gg.S * 2);
+            gg.rowexp = ws<double>(ctx, "grp_rowexp", (size_t)G * gg.U);
             // the genes that go on keep the order of the list (decreasing
             // entries: the pass's work order)
             int8_t* keep = ws<int8_t>(ctx, "keep", G);
             LAUNCH(launch_grp_irls_finalize(gg, (int)hint, act[nxt], cnt + nxt, beta, beta_f, iters,
                                             status, max_iter, eps, k, st, keep));
             LAUNCH(launch_compact_kept(act[cur], cnt + cur, 0, keep, act[nxt], cnt + nxt, st, dp.grp.wkey, thr,
-                                       nheavy + nxt));
+                                       nheavy + nxt, ctx->mapped_dev + (t & 3)));
         } else {
             LAUNCH(launch_irls_finalize(pb.partW, part_f64, nseg, tiles * plan.GT, dp.P, act[cur],
                                         cnt + cur, (int)hint, act[nxt], cnt + nxt, beta, beta_f,
                                         iters, status, max_iter, eps, k, st));
+            LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev + (t & 3), st));
         }
-        LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev + (t & 3), st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
     }
@@ -1571,9 +1574,10 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
         if (hint <= 0) break;
         const int tiles = (int)((hint + plan.GT - 1) / plan.GT);
         const int nseg = choose_nseg(ctx, dp, plan, tiles, form);
+        // (beta is fixed during the MLE loop: exp(x_u . beta) from its first pass)
         launch_pass(ctx, dp, PASS_MLE, plan, nseg, tiles, dp.fine_bound,
                     dp.fine_ptr, dp.nfine + 1, act[cur], cnt + cur, cnt + nxt, pb, prm, 0,
-                    ordered ? nheavy + cur : nullptr);
+                    ordered ? nheavy + cur : nullptr, ordered && t > 0);
         ++launched;
         const bool part_f64 = plan.engine != ENGINE_REG && plan.engine != ENGINE_TC && plan.engine != ENGINE_TCW;
         // the exclusive-column (one-hot) structure of a grouped design
@@ -1583,10 +1587,12 @@ void run_mle(devil_ctx* ctx, const DevProblem& dp, const float* beta_f, const do
                                    act[cur], cnt + cur, (int)hint, act[nxt], cnt + nxt, s, max_iter,
                                    cox_reid, nullptr, st, structured ? dp.grp.nA : 0,
                                    structured ? dp.grp.colA : nullptr, structured ? dp.grp.colD : nullptr));
+        // (the compaction mirrors the count for the host; otherwise a kernel does)
         if (ordered)
             LAUNCH(launch_compact_kept(act[cur], cnt + cur, 0, s.keep, act[nxt], cnt + nxt, st, dp.grp.wkey, thr,
-                                       nheavy + nxt));
-        LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev + (t & 3), st));
+                                       nheavy + nxt, ctx->mapped_dev + (t & 3)));
+        else
+            LAUNCH(launch_copy_i32_to_host_mapped(cnt + nxt, ctx->mapped_dev + (t & 3), st));
         CK(cudaEventRecord(ctx->ev[t & 3], st));
         if (t >= LAG) CK(cudaEventSynchronize(ctx->ev[(t - LAG) & 3]));
     }

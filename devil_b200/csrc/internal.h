@@ -166,7 +166,7 @@ struct GrpGeom {
     const int32_t* sl_key;    // [S] its key u * C + c
     const int32_t* kslice;    // [U*C + 1] first slice of every key (slices ordered by key)
     double* gsum;          // slice-major IRLS: [slots][S][NQ] per-(gene, slice) sums
-    double* rowexp;        // slice-major passes: [slots][U] exp(x_u . beta)
+    double* rowexp;        // slice-major passes: [G][U] exp(x_u . beta) by gene
     double* psitab;        // slice-major MLE: [slots][kGrpTab] psi tables, psi(a), psi1(a)
     const double* rs;      // [rules][kRuleCap] node offsets; rules 0..U-1 coarse, U.. fine
     const double* rw;      // [rules][kRuleCap] node weights
@@ -237,11 +237,12 @@ cudaError_t launch_new_od(const NodArgs& a, const double* Xcm, double* xcolsum, 
 
 cudaError_t launch_grp_pass(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm, int val_u16,
                             int max_slots, cudaStream_t st);
-// the IRLS and MLE passes of the design-group engine, slice-major: a block
-// stages one slice's exp(offset) in shared memory and runs `tile` genes over
-// it, then a block per gene assembles the p x p sums (geo.gsum: slots x S x
-// grp_slices_nq(kind) doubles; geo.rowexp: slots x U; geo.psitab, MLE:
-// slots x kGrpTab)
+// the IRLS, MLE, MOM and bread passes of the design-group engine,
+// slice-major: a block stages one slice's exp(offset) in shared memory and
+// runs its share of the genes over it, then a block per gene assembles the
+// p x p sums (geo.gsum: slots x S x grp_slices_nq(kind) doubles;
+// geo.rowexp: G x U exp(x_u . beta) by gene, recomputed first unless
+// rowexp_fresh; geo.psitab, MLE: slots x kGrpTab)
 int grp_slices_tile(int64_t hint, int S, int sm_count, int waves = 3);
 // key[g] = entries of gene g, idx[g] = g (sorted descending into the work
 // order of the slice-major passes)
@@ -249,13 +250,14 @@ cudaError_t launch_gene_entries(const int64_t* rowptr, int64_t G, int32_t* key, 
                                 cudaStream_t st);
 int grp_slices_nq(PassKind k);
 cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm,
-                              int val_u16, int max_slots, int tile, bool assemble, cudaStream_t st);
+                              int val_u16, int max_slots, int tile, bool assemble, cudaStream_t st,
+                              bool rowexp_fresh = false);
 // cells in key order: sl_cell / sl_loc per original cell, E in slice order
 cudaError_t launch_slice_cells(const int32_t* pnew, const int32_t* sl_start, int S, int64_t n,
                                const double* off, int32_t* cslice, int32_t* cloc, double* E,
                                cudaStream_t st);
 // beta_0 of a grouped design: geo.act / geo.n_act list every gene, geo.gsum
-// holds G x S doubles, geo.rowexp G x U; zero_beta is G x P zeros
+// holds G x S doubles; zero_beta is G x P zeros
 cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* zero_beta,
                                  const double* ginv, int64_t G, int tile, double* beta,
                                  float* beta_f, cudaStream_t st);
@@ -348,10 +350,12 @@ cudaError_t launch_mle_passes(const int32_t* it, const int32_t* phase, const dou
 cudaError_t launch_set_i32(int32_t* a, int32_t v, cudaStream_t st);
 // act_next = the genes g of act[0, n) (n = *n_act, or n_fixed when n_act is
 // null) with keep[g] != 0, in order; *n_next = their count
-// (wkey non-null: *n_heavy_next = the kept genes with wkey[g] >= thr)
+// (wkey non-null: *n_heavy_next = the kept genes with wkey[g] >= thr;
+// mirror non-null: the count also written there, a pinned mapped host slot)
 cudaError_t launch_compact_kept(const int32_t* act, const int32_t* n_act, int64_t n_fixed, const int8_t* keep,
                                 int32_t* act_next, int32_t* n_next, cudaStream_t st,
-                                const int32_t* wkey = nullptr, int32_t thr = 0, int32_t* n_heavy_next = nullptr);
+                                const int32_t* wkey = nullptr, int32_t thr = 0, int32_t* n_heavy_next = nullptr,
+                                volatile int32_t* mirror = nullptr);
 // *out = the number of leading entries of key (in descending order) >= thr
 cudaError_t launch_count_at_least(const int32_t* key, int64_t n, int32_t thr, int32_t* out, cudaStream_t st);
 cudaError_t launch_copy_i32_to_host_mapped(const int32_t* src, volatile int32_t* dst,

@@ -286,27 +286,40 @@ __global__ void grp_irls_finalize_kernel(GrpGeom geo, int32_t* act_next, int32_t
         warp_lu(H, LD, P, perm, step);
         x_own = warp_lu_solve(H, LD, P, perm, step, s_own);
     }
+    double b_own = 0.0;
     if (lane < P) {
-        const double b = beta[(int64_t)g * P + lane] + x_own;
-        beta[(int64_t)g * P + lane] = b;
-        beta_f[(int64_t)g * P + lane] = (float)b;
+        b_own = beta[(int64_t)g * P + lane] + x_own;
+        beta[(int64_t)g * P + lane] = b_own;
+        beta_f[(int64_t)g * P + lane] = (float)b_own;
     }
     double mx = lane < P ? fabs(x_own) : 0.0;
     mx = (mx == mx) ? mx : 0.0;  // NaN entries never compare greater
     mx = warp_max(mx);
     const double x0 = __shfl_sync(0xffffffffu, x_own, 0);
-    if (lane != 0) return;
     const int it = iters[g] + 1;
+    // (the same decision on every lane)
+    const bool more = (x0 == x0) && !(mx < eps) && it < max_iter;
+    if (more && geo.rowexp) {
+        // the next pass's exp(x_u . beta) of this gene (rows of the design
+        // in shared memory order, as grp_rowexp_kernel sums them); H is free
+        __syncwarp();
+        if (lane < P) H[lane] = b_own;
+        __syncwarp();
+        for (int uu = lane; uu < U; uu += 32) {
+            double a = 0.0;
+            for (int e = __ldg(geo.rptr + uu); e < __ldg(geo.rptr + uu + 1); ++e)
+                a += __ldg(geo.rval + e) * H[__ldg(geo.rcol + e)];
+            geo.rowexp[(int64_t)g * U + uu] = exp(a);
+        }
+    }
+    if (lane != 0) return;
     iters[g] = it;
-    bool more = false;
     if (!(x0 == x0)) {
         status[g] = 2;  // DEVIL_GENE_NAN
     } else if (mx < eps) {
         status[g] = 0;
     } else if (it >= max_iter) {
         status[g] = 1;
-    } else {
-        more = true;
     }
     if (keep) keep[g] = more ? 1 : 0;
     else if (more) act_next[atomicAdd(n_next, 1)] = g;

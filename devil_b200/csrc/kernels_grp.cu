@@ -868,7 +868,7 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
         if (it.j >= nheavy) it.j = nact;  // past the heavy part
         if (it.j < nact) {
             it.g = __ldg(geo.act + it.j);
-            it.A = __ldg(geo.rowexp + (int64_t)it.j * U + u);
+            it.A = __ldg(geo.rowexp + (int64_t)it.g * U + u);
             it.e0 = __ldg(geo.gptr + (int64_t)it.g * (S + 1) + s);
             it.e1 = __ldg(geo.gptr + (int64_t)it.g * (S + 1) + s + 1);
         }
@@ -1053,7 +1053,7 @@ __global__ void __launch_bounds__(kSlNT, 1) grp_slices_kernel(GrpGeom geo, typen
             SlItem it{jl < nlight ? nheavy + jl : -1, 0, 0.0, 0, 0};
             if (it.j >= 0) {
                 it.g = __ldg(geo.act + it.j);
-                it.A = __ldg(geo.rowexp + (int64_t)it.j * U + u);
+                it.A = __ldg(geo.rowexp + (int64_t)it.g * U + u);
                 it.e0 = __ldg(geo.gptr + (int64_t)it.g * (S + 1) + s);
                 it.e1 = __ldg(geo.gptr + (int64_t)it.g * (S + 1) + s + 1);
             }
@@ -1146,18 +1146,20 @@ __global__ void __launch_bounds__(32) grp_psi_tables_kernel(const int32_t* act, 
 }
 
 // exp(x_u . beta) for every (active gene, design group): the factor the
-// slice-major pass multiplies each cell's exp(offset) by
+// slice-major pass multiplies each cell's exp(offset) by, stored by gene
+// ([G][U]; the IRLS step refreshes a gene's row after its update)
 __global__ void grp_rowexp_kernel(GrpGeom geo, const double* beta_d, int64_t max_slots) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int U = geo.U, P = geo.P;
     const int64_t slot = i / U;
     if (slot >= *geo.n_act || slot >= max_slots) return;
     const int u = (int)(i - slot * U);
-    const double* b = beta_d + (int64_t)__ldg(geo.act + slot) * P;
+    const int64_t g = __ldg(geo.act + slot);
+    const double* b = beta_d + g * P;
     double a = 0.0;
     for (int e = __ldg(geo.rptr + u); e < __ldg(geo.rptr + u + 1); ++e)
         a += __ldg(geo.rval + e) * __ldg(b + __ldg(geo.rcol + e));
-    geo.rowexp[i] = exp(a);
+    geo.rowexp[g * U + u] = exp(a);
 }
 
 // Per active gene: group sums over the gene's slices (in slice order) and
@@ -1245,14 +1247,16 @@ int grp_slices_tile(int64_t hint, int S, int sm_count, int waves) {
 
 template <class Pass>
 static cudaError_t slices_run(const GrpGeom& geo, typename Pass::Params prm, int val_u16,
-                              int max_slots, int tile, bool assemble, cudaStream_t st) {
+                              int max_slots, int tile, bool assemble, bool rowexp_fresh, cudaStream_t st) {
     constexpr int NQ = Pass::NW + Pass::NV + Pass::NF + Pass::NS;
     const size_t smem = sl_smem_bytes<Pass>();
     if constexpr (Pass::TABLES)
         grp_psi_tables_kernel<<<(unsigned)max_slots, 32, 0, st>>>(geo.act, geo.n_act, prm.log_theta,
                                                                  geo.psitab);
-    const int64_t nrow = (int64_t)max_slots * geo.U;
-    grp_rowexp_kernel<<<nblk(nrow, 256), 256, 0, st>>>(geo, prm.beta_d, max_slots);
+    if (!rowexp_fresh) {
+        const int64_t nrow = (int64_t)max_slots * geo.U;
+        grp_rowexp_kernel<<<nblk(nrow, 256), 256, 0, st>>>(geo, prm.beta_d, max_slots);
+    }
     dim3 grid((unsigned)geo.S, (unsigned)((max_slots + tile - 1) / tile));
     auto go = [&](auto kern) -> cudaError_t {
         cudaError_t e = raise_dyn_smem(kern, smem);
@@ -1269,20 +1273,21 @@ static cudaError_t slices_run(const GrpGeom& geo, typename Pass::Params prm, int
 int grp_slices_nq(PassKind k) { return pass_nw(k) + pass_nv(k) + pass_nf(k) + pass_ns(k); }
 
 cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& pa,
-                              int val_u16, int max_slots, int tile, bool assemble, cudaStream_t st) {
+                              int val_u16, int max_slots, int tile, bool assemble, cudaStream_t st,
+                              bool rowexp_fresh) {
     if (max_slots <= 0) return cudaSuccess;
     if (kind == PASS_IRLS)
         return slices_run<PassIRLS>(geo, PassIRLS::Params{pa.beta, pa.beta_d, pa.k}, val_u16,
-                                    max_slots, tile, assemble, st);
+                                    max_slots, tile, assemble, rowexp_fresh, st);
     if (kind == PASS_MLE)
         return slices_run<PassMLE>(geo, PassMLE::Params{pa.beta, pa.beta_d, pa.log_theta}, val_u16,
-                                   max_slots, tile, assemble, st);
+                                   max_slots, tile, assemble, rowexp_fresh, st);
     if (kind == PASS_MOM)
         return slices_run<PassMOM>(geo, PassMOM::Params{pa.beta, pa.beta_d}, val_u16, max_slots, tile,
-                                   assemble, st);
+                                   assemble, rowexp_fresh, st);
     if (kind == PASS_SANDWICH)
         return slices_run<PassSandwich>(geo, PassSandwich::Params{pa.beta, pa.beta_d, pa.theta}, val_u16,
-                                        max_slots, tile, assemble, st);
+                                        max_slots, tile, assemble, rowexp_fresh, st);
     return cudaErrorInvalidValue;
 }
 
@@ -1327,8 +1332,7 @@ cudaError_t launch_grp_init_beta(const GrpGeom& geo, int val_u16, const double* 
     if (G <= 0) return cudaSuccess;
     PassInitZ::Params prm{nullptr, zero_beta};
     const size_t smem = sl_smem_bytes<PassInitZ>();
-    const int64_t nrow = G * geo.U;
-    grp_rowexp_kernel<<<nblk(nrow, 256), 256, 0, st>>>(geo, zero_beta, G);  // exp(0) = 1
+    // (beta_0's pass reads no exp(x_u . beta): no row factors)
     dim3 grid((unsigned)geo.S, (unsigned)((G + tile - 1) / tile));
     auto go = [&](auto kern) -> cudaError_t {
         cudaError_t e = raise_dyn_smem(kern, smem);

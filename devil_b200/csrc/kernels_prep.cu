@@ -920,7 +920,8 @@ __global__ void __launch_bounds__(kCompactNT) compact_kept_kernel(const int32_t*
                                                                   int64_t n_fixed, const int8_t* keep,
                                                                   int32_t* act_next, int32_t* n_next,
                                                                   const int32_t* wkey, int32_t thr,
-                                                                  int32_t* n_heavy_next) {
+                                                                  int32_t* n_heavy_next,
+                                                                  volatile int32_t* mirror) {
     __shared__ int wtot[kCompactR][32];
     __shared__ int batch_total;
     const int64_t n = n_act ? (int64_t)*n_act : n_fixed;
@@ -972,7 +973,10 @@ __global__ void __launch_bounds__(kCompactNT) compact_kept_kernel(const int32_t*
         base += batch_total;
         __syncthreads();  // wtot and batch_total are rewritten by the next batch
     }
-    if (t == 0) *n_next = base;
+    if (t == 0) {
+        *n_next = base;
+        if (mirror) *mirror = base;  // the host's copy (pinned, mapped)
+    }
     if (wkey) {
         heavy = __reduce_add_sync(0xffffffffu, heavy);
         if (lane == 0) wtot[0][w] = heavy;
@@ -986,9 +990,9 @@ __global__ void __launch_bounds__(kCompactNT) compact_kept_kernel(const int32_t*
 }
 cudaError_t launch_compact_kept(const int32_t* act, const int32_t* n_act, int64_t n_fixed, const int8_t* keep,
                                 int32_t* act_next, int32_t* n_next, cudaStream_t st, const int32_t* wkey,
-                                int32_t thr, int32_t* n_heavy_next) {
+                                int32_t thr, int32_t* n_heavy_next, volatile int32_t* mirror) {
     compact_kept_kernel<<<1, kCompactNT, 0, st>>>(act, n_act, n_fixed, keep, act_next, n_next, wkey, thr,
-                                                  n_heavy_next);
+                                                  n_heavy_next, mirror);
     return cudaGetLastError();
 }
 // *out = the number of leading entries of key (descending) that are >= thr
