@@ -489,8 +489,10 @@ __global__ void seg_scatter_kernel(const int64_t* rowptr, const int32_t* col, co
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            k[u] = c[u] >= 0 ? __ldg(ckey + c[u]) : -1;
-            lc[u] = c[u] >= 0 ? __ldg(cloc + c[u]) : 0;
+            // (cloc packs the slice and the index in it)
+            const uint32_t kl = c[u] >= 0 ? (uint32_t)__ldg(cloc + c[u]) : 0xffffffffu;
+            k[u] = c[u] >= 0 ? (int)(kl >> 16) : -1;
+            lc[u] = (int)(kl & 0xffffu);
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -1401,7 +1403,9 @@ __global__ void slice_cells_kernel(const int32_t* pnew, const int32_t* sl_start,
     }
     const int c = pnew[i];
     cslice[c] = lo;
-    cloc[c] = (int32_t)(i - sl_start[lo]);
+    // slice (high 16 bits: fewer than kMaxSlices < 2^16) and index in the
+    // slice (low 16 bits: fewer than kSliceCells), one gather for the copy
+    cloc[c] = (int32_t)(((uint32_t)lo << 16) | (uint32_t)(i - sl_start[lo]));
     E[i] = exp(off[c]);
 }
 
