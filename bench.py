@@ -777,7 +777,7 @@ def main():
             roof["tensor_note"] = (
                 "no dense contraction left for the tensor cores: the design has few distinct rows, "
                 "so the p x p terms are assembled from per-(gene, design row) sums, "
-                "U*p^2 FLOPs per gene-pass against 6 B per nonzero read")
+                "U*p^2 FLOPs per gene-pass against 4 B per nonzero read (slice-ordered copy)")
     passes = {name: {"launches": prof[k][0], "ms_per_step": round(prof[k][1] / args.steps, 3)}
               for k, name in enumerate(PASS_NAMES)}
     passes["other"] = {"ms_per_step": round(ms - sum(prof[k][1] for k in range(4)) / args.steps, 3),

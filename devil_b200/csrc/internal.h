@@ -252,7 +252,8 @@ int grp_slices_nq(PassKind k);
 cudaError_t launch_grp_slices(PassKind kind, const GrpGeom& geo, const PassParamsAny& prm,
                               int val_u16, int max_slots, int tile, bool assemble, cudaStream_t st,
                               bool rowexp_fresh = false);
-// cells in key order: sl_cell / sl_loc per original cell, E in slice order
+// cells in key order, per original cell: cslice = its slice, cloc = slice
+// << 16 | index within the slice; E in slice order
 cudaError_t launch_slice_cells(const int32_t* pnew, const int32_t* sl_start, int S, int64_t n,
                                const double* off, int32_t* cslice, int32_t* cloc, double* E,
                                cudaStream_t st);
@@ -286,8 +287,9 @@ int group_csr_segment(int64_t nnz, int64_t G, int K);  // entries per segment
 cudaError_t launch_group_segments(const int64_t* rowptr, int64_t G, int S, int64_t* segcnt,
                                   int64_t* segbase, void* scan_tmp, size_t* scan_bytes,
                                   cudaStream_t st);
-// hist: nsegs x K (nsegs = segbase[G]); ckey / cloc: slice and index within
-// the slice of every cell; gent: GrpEnt entries
+// hist: nsegs x K (nsegs = segbase[G]); ckey: the slice of every cell;
+// cloc: slice << 16 | index within the slice (one gather per entry for the
+// scatter); gent: GrpEnt entries
 cudaError_t launch_group_csr(const int64_t* rowptr, const int32_t* col, const void* val, int val_u16,
                              int64_t G, const int64_t* segbase, int S, const int32_t* ckey,
                              const int32_t* cloc, int K, int32_t* hist, int64_t nsegs,

@@ -459,9 +459,8 @@ __global__ void __launch_bounds__(kOffNT) seg_offsets_kernel(const int64_t* rowp
 
 template <class VT>
 __global__ void seg_scatter_kernel(const int64_t* rowptr, const int32_t* col, const VT* val,
-                                   int64_t G, const int64_t* segbase, int S, const int32_t* ckey,
-                                   const int32_t* cloc, int K, const int32_t* hist,
-                                   typename GrpEnt<VT>::T* gent) {
+                                   int64_t G, const int64_t* segbase, int S, const int32_t* cloc, int K,
+                                   const int32_t* hist, typename GrpEnt<VT>::T* gent) {
     extern __shared__ int32_t cur_all[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t s = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
@@ -1498,11 +1497,11 @@ cudaError_t launch_group_csr(const int64_t* rowptr, const int32_t* col, const vo
     if (grid > 0) {
         if (val_u16)
             seg_scatter_kernel<uint16_t><<<grid, 32 * wpb, smem, st>>>(
-                rowptr, col, static_cast<const uint16_t*>(val), G, segbase, S, ckey, cloc, K, hist,
+                rowptr, col, static_cast<const uint16_t*>(val), G, segbase, S, cloc, K, hist,
                 static_cast<GrpEnt<uint16_t>::T*>(gent));
         else
             seg_scatter_kernel<float><<<grid, 32 * wpb, smem, st>>>(
-                rowptr, col, static_cast<const float*>(val), G, segbase, S, ckey, cloc, K, hist,
+                rowptr, col, static_cast<const float*>(val), G, segbase, S, cloc, K, hist,
                 static_cast<GrpEnt<float>::T*>(gent));
     }
     return cudaGetLastError();
